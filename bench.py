@@ -1,0 +1,342 @@
+#!/usr/bin/env python3
+"""Throughput of the per-step particle hot path on B200: particle-steps/s.
+
+Workload: the 3D delta+-SPH dam break (sigmasph_b200.scenes.dambreak3d), 1,000,188 fluid
+particles at dx = 4.762 mm, reflecting tank walls.  A step is one SPHBase.step(): the
+neighbour rebuild with the reorder of every persistent field, the five pair passes of
+the delta+-SPH substep, advect, particle shifting and the walls.  The state (>= 0.9 GB
+with the neighbour lists) is far larger than the 126 MB L2, so no flush is needed
+between steps.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference]
+
+Under torchrun (N > 1) every rank runs an independent replica of the workload (the
+path does not shard at one-GPU scale: replicas only); the time is the max over ranks.
+`--impl reference` times the reference's algorithm on the host cores: the CPU
+restatement of the reference's kernels (the reference itself is Taichi, not installed
+and not installable here), float32, all host threads, on rank 0 only.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+if ROOT not in sys.path:
+    sys.path.insert(0, ROOT)
+
+METRIC = "particle-steps/s on 1 B200 (3D delta+-SPH dam break)"
+UNIT = "particle-steps/s"
+DX_1M = 0.004762
+
+# Algorithmic (compulsory, own-particle) bytes per particle of each kernel: the fields it
+# must read and write once in float32; neighbour data is assumed served on chip.
+ALGO_BYTES = {
+    "k_nbr_build": 16 + 16 + 4,        # pos + cell read, count write (list entries: design)
+    "k_lam": 16 + 4 + 32,              # pos read; lam + L (8 floats) write
+    "k_lamgrad_cont": 16 + 16 + 16 + 32 + 4 + 16 + 16,  # pos vel shift L lam read; lgrad, div write
+    "k_eos": 16 + 4 + 4 + 16 + 4 + 16,  # pos, div, V_lo, vel.m read; pos.V, V_lo, p, acc write
+    "k_force": 16 + 16 + 16 + 16 + 16 + 16,  # pos vel disp shift acc read; acc write
+    "k_advect": 16 + 16 + 16 + 16 + 16 + 16 + 16,
+    "k_pst": 16 + 16 + 4 + 16 + 16,   # pos vel lam lgrad read; shift write
+    "k_finish": 16 * 6 + 16 * 4,
+    "k_gather": 2 * (16 * 5 + 4) + 16 + 4,
+}
+
+
+def load_peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        with open(p) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+def read_traffic(kernel):
+    """dram bytes per launch at the bench size from the committed ncu summary, if any."""
+    p = os.path.join(ROOT, "profiles", f"{kernel}_dambreak3d.md")
+    if not os.path.exists(p):
+        return None
+    with open(p) as f:
+        for line in f:
+            if line.strip().startswith("dram_bytes_per_launch_at_bench_size:"):
+                try:
+                    return float(line.split(":", 1)[1].split()[0])
+                except ValueError:
+                    return None
+    return None
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled every 200 ms during a region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index):
+        self.gpu = gpu_index
+        self.proc = None
+        self.path = os.path.join(ROOT, "_work", f"clocks_{os.getpid()}.csv")
+
+    def start(self):
+        try:
+            os.makedirs(os.path.dirname(self.path), exist_ok=True)
+            self.f = open(self.path, "w")
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.gpu}", f"--query-gpu={self.FIELDS}",
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=self.f, stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+
+    def stop(self):
+        if self.proc is None:
+            return None
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        self.f.close()
+        sm, mx, reasons = [], None, set()
+        names = ("hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap")
+        with open(self.path) as f:
+            for line in f:
+                parts = [t.strip() for t in line.split(",")]
+                if len(parts) < 9:
+                    continue
+                try:
+                    sm.append(float(parts[1]))
+                    mx = float(parts[2])
+                except ValueError:
+                    continue
+                for nm, val in zip(names, parts[5:9]):
+                    if val.lower() == "active":
+                        reasons.add(nm)
+        try:
+            os.remove(self.path)
+        except OSError:
+            pass
+        if not sm:
+            return None
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": mx, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def dist_setup():
+    ws = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return ws, rank, local
+
+
+def cpu_baseline(ps, steps_target_s=15.0, max_steps=6, threads=None):
+    """The CPU restatement (float32, all host threads) on the same workload."""
+    from oracle.oracle import Oracle, state_from_sets
+    from sigmasph_b200.solver import build_params
+    nt = Oracle.threads(threads or os.cpu_count())
+    p = build_params(ps)
+    st = state_from_sets(ps.state_numpy())
+    orc = Oracle(p, ps.particle_max_num, fp64=False)
+    orc.set_state(st, p.CFL * p.support_radius / p.c_signal)
+    orc.stage(0)
+    t0 = time.perf_counter()
+    orc.step(1)       # warm-up step
+    t_warm = time.perf_counter() - t0
+    k = max(1, min(max_steps, int(steps_target_s / max(t_warm, 1e-3))))
+    t0 = time.perf_counter()
+    orc.step(k)
+    el = time.perf_counter() - t0
+    return {"value": ps.particle_max_num * k / el, "unit": UNIT, "cores": nt,
+            "kind": "port",
+            "sample": f"{k} step(s) of the full {ps.particle_max_num}-particle workload after 1 "
+                      f"warm-up step, CPU restatement of the reference kernels (float32, "
+                      f"OpenMP, {nt} threads); the reference's own Taichi run is not installable"}
+
+
+def run_reference(args):
+    ws, rank, local = dist_setup()
+    if rank != 0:
+        return 0
+    from sigmasph_b200.config import SimConfig
+    from sigmasph_b200.particle_system import ParticleSystem
+    from sigmasph_b200.scenes import dambreak3d
+    from oracle.oracle import Oracle, state_from_sets
+    from sigmasph_b200.solver import build_params
+    cfg = SimConfig(dambreak3d(dx=args.dx))
+    ps = ParticleSystem(cfg, device="cpu")
+    nt = Oracle.threads(os.cpu_count())
+    p = build_params(ps)
+    orc = Oracle(p, ps.particle_max_num, fp64=False)
+    orc.set_state(state_from_sets(ps.state_numpy()), p.CFL * p.support_radius / p.c_signal)
+    orc.stage(0)
+    t0 = time.perf_counter()
+    orc.step(args.warmup)
+    t_w = time.perf_counter() - t0
+    t0 = time.perf_counter()
+    orc.step(args.steps)
+    el = time.perf_counter() - t0
+    n = ps.particle_max_num
+    val = n * args.steps / el
+    line = {"impl": "reference", "metric": METRIC, "value": val, "unit": UNIT,
+            "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": 1000.0 * el / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": {"workload": "3D dam break, delta+-SPH, reflecting walls",
+                       "particles": n, "dx_m": args.dx, "support_dx": 2.6,
+                       "parallelism": "host threads"},
+            "cpu_baseline": {"value": val, "unit": UNIT, "cores": nt, "kind": "port",
+                             "sample": f"the full workload, {args.warmup} warm-up + {args.steps} "
+                                       "timed steps; CPU restatement of the reference kernels "
+                                       "(the reference's Taichi is not installable here)"},
+            "e2e": {"value": val, "unit": UNIT, "h2d_bytes_per_step": 0,
+                    "d2h_bytes_per_step": 0}}
+    print(json.dumps(line))
+    return 0
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=40)
+    ap.add_argument("--warmup", type=int, default=6)
+    ap.add_argument("--impl", default="b200", choices=("b200", "reference"))
+    ap.add_argument("--dx", type=float, default=DX_1M)
+    ap.add_argument("--e2e-steps", type=int, default=None)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--profile-steps", type=int, default=4)
+    args = ap.parse_args()
+    if args.warmup < 3:
+        args.warmup = 3
+    if args.impl == "reference":
+        return run_reference(args)
+
+    import torch
+    ws, rank, local = dist_setup()
+    torch.cuda.set_device(local)
+    dist = None
+    if ws > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+    from sigmasph_b200 import abi
+    from sigmasph_b200.config import SimConfig
+    from sigmasph_b200.particle_system import ParticleSystem
+    from sigmasph_b200.scenes import dambreak3d
+
+    cfg = SimConfig(dambreak3d(dx=args.dx))
+    ps = ParticleSystem(cfg, device=f"cuda:{local}")
+    n = ps.particle_max_num
+    cpu_ps = None
+    if rank == 0 and ws == 1 and not args.no_cpu_baseline:
+        cpu_ps = ParticleSystem(SimConfig(dambreak3d(dx=args.dx)), device="cpu")
+    solver = ps.build_solver()
+    solver.initialize()
+    stream = torch.cuda.current_stream()
+
+    # warm-up (builds the two-step CUDA graph)
+    solver.step_many(args.warmup + (args.warmup & 1))
+    torch.cuda.synchronize()
+
+    def barrier():
+        if dist is not None:
+            dist.barrier()
+
+    # ---------------------------------------------------------------- timed region
+    K = args.steps
+    clocks = ClockSampler(local)
+    barrier()
+    torch.cuda.synchronize()
+    clocks.start()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    solver.step_many(K)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    barrier()
+    ck = clocks.stop()
+    ms = e0.elapsed_time(e1)
+    if dist is not None:
+        t = torch.tensor([ms], device=f"cuda:{local}", dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+    err = solver.error_word()
+    value = ws * n * K / (ms / 1000.0)
+
+    # ---------------------------------------------------------------- e2e through the public API
+    # Per step, as the reference's driver loop does (run_simulation.py:1186-1209): write
+    # dt from page-locked host memory, solver.step(), read dt back (synchronises).
+    Ke = args.e2e_steps or K
+    dt = solver.dt[None]
+    barrier()
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for _ in range(Ke):
+        solver.dt[None] = dt
+        solver.step()
+        dt = solver.dt[None]
+    torch.cuda.synchronize()
+    el = time.perf_counter() - t0
+    if dist is not None:
+        t = torch.tensor([el], device=f"cuda:{local}", dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        el = float(t.item())
+    e2e = {"value": ws * n * Ke / el, "unit": UNIT, "h2d_bytes_per_step": 4,
+           "d2h_bytes_per_step": 4}
+
+    # ---------------------------------------------------------------- per-kernel timing
+    solver.profile(True)
+    for _ in range(args.profile_steps):
+        solver.step()
+    prof = solver.profile_read()
+    solver.profile(False)
+    launches_per_step = sum(c for _, c in prof.values()) / max(args.profile_steps, 1)
+    per_step_ms = {k: v[0] / args.profile_steps for k, v in prof.items()}
+    dom = max((k for k in prof if k in ALGO_BYTES), key=lambda k: per_step_ms[k])
+    dom_ms = prof[dom][0] / prof[dom][1]
+    peak, peak_kind = load_peaks()
+    achieved = ALGO_BYTES[dom] * n / (dom_ms / 1000.0) / 1e9
+    traffic = read_traffic(dom)
+    roofline = {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peak,
+                "unit": "GB/s", "frac": achieved / peak, "peak_source": peak_kind,
+                "algorithmic_bytes_per_particle": ALGO_BYTES[dom],
+                "launch_ms": dom_ms, "traffic": traffic}
+
+    if rank == 0:
+        line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": ws, "steps": K,
+                "warmup": args.warmup, "ms_per_step": ms / K, "higher_is_better": True,
+                "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+                "config": {"workload": "3D dam break, delta+-SPH, reflecting walls",
+                           "particles": n, "dx_m": args.dx, "support_dx": 2.6,
+                           "parallelism": "replicas" if ws > 1 else "single GPU",
+                           "l2": "inputs larger than L2 (state + neighbour lists ~1 GB)",
+                           "graph": "two-step CUDA graph replayed"},
+                "e2e": e2e, "gpu_launches": int(round(launches_per_step * K)),
+                "roofline": roofline,
+                "kernel_ms_per_step": {k: round(v, 5) for k, v in sorted(per_step_ms.items(),
+                                                                       key=lambda t: -t[1])},
+                "error_word": err}
+        if ck is not None:
+            line["clocks"] = ck
+        if cpu_ps is not None:
+            try:
+                line["cpu_baseline"] = cpu_baseline(cpu_ps)
+            except Exception as e:  # the baseline is reported, not required
+                line["cpu_baseline"] = {"value": None, "error": str(e)}
+        print(json.dumps(line))
+    if dist is not None:
+        dist.barrier()
+        dist.destroy_process_group()
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

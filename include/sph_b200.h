@@ -1,0 +1,271 @@
+/*
+ * sph_b200.h -- C-ABI of libsph_b200.so, the B200 (sm_100a) per-step particle hot path
+ * of the sigmaSPH delta+-SPH fluid and hypoelastic tensile-solid solvers.
+ *
+ * The reference has no FFI: its hot path sits behind the solver object's Python API
+ * (ParticleSystem fields, solver.initialize(), solver.step(), solver.dt[None], the
+ * energy/momentum reductions and get_constraint_data()).  Each entry point below
+ * replaces one of those calls; the reference method it stands in for is cited beside it
+ * by file:line within the sigmaSPH source tree.  The Python package sigmasph_b200 binds
+ * these with ctypes and keeps the reference's attribute names.
+ *
+ * Conventions
+ *  - Plain C types only.  Device pointers are passed as raw pointers; `stream` is a
+ *    cudaStream_t passed as void* (NULL = the legacy default stream).
+ *  - Every function returns an int status: 0 = SPH_OK, < 0 = error (sph_strerror()).
+ *    No exception crosses the boundary.
+ *  - The caller owns every per-particle buffer (PyTorch tensors in the Python host
+ *    layer).  The library allocates only scratch: sort keys, permutation, cell table,
+ *    neighbour lists, device scalars.
+ *  - The persistent particle state lives in TWO buffer sets (A and B).  Every neighbour
+ *    rebuild gathers the state from the current set into the other one in the new
+ *    order and flips the parity; sph_parity() says which set is current.
+ */
+#ifndef SPH_B200_H
+#define SPH_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define SPH_ABI_VERSION 3
+
+/* ---------------------------------------------------------------- status codes */
+#define SPH_OK                 0
+#define SPH_ERR_ARG           -1   /* bad argument (null pointer, n > n_max, ...)          */
+#define SPH_ERR_CUDA          -2   /* a CUDA runtime call failed                           */
+#define SPH_ERR_NOMEM         -3   /* scratch allocation failed                            */
+#define SPH_ERR_UNSUPPORTED   -4   /* option the library does not implement                */
+#define SPH_ERR_NOT_BOUND     -5   /* sph_bind() has not been called                       */
+#define SPH_ERR_NEIGHBOUR_CAP -6   /* reserved: neighbour-list overflow is handled in-kernel */
+#define SPH_ERR_TIMEOUT       -7   /* a bounded device wait ran out                        */
+#define SPH_ERR_SCRATCH_CAP   -8   /* request exceeds the fixed static scratch capacity    */
+
+/* Device error-word bits (SphScalars.err).  Set by kernels, never by a trap. */
+#define SPH_EW_NBR_OVERFLOW   0x1  /* a particle had more neighbours than the list holds;
+                                      its extra pairs were found by a direct search      */
+#define SPH_EW_HASHED_GRID    0x2  /* the occupied cell box did not fit the dense Morton
+                                      table; the step ran on the hashed fallback table   */
+#define SPH_EW_JC_NO_CONVERGE 0x4  /* a Johnson-Cook return map hit its iteration cap     */
+#define SPH_EW_STS_CAP        0x8  /* the hourglass sub-cycle count hit its cap          */
+
+/* ------------------------------------------------------------------ parameters */
+/* Flattened, resolved scene configuration.  Field meanings follow the reference's
+ * registry (params.py) and the solver constructors (DSPH.py:64-450, SOLID.py:138-1452).
+ * Appended-to only; struct_size guards the layout. */
+typedef struct SphParams {
+    int32_t struct_size;          /* sizeof(SphParams), checked by sph_create           */
+    int32_t is_solid;             /* simulationMethod == hypoElastic                    */
+    /* --- domain (particle_system.py:25-350) --- */
+    int32_t two_d;                /* plane_strain || axisymmetric                       */
+    int32_t axisymmetric;
+    int32_t plane_strain;
+    int32_t sym_y, sym_z;         /* Cartesian symmetry planes (mirror sweeps)          */
+    int32_t walls;                /* Domain.boundary == reflect                          */
+    int32_t displacement_positions;
+    int32_t compensated_volume;
+    float   support_radius;       /* h: kernel support == grid cell size                */
+    float   particle_diameter;    /* dx0                                                */
+    float   V0;                   /* dx0^2 (single layer) or dx0^3                      */
+    float   axi_r_min;            /* floor on r in axisymmetry                          */
+    float   domain_size[3];
+    float   padding;              /* wall offset == grid size                           */
+    float   wall_restitution;
+    /* --- fluid solver (DSPH.py) --- */
+    float   density0;
+    float   c0;
+    float   exponent;
+    float   stiffness;            /* c0^2 rho0 / exponent                               */
+    float   viscosity;
+    float   CFL;
+    float   delta_sph;
+    float   gravity[3];
+    int32_t allow_negative_pressure;
+    int32_t track_visc_work;
+    float   l_eig_tol_lam;        /* regularised-inverse tolerance for L (0.02)         */
+    float   c_signal;             /* CFL floor speed: c0 (fluid) or c_p (solid)         */
+    int32_t dt_pair_mode;         /* 0 off, 1 all pairs, 2 same-material pairs          */
+    /* --- particle shifting (DSPH.py:190-330, 943-1049) --- */
+    int32_t pst_enabled;
+    int32_t pst_colle;            /* 0 = Sun, 1 = Colle                                 */
+    int32_t pst_ma_mode;          /* 0 local, 1 global, 2 fixed                         */
+    int32_t pst_clamp_disp;
+    int32_t pst_clamp_vel;
+    int32_t pst_surface_none;
+    int32_t pst_normal_eigvec;
+    int32_t pst_ale_momentum;
+    float   pst_R;
+    int32_t pst_n;
+    float   pst_max_shift;
+    float   pst_ma_fixed;
+    float   pst_m_delta;
+    float   pst_lambda_lo;
+    float   pst_lambda_hi;
+    /* --- hypoelastic solid (SOLID.py); ignored unless is_solid --- */
+    int32_t n_materials;          /* rows used in the material tables below (<= 4)      */
+    float   mat_rho0[4];
+    float   mat_K[4];
+    float   mat_G[4];
+    float   mat_cp[4];            /* dilatational speed sqrt((K + 4G/3)/rho0)           */
+    float   mat_c0[4];            /* EOS sound speed sqrt(K/rho0)                       */
+    float   mat_delta[4];         /* per-material delta-SPH coefficient                 */
+    int32_t plastic_kind[4];      /* 0 none, 1 linear (J2), 2 Johnson-Cook              */
+    float   plastic_sy0[4];
+    float   plastic_H[4];
+    float   jc_A[4], jc_B[4], jc_n[4], jc_C[4], jc_eps0_dot[4];
+    int32_t kernel_correction;    /* grad v through the regularised inverse of E        */
+    float   l_eig_tol;            /* tolerance of that inverse (0.1)                    */
+    float   hourglass_alpha;
+    int32_t hourglass_sts;        /* 0 in-loop damper + dt clamp, 1 sub-cycled          */
+    int32_t hourglass_sts_cap;    /* max sub-cycle stages                               */
+    float   hourglass_sts_safety; /* 1.6 */
+    float   hg_S;                 /* lattice kernel sum of the damper (SOLID.py:1632)   */
+    float   hg_W_dx0;             /* W(dx0)                                            */
+    int32_t hg_sts_refresh;       /* recompute grad v after the half kick               */
+    int32_t ale_history;          /* ALE transport of s, eps_p                          */
+    int32_t transport_e;          /* ALE transport of e_int                             */
+    float   ale_diffusion;        /* xi of the upwind ALE diffusion (1.0)               */
+    int32_t num_constraints;      /* grips (<= 8)                                       */
+    float   ramp_time;
+    int32_t jc_surrogate;         /* 1: MLP return map with Newton fallback             */
+    float   jc_surrogate_tol;     /* |f_yield| / sigma_y acceptance (1e-3)              */
+    int32_t reserved[8];
+} SphParams;
+
+/* ------------------------------------------------------------------ buffers */
+/* One set of the persistent (sorted) per-particle state.  Row-major [n][k] float32
+ * unless noted.  Vector fields carry a fourth float so every record is one 16-byte
+ * load; the fourth slot holds a scalar field of the reference (named below). */
+typedef struct SphFieldSet {
+    float*   pos;      /* [n][4] x, y, z, V         (ps.x, ps.V)                         */
+    float*   vel;      /* [n][4] vx, vy, vz, m      (ps.v, ps.m)                         */
+    float*   x0;       /* [n][4] x0, y0, z0, V_lo   (ps.x_0, ps.V_lo)                    */
+    float*   disp;     /* [n][4] ux, uy, uz, p      (ps.u, ps.pressure)                  */
+    float*   shift;    /* [n][4] dr_x, dr_y, dr_z, e_int (ps.pst_shift, ps.e_int)        */
+    int32_t* pid;      /* [n] persistent particle id (index at creation)                 */
+    /* solid only (may be NULL for a fluid run) */
+    float*   sdev;     /* [n][8] s_xx, s_yy, s_zz, s_xy, s_xz, s_yz, eps_p, T            */
+    int32_t* bc;       /* [n][2] bc_flag, bc_id                                         */
+    float*   bcdisp;   /* [n][4] bc_disp xyz, eos_id (as float)                         */
+} SphFieldSet;
+
+/* Per-step derived fields (one copy, overwritten every step before they are read). */
+typedef struct SphBuffers {
+    SphFieldSet set[2];
+    float* acc;        /* [n][4] ax, ay, az, de_visc (de_int on the solid path)          */
+    float* lam;        /* [n]                                                            */
+    float* lsym;       /* [n][8] L_00, L_11, L_22, L_01, L_02, L_12, -, -                */
+    float* lgrad;      /* [n][4] grad lambda (or the min eigenvector under eigvec)       */
+    float* div;        /* [n][4] divergence, diffusion rate, -, -                        */
+    float* gradv;      /* [n][12] grad v (row-major 3x3) + 3 spare (solid)               */
+    float* aux;        /* [n][8] solid scratch: hg y_a, y_b, a (STS), d_eps_prod          */
+} SphBuffers;
+
+/* Device scalars copied back by sph_get_scalars (the reference's 0-d fields). */
+typedef struct SphScalars {
+    float   dt;               /* solver.dt[None]                                         */
+    float   max_c_sq;         /* solver.max_c_sq[None]                                   */
+    float   max_accel;        /* solver.max_accel[None]                                  */
+    float   max_v;            /* solver.max_v[None]                                      */
+    int32_t off_grid_num;     /* ps.off_grid_num[None]                                   */
+    int32_t err;              /* SPH_EW_* bits accumulated since the last reset           */
+    int32_t sts_stages;       /* last hourglass sub-cycle count                           */
+    int32_t pad0;
+    double  off_grid_mass;    /* ps.off_grid_mass[None]                                  */
+    double  wall_work;        /* SPHBase.wall_work                                       */
+    double  visc_work;        /* DSPHSolver.visc_work                                    */
+    double  diff_work;        /* DSPHSolver.diff_work                                    */
+    double  leftover_work;    /* DSPHSolver.leftover_work                                */
+    double  plastic_work;     /* HypoElasticSolver plastic work                          */
+    double  hg_work;          /* HypoElasticSolver hourglass work                        */
+    double  sim_time;         /* HypoElasticSolver.sim_time                              */
+    float   load_s, load_sdot;/* HypoElasticSolver.load_s / load_sdot                    */
+    double  constraint_force[8][3];
+    double  constraint_disp[8][3];
+} SphScalars;
+
+/* Reduction indices of sph_reduce(). */
+enum {
+    SPH_RED_KE = 0, SPH_RED_KE_OFFGRID, SPH_RED_PE, SPH_RED_SE, SPH_RED_IE,
+    SPH_RED_MASS, SPH_RED_PX, SPH_RED_PY, SPH_RED_PZ, SPH_RED_GROSS_P,
+    SPH_RED_ELASTIC, SPH_RED_COUNT
+};
+
+typedef struct SphHandle SphHandle;
+
+/* Library identity and layout checks. */
+int         sph_abi_version(void);
+size_t      sph_params_size(void);
+size_t      sph_scalars_size(void);
+const char* sph_strerror(int status);
+/* Writes "name=offset;..." for every SphParams field into buf (for the host layer's
+ * layout check).  Returns the number of bytes needed. */
+int         sph_params_layout(char* buf, int cap);
+
+/* Set-up: ParticleSystem.__init__ + build_solver (particle_system.py:25-475, :958-966,
+ * DSPH.py:64-450, SOLID.py:138-1452).  Allocates scratch for n_max particles. */
+int  sph_create(const SphParams* p, int64_t n_max, SphHandle** out);
+void sph_destroy(SphHandle* h);
+/* Attach the caller's buffers; n = particle_num[None] (particle_system.py:269). */
+int  sph_bind(SphHandle* h, const SphBuffers* b, int64_t n);
+/* Which SphFieldSet holds the current state (0 or 1). */
+int  sph_parity(const SphHandle* h);
+/* Upload per-material constraint/material tables after a change on the host. */
+int  sph_set_params(SphHandle* h, const SphParams* p);
+
+/* ParticleSystem.initialize_particle_system (particle_system.py:1342-1345): rebuild the
+ * cell table, reorder every persistent field, rebuild the neighbour lists. */
+int  sph_initialize(SphHandle* h, void* stream);
+/* SPHBase.step (sph_base.py:622-655) / HypoElasticSolver.step (SOLID.py:5227-5231),
+ * nsteps times, asynchronously on `stream`; dt stays on the device. */
+int  sph_step(SphHandle* h, int nsteps, void* stream);
+/* One named stage of the step, for stage-by-stage parity tests (SPH_STAGE_*). */
+int  sph_run_stage(SphHandle* h, int stage, void* stream);
+/* solver.dt[None] read/write (DSPH.py:124-131, run_simulation.py:1190-1211). */
+int  sph_set_dt(SphHandle* h, float dt, void* stream);
+/* solver.dt[None] read: 4 bytes device -> page-locked host (synchronises `stream`). */
+int  sph_get_dt(SphHandle* h, float* dt, void* stream);
+/* Copies the device scalars (synchronises `stream`). */
+int  sph_get_scalars(SphHandle* h, SphScalars* out, void* stream);
+int  sph_clear_error(SphHandle* h, void* stream);
+/* FP64 reductions: compute_kinetic_energy / _off_grid / potential / elastic /
+ * internal / total_mass (sph_base.py:425-557, DSPH.py:1670-1712) and compute_momentum /
+ * compute_gross_momentum (sph_base.py:560-620), into out[SPH_RED_COUNT]. */
+int  sph_reduce(SphHandle* h, double* out, void* stream);
+/* Neighbour pairs of the current bins (for_all_neighbors, particle_system.py:1348-1490):
+ * mode 0 = the list built at the last rebuild; mode 1 = a fresh search from the live
+ * positions against the stale bins (the PST sweep, DSPH.py:771-886).  Writes up to cap
+ * (i, j, mirror) triples as current-order indices and the total into *count. */
+int  sph_pairs(SphHandle* h, int mode, int32_t* pi, int32_t* pj, int32_t* mir,
+               int64_t cap, int64_t* count, void* stream);
+
+/* Per-kernel timing with CUDA events recorded on the launching stream around every
+ * kernel of eagerly launched steps (sph_step with nsteps == 1, sph_run_stage).  Off by
+ * default; graph replays are not instrumented. */
+int  sph_profile_enable(SphHandle* h, int on);
+/* Synchronises, then writes up to cap entries: '\n'-separated kernel names into names,
+ * total milliseconds into ms and launch counts into launches; *count = entries.  Resets
+ * the accumulators. */
+int  sph_profile_read(SphHandle* h, char* names, int names_cap, double* ms, int* launches,
+                      int cap, int* count);
+
+/* Stage ids for sph_run_stage. */
+enum {
+    SPH_STAGE_SORT = 0,        /* initialize_particle_system                           */
+    SPH_STAGE_LAM = 1,         /* DSPHSolver.compute_lam, both passes                  */
+    SPH_STAGE_CONTINUITY = 2,  /* compute_volume_evolution                             */
+    SPH_STAGE_FORCES = 3,      /* non-pressure + pressure accelerations (+ dt pair max) */
+    SPH_STAGE_DT = 4,          /* compute_adaptive_dt                                  */
+    SPH_STAGE_ADVECT = 5,      /* accumulate_step_work + advect                        */
+    SPH_STAGE_PST = 6,         /* apply_pst                                            */
+    SPH_STAGE_BOUNDARY = 7,    /* constraints / walls at the end of SPHBase.step       */
+    SPH_STAGE_COUNT_FLUID = 8
+};
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* SPH_B200_H */

@@ -1,0 +1,75 @@
+"""Builds libsph_b200.so in-tree for sm_100a (nvcc cross-compiles without a GPU).
+
+    python -m sigmasph_b200.build [--force]
+"""
+from __future__ import annotations
+
+import os
+import shutil
+import subprocess
+import sys
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.dirname(HERE)
+CSRC = os.path.join(HERE, "csrc")
+OUT_DIR = os.path.join(HERE, "_build")
+LIB = os.path.join(OUT_DIR, "libsph_b200.so")
+MAIN = os.path.join(CSRC, "sph_b200.cu")
+
+NVCC_FLAGS = [
+    "-gencode", "arch=compute_100a,code=sm_100a",
+    "-lineinfo", "-O3", "-std=c++17",
+    "-Xcompiler", "-fPIC", "-shared",
+]
+
+
+def _sources():
+    srcs = [os.path.join(CSRC, f) for f in os.listdir(CSRC) if f.endswith((".cu", ".cuh"))]
+    srcs.append(os.path.join(ROOT, "include", "sph_b200.h"))
+    return srcs
+
+
+def nvcc_path():
+    p = shutil.which("nvcc")
+    if p:
+        return p
+    cand = "/usr/local/cuda/bin/nvcc"
+    if os.path.exists(cand):
+        return cand
+    raise RuntimeError("nvcc not found")
+
+
+def host_compiler():
+    """nvcc's host compiler: the system g++ (a CXX from the environment may lack the
+    runtime specs)."""
+    for c in ("/usr/bin/g++", shutil.which("g++")):
+        if c and os.path.exists(c):
+            return c
+    return None
+
+
+def build(force=False, verbose=False):
+    os.makedirs(OUT_DIR, exist_ok=True)
+    if not force and os.path.exists(LIB):
+        t = os.path.getmtime(LIB)
+        if all(os.path.getmtime(s) <= t for s in _sources()):
+            return LIB
+    cmd = [nvcc_path()] + NVCC_FLAGS
+    cc = host_compiler()
+    if cc:
+        cmd += ["-ccbin", cc]
+    if verbose:
+        cmd += ["-Xptxas", "-v"]
+    tmp = LIB + ".tmp"
+    cmd += ["-o", tmp, MAIN]
+    r = subprocess.run(cmd, capture_output=True, text=True)
+    if r.returncode != 0:
+        raise RuntimeError("nvcc failed:\n" + r.stdout + r.stderr)
+    if verbose:
+        sys.stderr.write(r.stderr)
+    os.replace(tmp, LIB)
+    return LIB
+
+
+if __name__ == "__main__":
+    print(build(force="--force" in sys.argv, verbose="-v" in sys.argv))

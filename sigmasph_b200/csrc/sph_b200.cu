@@ -1,0 +1,647 @@
+// sph_b200.cu -- libsph_b200.so: the C-ABI of include/sph_b200.h over the sm_100a
+// kernels of sph_grid.cuh / sph_fluid.cuh / sph_solid.cuh.  One translation unit.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstddef>
+#include <string>
+#include <cstdio>
+#include <cstring>
+#include <new>
+#include <vector>
+
+#include "sph_fluid.cuh"
+#include "sph_solid.cuh"
+
+using namespace sph;
+
+struct SphHandle {
+    SphParams p;
+    Cst c;
+    int64_t n_max = 0;
+    int64_t n = 0;
+    int parity = 0;
+    bool bound = false;
+    SphBuffers buf;
+    int device = 0;
+    // scratch
+    int4* cell = nullptr;
+    int4* cell_tmp = nullptr;
+    int* key = nullptr;
+    int* rank = nullptr;
+    int* perm = nullptr;
+    int* hist = nullptr;
+    int* start = nullptr;
+    int* bsum = nullptr;
+    int* bbox = nullptr;
+    GridLayout* layout = nullptr;
+    int* nbr = nullptr;
+    int* nbr_cnt = nullptr;
+    DevScalars* sc = nullptr;
+    DevAccum* ac = nullptr;
+    SphScalars* pinned = nullptr;   // page-locked staging of the scalar copies
+    SolidScratch solid;
+    // CUDA graph of two consecutive steps (parity returns to where it started)
+    cudaGraphExec_t graph2 = nullptr;
+    cudaStream_t cap_stream = nullptr;
+    // per-kernel event profile of eager launches
+    bool prof_on = false;
+    bool capturing = false;
+    std::vector<std::pair<const char*, cudaEvent_t>> prof_marks;
+    std::vector<cudaEvent_t> prof_pool;
+    size_t prof_used = 0;
+};
+
+namespace {
+
+// Records an event after a launch when profiling an eager launch sequence; the kernel's
+// time is the interval since the previous mark.
+void prof_mark(SphHandle* h, const char* name, cudaStream_t st) {
+    if (!h->prof_on || h->capturing) return;
+    if (h->prof_used == h->prof_pool.size()) {
+        cudaEvent_t e;
+        if (cudaEventCreate(&e) != cudaSuccess) return;
+        h->prof_pool.push_back(e);
+    }
+    cudaEvent_t e = h->prof_pool[h->prof_used++];
+    cudaEventRecord(e, st);
+    h->prof_marks.emplace_back(name, e);
+}
+#define LAUNCH(name, ...)            \
+    do {                             \
+        __VA_ARGS__;                 \
+        prof_mark(h, name, st);      \
+    } while (0)
+
+#define CK(x)                                                                        \
+    do {                                                                             \
+        cudaError_t e_ = (x);                                                        \
+        if (e_ != cudaSuccess) {                                                     \
+            fprintf(stderr, "libsph_b200: %s failed: %s\n", #x, cudaGetErrorString(e_)); \
+            return SPH_ERR_CUDA;                                                     \
+        }                                                                            \
+    } while (0)
+
+inline int blocks_for(int64_t n) { return (int)((n + kBlock - 1) / kBlock) > 0 ? (int)((n + kBlock - 1) / kBlock) : 1; }
+inline cudaStream_t S(void* s) { return reinterpret_cast<cudaStream_t>(s); }
+
+// Smallest float t with sqrtf(t) >= h: |r| < h  <=>  |r|^2 < t for the rounded |r|^2.
+float d2_threshold(float h) {
+    float t = (float)((double)h * (double)h);
+    for (int k = 0; k < 64 && std::sqrt(std::nextafter(t, 0.0f)) >= h; ++k) t = std::nextafter(t, 0.0f);
+    for (int k = 0; k < 64 && std::sqrt(t) < h; ++k) t = std::nextafter(t, INFINITY);
+    return t;
+}
+
+void fill_constants(SphHandle* h) {
+    const SphParams& p = h->p;
+    Cst& c = h->c;
+    c.p = p;
+    c.n = (int)h->n;
+    double hd = p.support_radius;
+    double al = p.two_d ? 7.0 / (M_PI * hd * hd) : 21.0 / (2.0 * M_PI * hd * hd * hd);
+    c.h = (float)hd;
+    c.alpha = (float)al;
+    c.kgrad = (float)(20.0 * al / hd);
+    c.eta2 = (float)(0.01 * hd * hd);
+    {
+        float r = p.particle_diameter, q = r / c.h;
+        float W = 0.0f;
+        if (q < 1.0f) { float t = 1.0f - q; float t2 = t * t; W = c.alpha * (t2 * t2) * (4.0f * q + 1.0f); }
+        c.W_dx0 = W;
+    }
+    c.d2_lt = d2_threshold(c.h);
+    c.visc_coef = (float)(10.0 * (double)p.viscosity);
+    c.delta_coef = p.delta_sph * c.h * p.c0;
+    c.cfl_h = (float)((double)p.CFL * (double)p.support_radius);
+    for (int k = 0; k < 3; ++k) c.wall_hi[k] = (float)((double)p.domain_size[k] - (double)p.padding);
+    c.rest_1p = (float)(1.0 + (double)p.wall_restitution);
+    c.rest_loss = (float)(1.0 - (double)p.wall_restitution * (double)p.wall_restitution);
+    c.max_shift = (float)((double)p.pst_max_shift * (double)p.particle_diameter);
+    c.colle_coef = (float)(-2.0 * (double)p.support_radius);
+    c.sun_coef = -p.CFL;
+    c.mirror_y = (p.axisymmetric || p.sym_y) ? 1 : 0;
+    c.mirror_z = p.sym_z ? 1 : 0;
+    solid_fill_constants(c);
+}
+
+Ptr make_ptr(SphHandle* h) {
+    Ptr P;
+    P.cur = h->buf.set[h->parity];
+    P.nxt = h->buf.set[1 - h->parity];
+    P.acc = reinterpret_cast<float4*>(h->buf.acc);
+    P.lam = h->buf.lam;
+    P.lsym = reinterpret_cast<float4*>(h->buf.lsym);
+    P.lgrad = reinterpret_cast<float4*>(h->buf.lgrad);
+    P.div = reinterpret_cast<float4*>(h->buf.div);
+    P.gradv = h->buf.gradv;
+    P.aux = reinterpret_cast<float4*>(h->buf.aux);
+    P.cell = h->cell;
+    P.cell_tmp = h->cell_tmp;
+    P.key = h->key;
+    P.rank = h->rank;
+    P.perm = h->perm;
+    P.hist = h->hist;
+    P.start = h->start;
+    P.bsum = h->bsum;
+    P.bbox = h->bbox;
+    P.layout = h->layout;
+    P.nbr = h->nbr;
+    P.nbr_cnt = h->nbr_cnt;
+    P.sc = h->sc;
+    P.ac = h->ac;
+    return P;
+}
+
+void drop_graph(SphHandle* h) {
+    if (h->graph2) { cudaGraphExecDestroy(h->graph2); h->graph2 = nullptr; }
+}
+
+int scan_tiles(const SphHandle* h) { return (int)((h->c.mcap + 1 + kScanTile - 1) / kScanTile); }
+
+// initialize_particle_system + the neighbour-list rebuild.
+int rebuild(SphHandle* h, cudaStream_t st) {
+    const int nb = blocks_for(h->n);
+    Ptr P = make_ptr(h);
+    const Cst& c = h->c;
+    prof_mark(h, "", st);
+    LAUNCH("k_grid_reset", k_grid_reset<<<1, 32, 0, st>>>(P));
+    LAUNCH("k_cells", k_cells<<<nb, kBlock, 0, st>>>(c, P));
+    LAUNCH("k_layout", k_layout<<<1, 32, 0, st>>>(c, P));
+    int zb = (int)std::min<int64_t>((c.mcap + 2 + kBlock - 1) / kBlock, 148 * 16);
+    LAUNCH("k_zero_hist", k_zero_hist<<<zb, kBlock, 0, st>>>(c, P));
+    LAUNCH("k_keys", k_keys<<<nb, kBlock, 0, st>>>(c, P));
+    int tiles = scan_tiles(h);
+    int sb = std::min(tiles, 148 * 8);
+    LAUNCH("k_scan_reduce", k_scan_reduce<<<sb, kBlock, 0, st>>>(P));
+    LAUNCH("k_scan_bsum", k_scan_bsum<<<1, 1024, 0, st>>>(P));
+    LAUNCH("k_scan_apply", k_scan_apply<<<sb, kBlock, 0, st>>>(P));
+    LAUNCH("k_scatter", k_scatter<<<nb, kBlock, 0, st>>>(c, P));
+    LAUNCH("k_stabilise", k_stabilise<<<nb, kBlock, 0, st>>>(c, P));
+    LAUNCH("k_gather", k_gather<<<nb, kBlock, 0, st>>>(c, P));
+    h->parity ^= 1;
+    P = make_ptr(h);
+    LAUNCH("k_nbr_build", k_nbr_build<<<nb, kBlock, 0, st>>>(c, P));
+    return SPH_OK;
+}
+
+int fluid_substep_and_boundary(SphHandle* h, cudaStream_t st) {
+    const int nb = blocks_for(h->n);
+    const Cst& c = h->c;
+    Ptr P = make_ptr(h);
+    LAUNCH("k_lam", k_lam<<<nb, kBlock, 0, st>>>(c, P));
+    LAUNCH("k_lamgrad_cont", k_lamgrad_cont<<<nb, kBlock, 0, st>>>(c, P));
+    LAUNCH("k_eos", k_eos<<<nb, kBlock, 0, st>>>(c, P));
+    LAUNCH("k_force", k_force<<<nb, kBlock, 0, st>>>(c, P));
+    LAUNCH("k_dt", k_dt<<<1, 32, 0, st>>>(c, P));
+    LAUNCH("k_advect", k_advect<<<nb, kBlock, 0, st>>>(c, P));
+    if (h->p.pst_enabled) {
+        LAUNCH("k_pst", k_pst<<<nb, kBlock, 0, st>>>(c, P));
+        LAUNCH("k_finish", k_finish<<<nb, kBlock, 0, st>>>(c, P, 3));
+    } else {
+        LAUNCH("k_finish", k_finish<<<nb, kBlock, 0, st>>>(c, P, 2));
+    }
+    return SPH_OK;
+}
+
+int one_step(SphHandle* h, cudaStream_t st) {
+    int r;
+    if (h->p.is_solid) {
+        if ((r = solid_pre_step(h->c, make_ptr(h), h->solid, st)) != SPH_OK) return r;
+    }
+    if ((r = rebuild(h, st)) != SPH_OK) return r;
+    if (h->p.is_solid) return solid_substep_and_boundary(h->c, make_ptr(h), h->solid, (int)h->n, st);
+    return fluid_substep_and_boundary(h, st);
+}
+
+template <class T> int dalloc(T** p, size_t count) {
+    if (count == 0) count = 1;
+    cudaError_t e = cudaMalloc((void**)p, count * sizeof(T));
+    return e == cudaSuccess ? SPH_OK : SPH_ERR_NOMEM;
+}
+
+void free_all(SphHandle* h) {
+    drop_graph(h);
+    for (cudaEvent_t e : h->prof_pool) cudaEventDestroy(e);
+    h->prof_pool.clear();
+    if (h->cap_stream) cudaStreamDestroy(h->cap_stream);
+    void* ptrs[] = {h->cell, h->cell_tmp, h->key, h->rank, h->perm, h->hist, h->start, h->bsum,
+                    h->bbox, h->layout, h->nbr, h->nbr_cnt, h->sc, h->ac};
+    for (void* q : ptrs) if (q) cudaFree(q);
+    if (h->pinned) cudaFreeHost(h->pinned);
+    solid_free(h->solid);
+}
+
+bool valid_set(const SphFieldSet& s, bool solid) {
+    if (!s.pos || !s.vel || !s.x0 || !s.disp || !s.shift || !s.pid) return false;
+    if (solid && (!s.sdev || !s.bc || !s.bcdisp)) return false;
+    auto al = [](const void* q) { return (reinterpret_cast<uintptr_t>(q) & 15u) == 0; };
+    return al(s.pos) && al(s.vel) && al(s.x0) && al(s.disp) && al(s.shift) &&
+           (!solid || (al(s.sdev) && al(s.bcdisp) && (reinterpret_cast<uintptr_t>(s.bc) & 7u) == 0));
+}
+
+}  // namespace
+
+extern "C" {
+
+int sph_abi_version(void) { return SPH_ABI_VERSION; }
+size_t sph_params_size(void) { return sizeof(SphParams); }
+size_t sph_scalars_size(void) { return sizeof(SphScalars); }
+
+const char* sph_strerror(int status) {
+    switch (status) {
+        case SPH_OK: return "ok";
+        case SPH_ERR_ARG: return "invalid argument";
+        case SPH_ERR_CUDA: return "CUDA runtime error";
+        case SPH_ERR_NOMEM: return "device allocation failed";
+        case SPH_ERR_UNSUPPORTED: return "option not implemented by libsph_b200";
+        case SPH_ERR_NOT_BOUND: return "buffers not bound (sph_bind)";
+        case SPH_ERR_NEIGHBOUR_CAP: return "neighbour list overflow (export needs the full list)";
+        case SPH_ERR_TIMEOUT: return "bounded device wait ran out";
+        case SPH_ERR_SCRATCH_CAP: return "request exceeds the static scratch capacity";
+        default: return "unknown status";
+    }
+}
+
+int sph_params_layout(char* buf, int cap) {
+    std::string s;
+#define F(name) s += #name "=" + std::to_string(offsetof(SphParams, name)) + ";";
+    F(struct_size) F(is_solid) F(two_d) F(axisymmetric) F(plane_strain) F(sym_y) F(sym_z)
+    F(walls) F(displacement_positions) F(compensated_volume) F(support_radius)
+    F(particle_diameter) F(V0) F(axi_r_min) F(domain_size) F(padding) F(wall_restitution)
+    F(density0) F(c0) F(exponent) F(stiffness) F(viscosity) F(CFL) F(delta_sph) F(gravity)
+    F(allow_negative_pressure) F(track_visc_work) F(l_eig_tol_lam) F(c_signal) F(dt_pair_mode)
+    F(pst_enabled) F(pst_colle) F(pst_ma_mode) F(pst_clamp_disp) F(pst_clamp_vel)
+    F(pst_surface_none) F(pst_normal_eigvec) F(pst_ale_momentum) F(pst_R) F(pst_n)
+    F(pst_max_shift) F(pst_ma_fixed) F(pst_m_delta) F(pst_lambda_lo) F(pst_lambda_hi)
+    F(n_materials) F(mat_rho0) F(mat_K) F(mat_G) F(mat_cp) F(mat_c0) F(mat_delta)
+    F(plastic_kind) F(plastic_sy0) F(plastic_H) F(jc_A) F(jc_B) F(jc_n) F(jc_C) F(jc_eps0_dot)
+    F(kernel_correction) F(l_eig_tol) F(hourglass_alpha) F(hourglass_sts) F(hourglass_sts_cap)
+    F(hourglass_sts_safety) F(hg_S) F(hg_W_dx0) F(hg_sts_refresh) F(ale_history) F(transport_e)
+    F(ale_diffusion) F(num_constraints) F(ramp_time) F(jc_surrogate) F(jc_surrogate_tol)
+    F(reserved)
+#undef F
+    if (buf && cap > 0) {
+        size_t k = std::min<size_t>(s.size(), (size_t)cap - 1);
+        memcpy(buf, s.data(), k);
+        buf[k] = 0;
+    }
+    return (int)s.size();
+}
+
+int sph_create(const SphParams* p, int64_t n_max, SphHandle** out) {
+    if (!p || !out || n_max < 0 || n_max > (int64_t)kIdxMask) return SPH_ERR_ARG;
+    if (p->struct_size != (int32_t)sizeof(SphParams)) return SPH_ERR_ARG;
+    if (!(p->support_radius > 0.0f) || !(p->particle_diameter > 0.0f)) return SPH_ERR_ARG;
+    if (p->is_solid && (p->n_materials < 1 || p->n_materials > 4 || p->num_constraints < 0 ||
+                        p->num_constraints > 8))
+        return SPH_ERR_ARG;
+    *out = nullptr;
+    SphHandle* h = new (std::nothrow) SphHandle();
+    if (!h) return SPH_ERR_NOMEM;
+    h->p = *p;
+    h->n_max = n_max;
+    cudaGetDevice(&h->device);
+    // neighbour-list capacity from the lattice count at this support, with headroom
+    double ratio = (double)p->support_radius / (double)p->particle_diameter;
+    double est = p->two_d ? M_PI * ratio * ratio * 1.5 : (4.0 / 3.0) * M_PI * ratio * ratio * ratio;
+    int K = (int)std::ceil((1.5 * est + 16.0) / 32.0) * 32;
+    K = std::max(32, std::min(K, 512));
+    int64_t mcap = 131072;
+    while (mcap < 4 * n_max) mcap <<= 1;
+    int lg = 0;
+    while ((1ll << lg) < mcap) ++lg;
+    h->n = 0;
+    fill_constants(h);
+    h->c.K = K;
+    h->c.mcap = (int)mcap;
+    h->c.mcap_log2 = lg;
+    int r = SPH_OK;
+    const size_t N = (size_t)std::max<int64_t>(n_max, 1);
+    const size_t tiles = (size_t)((mcap + 1 + kScanTile - 1) / kScanTile) + 1;
+    if ((r = dalloc(&h->cell, N)) || (r = dalloc(&h->cell_tmp, N)) || (r = dalloc(&h->key, N)) ||
+        (r = dalloc(&h->rank, N)) || (r = dalloc(&h->perm, N)) ||
+        (r = dalloc(&h->hist, (size_t)mcap + 2)) || (r = dalloc(&h->start, (size_t)mcap + 2)) ||
+        (r = dalloc(&h->bsum, tiles)) || (r = dalloc(&h->bbox, 8)) ||
+        (r = dalloc(&h->layout, 1)) || (r = dalloc(&h->nbr, N * (size_t)K)) ||
+        (r = dalloc(&h->nbr_cnt, N)) || (r = dalloc(&h->sc, 1)) || (r = dalloc(&h->ac, 1)) ||
+        cudaMallocHost((void**)&h->pinned, sizeof(SphScalars)) != cudaSuccess) {
+        if (!r) r = SPH_ERR_NOMEM;
+        free_all(h);
+        delete h;
+        return r;
+    }
+    if (p->is_solid && (r = solid_alloc(h->solid, *p, n_max)) != SPH_OK) {
+        free_all(h);
+        delete h;
+        return r;
+    }
+    SphScalars s0;
+    memset(&s0, 0, sizeof(s0));
+    // DSPH.py:124-131: the initial step from the CFL on the signal speed
+    s0.dt = (float)((double)p->CFL * (double)p->support_radius / (double)p->c_signal);
+    DevAccum a0;
+    memset(&a0, 0, sizeof(a0));
+    if (cudaMemcpy(h->sc, &s0, sizeof(s0), cudaMemcpyHostToDevice) != cudaSuccess ||
+        cudaMemcpy(h->ac, &a0, sizeof(a0), cudaMemcpyHostToDevice) != cudaSuccess ||
+        cudaMemset(h->nbr_cnt, 0, N * sizeof(int)) != cudaSuccess) {
+        free_all(h);
+        delete h;
+        return SPH_ERR_CUDA;
+    }
+    *out = h;
+    return SPH_OK;
+}
+
+void sph_destroy(SphHandle* h) {
+    if (!h) return;
+    cudaDeviceSynchronize();
+    free_all(h);
+    delete h;
+}
+
+int sph_bind(SphHandle* h, const SphBuffers* b, int64_t n) {
+    if (!h || !b || n < 0 || n > h->n_max) return SPH_ERR_ARG;
+    if (!valid_set(b->set[0], h->p.is_solid) || !valid_set(b->set[1], h->p.is_solid)) return SPH_ERR_ARG;
+    if (!b->acc || !b->lam || !b->lsym || !b->lgrad || !b->div) return SPH_ERR_ARG;
+    if (h->p.is_solid && (!b->gradv || !b->aux)) return SPH_ERR_ARG;
+    drop_graph(h);
+    h->buf = *b;
+    h->n = n;
+    h->c.n = (int)n;
+    h->parity = 0;
+    h->bound = true;
+    return SPH_OK;
+}
+
+int sph_parity(const SphHandle* h) { return h ? h->parity : -1; }
+
+int sph_set_params(SphHandle* h, const SphParams* p) {
+    if (!h || !p || p->struct_size != (int32_t)sizeof(SphParams)) return SPH_ERR_ARG;
+    if (p->is_solid != h->p.is_solid) return SPH_ERR_ARG;
+    int K = h->c.K, mcap = h->c.mcap, lg = h->c.mcap_log2;
+    h->p = *p;
+    fill_constants(h);
+    h->c.K = K; h->c.mcap = mcap; h->c.mcap_log2 = lg; h->c.n = (int)h->n;
+    drop_graph(h);
+    return SPH_OK;
+}
+
+int sph_initialize(SphHandle* h, void* stream) {
+    if (!h) return SPH_ERR_ARG;
+    if (!h->bound) return SPH_ERR_NOT_BOUND;
+    if (h->n == 0) return SPH_OK;
+    int r = rebuild(h, S(stream));
+    if (r) return r;
+    CK(cudaGetLastError());
+    return SPH_OK;
+}
+
+int sph_step(SphHandle* h, int nsteps, void* stream) {
+    if (!h || nsteps < 0) return SPH_ERR_ARG;
+    if (!h->bound) return SPH_ERR_NOT_BOUND;
+    if (h->n == 0 || nsteps == 0) return SPH_OK;
+    cudaStream_t st = S(stream);
+    int pairs = nsteps / 2;
+    if (pairs > 0) {
+        if (!h->graph2) {
+            if (!h->cap_stream) CK(cudaStreamCreateWithFlags(&h->cap_stream, cudaStreamNonBlocking));
+            cudaGraph_t g;
+            // finish everything queued on the caller's stream before capturing
+            CK(cudaStreamSynchronize(st));
+            CK(cudaStreamBeginCapture(h->cap_stream, cudaStreamCaptureModeThreadLocal));
+            int p0 = h->parity;
+            h->capturing = true;
+            int r1 = one_step(h, h->cap_stream);
+            int r2 = r1 ? r1 : one_step(h, h->cap_stream);
+            cudaError_t ec = cudaStreamEndCapture(h->cap_stream, &g);
+            h->capturing = false;
+            h->parity = p0;
+            if (r2 != SPH_OK) { if (ec == cudaSuccess) cudaGraphDestroy(g); return r2; }
+            CK(ec);
+            cudaError_t ei = cudaGraphInstantiate(&h->graph2, g, 0);
+            cudaGraphDestroy(g);
+            CK(ei);
+        }
+        for (int k = 0; k < pairs; ++k) CK(cudaGraphLaunch(h->graph2, st));
+    }
+    if (nsteps & 1) {
+        int r = one_step(h, st);
+        if (r) return r;
+    }
+    CK(cudaGetLastError());
+    return SPH_OK;
+}
+
+int sph_run_stage(SphHandle* h, int stage, void* stream) {
+    if (!h) return SPH_ERR_ARG;
+    if (!h->bound) return SPH_ERR_NOT_BOUND;
+    if (h->n == 0) return SPH_OK;
+    cudaStream_t st = S(stream);
+    const int nb = blocks_for(h->n);
+    if (h->p.is_solid) {
+        int r = solid_run_stage(h->c, make_ptr(h), h->solid, (int)h->n, stage, st,
+                                [&]() { return rebuild(h, st); });
+        if (r) return r;
+        CK(cudaGetLastError());
+        return SPH_OK;
+    }
+    Ptr P = make_ptr(h);
+    const Cst& c = h->c;
+    switch (stage) {
+        case SPH_STAGE_SORT: { int r = rebuild(h, st); if (r) return r; break; }
+        case SPH_STAGE_LAM:
+            k_lam<<<nb, kBlock, 0, st>>>(c, P);
+            k_lamgrad_cont<<<nb, kBlock, 0, st>>>(c, P);
+            break;
+        case SPH_STAGE_CONTINUITY: k_eos<<<nb, kBlock, 0, st>>>(c, P); break;
+        case SPH_STAGE_FORCES: k_force<<<nb, kBlock, 0, st>>>(c, P); break;
+        case SPH_STAGE_DT: k_dt<<<1, 32, 0, st>>>(c, P); break;
+        case SPH_STAGE_ADVECT: k_advect<<<nb, kBlock, 0, st>>>(c, P); break;
+        case SPH_STAGE_PST:
+            if (h->p.pst_enabled) {
+                k_pst<<<nb, kBlock, 0, st>>>(c, P);
+                k_finish<<<nb, kBlock, 0, st>>>(c, P, 1);
+            }
+            break;
+        case SPH_STAGE_BOUNDARY: k_finish<<<nb, kBlock, 0, st>>>(c, P, 2); break;
+        default: return SPH_ERR_ARG;
+    }
+    CK(cudaGetLastError());
+    return SPH_OK;
+}
+
+int sph_set_dt(SphHandle* h, float dt, void* stream) {
+    if (!h) return SPH_ERR_ARG;
+    CK(cudaStreamSynchronize(S(stream)));
+    h->pinned->dt = dt;
+    CK(cudaMemcpyAsync(&h->sc->dt, &h->pinned->dt, sizeof(float), cudaMemcpyHostToDevice, S(stream)));
+    CK(cudaStreamSynchronize(S(stream)));
+    return SPH_OK;
+}
+
+int sph_get_dt(SphHandle* h, float* dt, void* stream) {
+    if (!h || !dt) return SPH_ERR_ARG;
+    CK(cudaMemcpyAsync(&h->pinned->dt, &h->sc->dt, sizeof(float), cudaMemcpyDeviceToHost, S(stream)));
+    CK(cudaStreamSynchronize(S(stream)));
+    *dt = h->pinned->dt;
+    return SPH_OK;
+}
+
+int sph_get_scalars(SphHandle* h, SphScalars* out, void* stream) {
+    if (!h || !out) return SPH_ERR_ARG;
+    CK(cudaMemcpyAsync(h->pinned, h->sc, sizeof(SphScalars), cudaMemcpyDeviceToHost, S(stream)));
+    CK(cudaStreamSynchronize(S(stream)));
+    memcpy(out, h->pinned, sizeof(SphScalars));
+    return SPH_OK;
+}
+
+int sph_clear_error(SphHandle* h, void* stream) {
+    if (!h) return SPH_ERR_ARG;
+    CK(cudaMemsetAsync(&h->sc->err, 0, sizeof(int), S(stream)));
+    return SPH_OK;
+}
+
+int sph_reduce(SphHandle* h, double* out, void* stream) {
+    if (!h || !out) return SPH_ERR_ARG;
+    if (!h->bound) return SPH_ERR_NOT_BOUND;
+    cudaStream_t st = S(stream);
+    CK(cudaMemsetAsync(h->ac->red, 0, sizeof(double) * SPH_RED_COUNT, st));
+    if (h->n > 0) {
+        Ptr P = make_ptr(h);
+        k_reduce<<<blocks_for(h->n), kBlock, 0, st>>>(h->c, P);
+        if (h->p.is_solid) solid_reduce_extra(h->c, P, (int)h->n, st);
+    }
+    CK(cudaMemcpyAsync(out, h->ac->red, sizeof(double) * SPH_RED_COUNT, cudaMemcpyDeviceToHost, st));
+    CK(cudaStreamSynchronize(st));
+    return SPH_OK;
+}
+
+}  // extern "C"
+
+namespace {
+__global__ void k_pairs_live(Cst c, Ptr P, const int* off, int* out_i, int* out_j, int* out_m, int write) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= c.n) return;
+    float4 pi = reinterpret_cast<const float4*>(P.cur.pos)[i];
+    F3 xi = f3(pi);
+    int cnt = 0;
+    if (!(isnan(xi.x) || isnan(xi.y) || isnan(xi.z))) {
+        const GridLayout L = *P.layout;
+        int cx = cell_of(xi.x, c.h), cy = cell_of(xi.y, c.h), cz = cell_of(xi.z, c.h);
+        int base = write ? off[i] : 0;
+        enumerate_neighbours(c, P, L, i, xi, cx, cy, cz, [&](int j, int mir, float4) {
+            if (write) { out_i[base + cnt] = i; out_j[base + cnt] = j; out_m[base + cnt] = mir; }
+            ++cnt;
+        });
+    }
+    if (!write) P.nbr_cnt[i] = cnt;  // reused as a count buffer; restored by the caller
+}
+}  // namespace
+
+extern "C" int sph_pairs(SphHandle* h, int mode, int32_t* pi, int32_t* pj, int32_t* mir,
+                         int64_t cap, int64_t* count, void* stream) {
+    if (!h || !count || (mode != 0 && mode != 1)) return SPH_ERR_ARG;
+    if (!h->bound) return SPH_ERR_NOT_BOUND;
+    cudaStream_t st = S(stream);
+    const int n = (int)h->n;
+    *count = 0;
+    if (n == 0) return SPH_OK;
+    std::vector<int> cnt(n);
+    if (mode == 0) {
+        CK(cudaMemcpyAsync(cnt.data(), h->nbr_cnt, n * sizeof(int), cudaMemcpyDeviceToHost, st));
+        std::vector<int> lst((size_t)n * h->c.K);
+        CK(cudaMemcpyAsync(lst.data(), h->nbr, lst.size() * sizeof(int), cudaMemcpyDeviceToHost, st));
+        CK(cudaStreamSynchronize(st));
+        int64_t k = 0;
+        for (int i = 0; i < n; ++i) {
+            if (cnt[i] > h->c.K) return SPH_ERR_NEIGHBOUR_CAP;
+            for (int t = 0; t < cnt[i]; ++t) {
+                int e = lst[(size_t)t * n + i];
+                if (k < cap && pi) { pi[k] = i; pj[k] = e & kIdxMask; mir[k] = e >> kMirShift; }
+                ++k;
+            }
+        }
+        *count = k;
+        return SPH_OK;
+    }
+    // mode 1: live search; nbr_cnt is borrowed as the count buffer and restored after.
+    std::vector<int> saved(n);
+    CK(cudaMemcpyAsync(saved.data(), h->nbr_cnt, n * sizeof(int), cudaMemcpyDeviceToHost, st));
+    Ptr P = make_ptr(h);
+    k_pairs_live<<<blocks_for(n), kBlock, 0, st>>>(h->c, P, nullptr, nullptr, nullptr, nullptr, 0);
+    CK(cudaMemcpyAsync(cnt.data(), h->nbr_cnt, n * sizeof(int), cudaMemcpyDeviceToHost, st));
+    CK(cudaStreamSynchronize(st));
+    std::vector<int> off(n);
+    int64_t tot = 0;
+    for (int i = 0; i < n; ++i) { off[i] = (int)tot; tot += cnt[i]; }
+    *count = tot;
+    int *doff = nullptr, *di = nullptr, *dj = nullptr, *dm = nullptr;
+    int r = SPH_OK;
+    if ((r = dalloc(&doff, n)) || (r = dalloc(&di, (size_t)tot)) || (r = dalloc(&dj, (size_t)tot)) ||
+        (r = dalloc(&dm, (size_t)tot))) {
+        cudaFree(doff); cudaFree(di); cudaFree(dj); cudaFree(dm);
+        return r;
+    }
+    cudaMemcpyAsync(doff, off.data(), n * sizeof(int), cudaMemcpyHostToDevice, st);
+    k_pairs_live<<<blocks_for(n), kBlock, 0, st>>>(h->c, P, doff, di, dj, dm, 1);
+    int64_t m = std::min<int64_t>(cap, tot);
+    if (pi && m > 0) {
+        cudaMemcpyAsync(pi, di, m * sizeof(int), cudaMemcpyDeviceToHost, st);
+        cudaMemcpyAsync(pj, dj, m * sizeof(int), cudaMemcpyDeviceToHost, st);
+        cudaMemcpyAsync(mir, dm, m * sizeof(int), cudaMemcpyDeviceToHost, st);
+    }
+    cudaMemcpyAsync(h->nbr_cnt, saved.data(), n * sizeof(int), cudaMemcpyHostToDevice, st);
+    cudaError_t e = cudaStreamSynchronize(st);
+    cudaFree(doff); cudaFree(di); cudaFree(dj); cudaFree(dm);
+    CK(e);
+    CK(cudaGetLastError());
+    return SPH_OK;
+}
+
+extern "C" int sph_profile_enable(SphHandle* h, int on) {
+    if (!h) return SPH_ERR_ARG;
+    h->prof_on = on != 0;
+    h->prof_marks.clear();
+    h->prof_used = 0;
+    return SPH_OK;
+}
+
+extern "C" int sph_profile_read(SphHandle* h, char* names, int names_cap, double* ms,
+                                int* launches, int cap, int* count) {
+    if (!h || !count) return SPH_ERR_ARG;
+    CK(cudaDeviceSynchronize());
+    std::vector<std::string> nm;
+    std::vector<double> tot;
+    std::vector<int> cnt;
+    for (size_t k = 1; k < h->prof_marks.size(); ++k) {
+        const char* name = h->prof_marks[k].first;
+        if (!name || !name[0]) continue;  // a sequence start
+        float t = 0.0f;
+        if (cudaEventElapsedTime(&t, h->prof_marks[k - 1].second, h->prof_marks[k].second) != cudaSuccess)
+            continue;
+        size_t idx = 0;
+        while (idx < nm.size() && nm[idx] != name) ++idx;
+        if (idx == nm.size()) { nm.push_back(name); tot.push_back(0.0); cnt.push_back(0); }
+        tot[idx] += t;
+        cnt[idx] += 1;
+    }
+    std::string joined;
+    int m = (int)std::min<size_t>(nm.size(), (size_t)std::max(cap, 0));
+    for (int k = 0; k < m; ++k) {
+        if (ms) ms[k] = tot[k];
+        if (launches) launches[k] = cnt[k];
+        joined += nm[k];
+        joined += "\n";
+    }
+    if (names && names_cap > 0) {
+        size_t L = std::min<size_t>(joined.size(), (size_t)names_cap - 1);
+        memcpy(names, joined.data(), L);
+        names[L] = 0;
+    }
+    *count = m;
+    h->prof_marks.clear();
+    h->prof_used = 0;
+    return SPH_OK;
+}

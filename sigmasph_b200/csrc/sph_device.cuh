@@ -1,0 +1,282 @@
+// sph_device.cuh -- launch-parameter structs and device helpers shared by every kernel
+// of libsph_b200 (sm_100a).
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "../../include/sph_b200.h"
+
+namespace sph {
+
+constexpr int kBlock = 256;          // threads per block of the particle-parallel kernels
+constexpr int kMirShift = 30;        // neighbour entry = j | (mirror code << 30)
+constexpr int kIdxMask = (1 << kMirShift) - 1;
+
+// Cell layout of the current rebuild, written by k_layout on the device.
+struct GridLayout {
+    int mode;          // 0 dense Morton table over the occupied cell box, 1 hashed table
+    int nbuckets;      // buckets in use; the off-grid bucket is index nbuckets
+    int cmin[3];
+    int cmax[3];
+    int bits[3];       // Morton bits per axis (dense mode)
+    int total_bits;
+};
+
+// Device copy of SphScalars (identical layout, so one memcpy returns it).
+typedef SphScalars DevScalars;
+
+// Per-step accumulators that are not part of the user-visible scalars.
+struct DevAccum {
+    double w_diff_step;      // sum_i -V_i p_i rate1_i of the continuity pass
+    double red[SPH_RED_COUNT];
+    unsigned int max_c_sq_bits;
+    unsigned int max_accel_bits;
+    unsigned int max_v_bits;
+    int pad;
+};
+
+// Constants of one handle, passed by value to every kernel.
+struct Cst {
+    SphParams p;
+    int n;               // active particles
+    int K;               // neighbour-list capacity per particle
+    int mcap;            // bucket capacity of the cell table (power of two)
+    int mcap_log2;
+    float h;             // support radius == cell size
+    float alpha;         // Wendland prefactor
+    float kgrad;         // 20 alpha / h
+    float eta2;          // 0.01 h^2
+    float W_dx0;         // W(dx0)
+    float d2_lt;         // |r| < h  <=>  d2 < d2_lt, with d2 = (dx^2 + dy^2) + dz^2 (RN)
+    float visc_coef;     // 2 (dim + 2) nu = 10 nu
+    float delta_coef;    // delta h c0
+    float cfl_h;         // CFL h
+    float wall_hi[3];    // domain_size - padding
+    float rest_1p;       // 1 + c_f
+    float rest_loss;     // 1 - c_f^2
+    float max_shift;     // pst_max_shift dx0
+    float colle_coef;    // -2 h
+    float sun_coef;      // -CFL
+    int mirror_y, mirror_z;
+};
+
+// Device pointers of one launch.
+struct Ptr {
+    SphFieldSet cur, nxt;
+    float4* acc;
+    float* lam;
+    float4* lsym;        // two float4 per particle
+    float4* lgrad;
+    float4* div;
+    float* gradv;
+    float4* aux;
+    // scratch
+    int4* cell;          // binned cell of the current order: x, y, z, key (-1 off-grid)
+    int4* cell_tmp;      // binned cell of the pre-sort order
+    int* key;            // bucket of each pre-sort particle
+    int* rank;           // slot within its bucket (arbitrary before the stabilise pass)
+    int* perm;           // new index -> old index
+    int* hist;           // [mcap + 2] bucket counts
+    int* start;          // [mcap + 2] exclusive scan of hist
+    int* bsum;           // block sums of the scan
+    int* bbox;           // [6] cell box min/max
+    GridLayout* layout;
+    int* nbr;            // [K][n] neighbour entries, k-major
+    int* nbr_cnt;        // [n]
+    DevScalars* sc;
+    DevAccum* ac;
+};
+
+// ------------------------------------------------------------------ small vector ops
+struct F3 { float x, y, z; };
+__device__ __forceinline__ F3 f3(float4 a) { return {a.x, a.y, a.z}; }
+__device__ __forceinline__ F3 operator+(F3 a, F3 b) { return {a.x + b.x, a.y + b.y, a.z + b.z}; }
+__device__ __forceinline__ F3 operator-(F3 a, F3 b) { return {a.x - b.x, a.y - b.y, a.z - b.z}; }
+__device__ __forceinline__ F3 operator*(float s, F3 a) { return {s * a.x, s * a.y, s * a.z}; }
+__device__ __forceinline__ F3 operator-(F3 a) { return {-a.x, -a.y, -a.z}; }
+__device__ __forceinline__ void operator+=(F3& a, F3 b) { a.x += b.x; a.y += b.y; a.z += b.z; }
+__device__ __forceinline__ float dot3(F3 a, F3 b) { return a.x * b.x + a.y * b.y + a.z * b.z; }
+__device__ __forceinline__ float norm3(F3 a) { return sqrtf(dot3(a, a)); }
+__device__ __forceinline__ F3 mirror3(int code, F3 a) {
+    return {a.x, (code & 1) ? -a.y : a.y, (code & 2) ? -a.z : a.z};
+}
+
+// Squared distance in the pinned order (dx^2 + dy^2) + dz^2, every operation rounded to
+// nearest with no contraction: the neighbour test must decide exactly as the reference's
+// float32 (x_i - x_j).norm() < h does.
+__device__ __forceinline__ float dist2_rn(F3 a, F3 b) {
+    float dx = __fsub_rn(a.x, b.x), dy = __fsub_rn(a.y, b.y), dz = __fsub_rn(a.z, b.z);
+    return __fadd_rn(__fadd_rn(__fmul_rn(dx, dx), __fmul_rn(dy, dy)), __fmul_rn(dz, dz));
+}
+
+// Cell of a position: floor(x / h) with a correctly rounded division
+// (particle_system.py:1220-1222).  Clamped far outside any grid so the integer
+// conversion stays defined.
+__device__ __forceinline__ int cell_of(float x, float h) {
+    float q = floorf(__fdiv_rn(x, h));
+    q = fminf(fmaxf(q, -1.0e9f), 1.0e9f);
+    return (int)q;
+}
+
+// Spatial hash of the reference (particle_system.py:1283-1293), the fallback table.
+__device__ __forceinline__ int hash_cell(int cx, int cy, int cz, int mcap) {
+    unsigned h = (unsigned)cx * 73856093u;
+    h ^= (unsigned)cy * 19349663u;
+    h ^= (unsigned)cz * 83492791u;
+    return (int)(h & (unsigned)(mcap - 1));
+}
+
+// Compact Morton code of a cell offset inside the occupied box: bits are interleaved
+// from the least significant end, x then y then z, each axis contributing only the
+// bits its extent needs.
+__device__ __forceinline__ int morton_key(int ox, int oy, int oz, const GridLayout& L) {
+    unsigned key = 0;
+    int pos = 0;
+    int nb = max(L.bits[0], max(L.bits[1], L.bits[2]));
+    for (int b = 0; b < nb; ++b) {
+        if (b < L.bits[0]) { key |= ((unsigned)(ox >> b) & 1u) << pos; ++pos; }
+        if (b < L.bits[1]) { key |= ((unsigned)(oy >> b) & 1u) << pos; ++pos; }
+        if (b < L.bits[2]) { key |= ((unsigned)(oz >> b) & 1u) << pos; ++pos; }
+    }
+    return (int)key;
+}
+
+// Bucket of a cell, or -1 if no particle can be binned there (outside the dense box).
+__device__ __forceinline__ int bucket_of(int cx, int cy, int cz, const GridLayout& L, int mcap) {
+    if (L.mode == 0) {
+        int ox = cx - L.cmin[0], oy = cy - L.cmin[1], oz = cz - L.cmin[2];
+        if (ox < 0 || oy < 0 || oz < 0 || cx > L.cmax[0] || cy > L.cmax[1] || cz > L.cmax[2])
+            return -1;
+        return morton_key(ox, oy, oz, L);
+    }
+    return hash_cell(cx, cy, cz, mcap);
+}
+
+// ------------------------------------------------------------------ Wendland C2 (sph_base.py:42-92)
+__device__ __forceinline__ float wendland_W(float r, const Cst& c) {
+    float q = r / c.h;
+    if (q < 1.0f) {
+        float t = 1.0f - q;
+        float t2 = t * t;
+        return c.alpha * (t2 * t2) * (4.0f * q + 1.0f);
+    }
+    return 0.0f;
+}
+// grad_i W for r = x_i - x_j given |r| (the caller has it already).
+__device__ __forceinline__ F3 wendland_dW(F3 r, float rn, const Cst& c) {
+    float q = rn / c.h;
+    if (q < 1.0f && rn > 1.0e-5f) {
+        float t = 1.0f - q;
+        float cc = -(c.kgrad * q * (t * t * t));
+        float f = cc / rn;
+        return f * r;
+    }
+    return {0.0f, 0.0f, 0.0f};
+}
+
+// SPH quadrature weight and its mass (particle_system.py:990-1004).
+__device__ __forceinline__ float w_of(float4 pos, const Cst& c) {
+    return c.p.axisymmetric ? pos.w / fmaxf(pos.y, c.p.axi_r_min) : pos.w;
+}
+__device__ __forceinline__ float mw_of(float m, float4 pos, const Cst& c) {
+    return c.p.axisymmetric ? m / fmaxf(pos.y, c.p.axi_r_min) : m;
+}
+
+// ------------------------------------------------------------------ reductions
+template <class T>
+__device__ __forceinline__ T warp_sum(T v) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    return v;
+}
+__device__ __forceinline__ float warp_max(float v) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v = fmaxf(v, __shfl_xor_sync(0xffffffffu, v, o));
+    return v;
+}
+// Block sum of a double, atomically added to *dst by one thread per block.
+__device__ __forceinline__ void block_sum_atomic(double v, double* dst) {
+    __shared__ double red[32];
+    v = warp_sum(v);
+    int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    if (lane == 0) red[wid] = v;
+    __syncthreads();
+    if (wid == 0) {
+        int nw = (blockDim.x + 31) >> 5;
+        double s = lane < nw ? red[lane] : 0.0;
+        s = warp_sum(s);
+        if (lane == 0 && s != 0.0) atomicAdd(dst, s);
+    }
+    __syncthreads();
+}
+// Block max of a non-negative float, atomically maxed into the bit pattern *dst
+// (order-preserving for non-negative IEEE floats).
+__device__ __forceinline__ void block_max_atomic(float v, unsigned int* dst) {
+    __shared__ float red[32];
+    v = warp_max(v);
+    int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    if (lane == 0) red[wid] = v;
+    __syncthreads();
+    if (wid == 0) {
+        int nw = (blockDim.x + 31) >> 5;
+        float s = lane < nw ? red[lane] : 0.0f;
+        s = warp_max(s);
+        if (lane == 0) atomicMax(dst, __float_as_uint(fmaxf(s, 0.0f)));
+    }
+    __syncthreads();
+}
+
+// ------------------------------------------------------------------ 3x3 symmetric eigen
+// Cyclic Jacobi (the same published method the oracle restates for ti.sym_eig).
+// A is overwritten; Q receives the eigenvectors as columns; ev the eigenvalues.
+template <class T>
+__device__ __forceinline__ void sym_eig3(T A[3][3], T ev[3], T Q[3][3]) {
+#pragma unroll
+    for (int i = 0; i < 3; ++i)
+#pragma unroll
+        for (int j = 0; j < 3; ++j) Q[i][j] = (i == j) ? T(1) : T(0);
+    const T eps = sizeof(T) == 4 ? T(1e-14) : T(1e-30);
+    for (int sweep = 0; sweep < 12; ++sweep) {
+        T off = A[0][1] * A[0][1] + A[0][2] * A[0][2] + A[1][2] * A[1][2];
+        T diag = A[0][0] * A[0][0] + A[1][1] * A[1][1] + A[2][2] * A[2][2];
+        if (!(off > eps * diag) || off == T(0)) break;
+#pragma unroll
+        for (int p = 0; p < 2; ++p) {
+#pragma unroll
+            for (int q = p + 1; q < 3; ++q) {
+                T apq = A[p][q];
+                if (apq == T(0)) continue;
+                T theta = (A[q][q] - A[p][p]) / (T(2) * apq);
+                T t = (theta >= T(0) ? T(1) : T(-1)) / (fabs(theta) + sqrt(theta * theta + T(1)));
+                T cs = T(1) / sqrt(t * t + T(1));
+                T s = t * cs;
+                T tau = s / (T(1) + cs);
+                A[p][p] -= t * apq;
+                A[q][q] += t * apq;
+                A[p][q] = A[q][p] = T(0);
+                const int r = 3 - p - q;
+                T arp = A[r][p], arq = A[r][q];
+                A[r][p] = A[p][r] = arp - s * (arq + tau * arp);
+                A[r][q] = A[q][r] = arq + s * (arp - tau * arq);
+#pragma unroll
+                for (int k = 0; k < 3; ++k) {
+                    T qkp = Q[k][p], qkq = Q[k][q];
+                    Q[k][p] = qkp - s * (qkq + tau * qkp);
+                    Q[k][q] = qkq + s * (qkp - tau * qkq);
+                }
+            }
+        }
+    }
+#pragma unroll
+    for (int k = 0; k < 3; ++k) ev[k] = A[k][k];
+}
+
+// spd_inverse.py:45-50
+template <class T>
+__device__ __forceinline__ T spd_weight(T e, T tol) {
+    T u = fmin(T(1), fmax(T(0), (e - tol) / tol));
+    T beta = u * u * (T(3) - T(2) * u);
+    return beta / fmax(e, tol) + (T(1) - beta);
+}
+
+}  // namespace sph

@@ -1,0 +1,578 @@
+// sph_fluid.cuh -- the delta+-SPH step (DSPH.py DSPHSolver.substep, :1854-1883) as
+// fused sm_100a kernels over the neighbour lists.
+//
+//   k_lam            compute_lam first pass: E, lambda, regularised L   (DSPH.py:611-681)
+//   k_lamgrad_cont   compute_lam second pass + the continuity pair sum  (:683-702, :1208-1338)
+//   k_eos            volume update, Tait pressure, gravity               (:1476-1521, :1642-1650)
+//   k_force          pressure + Morris viscosity + ALE momentum, and the pair sound-speed
+//                    and acceleration maxima of compute_adaptive_dt      (:1523-1640, :1340-1430)
+//   k_dt             the two CFL limits                                  (:1416-1430)
+//   k_advect         accumulate_step_work + advect                       (:1652-1763)
+//   k_pst            apply_pst first pass: live-position search against the stale bins
+//   k_finish         apply_pst second pass (displace) + SPHBase.step's constraints and walls
+//
+// Fusions relative to the reference: the grad-lambda sum and the continuity sum read the
+// same start-of-step state and share one neighbour sweep; the dt pair estimate reads the
+// post-EOS pressure the force pass reads and shares its sweep; the step-work reduction is
+// folded into advect; the displacement of the shift is folded into the boundary pass.
+#pragma once
+#include "sph_grid.cuh"
+
+namespace sph {
+
+__device__ __forceinline__ float4* as4(float* p) { return reinterpret_cast<float4*>(p); }
+__device__ __forceinline__ const float4* as4c(const float* p) { return reinterpret_cast<const float4*>(p); }
+
+// ------------------------------------------------------------------ compute_lam pass 1
+__global__ void __launch_bounds__(kBlock) k_lam(Cst c, Ptr P) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= c.n) return;
+    const float4* __restrict__ pos = as4c(P.cur.pos);
+    float4 pi = pos[i];
+    F3 xi = f3(pi);
+    float E[3][3] = {{0, 0, 0}, {0, 0, 0}, {0, 0, 0}};
+    for_each_neighbour(c, P, i, [&](int j, int mir) {
+        float4 pj = __ldg(pos + j);
+        F3 xj = f3(pj);
+        if (mir) xj = mirror3(mir, xj);
+        F3 d = xj - xi;
+        F3 r = xi - xj;
+        F3 g = wendland_dW(r, norm3(r), c);
+        float Vj = w_of(pj, c);
+        E[0][0] += Vj * (d.x * g.x); E[0][1] += Vj * (d.x * g.y);
+        E[1][0] += Vj * (d.y * g.x); E[1][1] += Vj * (d.y * g.y);
+        if (!c.p.two_d) {
+            E[0][2] += Vj * (d.x * g.z); E[1][2] += Vj * (d.y * g.z);
+            E[2][0] += Vj * (d.z * g.x); E[2][1] += Vj * (d.z * g.y); E[2][2] += Vj * (d.z * g.z);
+        }
+    });
+    const float tol = c.p.l_eig_tol_lam;
+    float L00, L11, L22, L01, L02, L12, lam;
+    float4 evec = make_float4(0.f, 0.f, 0.f, 0.f);
+    if (c.p.two_d) {
+        // eig_sym_2x2 (DSPH.py:35-47) on (E00, E01, E11) and spd_inverse_2x2 (spd_inverse.py:53-83)
+        float a = E[0][0], b0 = E[0][1], dd = E[1][1];
+        float det = sqrtf((a - dd) * (a - dd) + 4.0f * b0 * b0);
+        lam = fminf(1.0f, fmaxf(0.0f, 0.5f * (a + dd - det)));
+        float b = 0.5f * (E[0][1] + E[1][0]);
+        float disc = sqrtf(fmaxf((a - dd) * (a - dd) + 4.0f * b * b, 0.0f));
+        float e1 = 0.5f * (a + dd + disc), e2 = 0.5f * (a + dd - disc);
+        float n1x = 1.0f, n1y = 0.0f;
+        float scale = fabsf(a) + fabsf(dd) + 1e-30f;
+        if (disc > 1e-9f * scale) {
+            float v1x = b, v1y = e1 - a, v2x = e1 - dd, v2y = b;
+            float l1 = sqrtf(v1x * v1x + v1y * v1y), l2 = sqrtf(v2x * v2x + v2y * v2y);
+            if (l1 >= l2) { n1x = v1x / l1; n1y = v1y / l1; }
+            else { n1x = v2x / l2; n1y = v2y / l2; }
+        }
+        float n2x = -n1y, n2y = n1x;
+        float w1 = spd_weight(e1, tol), w2 = spd_weight(e2, tol);
+        L00 = w1 * (n1x * n1x) + w2 * (n2x * n2x);
+        L01 = w1 * (n1x * n1y) + w2 * (n2x * n2y);
+        L11 = w1 * (n1y * n1y) + w2 * (n2y * n2y);
+        L22 = 1.0f; L02 = 0.0f; L12 = 0.0f;
+        evec = make_float4(n2x, n2y, 0.0f, 0.0f);
+    } else {
+        float A[3][3], ev[3], Q[3][3];
+#pragma unroll
+        for (int a = 0; a < 3; ++a)
+#pragma unroll
+            for (int b = 0; b < 3; ++b) A[a][b] = 0.5f * (E[a][b] + E[b][a]);
+        sym_eig3(A, ev, Q);
+        float mine = fminf(ev[0], fminf(ev[1], ev[2]));
+        lam = fminf(1.0f, fmaxf(0.0f, mine));
+        float w0 = spd_weight(ev[0], tol), w1 = spd_weight(ev[1], tol), w2 = spd_weight(ev[2], tol);
+        L00 = w0 * (Q[0][0] * Q[0][0]) + w1 * (Q[0][1] * Q[0][1]) + w2 * (Q[0][2] * Q[0][2]);
+        L11 = w0 * (Q[1][0] * Q[1][0]) + w1 * (Q[1][1] * Q[1][1]) + w2 * (Q[1][2] * Q[1][2]);
+        L22 = w0 * (Q[2][0] * Q[2][0]) + w1 * (Q[2][1] * Q[2][1]) + w2 * (Q[2][2] * Q[2][2]);
+        L01 = w0 * (Q[0][0] * Q[1][0]) + w1 * (Q[0][1] * Q[1][1]) + w2 * (Q[0][2] * Q[1][2]);
+        L02 = w0 * (Q[0][0] * Q[2][0]) + w1 * (Q[0][1] * Q[2][1]) + w2 * (Q[0][2] * Q[2][2]);
+        L12 = w0 * (Q[1][0] * Q[2][0]) + w1 * (Q[1][1] * Q[2][1]) + w2 * (Q[1][2] * Q[2][2]);
+        int km = 0;
+        if (ev[1] < ev[km]) km = 1;
+        if (ev[2] < ev[km]) km = 2;
+        evec = make_float4(Q[0][km], Q[1][km], Q[2][km], 0.0f);
+    }
+    P.lam[i] = lam;
+    P.lsym[2 * i] = make_float4(L00, L11, L22, L01);
+    P.lsym[2 * i + 1] = make_float4(L02, L12, 0.0f, 0.0f);
+    if (c.p.pst_normal_eigvec) P.lgrad[i] = evec;
+}
+
+// ------------------------------------------------------------------ grad lambda + continuity
+__global__ void __launch_bounds__(kBlock) k_lamgrad_cont(Cst c, Ptr P) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    double wdiff = 0.0;
+    if (i < c.n) {
+        const float4* __restrict__ pos = as4c(P.cur.pos);
+        const float4* __restrict__ vel = as4c(P.cur.vel);
+        const float4* __restrict__ shf = as4c(P.cur.shift);
+        const float* __restrict__ lam = P.lam;
+        float4 pi = pos[i], vi4 = vel[i];
+        F3 xi = f3(pi), vi = f3(vi4);
+        float4 l0 = P.lsym[2 * i], l1 = P.lsym[2 * i + 1];
+        const float L00 = l0.x, L11 = l0.y, L22 = l0.z, L01 = l0.w, L02 = l1.x, L12 = l1.y;
+        const float lam_i = lam[i];
+        const float rho_i = vi4.w / pi.w;
+        const float dt = P.sc->dt;
+        const bool pst = c.p.pst_enabled;
+        const bool need_lgrad = !c.p.pst_normal_eigvec;
+        F3 du_i = {0, 0, 0};
+        if (pst) {
+            float4 s = shf[i];
+            du_i = {s.x / dt, s.y / dt, s.z / dt};
+        }
+        const F3 vhat_i = vi + du_i;
+        F3 lg = {0, 0, 0};
+        float r0 = 0.0f, r1 = 0.0f;
+        for_each_neighbour(c, P, i, [&](int j, int mir) {
+            float4 pj = __ldg(pos + j), vj4 = __ldg(vel + j);
+            F3 xj = f3(pj), vj = f3(vj4);
+            if (mir) { xj = mirror3(mir, xj); vj = mirror3(mir, vj); }
+            F3 r = xi - xj;
+            float rn = norm3(r);
+            F3 g = wendland_dW(r, rn, c);
+            float Vj = w_of(pj, c);
+            if (need_lgrad) {
+                float ld = __ldg(lam + j) - lam_i;
+                F3 Lg = {L00 * g.x + L01 * g.y + L02 * g.z,
+                         L01 * g.x + L11 * g.y + L12 * g.z,
+                         L02 * g.x + L12 * g.y + L22 * g.z};
+                lg += (Vj * ld) * Lg;
+            }
+            float rho_j = vj4.w / pj.w;
+            F3 vh_j = vj;
+            if (pst) {
+                float4 s = __ldg(shf + j);
+                F3 du_j = {s.x / dt, s.y / dt, s.z / dt};
+                if (mir) du_j = mirror3(mir, du_j);
+                vh_j += du_j;
+                r0 += Vj * dot3(rho_j * du_j - rho_i * du_i, g) / rho_i;
+            }
+            r0 += Vj * dot3(vhat_i - vh_j, g);
+            if (c.p.delta_sph > 0.0f) {
+                float rn2 = dot3(r, r);
+                float a2 = 2.0f * (rho_j - rho_i);
+                float den = rn2 + c.eta2;
+                F3 psi = {a2 * (-r.x) / den, a2 * (-r.y) / den, a2 * (-r.z) / den};
+                float rate = c.delta_coef * Vj * dot3(psi, g) / rho_i;
+                r0 += rate;
+                r1 += rate;
+            }
+        });
+        if (need_lgrad) {
+            if (c.p.two_d) lg.z = 0.0f;
+            P.lgrad[i] = make_float4(lg.x, lg.y, lg.z, 0.0f);
+        }
+        float dv = r0;
+        if (c.p.axisymmetric) dv -= vi.y / fmaxf(pi.y, c.p.axi_r_min);
+        P.div[i] = make_float4(dv, r1, 0.0f, 0.0f);
+        wdiff = -(double)pi.w * (double)__ldg(P.cur.disp + 4 * i + 3) * (double)r1;
+    }
+    block_sum_atomic(wdiff, &P.ac->w_diff_step);
+}
+
+// ------------------------------------------------------------------ volume update + EOS + gravity
+__device__ __forceinline__ float tait_p(float rho, const Cst& c) {
+    float p = c.p.stiffness * (powf(rho / c.p.density0, c.p.exponent) - 1.0f);
+    if (!c.p.allow_negative_pressure) p = fmaxf(p, 0.0f);
+    return p;
+}
+
+__global__ void __launch_bounds__(kBlock) k_eos(Cst c, Ptr P) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    const float dt = P.sc->dt;
+    if (i == 0) {
+        // end of compute_volume_evolution: diff_work += dt * w_diff_step (DSPH.py:1495)
+        P.sc->diff_work += (double)dt * P.ac->w_diff_step;
+        P.ac->w_diff_step = 0.0;
+        P.ac->max_c_sq_bits = __float_as_uint(c.p.c_signal * c.p.c_signal);
+        P.ac->max_accel_bits = __float_as_uint(1e-10f);
+    }
+    if (i >= c.n) return;
+    float4* pos = as4(P.cur.pos);
+    float4 pi = pos[i];
+    float V = pi.w;
+    float dVdt = -V * P.div[i].x;
+    if (c.p.compensated_volume) {
+        float* xo = P.cur.x0 + 4 * i + 3;
+        double s = (double)V + (double)(*xo) + (double)(dt * dVdt);
+        float hi = (float)s;
+        V = hi;
+        *xo = (float)(s - (double)hi);
+    } else {
+        V += dt * dVdt;
+    }
+    pi.w = V;
+    pos[i] = pi;
+    float m = P.cur.vel[4 * i + 3];
+    P.cur.disp[4 * i + 3] = tait_p(m / V, c);
+    P.acc[i] = make_float4(c.p.gravity[0], c.p.gravity[1], c.p.gravity[2], 0.0f);
+}
+
+// ------------------------------------------------------------------ pressure + viscosity + dt pairs
+__global__ void __launch_bounds__(kBlock) k_force(Cst c, Ptr P) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    float amag = 0.0f, csq = 0.0f;
+    if (i < c.n) {
+        const float4* __restrict__ pos = as4c(P.cur.pos);
+        const float4* __restrict__ vel = as4c(P.cur.vel);
+        const float4* __restrict__ dsp = as4c(P.cur.disp);
+        const float4* __restrict__ shf = as4c(P.cur.shift);
+        float4 pi = pos[i], vi4 = vel[i];
+        F3 xi = f3(pi), vi = f3(vi4);
+        const float p_i = dsp[i].w;
+        const float rho_i = vi4.w / pi.w;
+        const float w_i = w_of(pi, c);
+        const float mw_i = mw_of(vi4.w, pi, c);
+        const float dt = P.sc->dt;
+        const bool ale = c.p.pst_enabled && c.p.pst_ale_momentum;
+        F3 du_i = {0, 0, 0};
+        if (ale) {
+            float4 s = shf[i];
+            du_i = {s.x / dt, s.y / dt, s.z / dt};
+        }
+        const float eps_rho = 1e-3f * c.p.density0;
+        float cl = c.p.c_signal * c.p.c_signal;
+        F3 a = {0, 0, 0};
+        float dvisc = 0.0f;
+        for_each_neighbour(c, P, i, [&](int j, int mir) {
+            float4 pj = __ldg(pos + j), vj4 = __ldg(vel + j);
+            float p_j = __ldg(&dsp[j].w);
+            F3 xj = f3(pj), vj = f3(vj4);
+            if (mir) { xj = mirror3(mir, xj); vj = mirror3(mir, vj); }
+            F3 r = xi - xj;
+            float rn = norm3(r);
+            F3 g = wendland_dW(r, rn, c);
+            float w_j = w_of(pj, c);
+            float fp = -w_i * w_j * (p_i + p_j);
+            a += {fp * g.x / mw_i, fp * g.y / mw_i, fp * g.z / mw_i};
+            float vxy = dot3(vi - vj, r);
+            F3 fv = (c.visc_coef * w_j * vxy / (rn * rn + c.eta2)) * g;
+            a += fv;
+            dvisc += dot3(vi, fv);
+            float rho_j = vj4.w / pj.w;
+            if (ale) {
+                float4 s = __ldg(shf + j);
+                F3 du_j = {s.x / dt, s.y / dt, s.z / dt};
+                if (mir) du_j = mirror3(mir, du_j);
+                F3 t1 = (rho_j * dot3(du_j, g)) * vj - (rho_i * dot3(du_i, g)) * vi;
+                float b = dot3(rho_j * du_j - rho_i * du_i, g);
+                F3 t = t1 - b * vi;
+                a += {w_j * t.x / rho_i, w_j * t.y / rho_i, w_j * t.z / rho_i};
+            }
+            if (c.p.dt_pair_mode != 0) {
+                float drho = fabsf(rho_i - rho_j);
+                if (drho > eps_rho) {
+                    float cij = fabsf(p_i - p_j) / drho;
+                    if (cij > cl) cl = cij;
+                }
+            }
+        });
+        float4 a0 = P.acc[i];
+        F3 an = {a0.x + a.x, a0.y + a.y, a0.z + a.z};
+        P.acc[i] = make_float4(an.x, an.y, an.z, c.p.track_visc_work ? dvisc : 0.0f);
+        bool ongrid = !(isnan(pi.x) || isnan(pi.y) || isnan(pi.z));
+        if (ongrid) amag = norm3(an);
+        if (c.p.dt_pair_mode != 0) csq = cl;
+    }
+    block_max_atomic(amag, &P.ac->max_accel_bits);
+    block_max_atomic(csq, &P.ac->max_c_sq_bits);
+}
+
+// ------------------------------------------------------------------ compute_adaptive_dt tail
+__global__ void k_dt(Cst c, Ptr P) {
+    if (threadIdx.x != 0 || blockIdx.x != 0) return;
+    float mcs = __uint_as_float(P.ac->max_c_sq_bits);
+    float ma = __uint_as_float(P.ac->max_accel_bits);
+    P.sc->max_c_sq = mcs;
+    P.sc->max_accel = ma;
+    float cmax = sqrtf(mcs);
+    float dta = c.cfl_h / cmax;
+    float dtf = c.p.CFL * sqrtf(c.h / ma);
+    P.sc->dt = fminf(dta, dtf);
+    P.ac->max_v_bits = 0u;
+}
+
+// ------------------------------------------------------------------ step work + advect
+__global__ void __launch_bounds__(kBlock) k_advect(Cst c, Ptr P) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    const float dt = P.sc->dt;
+    double wl = 0.0, wv = 0.0;
+    float vmag = 0.0f;
+    if (i < c.n) {
+        float4 a4 = P.acc[i];
+        float4* vel = as4(P.cur.vel);
+        float4 v4 = vel[i];
+        const float gx = c.p.gravity[0], gy = c.p.gravity[1], gz = c.p.gravity[2];
+        float gsq = gx * gx + gy * gy + gz * gz;
+        F3 f = {a4.x - gx, a4.y - gy, a4.z - gz};
+        wl = (double)(0.5f * v4.w * dt * dt * (dot3(f, f) - gsq));
+        if (c.p.track_visc_work) wv = (double)v4.w * (double)a4.w;
+        v4.x += dt * a4.x; v4.y += dt * a4.y; v4.z += dt * a4.z;
+        vel[i] = v4;
+        float4* pos = as4(P.cur.pos);
+        float4 p = pos[i];
+        if (c.p.displacement_positions) {
+            float4* dsp = as4(P.cur.disp);
+            float4 u = dsp[i];
+            float4 x0 = as4(P.cur.x0)[i];
+            u.x += dt * v4.x; u.y += dt * v4.y; u.z += dt * v4.z;
+            dsp[i] = u;
+            p.x = x0.x + u.x; p.y = x0.y + u.y; p.z = x0.z + u.z;
+        } else {
+            p.x += dt * v4.x; p.y += dt * v4.y; p.z += dt * v4.z;
+        }
+        pos[i] = p;
+        if (c.p.pst_enabled && c.p.pst_ma_mode == 1 && !(isnan(p.x) || isnan(p.y) || isnan(p.z)))
+            vmag = sqrtf(v4.x * v4.x + v4.y * v4.y + v4.z * v4.z);
+    }
+    __shared__ double sh[2][32];
+    wl = warp_sum(wl);
+    wv = warp_sum(wv);
+    int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    if (lane == 0) { sh[0][wid] = wl; sh[1][wid] = wv; }
+    __syncthreads();
+    if (wid == 0) {
+        int nw = blockDim.x >> 5;
+        double a = lane < nw ? sh[0][lane] : 0.0, b = lane < nw ? sh[1][lane] : 0.0;
+        a = warp_sum(a);
+        b = warp_sum(b);
+        if (lane == 0) {
+            atomicAdd(&P.sc->leftover_work, a);
+            if (c.p.track_visc_work) atomicAdd(&P.sc->visc_work, (double)dt * b);
+        }
+    }
+    if (c.p.pst_enabled && c.p.pst_ma_mode == 1) block_max_atomic(vmag, &P.ac->max_v_bits);
+}
+
+// ------------------------------------------------------------------ apply_pst (DSPH.py:725-1046)
+__global__ void __launch_bounds__(kBlock) k_pst(Cst c, Ptr P) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= c.n) return;
+    const float4* __restrict__ pos = as4c(P.cur.pos);
+    const float4* __restrict__ vel = as4c(P.cur.vel);
+    float4 pi = pos[i];
+    F3 xi = f3(pi);
+    F3 sr = {0, 0, 0};
+    const float m_i = __ldg(&vel[i].w);
+    const float rho_i = m_i / pi.w;
+    if (!(isnan(xi.x) || isnan(xi.y) || isnan(xi.z))) {
+        const GridLayout L = *P.layout;
+        int cx = cell_of(xi.x, c.h), cy = cell_of(xi.y, c.h), cz = cell_of(xi.z, c.h);
+        const float Wd = c.W_dx0;
+        enumerate_neighbours(c, P, L, i, xi, cx, cy, cz, [&](int j, int mir, float4 pj) {
+            F3 xj = f3(pj);
+            if (mir) xj = mirror3(mir, xj);
+            F3 r = xi - xj;
+            float rn = norm3(r);
+            F3 g = wendland_dW(r, rn, c);
+            float Wij = wendland_W(rn, c);
+            float f = 0.0f;
+            if (Wd > 1e-10f) f = c.p.pst_R * powf(Wij / Wd, (float)c.p.pst_n);
+            if (c.p.pst_colle) {
+                float Vj = w_of(pj, c);
+                if (Vj > 1e-30f) sr += ((1.0f + f) * Vj) * g;
+            } else {
+                float mj_raw = __ldg(&vel[j].w);
+                float mj = mw_of(mj_raw, pj, c);
+                if (mj > 1e-10f) {
+                    float rho_j = mj_raw / pj.w;
+                    float ra = 0.5f * (rho_i + rho_j);
+                    if (ra > 1e-10f) sr += ((1.0f + f) * (mj / ra)) * g;
+                }
+            }
+        });
+    }
+    float4 vi4 = vel[i];
+    F3 vi = f3(vi4);
+    float Ma;
+    if (c.p.pst_ma_mode == 2) Ma = c.p.pst_ma_fixed;
+    else {
+        float vref = c.p.pst_ma_mode == 1 ? __uint_as_float(P.ac->max_v_bits) : norm3(vi);
+        Ma = vref / c.p.c0;
+    }
+    F3 dr;
+    if (c.p.pst_colle) {
+        float cc = c.colle_coef * c.p.c0 * Ma;
+        F3 dvv = cc * sr;
+        if (c.p.pst_clamp_vel) {
+            float cap = c.p.pst_m_delta * norm3(vi);
+            float dn = norm3(dvv);
+            if (dn > cap) dvv = (cap / fmaxf(dn, 1e-30f)) * dvv;
+        }
+        dr = P.sc->dt * dvv;
+    } else {
+        float cc = c.sun_coef * Ma * c.h * c.h;
+        dr = cc * sr;
+    }
+    if (c.p.pst_clamp_disp) {
+        float dn = norm3(dr);
+        if (dn > c.max_shift) dr = (c.max_shift / dn) * dr;
+    }
+    // pst_constrain (DSPH.py:888-941)
+    float li = P.lam[i];
+    bool surf = li < c.p.pst_lambda_hi;
+    if (c.p.pst_surface_none) {
+        if (surf) dr = {0, 0, 0};
+    } else if (surf) {
+        if (li < c.p.pst_lambda_lo) dr = {0, 0, 0};
+        else {
+            F3 ns = f3(P.lgrad[i]);
+            if (c.p.two_d) ns.z = 0.0f;
+            float nn = norm3(ns);
+            if (nn > 1e-10f) {
+                F3 nh = {ns.x / nn, ns.y / nn, ns.z / nn};
+                float dd = dot3(dr, nh);
+                dr = dr - dd * nh;
+            }
+        }
+    }
+    if (c.p.two_d) dr.z = 0.0f;
+    if (c.p.is_solid && P.cur.bc[2 * i] != 0) dr = {0, 0, 0};
+    float4* shf = as4(P.cur.shift);
+    float4 s = shf[i];
+    s.x = dr.x; s.y = dr.y; s.z = dr.z;
+    shf[i] = s;
+}
+
+// ------------------------------------------------------------------ displace + SPHBase.step boundary
+__device__ __forceinline__ void place_component(float4& p, float4& u, const float4& x0, int k,
+                                                float value, bool dpos) {
+    if (k == 0) { p.x = value; if (dpos) u.x = value - x0.x; }
+    else if (k == 1) { p.y = value; if (dpos) u.y = value - x0.y; }
+    else { p.z = value; if (dpos) u.z = value - x0.z; }
+}
+
+__global__ void __launch_bounds__(kBlock) k_finish(Cst c, Ptr P, int mode) {
+    const bool do_shift = mode & 1, do_bnd = mode & 2;
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    double ww = 0.0;
+    if (i < c.n) {
+        float4* pos = as4(P.cur.pos);
+        float4* vel = as4(P.cur.vel);
+        float4* dsp = as4(P.cur.disp);
+        float4 p = pos[i], v = vel[i], u = dsp[i];
+        const float4 x0 = as4(P.cur.x0)[i];
+        float4 a = P.acc[i];
+        const bool dpos = c.p.displacement_positions;
+        if (do_shift) {
+            float4 s = as4(P.cur.shift)[i];
+            if (dpos) {
+                u.x += s.x; u.y += s.y; u.z += s.z;
+                p.x = x0.x + u.x; p.y = x0.y + u.y; p.z = x0.z + u.z;
+            } else {
+                p.x += s.x; p.y += s.y; p.z += s.z;
+            }
+        }
+        auto walls = [&](bool wx, bool wylo, bool wyhi, bool wz) {
+            float4 q = p;
+            float cn[3] = {0.f, 0.f, 0.f};
+            const float qv[3] = {q.x, q.y, q.z};
+            const bool on[3] = {wx, true, wz};
+#pragma unroll
+            for (int k = 0; k < 3; ++k) {
+                if (!on[k]) continue;
+                bool hi_ok = k != 1 || wyhi, lo_ok = k != 1 || wylo;
+                if (hi_ok && qv[k] > c.wall_hi[k]) { cn[k] += 1.0f; place_component(p, u, x0, k, c.wall_hi[k], dpos); }
+                if (lo_ok && qv[k] <= c.p.padding) { cn[k] += -1.0f; place_component(p, u, x0, k, c.p.padding, dpos); }
+            }
+            float cl = sqrtf(cn[0] * cn[0] + cn[1] * cn[1] + cn[2] * cn[2]);
+            if (cl > 1e-6f) {
+                float nx = cn[0] / cl, ny = cn[1] / cl, nz = cn[2] / cl;
+                float vn = v.x * nx + v.y * ny + v.z * nz;
+                if (vn > 0.0f) {
+                    ww += (double)(0.5f * v.w * vn * vn * c.rest_loss);
+                    float k2 = c.rest_1p * vn;
+                    v.x -= k2 * nx; v.y -= k2 * ny; v.z -= k2 * nz;
+                }
+            }
+        };
+        if (!do_bnd) {
+        } else if (c.p.axisymmetric) {
+            v.z = 0.0f; a.z = 0.0f;
+            place_component(p, u, x0, 2, x0.z, dpos);
+            if (p.y < 0.0f) {
+                p.y = -p.y;
+                if (dpos) u.y = -u.y - 2.0f * x0.y;
+                v.y = -v.y;
+                a.y = -a.y;
+                if (c.p.is_solid) {  // M s M with M = diag(1, -1, 1): s_xy, s_yz flip
+                    float4* sd = reinterpret_cast<float4*>(P.cur.sdev);
+                    float4 s0 = sd[2 * i], s1 = sd[2 * i + 1];
+                    s0.w = -s0.w;      // s_xy
+                    s1.y = -s1.y;      // s_yz
+                    sd[2 * i] = s0; sd[2 * i + 1] = s1;
+                }
+            }
+            if (c.p.walls) walls(true, false, true, false);
+        } else {
+            if (c.p.sym_y && p.y < 0.0f) {
+                p.y = -p.y; if (dpos) u.y = -u.y - 2.0f * x0.y;
+                v.y = -v.y; a.y = -a.y;
+                if (c.p.is_solid) {
+                    float4* sd = reinterpret_cast<float4*>(P.cur.sdev);
+                    float4 s0 = sd[2 * i], s1 = sd[2 * i + 1];
+                    s0.w = -s0.w; s1.y = -s1.y;
+                    sd[2 * i] = s0; sd[2 * i + 1] = s1;
+                }
+            }
+            if (c.p.sym_z && p.z < 0.0f) {
+                p.z = -p.z; if (dpos) u.z = -u.z - 2.0f * x0.z;
+                v.z = -v.z; a.z = -a.z;
+                if (c.p.is_solid) {  // M = diag(1, 1, -1): s_xz, s_yz flip
+                    float4* sd = reinterpret_cast<float4*>(P.cur.sdev);
+                    float4 s1 = sd[2 * i + 1];
+                    s1.x = -s1.x; s1.y = -s1.y;
+                    sd[2 * i + 1] = s1;
+                }
+            }
+            if (c.p.walls) walls(true, true, true, !c.p.plane_strain);
+            if (c.p.plane_strain) {
+                v.z = 0.0f; a.z = 0.0f;
+                place_component(p, u, x0, 2, x0.z, dpos);
+            }
+        }
+        pos[i] = p; vel[i] = v; dsp[i] = u; P.acc[i] = a;
+    }
+    if (c.p.walls && do_bnd) block_sum_atomic(ww, &P.sc->wall_work);
+}
+
+// ------------------------------------------------------------------ FP64 reductions (sph_base.py:425-620)
+__global__ void __launch_bounds__(kBlock) k_reduce(Cst c, Ptr P) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    double r[SPH_RED_COUNT];
+#pragma unroll
+    for (int k = 0; k < SPH_RED_COUNT; ++k) r[k] = 0.0;
+    if (i < c.n) {
+        float4 p = as4c(P.cur.pos)[i];
+        float4 v = as4c(P.cur.vel)[i];
+        double m = (double)v.w;
+        float vv = v.x * v.x + v.y * v.y + v.z * v.z;
+        double ke = (double)(0.5f * v.w * vv);
+        bool ongrid = !(isnan(p.x) || isnan(p.y) || isnan(p.z));
+        r[SPH_RED_KE] = ke;
+        r[SPH_RED_KE_OFFGRID] = ongrid ? 0.0 : ke;
+        float gdx = c.p.gravity[0] * p.x + c.p.gravity[1] * p.y + c.p.gravity[2] * p.z;
+        r[SPH_RED_PE] = -m * (double)gdx;
+        // DSPHSolver.compute_elastic_energy: Tait compression energy in float64
+        double rho = m / (double)p.w, rho0 = (double)c.p.density0;
+        double S = (double)c.p.stiffness, gam = (double)c.p.exponent;
+        double x = rho / rho0, e;
+        if (fabs(gam - 1.0) < 1.0e-6) e = (S / rho0) * (log(x) + 1.0 / x - 1.0);
+        else e = (S / rho0) * ((pow(x, gam - 1.0) - 1.0) / (gam - 1.0) + 1.0 / x - 1.0);
+        if (!c.p.allow_negative_pressure && rho < rho0) e = 0.0;
+        r[SPH_RED_SE] = c.p.is_solid ? 0.0 : m * e;
+        r[SPH_RED_IE] = c.p.is_solid ? m * (double)as4c(P.cur.shift)[i].w : 0.0;
+        r[SPH_RED_MASS] = m;
+        r[SPH_RED_PX] = m * (double)v.x;
+        r[SPH_RED_PY] = m * (double)v.y;
+        r[SPH_RED_PZ] = m * (double)v.z;
+        double vx = v.x, vy = v.y, vz = v.z;
+        r[SPH_RED_GROSS_P] = m * sqrt(vx * vx + vy * vy + vz * vz);
+    }
+#pragma unroll
+    for (int k = 0; k < SPH_RED_COUNT; ++k) block_sum_atomic(r[k], &P.ac->red[k]);
+}
+
+}  // namespace sph
