@@ -130,7 +130,7 @@ REGISTRY = [
     ("PST_RELAX_STEPS", ("Shifting",), "initialRelaxation", "int", 0),
     ("HOURGLASS_ALPHA", ("Hourglass",), "alpha", "float", 0.0),
     ("HOURGLASS_FORM", ("Hourglass",), "form", "str", "rate"),
-    ("HOURGLASS_STS_MODE", ("Hourglass", "superTimeStepping"), "mode", "str", None),
+    ("HOURGLASS_STS_MODE", ("Hourglass", "superTimeStepping"), "mode", "str", "subcycle"),
     ("HOURGLASS_STS_STAGES", ("Hourglass", "superTimeStepping"), "stages", "int", 0),
     ("HOURGLASS_STS_REFRESH", ("Hourglass", "superTimeStepping"), "refreshGradV", "bool", True),
     ("HOURGLASS_STS_SAFETY", ("Hourglass", "superTimeStepping"), "safety", "float", 0.8),
@@ -148,7 +148,7 @@ UNSUPPORTED = {
     "DT_PAIR_SOUND_SPEED": ("all", "samematerial", "off"),
     "OBJECTIVE_RATE": ("jaumann",),
     "HOURGLASS_FORM": ("rate",),
-    "HOURGLASS_STS_MODE": (None, "subcycle"),
+    "HOURGLASS_STS_MODE": ("subcycle",),
 }
 
 # Cards the format knows, and those whose content is accepted but not read here
@@ -286,10 +286,9 @@ class SimConfig:
                 errors.append(f"{card}: expected an object")
                 continue
             walk(node, (card,))
-        # Hourglass.superTimeStepping present => the sub-cycled damper
+        # the presence of Hourglass.superTimeStepping is the switch (params.py:1330)
         hg = raw.get("Hourglass") or {}
-        if isinstance(hg, dict) and "superTimeStepping" in hg and "HOURGLASS_STS_MODE" not in given:
-            given["HOURGLASS_STS_MODE"] = "subcycle"
+        given["HOURGLASS_STS"] = bool(isinstance(hg, dict) and "superTimeStepping" in hg)
         return given
 
     def _build_materials(self, raw, given, errors):
