@@ -102,6 +102,7 @@ void fill_constants(SphHandle* h) {
     double hd = p.support_radius;
     double al = p.two_d ? 7.0 / (M_PI * hd * hd) : 21.0 / (2.0 * M_PI * hd * hd * hd);
     c.h = (float)hd;
+    c.inv_h = (float)(1.0 / hd);
     c.alpha = (float)al;
     c.kgrad = (float)(20.0 * al / hd);
     c.eta2 = (float)(0.01 * hd * hd);
@@ -197,6 +198,7 @@ int fluid_substep_and_boundary(SphHandle* h, cudaStream_t st) {
     LAUNCH("k_dt", k_dt<<<1, 32, 0, st>>>(c, P));
     LAUNCH("k_advect", k_advect<<<nb, kBlock, 0, st>>>(c, P));
     if (h->p.pst_enabled) {
+        LAUNCH("k_pst_search", k_pst_search<<<nb, kBlock, 0, st>>>(c, P));
         LAUNCH("k_pst", k_pst<<<nb, kBlock, 0, st>>>(c, P));
         LAUNCH("k_finish", k_finish<<<nb, kBlock, 0, st>>>(c, P, 3));
     } else {
@@ -461,6 +463,7 @@ int sph_run_stage(SphHandle* h, int stage, void* stream) {
         case SPH_STAGE_ADVECT: k_advect<<<nb, kBlock, 0, st>>>(c, P); break;
         case SPH_STAGE_PST:
             if (h->p.pst_enabled) {
+                k_pst_search<<<nb, kBlock, 0, st>>>(c, P);
                 k_pst<<<nb, kBlock, 0, st>>>(c, P);
                 k_finish<<<nb, kBlock, 0, st>>>(c, P, 1);
             }
@@ -559,7 +562,7 @@ extern "C" int sph_pairs(SphHandle* h, int mode, int32_t* pi, int32_t* pj, int32
             if (cnt[i] > h->c.K) return SPH_ERR_NEIGHBOUR_CAP;
             for (int t = 0; t < cnt[i]; ++t) {
                 int e = lst[(size_t)t * n + i];
-                if (k < cap && pi) { pi[k] = i; pj[k] = e & kIdxMask; mir[k] = e >> kMirShift; }
+                if (k < cap && pi) { pi[k] = i; pj[k] = e & kIdxMask; mir[k] = (int)((unsigned)e >> kMirShift); }
                 ++k;
             }
         }

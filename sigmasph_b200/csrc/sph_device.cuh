@@ -43,6 +43,7 @@ struct Cst {
     int mcap;            // bucket capacity of the cell table (power of two)
     int mcap_log2;
     float h;             // support radius == cell size
+    float inv_h;         // 1 / h
     float alpha;         // Wendland prefactor
     float kgrad;         // 20 alpha / h
     float eta2;          // 0.01 h^2
@@ -154,7 +155,7 @@ __device__ __forceinline__ int bucket_of(int cx, int cy, int cz, const GridLayou
 
 // ------------------------------------------------------------------ Wendland C2 (sph_base.py:42-92)
 __device__ __forceinline__ float wendland_W(float r, const Cst& c) {
-    float q = r / c.h;
+    float q = r * c.inv_h;
     if (q < 1.0f) {
         float t = 1.0f - q;
         float t2 = t * t;
@@ -164,14 +165,36 @@ __device__ __forceinline__ float wendland_W(float r, const Cst& c) {
 }
 // grad_i W for r = x_i - x_j given |r| (the caller has it already).
 __device__ __forceinline__ F3 wendland_dW(F3 r, float rn, const Cst& c) {
-    float q = rn / c.h;
+    float q = rn * c.inv_h;
     if (q < 1.0f && rn > 1.0e-5f) {
         float t = 1.0f - q;
         float cc = -(c.kgrad * q * (t * t * t));
-        float f = cc / rn;
+        float f = __fdividef(cc, rn);
         return f * r;
     }
     return {0.0f, 0.0f, 0.0f};
+}
+// |r| and grad_i W from the squared separation, one reciprocal square root.
+__device__ __forceinline__ F3 wendland_dW2(F3 r, float d2, float& rn, const Cst& c) {
+    rn = d2 > 0.0f ? d2 * rsqrtf(d2) : 0.0f;   // coincident pair: |r| = 0, grad W = 0
+    float q = rn * c.inv_h;
+    if (q < 1.0f && rn > 1.0e-5f) {
+        float t = 1.0f - q;
+        float f = -(c.kgrad * c.inv_h * (t * t * t));   // (-kgrad q (1-q)^3) / |r|
+        return f * r;
+    }
+    return {0.0f, 0.0f, 0.0f};
+}
+
+// x^n for the Monaghan tensile-correction exponent (an integer in every deck; any other
+// value goes through powf).
+__device__ __forceinline__ float ipow_or_pow(float x, int n) {
+    if (n >= 0 && n <= 8) {
+        float r = 1.0f;
+        for (int k = 0; k < n; ++k) r *= x;
+        return r;
+    }
+    return powf(x, (float)n);
 }
 
 // SPH quadrature weight and its mass (particle_system.py:990-1004).

@@ -37,7 +37,8 @@ __global__ void __launch_bounds__(kBlock) k_lam(Cst c, Ptr P) {
         if (mir) xj = mirror3(mir, xj);
         F3 d = xj - xi;
         F3 r = xi - xj;
-        F3 g = wendland_dW(r, norm3(r), c);
+        float rn;
+        F3 g = wendland_dW2(r, dot3(r, r), rn, c);
         float Vj = w_of(pj, c);
         E[0][0] += Vj * (d.x * g.x); E[0][1] += Vj * (d.x * g.y);
         E[1][0] += Vj * (d.y * g.x); E[1][1] += Vj * (d.y * g.y);
@@ -114,13 +115,15 @@ __global__ void __launch_bounds__(kBlock) k_lamgrad_cont(Cst c, Ptr P) {
         const float L00 = l0.x, L11 = l0.y, L22 = l0.z, L01 = l0.w, L02 = l1.x, L12 = l1.y;
         const float lam_i = lam[i];
         const float rho_i = vi4.w / pi.w;
+        const float inv_rho_i = 1.0f / rho_i;
         const float dt = P.sc->dt;
+        const float inv_dt = 1.0f / dt;
         const bool pst = c.p.pst_enabled;
         const bool need_lgrad = !c.p.pst_normal_eigvec;
         F3 du_i = {0, 0, 0};
         if (pst) {
             float4 s = shf[i];
-            du_i = {s.x / dt, s.y / dt, s.z / dt};
+            du_i = {s.x * inv_dt, s.y * inv_dt, s.z * inv_dt};
         }
         const F3 vhat_i = vi + du_i;
         F3 lg = {0, 0, 0};
@@ -130,8 +133,9 @@ __global__ void __launch_bounds__(kBlock) k_lamgrad_cont(Cst c, Ptr P) {
             F3 xj = f3(pj), vj = f3(vj4);
             if (mir) { xj = mirror3(mir, xj); vj = mirror3(mir, vj); }
             F3 r = xi - xj;
-            float rn = norm3(r);
-            F3 g = wendland_dW(r, rn, c);
+            float rn2 = dot3(r, r);
+            float rn;
+            F3 g = wendland_dW2(r, rn2, rn, c);
             float Vj = w_of(pj, c);
             if (need_lgrad) {
                 float ld = __ldg(lam + j) - lam_i;
@@ -140,22 +144,20 @@ __global__ void __launch_bounds__(kBlock) k_lamgrad_cont(Cst c, Ptr P) {
                          L02 * g.x + L12 * g.y + L22 * g.z};
                 lg += (Vj * ld) * Lg;
             }
-            float rho_j = vj4.w / pj.w;
+            float rho_j = __fdividef(vj4.w, pj.w);
             F3 vh_j = vj;
             if (pst) {
                 float4 s = __ldg(shf + j);
-                F3 du_j = {s.x / dt, s.y / dt, s.z / dt};
+                F3 du_j = {s.x * inv_dt, s.y * inv_dt, s.z * inv_dt};
                 if (mir) du_j = mirror3(mir, du_j);
                 vh_j += du_j;
-                r0 += Vj * dot3(rho_j * du_j - rho_i * du_i, g) / rho_i;
+                r0 += Vj * dot3(rho_j * du_j - rho_i * du_i, g) * inv_rho_i;
             }
             r0 += Vj * dot3(vhat_i - vh_j, g);
             if (c.p.delta_sph > 0.0f) {
-                float rn2 = dot3(r, r);
-                float a2 = 2.0f * (rho_j - rho_i);
-                float den = rn2 + c.eta2;
-                F3 psi = {a2 * (-r.x) / den, a2 * (-r.y) / den, a2 * (-r.z) / den};
-                float rate = c.delta_coef * Vj * dot3(psi, g) / rho_i;
+                // psi . grad W = 2 (rho_j - rho_i) (-r . grad W) / (|r|^2 + eta^2)
+                float psig = __fdividef(2.0f * (rho_j - rho_i) * (-dot3(r, g)), rn2 + c.eta2);
+                float rate = c.delta_coef * Vj * psig * inv_rho_i;
                 r0 += rate;
                 r1 += rate;
             }
@@ -233,6 +235,8 @@ __global__ void __launch_bounds__(kBlock) k_force(Cst c, Ptr P) {
             du_i = {s.x / dt, s.y / dt, s.z / dt};
         }
         const float eps_rho = 1e-3f * c.p.density0;
+        const float inv_mw_i = 1.0f / mw_i, inv_rho_i = 1.0f / rho_i, inv_dt = 1.0f / dt;
+        const float wi_mw = w_i * inv_mw_i;
         float cl = c.p.c_signal * c.p.c_signal;
         F3 a = {0, 0, 0};
         float dvisc = 0.0f;
@@ -242,24 +246,24 @@ __global__ void __launch_bounds__(kBlock) k_force(Cst c, Ptr P) {
             F3 xj = f3(pj), vj = f3(vj4);
             if (mir) { xj = mirror3(mir, xj); vj = mirror3(mir, vj); }
             F3 r = xi - xj;
-            float rn = norm3(r);
-            F3 g = wendland_dW(r, rn, c);
+            float rn;
+            F3 g = wendland_dW2(r, dot3(r, r), rn, c);
             float w_j = w_of(pj, c);
-            float fp = -w_i * w_j * (p_i + p_j);
-            a += {fp * g.x / mw_i, fp * g.y / mw_i, fp * g.z / mw_i};
+            // -w_i w_j (p_i + p_j) grad W / mw_i
+            a += (-wi_mw * w_j * (p_i + p_j)) * g;
             float vxy = dot3(vi - vj, r);
-            F3 fv = (c.visc_coef * w_j * vxy / (rn * rn + c.eta2)) * g;
+            F3 fv = __fdividef(c.visc_coef * w_j * vxy, rn * rn + c.eta2) * g;
             a += fv;
             dvisc += dot3(vi, fv);
-            float rho_j = vj4.w / pj.w;
+            float rho_j = __fdividef(vj4.w, pj.w);
             if (ale) {
                 float4 s = __ldg(shf + j);
-                F3 du_j = {s.x / dt, s.y / dt, s.z / dt};
+                F3 du_j = {s.x * inv_dt, s.y * inv_dt, s.z * inv_dt};
                 if (mir) du_j = mirror3(mir, du_j);
                 F3 t1 = (rho_j * dot3(du_j, g)) * vj - (rho_i * dot3(du_i, g)) * vi;
                 float b = dot3(rho_j * du_j - rho_i * du_i, g);
                 F3 t = t1 - b * vi;
-                a += {w_j * t.x / rho_i, w_j * t.y / rho_i, w_j * t.z / rho_i};
+                a += (w_j * inv_rho_i) * t;
             }
             if (c.p.dt_pair_mode != 0) {
                 float drho = fabsf(rho_i - rho_j);
@@ -347,6 +351,54 @@ __global__ void __launch_bounds__(kBlock) k_advect(Cst c, Ptr P) {
 }
 
 // ------------------------------------------------------------------ apply_pst (DSPH.py:725-1046)
+// First the neighbour search of the shift: live positions after advect against the bins
+// of the step's rebuild (particle_system.py:1377-1411).  The pairs are compacted into the
+// neighbour list, whose pre-advect content is dead once the force pass has run, so the
+// evaluation below runs warp-coherent over ~80 pairs instead of inside the divergent
+// candidate loop.
+__global__ void __launch_bounds__(kBlock) k_pst_search(Cst c, Ptr P) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= c.n) return;
+    F3 xi = f3(as4c(P.cur.pos)[i]);
+    int cnt = 0;
+    if (!(isnan(xi.x) || isnan(xi.y) || isnan(xi.z))) {
+        const GridLayout L = *P.layout;
+        int cx = cell_of(xi.x, c.h), cy = cell_of(xi.y, c.h), cz = cell_of(xi.z, c.h);
+        const int n = c.n, K = c.K;
+        int* __restrict__ nb = P.nbr;
+        enumerate_neighbours(c, P, L, i, xi, cx, cy, cz, [&](int j, int mir, float4) {
+            if (cnt < K) nb[(size_t)cnt * n + i] = j | (mir << kMirShift);
+            ++cnt;
+        });
+        if (cnt > K) atomicOr(&P.sc->err, SPH_EW_NBR_OVERFLOW);
+    }
+    P.nbr_cnt[i] = cnt;
+}
+
+// Pairs of the shift search: the stored list, then (past the list's capacity) the same
+// live search again with the first K skipped.
+template <class F>
+__device__ __forceinline__ void for_each_live_neighbour(const Cst& c, const Ptr& P, int i, F3 xi, F&& f) {
+    const int cnt = __ldg(P.nbr_cnt + i);
+    const int m = cnt < c.K ? cnt : c.K;
+    const int* __restrict__ nb = P.nbr + i;
+    const size_t n = (size_t)c.n;
+#pragma unroll 4
+    for (int k = 0; k < m; ++k) {
+        int e = __ldg(nb + (size_t)k * n);
+        f(e & kIdxMask, (int)((unsigned)e >> kMirShift));
+    }
+    if (cnt > c.K) {
+        const GridLayout L = *P.layout;
+        int cx = cell_of(xi.x, c.h), cy = cell_of(xi.y, c.h), cz = cell_of(xi.z, c.h);
+        int k = 0;
+        enumerate_neighbours(c, P, L, i, xi, cx, cy, cz, [&](int j, int mir, float4) {
+            if (k >= c.K) f(j, mir);
+            ++k;
+        });
+    }
+}
+
 __global__ void __launch_bounds__(kBlock) k_pst(Cst c, Ptr P) {
     int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= c.n) return;
@@ -357,19 +409,19 @@ __global__ void __launch_bounds__(kBlock) k_pst(Cst c, Ptr P) {
     F3 sr = {0, 0, 0};
     const float m_i = __ldg(&vel[i].w);
     const float rho_i = m_i / pi.w;
-    if (!(isnan(xi.x) || isnan(xi.y) || isnan(xi.z))) {
-        const GridLayout L = *P.layout;
-        int cx = cell_of(xi.x, c.h), cy = cell_of(xi.y, c.h), cz = cell_of(xi.z, c.h);
+    {
         const float Wd = c.W_dx0;
-        enumerate_neighbours(c, P, L, i, xi, cx, cy, cz, [&](int j, int mir, float4 pj) {
+        const float inv_Wd = Wd > 0.0f ? 1.0f / Wd : 0.0f;
+        for_each_live_neighbour(c, P, i, xi, [&](int j, int mir) {
+            float4 pj = __ldg(pos + j);
             F3 xj = f3(pj);
             if (mir) xj = mirror3(mir, xj);
             F3 r = xi - xj;
-            float rn = norm3(r);
-            F3 g = wendland_dW(r, rn, c);
+            float rn;
+            F3 g = wendland_dW2(r, dot3(r, r), rn, c);
             float Wij = wendland_W(rn, c);
             float f = 0.0f;
-            if (Wd > 1e-10f) f = c.p.pst_R * powf(Wij / Wd, (float)c.p.pst_n);
+            if (Wd > 1e-10f) f = c.p.pst_R * ipow_or_pow(Wij * inv_Wd, c.p.pst_n);
             if (c.p.pst_colle) {
                 float Vj = w_of(pj, c);
                 if (Vj > 1e-30f) sr += ((1.0f + f) * Vj) * g;

@@ -385,7 +385,7 @@ __device__ __forceinline__ void for_each_neighbour(const Cst& c, const Ptr& P, i
 #pragma unroll 4
     for (int k = 0; k < m; ++k) {
         int e = __ldg(nb + (size_t)k * n);
-        f(e & kIdxMask, e >> kMirShift);
+        f(e & kIdxMask, (int)((unsigned)e >> kMirShift));
     }
     if (cnt > c.K) {
         const GridLayout L = *P.layout;
