@@ -205,6 +205,37 @@ __device__ __forceinline__ float mw_of(float m, float4 pos, const Cst& c) {
     return c.p.axisymmetric ? m / fmaxf(pos.y, c.p.axi_r_min) : m;
 }
 
+// One particle's terms of every FP64 reduction.
+__device__ __forceinline__ void reduce_terms(const Cst& c, float4 p, float4 v, float e_int,
+                                             double r[SPH_RED_COUNT]) {
+    {
+        double m = (double)v.w;
+        float vv = v.x * v.x + v.y * v.y + v.z * v.z;
+        double ke = (double)(0.5f * v.w * vv);
+        bool ongrid = !(isnan(p.x) || isnan(p.y) || isnan(p.z));
+        r[SPH_RED_KE] = ke;
+        r[SPH_RED_KE_OFFGRID] = ongrid ? 0.0 : ke;
+        float gdx = c.p.gravity[0] * p.x + c.p.gravity[1] * p.y + c.p.gravity[2] * p.z;
+        r[SPH_RED_PE] = -m * (double)gdx;
+        // DSPHSolver.compute_elastic_energy: Tait compression energy in float64
+        double rho = m / (double)p.w, rho0 = (double)c.p.density0;
+        double S = (double)c.p.stiffness, gam = (double)c.p.exponent;
+        double x = rho / rho0, e;
+        if (fabs(gam - 1.0) < 1.0e-6) e = (S / rho0) * (log(x) + 1.0 / x - 1.0);
+        else e = (S / rho0) * ((pow(x, gam - 1.0) - 1.0) / (gam - 1.0) + 1.0 / x - 1.0);
+        if (!c.p.allow_negative_pressure && rho < rho0) e = 0.0;
+        r[SPH_RED_SE] = c.p.is_solid ? 0.0 : m * e;
+        r[SPH_RED_IE] = c.p.is_solid ? m * (double)e_int : 0.0;
+        r[SPH_RED_MASS] = m;
+        r[SPH_RED_PX] = m * (double)v.x;
+        r[SPH_RED_PY] = m * (double)v.y;
+        r[SPH_RED_PZ] = m * (double)v.z;
+        double vx = v.x, vy = v.y, vz = v.z;
+        r[SPH_RED_GROSS_P] = m * sqrt(vx * vx + vy * vy + vz * vz);
+        r[SPH_RED_ELASTIC] = 0.0;
+    }
+}
+
 // ------------------------------------------------------------------ reductions
 template <class T>
 __device__ __forceinline__ T warp_sum(T v) {

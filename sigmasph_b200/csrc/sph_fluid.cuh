@@ -144,7 +144,7 @@ __global__ void __launch_bounds__(kBlock) k_lamgrad_cont(Cst c, Ptr P) {
                          L02 * g.x + L12 * g.y + L22 * g.z};
                 lg += (Vj * ld) * Lg;
             }
-            float rho_j = __fdividef(vj4.w, pj.w);
+            float rho_j = vj4.w / pj.w;   // exact: rho_j - rho_i is a small difference
             F3 vh_j = vj;
             if (pst) {
                 float4 s = __ldg(shf + j);
@@ -255,7 +255,7 @@ __global__ void __launch_bounds__(kBlock) k_force(Cst c, Ptr P) {
             F3 fv = __fdividef(c.visc_coef * w_j * vxy, rn * rn + c.eta2) * g;
             a += fv;
             dvisc += dot3(vi, fv);
-            float rho_j = __fdividef(vj4.w, pj.w);
+            float rho_j = vj4.w / pj.w;   // exact: rho_j - rho_i is a small difference
             if (ale) {
                 float4 s = __ldg(shf + j);
                 F3 du_j = {s.x * inv_dt, s.y * inv_dt, s.z * inv_dt};
@@ -596,33 +596,8 @@ __global__ void __launch_bounds__(kBlock) k_reduce(Cst c, Ptr P) {
     double r[SPH_RED_COUNT];
 #pragma unroll
     for (int k = 0; k < SPH_RED_COUNT; ++k) r[k] = 0.0;
-    if (i < c.n) {
-        float4 p = as4c(P.cur.pos)[i];
-        float4 v = as4c(P.cur.vel)[i];
-        double m = (double)v.w;
-        float vv = v.x * v.x + v.y * v.y + v.z * v.z;
-        double ke = (double)(0.5f * v.w * vv);
-        bool ongrid = !(isnan(p.x) || isnan(p.y) || isnan(p.z));
-        r[SPH_RED_KE] = ke;
-        r[SPH_RED_KE_OFFGRID] = ongrid ? 0.0 : ke;
-        float gdx = c.p.gravity[0] * p.x + c.p.gravity[1] * p.y + c.p.gravity[2] * p.z;
-        r[SPH_RED_PE] = -m * (double)gdx;
-        // DSPHSolver.compute_elastic_energy: Tait compression energy in float64
-        double rho = m / (double)p.w, rho0 = (double)c.p.density0;
-        double S = (double)c.p.stiffness, gam = (double)c.p.exponent;
-        double x = rho / rho0, e;
-        if (fabs(gam - 1.0) < 1.0e-6) e = (S / rho0) * (log(x) + 1.0 / x - 1.0);
-        else e = (S / rho0) * ((pow(x, gam - 1.0) - 1.0) / (gam - 1.0) + 1.0 / x - 1.0);
-        if (!c.p.allow_negative_pressure && rho < rho0) e = 0.0;
-        r[SPH_RED_SE] = c.p.is_solid ? 0.0 : m * e;
-        r[SPH_RED_IE] = c.p.is_solid ? m * (double)as4c(P.cur.shift)[i].w : 0.0;
-        r[SPH_RED_MASS] = m;
-        r[SPH_RED_PX] = m * (double)v.x;
-        r[SPH_RED_PY] = m * (double)v.y;
-        r[SPH_RED_PZ] = m * (double)v.z;
-        double vx = v.x, vy = v.y, vz = v.z;
-        r[SPH_RED_GROSS_P] = m * sqrt(vx * vx + vy * vy + vz * vz);
-    }
+    if (i < c.n)
+        reduce_terms(c, as4c(P.cur.pos)[i], as4c(P.cur.vel)[i], as4c(P.cur.shift)[i].w, r);
 #pragma unroll
     for (int k = 0; k < SPH_RED_COUNT; ++k) block_sum_atomic(r[k], &P.ac->red[k]);
 }

@@ -2,7 +2,8 @@
 
 Tolerances (float32 arithmetic on both sides, different summation order):
   * neighbour pair sets: bit-exact (as sets of (pid_i, pid_j, mirror));
-  * one stage vs the float32 oracle: max |g - r| / max |r| <= 2e-5 per field;
+  * one stage vs the float32 oracle: max |g - r| / max |r| <= 2e-5 per field, the Tait
+    pressure <= 2e-4 (see LOOSE32);
   * one stage vs the float64 oracle: <= 1e-4, pressure and acceleration <= 5e-4 (the
     float32 EOS rounds rho / rho0 to one ulp, i.e. a Tait pressure noise of
     gamma * 2^-23 * B that the float64 oracle does not have);
@@ -33,6 +34,10 @@ STAGE_FIELDS = {
     abi.STAGE_BOUNDARY: ["x", "v", "u"],
 }
 LOOSE64 = {"pressure": 5e-4, "acc": 5e-4, "divergence": 5e-4}
+# The Tait pressure S((rho/rho0)^gamma - 1) cancels: a relative difference d in V (the
+# float32 sum-order noise, ~7e-8) becomes gamma d / ((rho/rho0)^gamma - 1) ~ 300 d in p,
+# and libm's and CUDA's powf differ by an ulp on top.
+LOOSE32 = {"pressure": 2e-4}
 
 
 def small_scene(n=8000, **kw):
@@ -130,7 +135,7 @@ def test_stages_match_oracle(cuda, scene_fn):
         e32 = field_errors(g, oracle_fields(o32), STAGE_FIELDS[s])
         e64 = field_errors(g, oracle_fields(o64), STAGE_FIELDS[s])
         for k, e in e32.items():
-            assert e <= 2e-5, (s, k, e)
+            assert e <= LOOSE32.get(k, 2e-5), (s, k, e)
         for k, e in e64.items():
             assert e <= LOOSE64.get(k, 1e-4), (s, k, e)
         if s == abi.STAGE_ADVECT:
@@ -206,9 +211,13 @@ def test_momentum_conserved_without_external_agents(cuda):
 def test_nan_particle_is_quarantined(cuda):
     cfg = SimConfig(small_scene(5000))
     ps = ParticleSystem(cfg, device="cuda")
+    # x is re-formed as x_0 + u at every displacement, so the poison goes into u too
     x = ps.x.to_numpy()
     x[17, 1] = np.nan
     ps.x.from_numpy(x)
+    u = ps.u.to_numpy()
+    u[17, 1] = np.nan
+    ps.u.from_numpy(u)
     m17 = float(ps.m.to_numpy()[17])
     sv = ps.build_solver()
     sv.initialize()
