@@ -252,6 +252,24 @@ int  sph_profile_enable(SphHandle* h, int on);
 int  sph_profile_read(SphHandle* h, char* names, int names_cap, double* ms, int* launches,
                       int cap, int* count);
 
+/* The FP64 reductions of sph_reduce without a handle and without allocating: no
+ * counterpart in the reference.  For callers that cannot call cudaMalloc (a host running
+ * inside another framework's fixed device-memory pool, code that may not allocate while
+ * a CUDA graph is being captured, FFI callers that hold only raw device pointers).  The
+ * caller passes the current buffer set's pos, vel and shift arrays ([n][4] float32,
+ * 16-byte aligned; shift may be NULL for a fluid) and `out`, a device array of
+ * SPH_RED_COUNT doubles it owns; the result is written there asynchronously on `stream`.
+ * The scratch is a fixed array compiled into the library (1.44 MB on each GPU that loads
+ * it, held until the process exits), which caps n at SPH_NOALLOC_MAX_PARTICLES: larger n
+ * returns SPH_ERR_SCRATCH_CAP and launches nothing.  The first call on a device looks up
+ * that array's device address (cudaGetSymbolAddress) with the device current; make it
+ * before any stream capture.  All calls share the array, so calls whose GPU work overlaps
+ * (other streams, other host threads) race: serialise them.  The sum is deterministic
+ * (per-block partials added in a fixed order). */
+#define SPH_NOALLOC_MAX_PARTICLES 4194304
+int  sph_reduce_noalloc(const SphParams* p, const float* pos, const float* vel,
+                        const float* shift, int64_t n, double* out, void* stream);
+
 /* Stage ids for sph_run_stage. */
 enum {
     SPH_STAGE_SORT = 0,        /* initialize_particle_system                           */

@@ -61,7 +61,7 @@ def build(force=False, verbose=False):
     if verbose:
         cmd += ["-Xptxas", "-v"]
     tmp = LIB + ".tmp"
-    cmd += ["-o", tmp, MAIN]
+    cmd += ["-o", tmp, MAIN, os.path.join(CSRC, "sph_noalloc.cu")]
     r = subprocess.run(cmd, capture_output=True, text=True)
     if r.returncode != 0:
         raise RuntimeError("nvcc failed:\n" + r.stdout + r.stderr)
