@@ -116,6 +116,13 @@ typedef struct SphParams {
     float   plastic_sy0[4];
     float   plastic_H[4];
     float   jc_A[4], jc_B[4], jc_n[4], jc_C[4], jc_eps0_dot[4];
+    float   jc_T0[4], jc_Tm[4], jc_m[4], jc_chi[4];
+    float   mat_cv[4];            /* specific heat (0: temperature stays at T0)         */
+    float   mat_stiff[4];         /* EOS stiffness: K (linear) or c0^2 rho0 / gamma     */
+    float   mat_gamma[4];         /* EOS exponent (1 for linear)                        */
+    float   mat_T0[4];            /* reference temperature                              */
+    int32_t axi_conservative_x;   /* axisymmetric conservative axial momentum form      */
+    float   hg_rate;              /* alpha c_p / h_min * S * axis ratio (1/time)        */
     int32_t kernel_correction;    /* grad v through the regularised inverse of E        */
     float   l_eig_tol;            /* tolerance of that inverse (0.1)                    */
     float   hourglass_alpha;
@@ -132,6 +139,7 @@ typedef struct SphParams {
     float   ramp_time;
     int32_t jc_surrogate;         /* 1: MLP return map with Newton fallback             */
     float   jc_surrogate_tol;     /* |f_yield| / sigma_y acceptance (1e-3)              */
+    int32_t hg_sts_fixed;         /* > 0: that many damper sub-steps, else automatic    */
     int32_t reserved[8];
 } SphParams;
 
@@ -150,6 +158,8 @@ typedef struct SphFieldSet {
     float*   sdev;     /* [n][8] s_xx, s_yy, s_zz, s_xy, s_xz, s_yz, eps_p, T            */
     int32_t* bc;       /* [n][2] bc_flag, bc_id                                         */
     float*   bcdisp;   /* [n][4] bc_disp xyz, eos_id (as float)                         */
+    float*   acc;      /* [n][4] acceleration, de_int: carried across the sort, since the
+                          next step's energy update reads them (SOLID.py:2071-2237)      */
 } SphFieldSet;
 
 /* Per-step derived fields (one copy, overwritten every step before they are read). */
@@ -161,7 +171,8 @@ typedef struct SphBuffers {
     float* lgrad;      /* [n][4] grad lambda (or the min eigenvector under eigvec)       */
     float* div;        /* [n][4] divergence, diffusion rate, -, -                        */
     float* gradv;      /* [n][12] grad v (row-major 3x3) + 3 spare (solid)               */
-    float* aux;        /* [n][8] solid scratch: hg y_a, y_b, a (STS), d_eps_prod          */
+    float* aux;        /* [n][24] solid per-step scratch: updated s, eps_p, e, T; the
+                          kernel-correction inverse; the damper's velocity buffers        */
 } SphBuffers;
 
 /* Device scalars copied back by sph_get_scalars (the reference's 0-d fields). */

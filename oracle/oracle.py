@@ -27,15 +27,22 @@ def build(force=False):
     return LIB
 
 
+STATE_KEYS = ("x", "x0", "u", "v", "acc", "V", "V_lo", "m", "pressure", "pst_shift", "pid",
+              "sdev", "eps_p", "e_int", "temperature", "de_int", "bc_flag", "bc_id", "bc_disp",
+              "eos_id")
+INT_KEYS = ("pid", "bc_flag", "bc_id", "eos_id")
+
+
 class _State(C.Structure):
-    _fields_ = [(k, C.c_void_p) for k in ("x", "x0", "u", "v", "acc", "V", "V_lo", "m",
-                                          "pressure", "pst_shift", "pid")]
+    _fields_ = [(k, C.c_void_p) for k in STATE_KEYS]
 
 
 class _Out(C.Structure):
     _fields_ = [(k, C.c_void_p) for k in ("x", "x0", "u", "v", "acc", "V", "V_lo", "m",
                                           "pressure", "pst_shift", "pid", "lam", "L_sym",
-                                          "lam_grad", "divergence", "de_visc")]
+                                          "lam_grad", "divergence", "de_visc", "sdev", "eps_p",
+                                          "e_int", "temperature", "de_int", "bc_flag",
+                                          "grad_v")]
 
 
 _L = None
@@ -63,12 +70,18 @@ def lib():
         L.orc_sym_eig3.argtypes = [vp, vp, vp]
         L.orc_sym_eig3_f32.argtypes = [vp, vp, vp]
         L.orc_spd_inverse3.argtypes = [vp, C.c_double, vp]
+        L.orc_j2_return.restype = C.c_double
+        L.orc_j2_return.argtypes = [vp, C.c_double, C.c_double, C.c_double, C.c_double, vp]
+        L.orc_jc_return.restype = C.c_double
+        L.orc_jc_return.argtypes = [vp, vp, C.c_double, C.c_double, C.c_double, vp, vp]
         _L = L
     return _L
 
 
 SCALARS = ("dt", "max_c_sq", "max_accel", "max_v", "off_grid_num", "off_grid_mass",
-           "wall_work", "visc_work", "diff_work", "leftover_work")
+           "wall_work", "visc_work", "diff_work", "leftover_work", "sim_time", "plastic_work",
+           "hg_work", "load_s", "load_sdot", "sts_stages")
+N_SCALAR_SLOTS = 64
 
 
 class Oracle:
@@ -98,17 +111,12 @@ class Oracle:
         """st: dict with x, x0, u, v, V, V_lo, m, pressure, pst_shift, pid (reference layout)."""
         keep = {}
         s = _State()
-        for k in ("x", "x0", "u", "v", "V", "V_lo", "m", "pressure", "pst_shift"):
-            a = np.ascontiguousarray(st[k], dtype=np.float64)
+        for k in STATE_KEYS:
+            if st.get(k) is None:
+                continue
+            a = np.ascontiguousarray(st[k], dtype=np.int32 if k in INT_KEYS else np.float64)
             keep[k] = a
             setattr(s, k, a.ctypes.data)
-        if st.get("acc") is not None:
-            a = np.ascontiguousarray(st["acc"], dtype=np.float64)
-            keep["acc"] = a
-            s.acc = a.ctypes.data
-        p = np.ascontiguousarray(st["pid"], dtype=np.int32)
-        keep["pid"] = p
-        s.pid = p.ctypes.data
         self.L.orc_set_state(self.h, C.byref(s))
         self.L.orc_set_dt(self.h, float(dt))
 
@@ -119,6 +127,11 @@ class Oracle:
                                              "de_visc")})
         out["L_sym"] = np.zeros((n, 6))
         out["pid"] = np.zeros(n, dtype=np.int32)
+        if self._params.is_solid:
+            out.update({k: np.zeros(n) for k in ("eps_p", "e_int", "temperature", "de_int")})
+            out["sdev"] = np.zeros((n, 6))
+            out["grad_v"] = np.zeros((n, 9))
+            out["bc_flag"] = np.zeros(n, dtype=np.int32)
         o = _Out()
         for k, a in out.items():
             setattr(o, k, a.ctypes.data)
@@ -126,9 +139,12 @@ class Oracle:
         return out
 
     def scalars(self):
-        a = (C.c_double * len(SCALARS))()
+        a = (C.c_double * N_SCALAR_SLOTS)()
         self.L.orc_get_scalars(self.h, a)
-        return dict(zip(SCALARS, list(a)))
+        out = dict(zip(SCALARS, list(a)))
+        out["constraint_force"] = np.array(a[16:40]).reshape(8, 3)
+        out["constraint_disp"] = np.array(a[40:64]).reshape(8, 3)
+        return out
 
     def step(self, k=1):
         self.L.orc_step(self.h, int(k))
@@ -148,9 +164,17 @@ class Oracle:
 def state_from_sets(sets_np):
     """Reference-layout state from one buffer set of sigmasph_b200 (numpy copies)."""
     s = sets_np
-    return {"x": s["pos"][:, :3], "V": s["pos"][:, 3], "v": s["vel"][:, :3], "m": s["vel"][:, 3],
-            "x0": s["x0"][:, :3], "V_lo": s["x0"][:, 3], "u": s["disp"][:, :3],
-            "pressure": s["disp"][:, 3], "pst_shift": s["shift"][:, :3], "pid": s["pid"]}
+    out = {"x": s["pos"][:, :3], "V": s["pos"][:, 3], "v": s["vel"][:, :3], "m": s["vel"][:, 3],
+           "x0": s["x0"][:, :3], "V_lo": s["x0"][:, 3], "u": s["disp"][:, :3],
+           "pressure": s["disp"][:, 3], "pst_shift": s["shift"][:, :3], "pid": s["pid"]}
+    if "sdev" in s:
+        out.update({"sdev": s["sdev"][:, :6], "eps_p": s["sdev"][:, 6],
+                    "temperature": s["sdev"][:, 7], "e_int": s["shift"][:, 3],
+                    "bc_flag": s["bc"][:, 0], "bc_id": s["bc"][:, 1],
+                    "bc_disp": s["bcdisp"][:, :3],
+                    "eos_id": np.rint(s["bcdisp"][:, 3]).astype(np.int32),
+                    "acc": s["acc"][:, :3], "de_int": s["acc"][:, 3]})
+    return out
 
 
 def sym_eig3(A, f32=False):
@@ -174,3 +198,23 @@ def spd_inverse3(E, tol):
     out = np.zeros((3, 3))
     L.orc_spd_inverse3(a.ctypes.data, float(tol), out.ctypes.data)
     return out
+
+
+def j2_return(s, G, sy0, H, eps_p):
+    """Linear-hardening radial return of one deviator: (s_new, d_eps_p)."""
+    a = np.ascontiguousarray(s, dtype=np.float64).reshape(9)
+    out = np.zeros(9)
+    d = lib().orc_j2_return(a.ctypes.data, float(G), float(sy0), float(H), float(eps_p),
+                            out.ctypes.data)
+    return out.reshape(3, 3), d
+
+
+def jc_return(s, G, A, B, n, C_rate, eps0_dot, T0, Tm, m, eps_p, temp, dt):
+    """Johnson-Cook radial return of one deviator: (s_new, d_eps_p, iterations)."""
+    a = np.ascontiguousarray(s, dtype=np.float64).reshape(9)
+    k = np.array([G, A, B, n, C_rate, eps0_dot, T0, Tm, m], dtype=np.float64)
+    out = np.zeros(9)
+    it = C.c_int(0)
+    d = lib().orc_jc_return(a.ctypes.data, k.ctypes.data, float(eps_p), float(temp), float(dt),
+                            out.ctypes.data, C.byref(it))
+    return out.reshape(3, 3), d, it.value

@@ -43,6 +43,18 @@ struct Sim {
     double off_grid_mass = 0, wall_work = 0, visc_work = 0, diff_work = 0, leftover_work = 0;
     // ---- constants folded the way the reference folds them
     R h = 0, alpha = 0, kgrad = 0, eta2 = 0, W_dx0 = 0;
+    // ---- hypoelastic solid (SOLID.py); sorted unless noted
+    std::vector<M3<R>> sdev;                    // deviatoric stress (symmetric)
+    std::vector<R> eps_p, e_int, temperature, de_int;
+    std::vector<int32_t> bc_flag, bc_id, eos_id;
+    std::vector<V3<R>> bc_disp;
+    std::vector<M3<R>> grad_v, dsigma;          // derived
+    std::vector<R> d_eps_p_rate, ale_adv, ale_diff;
+    std::vector<V3<R>> hg_yb, hg_a, hg_v_sync;
+    double sim_time = 0, plastic_work = 0, hg_work = 0, hg_ke_pre = 0;
+    R load_s = 0, load_sdot = 0;
+    double constraint_force[8][3] = {}, constraint_disp[8][3] = {};
+    int sts_last = 0;
 
     void setup(const SphParams& p, int64_t nn) {
         P = p;
@@ -66,6 +78,14 @@ struct Sim {
         kgrad = R(20.0 * al / hd);
         eta2 = R(0.01 * hd * hd);
         W_dx0 = W(R(P.particle_diameter));
+        if (P.is_solid) {
+            sdev.assign(n, M3<R>()); eps_p.assign(n, 0); e_int.assign(n, 0);
+            temperature.assign(n, 0); de_int.assign(n, 0);
+            bc_flag.assign(n, 0); bc_id.assign(n, -1); eos_id.assign(n, 0); bc_disp.assign(n, {});
+            grad_v.assign(n, M3<R>()); dsigma.assign(n, M3<R>());
+            d_eps_p_rate.assign(n, 0); ale_adv.assign(n, 0); ale_diff.assign(n, 0);
+            hg_yb.assign(n, {}); hg_a.assign(n, {}); hg_v_sync.assign(n, {});
+        }
     }
 
     // ------------------------------------------------------------ kernel (sph_base.py:42-92)
@@ -113,6 +133,10 @@ struct Sim {
     template <class F> void for_each_sorted(F&& f) {
         f(x); f(x0); f(u); f(v); f(acc); f(pst_shift); f(V); f(V_lo); f(m); f(pressure); f(pid);
         f(cell_id); f(grid_ids);
+        if (P.is_solid) {
+            f(sdev); f(eps_p); f(e_int); f(temperature); f(de_int); f(bc_flag); f(bc_id);
+            f(eos_id); f(bc_disp);
+        }
     }
 
     void initialize_particle_system() {
@@ -291,12 +315,22 @@ struct Sim {
                 }
                 V3<R> vd = vi - vj;
                 r0 += w(j) * dot(vd, g);
-                if (P.delta_sph > 0.0f) {
+                // the solid's pair_delta (SOLID.py:4103-4114) on same-material pairs only
+                R cpair = coef;
+                bool diffuse = P.delta_sph > 0.0f;
+                if (P.is_solid) {
+                    R di = R(P.mat_delta[eos_id[i]]), dj = R(P.mat_delta[eos_id[j]]);
+                    R den = di + dj;
+                    R dl = den > R(1e-12) ? R(2) * di * dj / den : R(0);
+                    diffuse = eos_id[i] == eos_id[j] && dl > R(0);
+                    cpair = dl * h * R(P.c0);
+                }
+                if (diffuse) {
                     R rn2 = dot(r, r);
                     R a2 = R(2) * (rho_j - rho_i);
                     R den = rn2 + eta2;
                     V3<R> psi = {a2 * (-r[0]) / den, a2 * (-r[1]) / den, a2 * (-r[2]) / den};
-                    R diffusion = coef * w(j) * dot(psi, g);
+                    R diffusion = cpair * w(j) * dot(psi, g);
                     R rate = diffusion / rho_i;
                     r0 += rate;
                     r1 += rate;
@@ -385,6 +419,7 @@ struct Sim {
                 R c = cs2;
                 const R rho_i = m[i] / V[i];
                 for_all_neighbors(i, [&](int64_t j, int) {
+                    if (P.is_solid && P.dt_pair_mode == 2 && eos_id[i] != eos_id[j]) return;
                     R dp = std::fabs(pressure[i] - pressure[j]);
                     R rho_j = m[j] / V[j];
                     R drho = std::fabs(rho_i - rho_j);
@@ -475,6 +510,7 @@ struct Sim {
             }
         }
         if (P.two_d) dr[2] = 0;
+        if (P.is_solid && bc_flag[i] != 0) dr = {};
         return dr;
     }
     void apply_pst() {
@@ -551,14 +587,21 @@ struct Sim {
                     reflect_component(i, 1);
                     v[i][1] = -v[i][1];
                     acc[i][1] = -acc[i][1];
+                    if (P.is_solid) sdev[i] = mirror_mat(1, sdev[i]);
                 }
             }
             if (P.walls) enforce_walls(1 | 4);
         } else {
             if (P.sym_y || P.sym_z) {
                 for (int64_t i = 0; i < n; ++i) {
-                    if (P.sym_y && x[i][1] < R(0)) { reflect_component(i, 1); v[i][1] = -v[i][1]; acc[i][1] = -acc[i][1]; }
-                    if (P.sym_z && x[i][2] < R(0)) { reflect_component(i, 2); v[i][2] = -v[i][2]; acc[i][2] = -acc[i][2]; }
+                    if (P.sym_y && x[i][1] < R(0)) {
+                        reflect_component(i, 1); v[i][1] = -v[i][1]; acc[i][1] = -acc[i][1];
+                        if (P.is_solid) sdev[i] = mirror_mat(1, sdev[i]);
+                    }
+                    if (P.sym_z && x[i][2] < R(0)) {
+                        reflect_component(i, 2); v[i][2] = -v[i][2]; acc[i][2] = -acc[i][2];
+                        if (P.is_solid) sdev[i] = mirror_mat(2, sdev[i]);
+                    }
                 }
             }
             if (P.walls) enforce_walls(P.plane_strain ? (1 | 2 | 4) : (1 | 2 | 4 | 8));
@@ -568,6 +611,525 @@ struct Sim {
                     place_component(i, 2, x0[i][2]);
                 }
             }
+        }
+    }
+
+    // ============================================================ hypoelastic solid (SOLID.py)
+    static M3<R> mirror_mat(int code, const M3<R>& T) {
+        R s[3] = {R(1), (code & 1) ? R(-1) : R(1), (code & 2) ? R(-1) : R(1)};
+        M3<R> o;
+        for (int a = 0; a < 3; ++a) for (int b = 0; b < 3; ++b) o[a][b] = s[a] * T[a][b] * s[b];
+        return o;
+    }
+    R matc_G(int64_t p) const { return R(P.mat_G[eos_id[p]]); }
+    R r_of(int64_t p) const { return std::max(x[p][1], R(P.axi_r_min)); }
+
+    // SOLID.py:5001-5017
+    void update_load_factor() {
+        double T = P.ramp_time;
+        if (T <= 0.0) { load_s = R(1); load_sdot = R(0); return; }
+        double uu = std::min(1.0, std::max(0.0, sim_time / T));
+        load_s = R(uu * uu * (3.0 - 2.0 * uu));
+        load_sdot = R(6.0 * uu * (1.0 - uu) / T);
+    }
+
+    // SOLID.py:1721-1794
+    void compute_velocity_gradient() {
+#pragma omp parallel for schedule(dynamic, 256)
+        for (int64_t i = 0; i < n; ++i) {
+            M3<R> G;
+            for_all_neighbors(i, [&](int64_t j, int mir) {
+                V3<R> xj = xj_of(j, mir), vj = vj_of(j, mir);
+                V3<R> g = dW(x[i] - xj);
+                V3<R> dv = vj - v[i];
+                R wj = w(j);
+                for (int a = 0; a < 3; ++a) for (int b = 0; b < 3; ++b) G[a][b] += wj * (dv[a] * g[b]);
+            });
+            if (P.kernel_correction) {
+                M3<R> E;
+                for_all_neighbors(i, [&](int64_t j, int mir) {
+                    V3<R> xj = xj_of(j, mir);
+                    V3<R> d = xj - x[i];
+                    V3<R> g = dW(x[i] - xj);
+                    R Vj = w(j);
+                    for (int a = 0; a < 3; ++a) for (int b = 0; b < 3; ++b) E[a][b] += Vj * (d[a] * g[b]);
+                });
+                M3<R> L;
+                if (P.two_d) {
+                    R L2[2][2];
+                    spd_inverse_2x2(E[0][0], E[0][1], E[1][0], E[1][1], R(P.l_eig_tol), L2);
+                    L[0][0] = L2[0][0]; L[0][1] = L2[0][1]; L[1][0] = L2[1][0]; L[1][1] = L2[1][1];
+                    L[2][2] = R(1);
+                } else {
+                    L = spd_inverse_3x3(E, R(P.l_eig_tol));
+                }
+                M3<R> GL;
+                for (int a = 0; a < 3; ++a) for (int b = 0; b < 3; ++b) {
+                    R s = 0;
+                    for (int k = 0; k < 3; ++k) s += G[a][k] * L[k][b];
+                    GL[a][b] = s;
+                }
+                G = GL;
+            }
+            if (P.two_d) for (int d = 0; d < 3; ++d) { G[2][d] = 0; G[d][2] = 0; }
+            if (P.axisymmetric) G[2][2] = v[i][1] / r_axi(i);
+            grad_v[i] = G;
+        }
+    }
+
+    // MAT001_linear_plasticity.py:65-81
+    static R vm_of(const M3<R>& s) {
+        R t = 0;
+        for (int a = 0; a < 3; ++a) for (int b = 0; b < 3; ++b) t += s[a][b] * s[a][b];
+        return std::sqrt(R(1.5) * t);
+    }
+    static R j2_return(M3<R>& s, R G, R sy, R H, R ep) {
+        R d = 0;
+        if (sy > R(0)) {
+            R vm = vm_of(s);
+            R sigy = sy + H * ep;
+            if (vm > sigy && (R(3) * G + H) > R(0)) {
+                d = (vm - sigy) / (R(3) * G + H);
+                R sc = (sigy + H * d) / vm;
+                for (int a = 0; a < 3; ++a) for (int b = 0; b < 3; ++b) s[a][b] = s[a][b] * sc;
+            }
+        }
+        return d;
+    }
+    // MAT002_johnson_cook.py:251-354 (bracketed Newton-bisection)
+    static void jc_residual(R d, R vm, R G, R A, R B, R nn, R C, R e0d, R mt, R ep, R dt, R& g, R& dg) {
+        R et = ep + d;
+        R ss = A, ds = 0;
+        if (et > R(0) && B > R(0) && nn > R(0)) {
+            ss += B * std::pow(et, nn);
+            if (et > R(1e-12)) ds = nn * B * std::pow(et, nn - R(1));
+        }
+        R rate = 1;
+        if (dt > R(0) && e0d > R(0)) rate = (d / dt) / e0d;
+        R mr = 1, dmr = 0;
+        if (rate > R(1) && C > R(0)) { mr = R(1) + C * std::log(rate); dmr = C / std::max(R(1e-12), d); }
+        R sy = ss * mr * mt;
+        R dsy = (ds * mr + ss * dmr) * mt;
+        g = vm - R(3) * G * d - sy;
+        dg = -R(3) * G - dsy;
+    }
+    R jc_return(M3<R>& s, int k, R ep, R temp, R dt, int* iters = nullptr) const {
+        return jc_return_of(s, R(P.mat_G[k]), R(P.jc_A[k]), R(P.jc_B[k]), R(P.jc_n[k]),
+                            R(P.jc_C[k]), R(P.jc_eps0_dot[k]), R(P.jc_T0[k]), R(P.jc_Tm[k]),
+                            R(P.jc_m[k]), ep, temp, dt, iters);
+    }
+    static R jc_return_of(M3<R>& s, R G, R A, R B, R nn, R C, R e0d, R T0, R Tm, R mexp,
+                          R ep, R temp, R dt, int* iters = nullptr) {
+        R d = 0;
+        if (!(G > R(0) && A > R(0))) return 0;
+        R vm = vm_of(s);
+        R mt = 1;
+        if (Tm > T0 && temp > T0) {
+            R ts = std::min(R(1), std::max(R(0), (temp - T0) / (Tm - T0)));
+            mt = std::max(R(0), R(1) - std::pow(ts, mexp));
+        }
+        R s0 = A;
+        if (ep > R(0) && B > R(0) && nn > R(0)) s0 += B * std::pow(ep, nn);
+        R sy0 = s0 * mt;
+        if (!(vm > sy0 && sy0 > R(0))) return 0;
+        R lo = 0, hi = (vm - sy0) / (R(3) * G);
+        R dref = 0;
+        if (dt > R(0) && e0d > R(0) && C > R(0)) dref = dt * e0d;
+        if (dref > R(0) && dref < hi) {
+            R g, dg;
+            jc_residual(dref, vm, G, A, B, nn, C, e0d, mt, ep, dt, g, dg);
+            if (g > R(0)) lo = dref; else hi = dref;
+        }
+        d = hi;
+        if (lo > R(0)) d = lo;
+        int it = 0;
+        for (; it < 40; ++it) {
+            R g, dg;
+            jc_residual(d, vm, G, A, B, nn, C, e0d, mt, ep, dt, g, dg);
+            if (g > R(0)) lo = d; else hi = d;
+            if (std::fabs(g) <= R(1e-6) * vm || hi - lo <= R(1e-6) * hi) break;
+            R dn = d - g / dg;
+            if (!(dn > lo && dn < hi)) dn = lo > R(0) ? std::sqrt(lo * hi) : R(0.5) * hi;
+            if (std::fabs(dn - d) <= R(1e-6) * d) { d = dn; break; }
+            d = dn;
+        }
+        if (iters) *iters = it;
+        R syf = std::max(R(0), vm - R(3) * G * d);
+        R sc = syf / vm;
+        for (int a = 0; a < 3; ++a) for (int b = 0; b < 3; ++b) s[a][b] = s[a][b] * sc;
+        return d;
+    }
+
+    // SOLID.py:2691-3004 with the ALE tasks :1799-1862
+    void update_stress() {
+        const R dtl = dt;
+        const bool ale = P.ale_history != 0;
+        const bool plastic_any = [&] {
+            for (int k = 0; k < P.n_materials; ++k) if (P.plastic_sy0[k] > 0.0f) return true;
+            return false;
+        }();
+#pragma omp parallel for schedule(dynamic, 256)
+        for (int64_t i = 0; i < n; ++i) {
+            const M3<R>& Lv = grad_v[i];
+            M3<R> ed, sp;
+            for (int a = 0; a < 3; ++a) for (int b = 0; b < 3; ++b) {
+                ed[a][b] = R(0.5) * (Lv[a][b] + Lv[b][a]);
+                sp[a][b] = R(0.5) * (Lv[a][b] - Lv[b][a]);
+            }
+            R tr = ed[0][0] + ed[1][1] + ed[2][2];
+            const M3<R>& s = sdev[i];
+            R G2 = R(2) * matc_G(i);
+            M3<R> sd;
+            for (int a = 0; a < 3; ++a) for (int b = 0; b < 3; ++b) {
+                R dev = ed[a][b] - ((a == b) ? tr / R(3) : R(0));
+                R ws = 0, sw = 0;
+                for (int k = 0; k < 3; ++k) { ws += sp[a][k] * s[k][b]; sw += s[a][k] * sp[k][b]; }
+                sd[a][b] = G2 * dev + (ws - sw);
+            }
+            R dep = 0;
+            if (ale) {
+                M3<R> A;
+                const V3<R> du_i = {pst_shift[i][0] / dtl, pst_shift[i][1] / dtl, pst_shift[i][2] / dtl};
+                const R rho_i = m[i] / V[i];
+                for_all_neighbors(i, [&](int64_t j, int mir) {
+                    V3<R> xj = xj_of(j, mir);
+                    V3<R> du_j = {pst_shift[j][0] / dtl, pst_shift[j][1] / dtl, pst_shift[j][2] / dtl};
+                    M3<R> sj = sdev[j];
+                    if (mir) { du_j = mirror(mir, du_j); sj = mirror_mat(mir, sj); }
+                    V3<R> g = dW(x[i] - xj);
+                    R rho_j = m[j] / V[j];
+                    R a_j = rho_j * dot(du_j, g), a_i = rho_i * dot(du_i, g);
+                    R div = dot(rho_j * du_j - rho_i * du_i, g);
+                    R wj = w(j);
+                    for (int a = 0; a < 3; ++a) for (int b = 0; b < 3; ++b) {
+                        R flux = a_j * sj[a][b] - a_i * s[a][b];
+                        A[a][b] += wj * (flux - s[a][b] * div) / rho_i;
+                    }
+                    if (plastic_any) {
+                        R flux = a_j * eps_p[j] - a_i * eps_p[i];
+                        dep += wj * (flux - eps_p[i] * div) / rho_i;
+                    }
+                });
+                for (int a = 0; a < 3; ++a) for (int b = 0; b < 3; ++b) sd[a][b] += A[a][b];
+            }
+            dsigma[i] = sd;
+            d_eps_p_rate[i] = dep;
+        }
+        double pw = 0;
+#pragma omp parallel for schedule(static) reduction(+ : pw)
+        for (int64_t i = 0; i < n; ++i) {
+            M3<R> sn;
+            for (int a = 0; a < 3; ++a) for (int b = 0; b < 3; ++b) sn[a][b] = sdev[i][a][b] + dtl * dsigma[i][a][b];
+            M3<R> ss;
+            for (int a = 0; a < 3; ++a) for (int b = 0; b < 3; ++b) ss[a][b] = R(0.5) * (sn[a][b] + sn[b][a]);
+            R tr3 = (ss[0][0] + ss[1][1] + ss[2][2]) / R(3);
+            for (int a = 0; a < 3; ++a) ss[a][a] -= tr3;
+            if (matc_G(i) <= R(0)) ss = M3<R>();
+            if (ale && plastic_any) eps_p[i] = std::max(R(0), eps_p[i] + dtl * d_eps_p_rate[i]);
+            R dprod = 0;
+            if (plastic_any) {
+                int k = eos_id[i];
+                if (P.plastic_kind[k] == 2) dprod = jc_return(ss, k, eps_p[i], temperature[i], dtl);
+                else dprod = j2_return(ss, matc_G(i), R(P.plastic_sy0[k]), R(P.plastic_H[k]), eps_p[i]);
+                eps_p[i] += dprod;
+                if (dprod > R(0)) pw += (double)(V[i] * vm_of(ss) * dprod);
+            }
+            sdev[i] = ss;
+        }
+        plastic_work += pw;
+    }
+
+    // SOLID.py:1949-2069 (ALE advection and upwind diffusion of e)
+    void compute_ale_e_rates() {
+        const R dtl = dt;
+#pragma omp parallel for schedule(dynamic, 256)
+        for (int64_t i = 0; i < n; ++i) {
+            R adv = 0, dif = 0;
+            const V3<R> du_i = {pst_shift[i][0] / dtl, pst_shift[i][1] / dtl, pst_shift[i][2] / dtl};
+            const R rho_i = m[i] / V[i];
+            for_all_neighbors(i, [&](int64_t j, int mir) {
+                V3<R> xj = xj_of(j, mir);
+                V3<R> du_j = {pst_shift[j][0] / dtl, pst_shift[j][1] / dtl, pst_shift[j][2] / dtl};
+                if (mir) du_j = mirror(mir, du_j);
+                V3<R> g = dW(x[i] - xj);
+                R rho_j = m[j] / V[j];
+                adv += w(j) * rho_j * (e_int[j] - e_int[i]) * dot(du_j, g) / rho_i;
+                if (P.ale_diffusion > 0.0f && eos_id[i] == eos_id[j]) {
+                    V3<R> r = x[i] - xj;
+                    R sc = R(2) * (e_int[j] - e_int[i]);
+                    R den = dot(r, r) + eta2;
+                    V3<R> psi = {sc * (-r[0]) / den, sc * (-r[1]) / den, sc * (-r[2]) / den};
+                    R rb = R(0.5) * (rho_i + rho_j);
+                    R sp = R(0.5) * norm(du_i + du_j);
+                    dif += R(P.ale_diffusion) * R(0.5) * R(P.particle_diameter) * sp * w(j) * dot(psi, g) * rb / rho_i;
+                }
+            });
+            ale_adv[i] = adv;
+            ale_diff[i] = dif;
+        }
+    }
+
+    // SOLID.py:2071-2237 (state part) and :2239-2293
+    void update_internal_energy() {
+        const R dtl = dt;
+        V3<R> g = {R(P.gravity[0]), R(P.gravity[1]), R(P.gravity[2])};
+        R gsq = dot(g, g);
+        double wl = 0;
+        for (int64_t i = 0; i < n; ++i) {
+            R de = de_int[i];
+            if (P.transport_e) de += ale_adv[i] + ale_diff[i];
+            e_int[i] += dtl * de;
+            V3<R> f = acc[i] - g;
+            wl += (double)(R(0.5) * m[i] * dtl * dtl * (dot(f, f) - gsq));
+        }
+        leftover_work += wl;
+    }
+    void update_temperature() {
+        for (int64_t i = 0; i < n; ++i) {
+            int k = eos_id[i];
+            R cv = R(P.mat_cv[k]);
+            if (!(cv > R(0))) continue;
+            double rho = (double)m[i] / (double)V[i], rho0 = (double)(R)P.mat_rho0[k];
+            double S = (double)(R)P.mat_stiff[k], gam = (double)(R)P.mat_gamma[k];
+            double xx = rho / rho0, ec;
+            if (std::fabs(gam - 1.0) < 1.0e-6) ec = (S / rho0) * (std::log(xx) + 1.0 / xx - 1.0);
+            else ec = (S / rho0) * ((std::pow(xx, gam - 1.0) - 1.0) / (gam - 1.0) + 1.0 / xx - 1.0);
+            if (!P.allow_negative_pressure && rho < rho0) ec = 0.0;
+            double eth = (double)e_int[i] - ec - 0.0;
+            temperature[i] = R(P.mat_T0[k]) + (R)(eth / (double)cv);
+        }
+    }
+
+    R solid_pressure(int64_t i, R rho) const {
+        int k = eos_id[i];
+        R rho0 = R(P.mat_rho0[k]), S = R(P.mat_stiff[k]), gam = R(P.mat_gamma[k]);
+        bool all_one = true;
+        for (int q = 0; q < P.n_materials; ++q) if (P.mat_gamma[q] != 1.0f) all_one = false;
+        R p = all_one ? S * (rho / rho0 - R(1)) : S * (std::pow(rho / rho0, gam) - R(1));
+        if (!P.allow_negative_pressure) p = std::max(p, R(0));
+        return p;
+    }
+
+    // SOLID.py:3204-3852
+    void compute_stress_accelerations() {
+        for (int64_t i = 0; i < n; ++i) {
+            acc[i] = {R(P.gravity[0]), R(P.gravity[1]), R(P.gravity[2])};
+            pressure[i] = solid_pressure(i, m[i] / V[i]);
+            de_int[i] = 0;
+        }
+        const R dtl = dt;
+        const R visc = R(10.0 * (double)P.viscosity);
+        const bool hg_inloop = P.hourglass_alpha > 0.0f && !P.hourglass_sts;
+        const bool ale = P.pst_enabled && P.pst_ale_momentum;
+        double hgw = 0;
+#pragma omp parallel for schedule(dynamic, 256) reduction(+ : hgw)
+        for (int64_t i = 0; i < n; ++i) {
+            V3<R> dv;
+            R dei = 0, dhg = 0;
+            const R rho_i = m[i] / V[i];
+            const R mwi = mw(i), wi = w(i);
+            for_all_neighbors(i, [&](int64_t j, int mir) {
+                V3<R> xj = xj_of(j, mir), vj = vj_of(j, mir);
+                M3<R> sj = sdev[j];
+                if (mir) sj = mirror_mat(mir, sj);
+                V3<R> r = x[i] - xj;
+                V3<R> g = dW(r);
+                V3<R> f;
+                for (int a = 0; a < 3; ++a) {
+                    R t = 0;
+                    for (int b = 0; b < 3; ++b) {
+                        R sig = (sdev[i][a][b] + sj[a][b]) - ((a == b) ? (pressure[i] + pressure[j]) : R(0));
+                        t += sig * g[b];
+                    }
+                    f[a] = wi * w(j) * t;
+                }
+                if (P.axisymmetric && P.axi_conservative_x) f[0] = f[0] * (R(0.5) * (r_of(i) + r_of(j)) / r_of(i));
+                dv += {f[0] / mwi, f[1] / mwi, f[2] / mwi};
+                V3<R> vij = v[i] - vj;
+                dei += -R(0.5) * dot(f, vij) / mwi;
+                R vxy = dot(vij, r);
+                R rn = norm(r);
+                V3<R> am = (visc * w(j) * vxy / (rn * rn + eta2)) * g;
+                dv += am;
+                if (P.viscosity > 0.0f) dei += -R(0.5) * dot(am, vij);
+                if (hg_inloop && rn > R(1e-9)) {
+                    V3<R> rh = {-r[0] / rn, -r[1] / rn, -r[2] / rn};
+                    M3<R> gvj = grad_v[j];
+                    if (mir) gvj = mirror_mat(mir, gvj);
+                    V3<R> dvh;
+                    for (int a = 0; a < 3; ++a) {
+                        R t = 0;
+                        for (int b = 0; b < 3; ++b) t += R(0.5) * (grad_v[i][a][b] + gvj[a][b]) * (-r[b]);
+                        dvh[a] = (vj[a] - v[i][a]) - t;
+                    }
+                    R hg = dot(dvh, rh);
+                    R Wij = W(rn);
+                    int k = eos_id[i];
+                    R damp = R(P.hourglass_alpha) * (R(P.mat_rho0[k]) / rho_i) * (R(P.mat_cp[k]) / h)
+                             * (w(j) / R(P.V0)) * (Wij / R(P.hg_W_dx0)) * hg;
+                    V3<R> ah = damp * rh;
+                    if (P.axisymmetric && P.axi_conservative_x) ah[0] = ah[0] * (R(0.5) * (r_of(i) + r_of(j)) / r_of(i));
+                    dv += ah;
+                    dhg += -R(0.5) * dot(ah, vij);
+                }
+                if (ale) {
+                    V3<R> du_i = {pst_shift[i][0] / dtl, pst_shift[i][1] / dtl, pst_shift[i][2] / dtl};
+                    V3<R> du_j = {pst_shift[j][0] / dtl, pst_shift[j][1] / dtl, pst_shift[j][2] / dtl};
+                    if (mir) du_j = mirror(mir, du_j);
+                    R rho_j = m[j] / V[j];
+                    V3<R> a = (rho_j * dot(du_j, g)) * vj - (rho_i * dot(du_i, g)) * v[i];
+                    R b = dot(rho_j * du_j - rho_i * du_i, g);
+                    V3<R> t = a - b * v[i];
+                    R c = w(j);
+                    dv += {c * t[0] / rho_i, c * t[1] / rho_i, c * t[2] / rho_i};
+                }
+            });
+            if (P.axisymmetric) {
+                R inv = R(1) / (rho_i * r_axi(i));
+                dv[1] += (sdev[i][1][1] - sdev[i][2][2]) * inv;
+            }
+            acc[i] += dv;
+            de_int[i] = dei;
+            hgw += (double)(mwi * dhg);
+        }
+        hg_step_power = hgw;
+    }
+    double hg_step_power = 0;
+
+    // SOLID.py:4241-4309 (the damper operator on the sub-stepped velocity y)
+    void compute_hg_accel() {
+#pragma omp parallel for schedule(dynamic, 256)
+        for (int64_t i = 0; i < n; ++i) {
+            V3<R> a;
+            const R rho_i = m[i] / V[i];
+            for_all_neighbors(i, [&](int64_t j, int mir) {
+                V3<R> xj = xj_of(j, mir);
+                V3<R> yj = hg_yb[j];
+                M3<R> gvj = grad_v[j];
+                if (mir) { yj = mirror(mir, yj); gvj = mirror_mat(mir, gvj); }
+                V3<R> r = x[i] - xj;
+                R rn = norm(r);
+                if (!(rn > R(1e-9))) return;
+                V3<R> rh = {-r[0] / rn, -r[1] / rn, -r[2] / rn};
+                V3<R> dvh;
+                for (int q = 0; q < 3; ++q) {
+                    R t = 0;
+                    for (int b = 0; b < 3; ++b) t += R(0.5) * (grad_v[i][q][b] + gvj[q][b]) * (-r[b]);
+                    dvh[q] = (yj[q] - hg_yb[i][q]) - t;
+                }
+                R hg = dot(dvh, rh);
+                R Wij = W(rn);
+                int k = eos_id[i];
+                R damp = R(P.hourglass_alpha) * (R(P.mat_rho0[k]) / rho_i) * (R(P.mat_cp[k]) / h)
+                         * (w(j) / R(P.V0)) * (Wij / R(P.hg_W_dx0)) * hg;
+                V3<R> ah = damp * rh;
+                if (P.axisymmetric && P.axi_conservative_x) ah[0] = ah[0] * (R(0.5) * (r_of(i) + r_of(j)) / r_of(i));
+                a += ah;
+            });
+            hg_a[i] = a;
+        }
+    }
+    double kinetic() const {
+        double ke = 0;
+        for (int64_t i = 0; i < n; ++i) ke += (double)(R(0.5) * m[i] * dot(v[i], v[i]));
+        return ke;
+    }
+
+    // SOLID.py:5019-5055
+    void apply_constraints() {
+        for (int k = 0; k < 8; ++k) for (int d = 0; d < 3; ++d) { constraint_force[k][d] = 0; constraint_disp[k][d] = 0; }
+        const R s = load_s, sd = load_sdot;
+        const R scale = P.axisymmetric ? R(2.0 * kPi) : R(1);
+        for (int64_t i = 0; i < n; ++i) {
+            int fl = bc_flag[i];
+            if (!fl) continue;
+            int cid = bc_id[i];
+            for (int d = 0; d < 3; ++d) {
+                if (!(fl & (1 << d))) continue;
+                if (P.num_constraints > 0 && cid >= 0) {
+                    constraint_force[cid][d] += (double)(scale * m[i] * acc[i][d]);
+                    constraint_disp[cid][d] = (double)(bc_disp[i][d] * s);
+                }
+                u[i][d] = bc_disp[i][d] * s;
+                x[i][d] = x0[i][d] + u[i][d];
+                v[i][d] = bc_disp[i][d] * sd;
+                acc[i][d] = 0;
+            }
+        }
+    }
+
+    // The step in the stage grouping of the GPU (SPH_STAGE_*), for stage-by-stage checks.
+    void stage_solid(int s) {
+        switch (s) {
+            case SPH_STAGE_SORT: update_load_factor(); initialize_particle_system(); break;
+            case SPH_STAGE_LAM: {
+                compute_lam();
+                compute_velocity_gradient();
+                update_stress();
+                if (P.transport_e) compute_ale_e_rates();
+                update_internal_energy();
+                bool thermal = false;
+                for (int k = 0; k < P.n_materials; ++k) if (P.mat_cv[k] > 0.0f) thermal = true;
+                if (thermal) update_temperature();
+                break;
+            }
+            case SPH_STAGE_CONTINUITY: compute_volume_evolution(); break;
+            case SPH_STAGE_FORCES: compute_stress_accelerations(); break;
+            case SPH_STAGE_DT: solid_dt(); break;
+            case SPH_STAGE_ADVECT: solid_advect(); apply_constraints(); break;
+            case SPH_STAGE_PST: if (P.pst_enabled) apply_pst(); break;
+            case SPH_STAGE_BOUNDARY: boundary(); sim_time += (double)dt; break;
+            default: break;
+        }
+    }
+    void solid_dt() {
+        compute_adaptive_dt();
+        const bool hg = P.hourglass_alpha > 0.0f;
+        sts_last = 0;
+        if (!P.hourglass_sts) {
+            if (hg) dt = std::min(dt, R(1.6 / (double)P.hg_rate));
+            hg_work += (double)dt * hg_step_power;
+        } else if (hg) {
+            int s = 1;
+            if (P.hg_rate > 0.0f) {
+                double want = (double)P.hg_rate * (double)dt;
+                s = P.hg_sts_fixed > 0 ? P.hg_sts_fixed : std::max(1, (int)std::ceil(want / 1.6));
+                s = std::min(s, 32);
+                double cap = s * 1.6 / (double)P.hg_rate;
+                if ((double)dt > cap) dt = R(cap);
+            }
+            sts_last = s;
+        }
+    }
+    void step_solid() {
+        for (int s = SPH_STAGE_SORT; s <= SPH_STAGE_BOUNDARY; ++s) stage_solid(s);
+    }
+    void solid_advect() {
+        const bool hg = P.hourglass_alpha > 0.0f;
+        if (P.hourglass_sts && hg) {
+            const int s = sts_last;
+            for (int64_t i = 0; i < n; ++i) { v[i] += (R(0.5) * dt) * acc[i]; hg_v_sync[i] = v[i]; }
+            if (P.hg_sts_refresh) compute_velocity_gradient();
+            hg_ke_pre = kinetic();
+            for (int64_t i = 0; i < n; ++i) hg_yb[i] = v[i];
+            R sub = R((double)dt / s);
+            for (int st = 0; st < s; ++st) {
+                compute_hg_accel();
+                for (int64_t i = 0; i < n; ++i) hg_yb[i] = hg_yb[i] + sub * hg_a[i];
+            }
+            for (int64_t i = 0; i < n; ++i) v[i] = hg_yb[i];
+            hg_work += hg_ke_pre - kinetic();
+            R hh = R(0.5) * dt;
+            double wsum = 0;
+            for (int64_t i = 0; i < n; ++i) {
+                V3<R> dvv = v[i] - hg_v_sync[i];
+                wsum += (double)(m[i] * dot(dvv, hh * acc[i]));
+                v[i] += hh * acc[i];
+            }
+            leftover_work += wsum;
+            for (int64_t i = 0; i < n; ++i) displace(i, dt * v[i]);
+        } else {
+            for (int64_t i = 0; i < n; ++i) { v[i] += dt * acc[i]; displace(i, dt * v[i]); }
         }
     }
 
@@ -581,11 +1143,13 @@ struct Sim {
         if (P.pst_enabled) apply_pst();
     }
     void step() {
+        if (P.is_solid) { step_solid(); return; }
         initialize_particle_system();
         substep();
         boundary();
     }
     void stage(int s) {
+        if (P.is_solid) { stage_solid(s); return; }
         switch (s) {
             case SPH_STAGE_SORT: initialize_particle_system(); break;
             case SPH_STAGE_LAM: compute_lam(); break;
@@ -615,11 +1179,17 @@ struct OracleState {
     const double* x; const double* x0; const double* u; const double* v; const double* acc;
     const double* V; const double* V_lo; const double* m; const double* pressure;
     const double* pst_shift; const int32_t* pid;
+    // solid (may be NULL for a fluid)
+    const double* sdev; const double* eps_p; const double* e_int; const double* temperature;
+    const double* de_int; const int32_t* bc_flag; const int32_t* bc_id; const double* bc_disp;
+    const int32_t* eos_id;
 };
 struct OracleOut {
     double* x; double* x0; double* u; double* v; double* acc;
     double* V; double* V_lo; double* m; double* pressure; double* pst_shift; int32_t* pid;
     double* lam; double* L_sym; double* lam_grad; double* divergence; double* de_visc;
+    double* sdev; double* eps_p; double* e_int; double* temperature; double* de_int;
+    int32_t* bc_flag; double* grad_v;
 };
 
 struct Handle {
@@ -640,6 +1210,21 @@ template <class R> void put(Sim<R>& s, const OracleState* st) {
         }
         s.V[i] = (R)st->V[i]; s.V_lo[i] = (R)st->V_lo[i]; s.m[i] = (R)st->m[i];
         s.pressure[i] = (R)st->pressure[i]; s.pid[i] = st->pid[i];
+        if (s.P.is_solid && st->sdev) {
+            const double* q = st->sdev + 6 * i;
+            M3<R> S;
+            S[0][0] = (R)q[0]; S[1][1] = (R)q[1]; S[2][2] = (R)q[2];
+            S[0][1] = S[1][0] = (R)q[3]; S[0][2] = S[2][0] = (R)q[4]; S[1][2] = S[2][1] = (R)q[5];
+            s.sdev[i] = S;
+            s.eps_p[i] = (R)st->eps_p[i];
+            s.e_int[i] = (R)st->e_int[i];
+            s.temperature[i] = (R)st->temperature[i];
+            s.de_int[i] = st->de_int ? (R)st->de_int[i] : R(0);
+            s.bc_flag[i] = st->bc_flag[i];
+            s.bc_id[i] = st->bc_id[i];
+            s.eos_id[i] = st->eos_id[i];
+            for (int k = 0; k < 3; ++k) s.bc_disp[i][k] = (R)st->bc_disp[3 * i + k];
+        }
     }
 }
 template <class R> void get(const Sim<R>& s, OracleOut* o) {
@@ -662,6 +1247,19 @@ template <class R> void get(const Sim<R>& s, OracleOut* o) {
         if (o->divergence) o->divergence[i] = s.divergence[i];
         if (o->de_visc) o->de_visc[i] = s.de_visc[i];
         if (o->L_sym) for (int k = 0; k < 6; ++k) o->L_sym[6 * i + k] = s.L_sym[i][k];
+        if (s.P.is_solid) {
+            const M3<R>& S = s.sdev[i];
+            if (o->sdev) {
+                double* q = o->sdev + 6 * i;
+                q[0] = S[0][0]; q[1] = S[1][1]; q[2] = S[2][2]; q[3] = S[0][1]; q[4] = S[0][2]; q[5] = S[1][2];
+            }
+            if (o->eps_p) o->eps_p[i] = s.eps_p[i];
+            if (o->e_int) o->e_int[i] = s.e_int[i];
+            if (o->temperature) o->temperature[i] = s.temperature[i];
+            if (o->de_int) o->de_int[i] = s.de_int[i];
+            if (o->bc_flag) o->bc_flag[i] = s.bc_flag[i];
+            if (o->grad_v) for (int a = 0; a < 3; ++a) for (int b = 0; b < 3; ++b) o->grad_v[9 * i + 3 * a + b] = s.grad_v[i][a][b];
+        }
     }
 }
 
@@ -697,6 +1295,13 @@ void orc_get_scalars(void* hp, double* out) {
         out[0] = s.dt; out[1] = s.max_c_sq; out[2] = s.max_accel; out[3] = s.max_v;
         out[4] = s.off_grid_num; out[5] = s.off_grid_mass; out[6] = s.wall_work;
         out[7] = s.visc_work; out[8] = s.diff_work; out[9] = s.leftover_work;
+        out[10] = s.sim_time; out[11] = s.plastic_work; out[12] = s.hg_work;
+        out[13] = s.load_s; out[14] = s.load_sdot; out[15] = s.sts_last;
+        for (int k = 0; k < 8; ++k)
+            for (int d = 0; d < 3; ++d) {
+                out[16 + 3 * k + d] = s.constraint_force[k][d];
+                out[40 + 3 * k + d] = s.constraint_disp[k][d];
+            }
     };
     if (h->fp64) fill(h->d); else fill(h->f);
 }
@@ -724,6 +1329,24 @@ void orc_sym_eig3_f32(const float* A, float* ev, float* Q) {
     for (int i = 0; i < 3; ++i) for (int j = 0; j < 3; ++j) M[i][j] = A[3 * i + j];
     sym_eig3(M, ev, QQ);
     for (int i = 0; i < 3; ++i) for (int j = 0; j < 3; ++j) Q[3 * i + j] = QQ[i][j];
+}
+// Return maps on one deviator (row-major 3x3), for the known-answer tests.
+double orc_j2_return(const double* s_in, double G, double sy, double H, double ep, double* s_out) {
+    M3<double> s;
+    for (int a = 0; a < 3; ++a) for (int b = 0; b < 3; ++b) s[a][b] = s_in[3 * a + b];
+    double d = Sim<double>::j2_return(s, G, sy, H, ep);
+    for (int a = 0; a < 3; ++a) for (int b = 0; b < 3; ++b) s_out[3 * a + b] = s[a][b];
+    return d;
+}
+double orc_jc_return(const double* s_in, const double* k11, double ep, double temp, double dt,
+                     double* s_out, int* iters) {
+    // k11 = {G, A, B, n, C, eps0_dot, T0, Tm, m}
+    M3<double> s;
+    for (int a = 0; a < 3; ++a) for (int b = 0; b < 3; ++b) s[a][b] = s_in[3 * a + b];
+    double d = Sim<double>::jc_return_of(s, k11[0], k11[1], k11[2], k11[3], k11[4], k11[5],
+                                         k11[6], k11[7], k11[8], ep, temp, dt, iters);
+    for (int a = 0; a < 3; ++a) for (int b = 0; b < 3; ++b) s_out[3 * a + b] = s[a][b];
+    return d;
 }
 void orc_spd_inverse3(const double* E, double tol, double* L) {
     M3<double> M;

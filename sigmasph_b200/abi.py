@@ -59,12 +59,15 @@ PARAM_FIELDS = [
     ("plastic_kind", _i32 * 4), ("plastic_sy0", _f32 * 4), ("plastic_H", _f32 * 4),
     ("jc_A", _f32 * 4), ("jc_B", _f32 * 4), ("jc_n", _f32 * 4), ("jc_C", _f32 * 4),
     ("jc_eps0_dot", _f32 * 4),
+    ("jc_T0", _f32 * 4), ("jc_Tm", _f32 * 4), ("jc_m", _f32 * 4), ("jc_chi", _f32 * 4),
+    ("mat_cv", _f32 * 4), ("mat_stiff", _f32 * 4), ("mat_gamma", _f32 * 4),
+    ("mat_T0", _f32 * 4), ("axi_conservative_x", _i32), ("hg_rate", _f32),
     ("kernel_correction", _i32), ("l_eig_tol", _f32), ("hourglass_alpha", _f32),
     ("hourglass_sts", _i32), ("hourglass_sts_cap", _i32),
     ("hourglass_sts_safety", _f32), ("hg_S", _f32), ("hg_W_dx0", _f32),
     ("hg_sts_refresh", _i32), ("ale_history", _i32), ("transport_e", _i32),
     ("ale_diffusion", _f32), ("num_constraints", _i32), ("ramp_time", _f32),
-    ("jc_surrogate", _i32), ("jc_surrogate_tol", _f32),
+    ("jc_surrogate", _i32), ("jc_surrogate_tol", _f32), ("hg_sts_fixed", _i32),
     ("reserved", _i32 * 8),
 ]
 
@@ -76,7 +79,8 @@ class SphParams(C.Structure):
 class SphFieldSet(C.Structure):
     _fields_ = [("pos", C.c_void_p), ("vel", C.c_void_p), ("x0", C.c_void_p),
                 ("disp", C.c_void_p), ("shift", C.c_void_p), ("pid", C.c_void_p),
-                ("sdev", C.c_void_p), ("bc", C.c_void_p), ("bcdisp", C.c_void_p)]
+                ("sdev", C.c_void_p), ("bc", C.c_void_p), ("bcdisp", C.c_void_p),
+                ("acc", C.c_void_p)]
 
 
 class SphBuffers(C.Structure):

@@ -96,7 +96,8 @@ Ptr make_ptr(SphHandle* h) {
     Ptr P;
     P.cur = h->buf.set[h->parity];
     P.nxt = h->buf.set[1 - h->parity];
-    P.acc = reinterpret_cast<float4*>(h->buf.acc);
+    // the solid's acceleration (and de_int) is persistent, carried in the field sets
+    P.acc = reinterpret_cast<float4*>(h->p.is_solid ? P.cur.acc : h->buf.acc);
     P.lam = h->buf.lam;
     P.lsym = reinterpret_cast<float4*>(h->buf.lsym);
     P.lgrad = reinterpret_cast<float4*>(h->buf.lgrad);
@@ -178,7 +179,9 @@ int one_step(SphHandle* h, cudaStream_t st) {
         if ((r = solid_pre_step(h->c, make_ptr(h), h->solid, st)) != SPH_OK) return r;
     }
     if ((r = rebuild(h, st)) != SPH_OK) return r;
-    if (h->p.is_solid) return solid_substep_and_boundary(h->c, make_ptr(h), h->solid, (int)h->n, st);
+    if (h->p.is_solid)
+        return solid_substep_launch(h->c, make_ptr(h), (int)h->n, st,
+                                    [&](const char* name) { prof_mark(h, name, st); });
     return fluid_substep_and_boundary(h, st);
 }
 
@@ -202,7 +205,8 @@ void free_all(SphHandle* h) {
 
 bool valid_set(const SphFieldSet& s, bool solid) {
     if (!s.pos || !s.vel || !s.x0 || !s.disp || !s.shift || !s.pid) return false;
-    if (solid && (!s.sdev || !s.bc || !s.bcdisp)) return false;
+    if (solid && (!s.sdev || !s.bc || !s.bcdisp || !s.acc)) return false;
+    if (solid && (reinterpret_cast<uintptr_t>(s.acc) & 15u) != 0) return false;
     auto al = [](const void* q) { return (reinterpret_cast<uintptr_t>(q) & 15u) == 0; };
     return al(s.pos) && al(s.vel) && al(s.x0) && al(s.disp) && al(s.shift) &&
            (!solid || (al(s.sdev) && al(s.bcdisp) && (reinterpret_cast<uintptr_t>(s.bc) & 7u) == 0));
@@ -244,6 +248,8 @@ int sph_params_layout(char* buf, int cap) {
     F(pst_max_shift) F(pst_ma_fixed) F(pst_m_delta) F(pst_lambda_lo) F(pst_lambda_hi)
     F(n_materials) F(mat_rho0) F(mat_K) F(mat_G) F(mat_cp) F(mat_c0) F(mat_delta)
     F(plastic_kind) F(plastic_sy0) F(plastic_H) F(jc_A) F(jc_B) F(jc_n) F(jc_C) F(jc_eps0_dot)
+    F(jc_T0) F(jc_Tm) F(jc_m) F(jc_chi) F(mat_cv) F(mat_stiff) F(mat_gamma) F(mat_T0)
+    F(axi_conservative_x) F(hg_rate) F(hg_sts_fixed)
     F(kernel_correction) F(l_eig_tol) F(hourglass_alpha) F(hourglass_sts) F(hourglass_sts_cap)
     F(hourglass_sts_safety) F(hg_S) F(hg_W_dx0) F(hg_sts_refresh) F(ale_history) F(transport_e)
     F(ale_diffusion) F(num_constraints) F(ramp_time) F(jc_surrogate) F(jc_surrogate_tol)
@@ -331,7 +337,7 @@ void sph_destroy(SphHandle* h) {
 int sph_bind(SphHandle* h, const SphBuffers* b, int64_t n) {
     if (!h || !b || n < 0 || n > h->n_max) return SPH_ERR_ARG;
     if (!valid_set(b->set[0], h->p.is_solid) || !valid_set(b->set[1], h->p.is_solid)) return SPH_ERR_ARG;
-    if (!b->acc || !b->lam || !b->lsym || !b->lgrad || !b->div) return SPH_ERR_ARG;
+    if ((!h->p.is_solid && !b->acc) || !b->lam || !b->lsym || !b->lgrad || !b->div) return SPH_ERR_ARG;
     if (h->p.is_solid && (!b->gradv || !b->aux)) return SPH_ERR_ARG;
     drop_graph(h);
     h->buf = *b;
@@ -408,8 +414,15 @@ int sph_run_stage(SphHandle* h, int stage, void* stream) {
     cudaStream_t st = S(stream);
     const int nb = blocks_for(h->n);
     if (h->p.is_solid) {
-        int r = solid_run_stage(h->c, make_ptr(h), h->solid, (int)h->n, stage, st,
-                                [&]() { return rebuild(h, st); });
+        if (stage < SPH_STAGE_SORT || stage > SPH_STAGE_BOUNDARY) return SPH_ERR_ARG;
+        int r = SPH_OK;
+        if (stage == SPH_STAGE_SORT) {
+            r = solid_pre_step(h->c, make_ptr(h), h->solid, st);
+            if (!r) r = rebuild(h, st);
+        } else {
+            r = solid_substep_launch(h->c, make_ptr(h), (int)h->n, st,
+                                     [&](const char* name) { prof_mark(h, name, st); }, stage, stage);
+        }
         if (r) return r;
         CK(cudaGetLastError());
         return SPH_OK;

@@ -33,6 +33,7 @@ struct DevAccum {
     unsigned int max_accel_bits;
     unsigned int max_v_bits;
     int pad;
+    double hg_power;         // sum_i mw_i de_hg_i of the in-loop damper (solid)
 };
 
 // Constants of one handle, passed by value to every kernel.

@@ -255,6 +255,7 @@ __global__ void __launch_bounds__(kBlock) k_gather(Cst c, Ptr P) {
         sb[2 * d + 1] = __ldg(sa + 2 * s + 1);
         reinterpret_cast<int2*>(B.bc)[d] = __ldg(reinterpret_cast<const int2*>(A.bc) + s);
         reinterpret_cast<float4*>(B.bcdisp)[d] = __ldg(reinterpret_cast<const float4*>(A.bcdisp) + s);
+        reinterpret_cast<float4*>(B.acc)[d] = __ldg(reinterpret_cast<const float4*>(A.acc) + s);
     }
     int4 cl = P.cell_tmp[s];
     cl.w = cl.w < 0 ? -1 : P.key[s];

@@ -1,24 +1,934 @@
-// sph_solid.cuh -- hypoelastic tensile-solid step (SOLID.py HypoElasticSolver).
+// sph_solid.cuh -- the hypoelastic tensile-solid step (SOLID.py HypoElasticSolver.substep,
+// :5060-5196, and step, :5227-5231) as sm_100a kernels over the neighbour lists.
+//
+//   k_solid_load     update_load_factor (SOLID.py:5001-5017), on the device clock
+//   (rebuild, k_lam as for the fluid; k_lam also forms the kernel-correction inverse)
+//   k_solid_a        grad lambda + continuity + grad v, one sweep      (DSPH.py:683-702,
+//                    :1208-1338, SOLID.py:1721-1794)
+//   k_solid_b        ALE transport of s, eps_p, e (one sweep); epilogue: Jaumann update,
+//                    J2 / Johnson-Cook return, energy and temperature  (SOLID.py:1799-2293,
+//                    :2691-3004)
+//   k_solid_commit   the updated history, volume update, per-material EOS, gravity
+//   k_solid_force    stress divergence + Morris + in-loop hourglass + ALE momentum, the
+//                    work conjugate de_int, the dt pair estimate    (SOLID.py:3204-3852)
+//   k_solid_dt       CFL limits, the damper cap or sub-step count  (SOLID.py:4116-4161,
+//                    :4510-4539)
+//   k_half_kick, k_gradv, k_hg_stage x32, k_sts_finish   the sub-cycled damper between
+//                    the half kicks, with a device-side stage count (SOLID.py:4485-4615)
+//   k_solid_advect   plain advect when the damper is in-loop
+//   k_constraints    grip kinematics and FP64 grip force          (SOLID.py:5019-5055)
+//   (k_pst_search, k_pst, k_finish as for the fluid)
+//
+// Per-step scratch in aux ([n][24] floats = 6 float4):
+//   aux[0]  s_new xx yy zz xy     aux[1]  s_new xz yz, eps_p_new, e_new
+//   aux[2]  T_new, -, -, -        aux[3]  kernel-correction inverse L00 L11 L22 L01
+//   aux[4]  L02 L12 | v_sync.xy   aux[5]  v_sync.z | -
+// The damper's sub-stepped velocity ping-pongs between aux[0..1] and aux[2..3]-free
+// slots: y_a = aux float4 slot 0 (xyz), y_b = slot 2 (xyz), used only after the history
+// has been committed.
 #pragma once
 #include "sph_fluid.cuh"
 
 namespace sph {
+
+constexpr int kStsMaxStages = 32;
 
 struct SolidScratch {
     int unused = 0;
 };
 
 inline void solid_fill_constants(Cst&) {}
-inline int solid_alloc(SolidScratch&, const SphParams&, int64_t) { return SPH_ERR_UNSUPPORTED; }
+inline int solid_alloc(SolidScratch&, const SphParams&, int64_t) { return SPH_OK; }
 inline void solid_free(SolidScratch&) {}
-inline int solid_pre_step(const Cst&, const Ptr&, SolidScratch&, cudaStream_t) { return SPH_ERR_UNSUPPORTED; }
-inline int solid_substep_and_boundary(const Cst&, const Ptr&, SolidScratch&, int, cudaStream_t) {
-    return SPH_ERR_UNSUPPORTED;
+
+// ------------------------------------------------------------------ helpers
+struct Sym { float xx, yy, zz, xy, xz, yz; };
+__device__ __forceinline__ Sym load_s(const float* sdev, int i) {
+    const float4* s = reinterpret_cast<const float4*>(sdev) + 2 * i;
+    float4 a = __ldg(s), b = __ldg(s + 1);
+    return {a.x, a.y, a.z, a.w, b.x, b.y};
 }
-template <class Rebuild>
-inline int solid_run_stage(const Cst&, const Ptr&, SolidScratch&, int, int, cudaStream_t, Rebuild&&) {
-    return SPH_ERR_UNSUPPORTED;
+__device__ __forceinline__ Sym mirror_sym(int code, Sym s) {
+    // M s M with M = diag(1, sy, sz): s_xy *= sy, s_xz *= sz, s_yz *= sy sz
+    float sy = (code & 1) ? -1.0f : 1.0f, sz = (code & 2) ? -1.0f : 1.0f;
+    return {s.xx, s.yy, s.zz, s.xy * sy, s.xz * sz, s.yz * sy * sz};
 }
+__device__ __forceinline__ float vm_sym(const Sym& s) {
+    float t = s.xx * s.xx + s.yy * s.yy + s.zz * s.zz + 2.0f * (s.xy * s.xy + s.xz * s.xz + s.yz * s.yz);
+    return sqrtf(1.5f * t);
+}
+__device__ __forceinline__ int eos_of(const Ptr& P, int i) {
+    return (int)__ldg(P.cur.bcdisp + 4 * i + 3);
+}
+__device__ __forceinline__ float r_axi_of(float y, const Cst& c) { return fmaxf(y, c.p.axi_r_min); }
+
+// Per-material pressure: S((rho/rho0)^gamma - 1), exactly linear when every material's
+// gamma is 1 (SOLID.py:3009-3038).
+__device__ __forceinline__ float solid_pressure(const Cst& c, int k, float rho) {
+    bool all_one = true;
+    for (int q = 0; q < c.p.n_materials; ++q) all_one = all_one && (c.p.mat_gamma[q] == 1.0f);
+    float rho0 = c.p.mat_rho0[k], S = c.p.mat_stiff[k];
+    float p = all_one ? S * (rho / rho0 - 1.0f) : S * (powf(rho / rho0, c.p.mat_gamma[k]) - 1.0f);
+    if (!c.p.allow_negative_pressure) p = fmaxf(p, 0.0f);
+    return p;
+}
+
+// ------------------------------------------------------------------ load factor
+__global__ void k_solid_load(Cst c, Ptr P) {
+    if (threadIdx.x != 0 || blockIdx.x != 0) return;
+    double T = c.p.ramp_time;
+    if (T <= 0.0) { P.sc->load_s = 1.0f; P.sc->load_sdot = 0.0f; return; }
+    double u = fmin(1.0, fmax(0.0, P.sc->sim_time / T));
+    P.sc->load_s = (float)(u * u * (3.0 - 2.0 * u));
+    P.sc->load_sdot = (float)(6.0 * u * (1.0 - u) / T);
+}
+
+// Velocity gradient sum G = sum_j w_j (v_j - v_i) (x) grad W (SOLID.py:1721-1794) with
+// the optional correction G L, single-layer zeroing and the axisymmetric hoop rate.
+template <class Extra>
+__device__ __forceinline__ void grad_v_finish(const Cst& c, const Ptr& P, int i, float G[3][3],
+                                              float4 pi, float vy) {
+    if (c.p.kernel_correction) {
+        float4 a = P.aux[6 * i + 3], b = P.aux[6 * i + 4];
+        float L[3][3] = {{a.x, a.w, b.x}, {a.w, a.y, b.y}, {b.x, b.y, a.z}};
+        float R[3][3];
+#pragma unroll
+        for (int r = 0; r < 3; ++r)
+#pragma unroll
+            for (int q = 0; q < 3; ++q) R[r][q] = G[r][0] * L[0][q] + G[r][1] * L[1][q] + G[r][2] * L[2][q];
+#pragma unroll
+        for (int r = 0; r < 3; ++r)
+#pragma unroll
+            for (int q = 0; q < 3; ++q) G[r][q] = R[r][q];
+    }
+    if (c.p.two_d) {
+#pragma unroll
+        for (int d = 0; d < 3; ++d) { G[2][d] = 0.0f; G[d][2] = 0.0f; }
+    }
+    if (c.p.axisymmetric) G[2][2] = vy / r_axi_of(pi.y, c);
+    float* g = P.gradv + 12 * i;
+    reinterpret_cast<float4*>(g)[0] = make_float4(G[0][0], G[0][1], G[0][2], G[1][0]);
+    reinterpret_cast<float4*>(g)[1] = make_float4(G[1][1], G[1][2], G[2][0], G[2][1]);
+    reinterpret_cast<float4*>(g)[2] = make_float4(G[2][2], 0.0f, 0.0f, 0.0f);
+}
+struct NoExtra {};
+
+__device__ __forceinline__ void load_gradv(const Ptr& P, int j, float G[3][3]) {
+    const float4* g = reinterpret_cast<const float4*>(P.gradv + 12 * j);
+    float4 a = __ldg(g), b = __ldg(g + 1), d = __ldg(g + 2);
+    G[0][0] = a.x; G[0][1] = a.y; G[0][2] = a.z; G[1][0] = a.w;
+    G[1][1] = b.x; G[1][2] = b.y; G[2][0] = b.z; G[2][1] = b.w; G[2][2] = d.x;
+}
+__device__ __forceinline__ void mirror_mat3(int code, float G[3][3]) {
+    float s[3] = {1.0f, (code & 1) ? -1.0f : 1.0f, (code & 2) ? -1.0f : 1.0f};
+#pragma unroll
+    for (int a = 0; a < 3; ++a)
+#pragma unroll
+        for (int b = 0; b < 3; ++b) G[a][b] *= s[a] * s[b];
+}
+
+// ------------------------------------------------------------------ kernel-correction inverse
+// The regularised inverse of E at the consumer's tolerance (spd_inverse.py:86-101), formed
+// from the lambda pass's E.  Near a free surface (lambda below 0.75) the eigen-problem is
+// solved in float64: there the smallest eigenvalues approach the tolerance and decide the
+// correction.
+__device__ __forceinline__ void store_kc_inverse(const Cst& c, const Ptr& P, int i, const float E[3][3],
+                                                 float lam) {
+    const float tol = c.p.l_eig_tol;
+    float L00, L11, L22, L01, L02, L12;
+    if (c.p.two_d) {
+        float a = E[0][0], b = 0.5f * (E[0][1] + E[1][0]), dd = E[1][1];
+        float disc = sqrtf(fmaxf((a - dd) * (a - dd) + 4.0f * b * b, 0.0f));
+        float e1 = 0.5f * (a + dd + disc), e2 = 0.5f * (a + dd - disc);
+        float n1x = 1.0f, n1y = 0.0f;
+        float scale = fabsf(a) + fabsf(dd) + 1e-30f;
+        if (disc > 1e-9f * scale) {
+            float v1x = b, v1y = e1 - a, v2x = e1 - dd, v2y = b;
+            float l1 = sqrtf(v1x * v1x + v1y * v1y), l2 = sqrtf(v2x * v2x + v2y * v2y);
+            if (l1 >= l2) { n1x = v1x / l1; n1y = v1y / l1; } else { n1x = v2x / l2; n1y = v2y / l2; }
+        }
+        float n2x = -n1y, n2y = n1x;
+        float w1 = spd_weight(e1, tol), w2 = spd_weight(e2, tol);
+        L00 = w1 * (n1x * n1x) + w2 * (n2x * n2x);
+        L01 = w1 * (n1x * n1y) + w2 * (n2x * n2y);
+        L11 = w1 * (n1y * n1y) + w2 * (n2y * n2y);
+        L22 = 1.0f; L02 = 0.0f; L12 = 0.0f;
+    } else if (lam < 0.75f) {
+        double A[3][3], ev[3], Q[3][3];
+        for (int a = 0; a < 3; ++a)
+            for (int b = 0; b < 3; ++b) A[a][b] = 0.5 * ((double)E[a][b] + (double)E[b][a]);
+        sym_eig3(A, ev, Q);
+        double w[3];
+        for (int k = 0; k < 3; ++k) w[k] = spd_weight(ev[k], (double)tol);
+        double M[3][3];
+        for (int a = 0; a < 3; ++a)
+            for (int b = 0; b < 3; ++b) M[a][b] = w[0] * Q[a][0] * Q[b][0] + w[1] * Q[a][1] * Q[b][1] + w[2] * Q[a][2] * Q[b][2];
+        L00 = (float)M[0][0]; L11 = (float)M[1][1]; L22 = (float)M[2][2];
+        L01 = (float)M[0][1]; L02 = (float)M[0][2]; L12 = (float)M[1][2];
+    } else {
+        float A[3][3], ev[3], Q[3][3];
+        for (int a = 0; a < 3; ++a)
+            for (int b = 0; b < 3; ++b) A[a][b] = 0.5f * (E[a][b] + E[b][a]);
+        sym_eig3(A, ev, Q);
+        float w[3];
+        for (int k = 0; k < 3; ++k) w[k] = spd_weight(ev[k], tol);
+        L00 = w[0] * Q[0][0] * Q[0][0] + w[1] * Q[0][1] * Q[0][1] + w[2] * Q[0][2] * Q[0][2];
+        L11 = w[0] * Q[1][0] * Q[1][0] + w[1] * Q[1][1] * Q[1][1] + w[2] * Q[1][2] * Q[1][2];
+        L22 = w[0] * Q[2][0] * Q[2][0] + w[1] * Q[2][1] * Q[2][1] + w[2] * Q[2][2] * Q[2][2];
+        L01 = w[0] * Q[0][0] * Q[1][0] + w[1] * Q[0][1] * Q[1][1] + w[2] * Q[0][2] * Q[1][2];
+        L02 = w[0] * Q[0][0] * Q[2][0] + w[1] * Q[0][1] * Q[2][1] + w[2] * Q[0][2] * Q[2][2];
+        L12 = w[0] * Q[1][0] * Q[2][0] + w[1] * Q[1][1] * Q[2][1] + w[2] * Q[1][2] * Q[2][2];
+    }
+    P.aux[6 * i + 3] = make_float4(L00, L11, L22, L01);
+    float4 b = P.aux[6 * i + 4];
+    b.x = L02; b.y = L12;
+    P.aux[6 * i + 4] = b;
+}
+
+__global__ void __launch_bounds__(kBlock) k_kc_inverse(Cst c, Ptr P) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= c.n) return;
+    const float4* __restrict__ pos = as4c(P.cur.pos);
+    F3 xi = f3(pos[i]);
+    float E[3][3] = {{0, 0, 0}, {0, 0, 0}, {0, 0, 0}};
+    for_each_neighbour(c, P, i, [&](int j, int mir) {
+        float4 pj = __ldg(pos + j);
+        F3 xj = f3(pj);
+        if (mir) xj = mirror3(mir, xj);
+        F3 d = xj - xi, r = xi - xj;
+        float rn;
+        F3 g = wendland_dW2(r, dot3(r, r), rn, c);
+        float Vj = w_of(pj, c);
+        E[0][0] += Vj * (d.x * g.x); E[0][1] += Vj * (d.x * g.y); E[0][2] += Vj * (d.x * g.z);
+        E[1][0] += Vj * (d.y * g.x); E[1][1] += Vj * (d.y * g.y); E[1][2] += Vj * (d.y * g.z);
+        E[2][0] += Vj * (d.z * g.x); E[2][1] += Vj * (d.z * g.y); E[2][2] += Vj * (d.z * g.z);
+    });
+    store_kc_inverse(c, P, i, E, P.lam[i]);
+}
+
+// ------------------------------------------------------------------ pass A
+__global__ void __launch_bounds__(kBlock) k_solid_a(Cst c, Ptr P) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    double wdiff = 0.0;
+    if (i < c.n) {
+        const float4* __restrict__ pos = as4c(P.cur.pos);
+        const float4* __restrict__ vel = as4c(P.cur.vel);
+        const float4* __restrict__ shf = as4c(P.cur.shift);
+        const float* __restrict__ lam = P.lam;
+        float4 pi = pos[i], vi4 = vel[i];
+        F3 xi = f3(pi), vi = f3(vi4);
+        float4 l0 = P.lsym[2 * i], l1 = P.lsym[2 * i + 1];
+        const float L00 = l0.x, L11 = l0.y, L22 = l0.z, L01 = l0.w, L02 = l1.x, L12 = l1.y;
+        const float lam_i = lam[i];
+        const float rho_i = vi4.w / pi.w, inv_rho_i = 1.0f / rho_i;
+        const float dt = P.sc->dt, inv_dt = 1.0f / dt;
+        const bool pst = c.p.pst_enabled;
+        const int ki = eos_of(P, i);
+        const float di = c.p.mat_delta[ki];
+        F3 du_i = {0, 0, 0};
+        if (pst) { float4 s = shf[i]; du_i = {s.x * inv_dt, s.y * inv_dt, s.z * inv_dt}; }
+        const F3 vhat_i = vi + du_i;
+        F3 lg = {0, 0, 0};
+        float r0 = 0.0f, r1 = 0.0f;
+        float G[3][3] = {{0, 0, 0}, {0, 0, 0}, {0, 0, 0}};
+        for_each_neighbour(c, P, i, [&](int j, int mir) {
+            float4 pj = __ldg(pos + j), vj4 = __ldg(vel + j);
+            F3 xj = f3(pj), vj = f3(vj4);
+            if (mir) { xj = mirror3(mir, xj); vj = mirror3(mir, vj); }
+            F3 r = xi - xj;
+            float rn2 = dot3(r, r), rn;
+            F3 g = wendland_dW2(r, rn2, rn, c);
+            float Vj = w_of(pj, c);
+            float ld = __ldg(lam + j) - lam_i;
+            F3 Lg = {L00 * g.x + L01 * g.y + L02 * g.z, L01 * g.x + L11 * g.y + L12 * g.z,
+                     L02 * g.x + L12 * g.y + L22 * g.z};
+            lg += (Vj * ld) * Lg;
+            F3 dv = vj - vi;
+            G[0][0] += Vj * (dv.x * g.x); G[0][1] += Vj * (dv.x * g.y); G[0][2] += Vj * (dv.x * g.z);
+            G[1][0] += Vj * (dv.y * g.x); G[1][1] += Vj * (dv.y * g.y); G[1][2] += Vj * (dv.y * g.z);
+            G[2][0] += Vj * (dv.z * g.x); G[2][1] += Vj * (dv.z * g.y); G[2][2] += Vj * (dv.z * g.z);
+            float rho_j = vj4.w / pj.w;
+            F3 vh_j = vj;
+            if (pst) {
+                float4 s = __ldg(shf + j);
+                F3 du_j = {s.x * inv_dt, s.y * inv_dt, s.z * inv_dt};
+                if (mir) du_j = mirror3(mir, du_j);
+                vh_j += du_j;
+                r0 += Vj * dot3(rho_j * du_j - rho_i * du_i, g) * inv_rho_i;
+            }
+            r0 += Vj * dot3(vhat_i - vh_j, g);
+            int kj = eos_of(P, j);
+            if (kj == ki) {   // pair_delta (SOLID.py:4103-4114) on same-material pairs
+                float dj = c.p.mat_delta[kj];
+                float den = di + dj;
+                float dl = den > 1e-12f ? 2.0f * di * dj / den : 0.0f;
+                if (dl > 0.0f) {
+                    float psig = __fdividef(2.0f * (rho_j - rho_i) * (-dot3(r, g)), rn2 + c.eta2);
+                    float rate = dl * c.h * c.p.c0 * Vj * psig * inv_rho_i;
+                    r0 += rate;
+                    r1 += rate;
+                }
+            }
+        });
+        if (c.p.two_d) lg.z = 0.0f;
+        P.lgrad[i] = make_float4(lg.x, lg.y, lg.z, 0.0f);
+        float dvg = r0;
+        if (c.p.axisymmetric) dvg -= vi.y / r_axi_of(pi.y, c);
+        P.div[i] = make_float4(dvg, r1, 0.0f, 0.0f);
+        wdiff = -(double)pi.w * (double)__ldg(P.cur.disp + 4 * i + 3) * (double)r1;
+        grad_v_finish<NoExtra>(c, P, i, G, pi, vi.y);
+    }
+    block_sum_atomic(wdiff, &P.ac->w_diff_step);
+}
+
+// ------------------------------------------------------------------ grad v alone (damper refresh)
+__global__ void __launch_bounds__(kBlock) k_gradv(Cst c, Ptr P) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= c.n) return;
+    const float4* __restrict__ pos = as4c(P.cur.pos);
+    const float4* __restrict__ vel = as4c(P.cur.vel);
+    float4 pi = pos[i];
+    F3 xi = f3(pi), vi = f3(vel[i]);
+    float G[3][3] = {{0, 0, 0}, {0, 0, 0}, {0, 0, 0}};
+    for_each_neighbour(c, P, i, [&](int j, int mir) {
+        float4 pj = __ldg(pos + j);
+        F3 xj = f3(pj), vj = f3(__ldg(vel + j));
+        if (mir) { xj = mirror3(mir, xj); vj = mirror3(mir, vj); }
+        F3 r = xi - xj;
+        float rn;
+        F3 g = wendland_dW2(r, dot3(r, r), rn, c);
+        float Vj = w_of(pj, c);
+        F3 dv = vj - vi;
+        G[0][0] += Vj * (dv.x * g.x); G[0][1] += Vj * (dv.x * g.y); G[0][2] += Vj * (dv.x * g.z);
+        G[1][0] += Vj * (dv.y * g.x); G[1][1] += Vj * (dv.y * g.y); G[1][2] += Vj * (dv.y * g.z);
+        G[2][0] += Vj * (dv.z * g.x); G[2][1] += Vj * (dv.z * g.y); G[2][2] += Vj * (dv.z * g.z);
+    });
+    grad_v_finish<NoExtra>(c, P, i, G, pi, vi.y);
+}
+
+// ------------------------------------------------------------------ return maps
+// MAT001_linear_plasticity.py:65-81
+__device__ __forceinline__ float j2_return(Sym& s, float G, float sy, float H, float ep) {
+    float d = 0.0f;
+    if (sy > 0.0f) {
+        float vm = vm_sym(s);
+        float sigy = sy + H * ep;
+        if (vm > sigy && (3.0f * G + H) > 0.0f) {
+            d = (vm - sigy) / (3.0f * G + H);
+            float sc = (sigy + H * d) / vm;
+            s = {s.xx * sc, s.yy * sc, s.zz * sc, s.xy * sc, s.xz * sc, s.yz * sc};
+        }
+    }
+    return d;
+}
+__device__ __forceinline__ void jc_residual(float d, float vm, float G, float A, float B, float nn,
+                                            float C, float e0d, float mt, float ep, float dt,
+                                            float& g, float& dg) {
+    float et = ep + d;
+    float ss = A, ds = 0.0f;
+    if (et > 0.0f && B > 0.0f && nn > 0.0f) {
+        ss += B * powf(et, nn);
+        if (et > 1e-12f) ds = nn * B * powf(et, nn - 1.0f);
+    }
+    float rate = 1.0f;
+    if (dt > 0.0f && e0d > 0.0f) rate = (d / dt) / e0d;
+    float mr = 1.0f, dmr = 0.0f;
+    if (rate > 1.0f && C > 0.0f) { mr = 1.0f + C * logf(rate); dmr = C / fmaxf(1e-12f, d); }
+    float sy = ss * mr * mt;
+    float dsy = (ds * mr + ss * dmr) * mt;
+    g = vm - 3.0f * G * d - sy;
+    dg = -3.0f * G - dsy;
+}
+// MAT002_johnson_cook.py:277-354: bracketed Newton-bisection, at most 40 iterations.
+__device__ __forceinline__ float jc_return(Sym& s, const Cst& c, int k, float ep, float temp, float dt,
+                                           bool& capped) {
+    const float G = c.p.mat_G[k], A = c.p.jc_A[k], B = c.p.jc_B[k], nn = c.p.jc_n[k];
+    const float C = c.p.jc_C[k], e0d = c.p.jc_eps0_dot[k], T0 = c.p.jc_T0[k], Tm = c.p.jc_Tm[k];
+    capped = false;
+    if (!(G > 0.0f && A > 0.0f)) return 0.0f;
+    float vm = vm_sym(s);
+    float mt = 1.0f;
+    if (Tm > T0 && temp > T0) {
+        float ts = fminf(1.0f, fmaxf(0.0f, (temp - T0) / (Tm - T0)));
+        mt = fmaxf(0.0f, 1.0f - powf(ts, c.p.jc_m[k]));
+    }
+    float s0 = A;
+    if (ep > 0.0f && B > 0.0f && nn > 0.0f) s0 += B * powf(ep, nn);
+    float sy0 = s0 * mt;
+    if (!(vm > sy0 && sy0 > 0.0f)) return 0.0f;
+    float lo = 0.0f, hi = (vm - sy0) / (3.0f * G);
+    float dref = 0.0f;
+    if (dt > 0.0f && e0d > 0.0f && C > 0.0f) dref = dt * e0d;
+    if (dref > 0.0f && dref < hi) {
+        float g, dg;
+        jc_residual(dref, vm, G, A, B, nn, C, e0d, mt, ep, dt, g, dg);
+        if (g > 0.0f) lo = dref; else hi = dref;
+    }
+    float d = lo > 0.0f ? lo : hi;
+    int it = 0;
+    for (; it < 40; ++it) {
+        float g, dg;
+        jc_residual(d, vm, G, A, B, nn, C, e0d, mt, ep, dt, g, dg);
+        if (g > 0.0f) lo = d; else hi = d;
+        if (fabsf(g) <= 1e-6f * vm || hi - lo <= 1e-6f * hi) break;
+        float dn = d - g / dg;
+        if (!(dn > lo && dn < hi)) dn = lo > 0.0f ? sqrtf(lo * hi) : 0.5f * hi;
+        if (fabsf(dn - d) <= 1e-6f * d) { d = dn; break; }
+        d = dn;
+    }
+    capped = it >= 40;
+    float syf = fmaxf(0.0f, vm - 3.0f * G * d);
+    float sc = syf / vm;
+    s = {s.xx * sc, s.yy * sc, s.zz * sc, s.xy * sc, s.xz * sc, s.yz * sc};
+    return d;
+}
+
+// ------------------------------------------------------------------ pass B
+__global__ void __launch_bounds__(kBlock) k_solid_b(Cst c, Ptr P) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    double pw = 0.0, wl = 0.0;
+    bool capped_any = false;
+    if (i < c.n) {
+        const float4* __restrict__ pos = as4c(P.cur.pos);
+        const float4* __restrict__ vel = as4c(P.cur.vel);
+        const float4* __restrict__ shf = as4c(P.cur.shift);
+        const float* __restrict__ sdev = P.cur.sdev;
+        float4 pi = pos[i], vi4 = vel[i], shi = shf[i];
+        F3 xi = f3(pi);
+        const float rho_i = vi4.w / pi.w, inv_rho_i = 1.0f / rho_i;
+        const float dt = P.sc->dt, inv_dt = 1.0f / dt;
+        const int ki = eos_of(P, i);
+        const Sym s = load_s(sdev, i);
+        const float4 sd1 = __ldg(reinterpret_cast<const float4*>(sdev) + 2 * i + 1);
+        float ep = sd1.z;
+        const float T_old = sd1.w;
+        const float e_i = shi.w;
+        const bool ale = c.p.ale_history != 0;
+        bool plastic_any = false;
+        for (int q = 0; q < c.p.n_materials; ++q) plastic_any = plastic_any || (c.p.plastic_sy0[q] > 0.0f);
+        const F3 du_i = {shi.x * inv_dt, shi.y * inv_dt, shi.z * inv_dt};
+        Sym A = {0, 0, 0, 0, 0, 0};
+        float dep = 0.0f, adv = 0.0f, dif = 0.0f;
+        if (ale) {
+            for_each_neighbour(c, P, i, [&](int j, int mir) {
+                float4 pj = __ldg(pos + j), vj4 = __ldg(vel + j), shj = __ldg(shf + j);
+                F3 xj = f3(pj);
+                F3 du_j = {shj.x * inv_dt, shj.y * inv_dt, shj.z * inv_dt};
+                Sym sj = load_s(sdev, j);
+                if (mir) { xj = mirror3(mir, xj); du_j = mirror3(mir, du_j); sj = mirror_sym(mir, sj); }
+                F3 r = xi - xj;
+                float rn2 = dot3(r, r), rn;
+                F3 g = wendland_dW2(r, rn2, rn, c);
+                float rho_j = vj4.w / pj.w;
+                float wj = w_of(pj, c);
+                float a_j = rho_j * dot3(du_j, g), a_i = rho_i * dot3(du_i, g);
+                float dv = dot3(rho_j * du_j - rho_i * du_i, g);
+                float k = wj * inv_rho_i;
+                A.xx += k * (a_j * sj.xx - a_i * s.xx - s.xx * dv);
+                A.yy += k * (a_j * sj.yy - a_i * s.yy - s.yy * dv);
+                A.zz += k * (a_j * sj.zz - a_i * s.zz - s.zz * dv);
+                A.xy += k * (a_j * sj.xy - a_i * s.xy - s.xy * dv);
+                A.xz += k * (a_j * sj.xz - a_i * s.xz - s.xz * dv);
+                A.yz += k * (a_j * sj.yz - a_i * s.yz - s.yz * dv);
+                if (plastic_any) {
+                    float epj = __ldg(sdev + 8 * j + 6);
+                    dep += k * (a_j * epj - a_i * ep - ep * dv);
+                }
+                if (c.p.transport_e) {
+                    float e_j = shj.w;
+                    adv += wj * rho_j * (e_j - e_i) * dot3(du_j, g) * inv_rho_i;
+                    if (c.p.ale_diffusion > 0.0f && eos_of(P, j) == ki) {
+                        float psig = __fdividef(2.0f * (e_j - e_i) * (-dot3(r, g)), rn2 + c.eta2);
+                        float rb = 0.5f * (rho_i + rho_j);
+                        F3 su = du_i + du_j;
+                        float sp = 0.5f * norm3(su);
+                        dif += c.p.ale_diffusion * 0.5f * c.p.particle_diameter * sp * wj * psig * rb * inv_rho_i;
+                    }
+                }
+            });
+        }
+        // update_stress (SOLID.py:2691-3004): Jaumann rate, trace-free symmetric update
+        float Lg[3][3];
+        load_gradv(P, i, Lg);
+        float ed[3][3], sp[3][3];
+#pragma unroll
+        for (int a = 0; a < 3; ++a)
+#pragma unroll
+            for (int b = 0; b < 3; ++b) { ed[a][b] = 0.5f * (Lg[a][b] + Lg[b][a]); sp[a][b] = 0.5f * (Lg[a][b] - Lg[b][a]); }
+        float tr = ed[0][0] + ed[1][1] + ed[2][2];
+        float S[3][3] = {{s.xx, s.xy, s.xz}, {s.xy, s.yy, s.yz}, {s.xz, s.yz, s.zz}};
+        const float G2 = 2.0f * c.p.mat_G[ki];
+        float Sn[3][3];
+#pragma unroll
+        for (int a = 0; a < 3; ++a)
+#pragma unroll
+            for (int b = 0; b < 3; ++b) {
+                float dev = ed[a][b] - ((a == b) ? tr / 3.0f : 0.0f);
+                float ws = sp[a][0] * S[0][b] + sp[a][1] * S[1][b] + sp[a][2] * S[2][b];
+                float sw = S[a][0] * sp[0][b] + S[a][1] * sp[1][b] + S[a][2] * sp[2][b];
+                Sn[a][b] = G2 * dev + (ws - sw);
+            }
+        Sn[0][0] += A.xx; Sn[1][1] += A.yy; Sn[2][2] += A.zz;
+        Sn[0][1] += A.xy; Sn[1][0] += A.xy; Sn[0][2] += A.xz; Sn[2][0] += A.xz; Sn[1][2] += A.yz; Sn[2][1] += A.yz;
+#pragma unroll
+        for (int a = 0; a < 3; ++a)
+#pragma unroll
+            for (int b = 0; b < 3; ++b) Sn[a][b] = S[a][b] + dt * Sn[a][b];
+        Sym sn = {Sn[0][0], Sn[1][1], Sn[2][2], 0.5f * (Sn[0][1] + Sn[1][0]), 0.5f * (Sn[0][2] + Sn[2][0]),
+                  0.5f * (Sn[1][2] + Sn[2][1])};
+        float tr3 = (sn.xx + sn.yy + sn.zz) / 3.0f;
+        sn.xx -= tr3; sn.yy -= tr3; sn.zz -= tr3;
+        if (c.p.mat_G[ki] <= 0.0f) sn = {0, 0, 0, 0, 0, 0};
+        if (ale && plastic_any) ep = fmaxf(0.0f, ep + dt * dep);
+        float dprod = 0.0f;
+        if (plastic_any) {
+            if (c.p.plastic_kind[ki] == 2) {
+                bool capped;
+                dprod = jc_return(sn, c, ki, ep, T_old, dt, capped);
+                capped_any = capped;
+            } else {
+                dprod = j2_return(sn, c.p.mat_G[ki], c.p.plastic_sy0[ki], c.p.plastic_H[ki], ep);
+            }
+            ep += dprod;
+            if (dprod > 0.0f) pw = (double)(pi.w * vm_sym(sn) * dprod);
+        }
+        // update_internal_energy (SOLID.py:2071-2237): the previous force pass's de_int
+        // plus this step's transport; the leftover with the previous acceleration.
+        float4 ap = P.cur.acc ? reinterpret_cast<const float4*>(P.cur.acc)[i] : make_float4(0, 0, 0, 0);
+        float de = ap.w;
+        if (c.p.transport_e) de += adv + dif;
+        float e_new = e_i + dt * de;
+        {
+            const float gx = c.p.gravity[0], gy = c.p.gravity[1], gz = c.p.gravity[2];
+            F3 f = {ap.x - gx, ap.y - gy, ap.z - gz};
+            wl = (double)(0.5f * vi4.w * dt * dt * (dot3(f, f) - (gx * gx + gy * gy + gz * gz)));
+        }
+        // update_temperature (SOLID.py:2239-2293) from the new energy and the current V
+        float T_new = T_old;
+        const float cv = c.p.mat_cv[ki];
+        if (cv > 0.0f) {
+            double rho = (double)vi4.w / (double)pi.w, rho0 = (double)c.p.mat_rho0[ki];
+            double St = (double)c.p.mat_stiff[ki], gam = (double)c.p.mat_gamma[ki];
+            double xx = rho / rho0, ec;
+            if (fabs(gam - 1.0) < 1.0e-6) ec = (St / rho0) * (log(xx) + 1.0 / xx - 1.0);
+            else ec = (St / rho0) * ((pow(xx, gam - 1.0) - 1.0) / (gam - 1.0) + 1.0 / xx - 1.0);
+            if (!c.p.allow_negative_pressure && rho < rho0) ec = 0.0;
+            double eth = (double)e_new - ec;
+            T_new = c.p.mat_T0[ki] + (float)(eth / (double)cv);
+        }
+        P.aux[6 * i + 0] = make_float4(sn.xx, sn.yy, sn.zz, sn.xy);
+        P.aux[6 * i + 1] = make_float4(sn.xz, sn.yz, ep, e_new);
+        float4 a2 = P.aux[6 * i + 2];
+        a2.x = T_new;
+        P.aux[6 * i + 2] = a2;
+    }
+    if (__syncthreads_or(capped_any) && threadIdx.x == 0) atomicOr(&P.sc->err, SPH_EW_JC_NO_CONVERGE);
+    block_sum_atomic(pw, &P.sc->plastic_work);
+    block_sum_atomic(wl, &P.sc->leftover_work);
+}
+
+// ------------------------------------------------------------------ commit + volume + EOS
+__global__ void __launch_bounds__(kBlock) k_solid_commit(Cst c, Ptr P) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    const float dt = P.sc->dt;
+    if (i == 0) {
+        P.sc->diff_work += (double)dt * P.ac->w_diff_step;
+        P.ac->w_diff_step = 0.0;
+        P.ac->max_c_sq_bits = __float_as_uint(c.p.c_signal * c.p.c_signal);
+        P.ac->max_accel_bits = __float_as_uint(1e-10f);
+    }
+    if (i >= c.n) return;
+    float4 a0 = P.aux[6 * i + 0], a1 = P.aux[6 * i + 1], a2 = P.aux[6 * i + 2];
+    float4* sd = reinterpret_cast<float4*>(P.cur.sdev) + 2 * i;
+    sd[0] = a0;
+    sd[1] = make_float4(a1.x, a1.y, a1.z, a2.x);
+    float4* sh = as4(P.cur.shift) + i;
+    float4 s = *sh;
+    s.w = a1.w;
+    *sh = s;
+    float4* pos = as4(P.cur.pos);
+    float4 pi = pos[i];
+    float V = pi.w;
+    float dVdt = -V * P.div[i].x;
+    if (c.p.compensated_volume) {
+        float* xo = P.cur.x0 + 4 * i + 3;
+        double sv = (double)V + (double)(*xo) + (double)(dt * dVdt);
+        float hi = (float)sv;
+        V = hi;
+        *xo = (float)(sv - (double)hi);
+    } else {
+        V += dt * dVdt;
+    }
+    pi.w = V;
+    pos[i] = pi;
+    float m = P.cur.vel[4 * i + 3];
+    P.cur.disp[4 * i + 3] = solid_pressure(c, eos_of(P, i), m / V);
+    // gravity; de_int restarts for this step's force pass
+    P.acc[i] = make_float4(c.p.gravity[0], c.p.gravity[1], c.p.gravity[2], 0.0f);
+}
+
+// ------------------------------------------------------------------ stress force
+__global__ void __launch_bounds__(kBlock) k_solid_force(Cst c, Ptr P) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    float amag = 0.0f, csq = 0.0f;
+    double hgp = 0.0;
+    if (i < c.n) {
+        const float4* __restrict__ pos = as4c(P.cur.pos);
+        const float4* __restrict__ vel = as4c(P.cur.vel);
+        const float4* __restrict__ dsp = as4c(P.cur.disp);
+        const float4* __restrict__ shf = as4c(P.cur.shift);
+        const float* __restrict__ sdev = P.cur.sdev;
+        float4 pi = pos[i], vi4 = vel[i];
+        F3 xi = f3(pi), vi = f3(vi4);
+        const float p_i = dsp[i].w;
+        const float rho_i = vi4.w / pi.w, inv_rho_i = 1.0f / rho_i;
+        const float w_i = w_of(pi, c), mw_i = mw_of(vi4.w, pi, c), inv_mw = 1.0f / mw_i;
+        const float dt = P.sc->dt, inv_dt = 1.0f / dt;
+        const int ki = eos_of(P, i);
+        const Sym s = load_s(sdev, i);
+        const bool ale = c.p.pst_enabled && c.p.pst_ale_momentum;
+        const bool hg_inloop = c.p.hourglass_alpha > 0.0f && !c.p.hourglass_sts;
+        const bool axc = c.p.axisymmetric && c.p.axi_conservative_x;
+        const float ri = r_axi_of(pi.y, c), inv_ri = 1.0f / ri;
+        float Gi[3][3];
+        if (hg_inloop) load_gradv(P, i, Gi);
+        const float hg_pre = c.p.hourglass_alpha * (c.p.mat_rho0[ki] * inv_rho_i) * (c.p.mat_cp[ki] * c.inv_h)
+                             / (c.p.V0 * (float)c.p.hg_W_dx0);
+        F3 du_i = {0, 0, 0};
+        if (ale) { float4 q = shf[i]; du_i = {q.x * inv_dt, q.y * inv_dt, q.z * inv_dt}; }
+        const float eps_rho = 1e-3f * c.p.density0;
+        float cl = c.p.c_signal * c.p.c_signal;
+        F3 a = {0, 0, 0};
+        float dei = 0.0f, dhg = 0.0f;
+        for_each_neighbour(c, P, i, [&](int j, int mir) {
+            float4 pj = __ldg(pos + j), vj4 = __ldg(vel + j);
+            float p_j = __ldg(&dsp[j].w);
+            F3 xj = f3(pj), vj = f3(vj4);
+            Sym sj = load_s(sdev, j);
+            if (mir) { xj = mirror3(mir, xj); vj = mirror3(mir, vj); sj = mirror_sym(mir, sj); }
+            F3 r = xi - xj;
+            float rn2 = dot3(r, r), rn;
+            F3 g = wendland_dW2(r, rn2, rn, c);
+            float w_j = w_of(pj, c);
+            float pp = p_i + p_j;
+            Sym ss = {s.xx + sj.xx - pp, s.yy + sj.yy - pp, s.zz + sj.zz - pp, s.xy + sj.xy, s.xz + sj.xz, s.yz + sj.yz};
+            float ww = w_i * w_j;
+            F3 f = {ww * (ss.xx * g.x + ss.xy * g.y + ss.xz * g.z),
+                    ww * (ss.xy * g.x + ss.yy * g.y + ss.yz * g.z),
+                    ww * (ss.xz * g.x + ss.yz * g.y + ss.zz * g.z)};
+            const float rj = r_axi_of(pj.y, c);
+            const float ratio = axc ? 0.5f * (ri + rj) * inv_ri : 1.0f;
+            f.x *= ratio;
+            a += inv_mw * f;
+            F3 vij = vi - vj;
+            dei += -0.5f * dot3(f, vij) * inv_mw;
+            float vxy = dot3(vij, r);
+            F3 am = __fdividef(c.visc_coef * w_j * vxy, rn * rn + c.eta2) * g;
+            a += am;
+            if (c.p.viscosity > 0.0f) dei += -0.5f * dot3(am, vij);
+            if (hg_inloop && rn > 1e-9f) {
+                float inv_rn = 1.0f / rn;
+                F3 rh = {-r.x * inv_rn, -r.y * inv_rn, -r.z * inv_rn};
+                float Gj[3][3];
+                load_gradv(P, j, Gj);
+                if (mir) mirror_mat3(mir, Gj);
+                F3 mr = -r;
+                F3 dvh = {(vj.x - vi.x) - 0.5f * ((Gi[0][0] + Gj[0][0]) * mr.x + (Gi[0][1] + Gj[0][1]) * mr.y + (Gi[0][2] + Gj[0][2]) * mr.z),
+                          (vj.y - vi.y) - 0.5f * ((Gi[1][0] + Gj[1][0]) * mr.x + (Gi[1][1] + Gj[1][1]) * mr.y + (Gi[1][2] + Gj[1][2]) * mr.z),
+                          (vj.z - vi.z) - 0.5f * ((Gi[2][0] + Gj[2][0]) * mr.x + (Gi[2][1] + Gj[2][1]) * mr.y + (Gi[2][2] + Gj[2][2]) * mr.z)};
+                float hg = dot3(dvh, rh);
+                float damp = hg_pre * w_j * wendland_W(rn, c) * hg;
+                F3 ah = damp * rh;
+                ah.x *= ratio;
+                a += ah;
+                dhg += -0.5f * dot3(ah, vij);
+            }
+            float rho_j = vj4.w / pj.w;
+            if (ale) {
+                float4 q = __ldg(shf + j);
+                F3 du_j = {q.x * inv_dt, q.y * inv_dt, q.z * inv_dt};
+                if (mir) du_j = mirror3(mir, du_j);
+                F3 t1 = (rho_j * dot3(du_j, g)) * vj - (rho_i * dot3(du_i, g)) * vi;
+                float b = dot3(rho_j * du_j - rho_i * du_i, g);
+                F3 t = t1 - b * vi;
+                a += (w_j * inv_rho_i) * t;
+            }
+            if (c.p.dt_pair_mode != 0 && (c.p.dt_pair_mode != 2 || eos_of(P, j) == ki)) {
+                float drho = fabsf(rho_i - rho_j);
+                if (drho > eps_rho) {
+                    float cij = fabsf(p_i - p_j) / drho;
+                    if (cij > cl) cl = cij;
+                }
+            }
+        });
+        if (c.p.axisymmetric) a.y += (s.yy - s.zz) / (rho_i * ri);
+        float4 a0 = P.acc[i];
+        F3 an = {a0.x + a.x, a0.y + a.y, a0.z + a.z};
+        P.acc[i] = make_float4(an.x, an.y, an.z, dei);
+        bool ongrid = !(isnan(pi.x) || isnan(pi.y) || isnan(pi.z));
+        if (ongrid) amag = norm3(an);
+        if (c.p.dt_pair_mode != 0) csq = cl;
+        hgp = (double)(mw_i * dhg);
+    }
+    block_max_atomic(amag, &P.ac->max_accel_bits);
+    block_max_atomic(csq, &P.ac->max_c_sq_bits);
+    if (c.p.hourglass_alpha > 0.0f && !c.p.hourglass_sts) block_sum_atomic(hgp, &P.ac->hg_power);
+}
+
+// ------------------------------------------------------------------ dt, damper cap / stage count
+__global__ void k_solid_dt(Cst c, Ptr P) {
+    if (threadIdx.x != 0 || blockIdx.x != 0) return;
+    float mcs = __uint_as_float(P.ac->max_c_sq_bits);
+    float ma = __uint_as_float(P.ac->max_accel_bits);
+    P.sc->max_c_sq = mcs;
+    P.sc->max_accel = ma;
+    float dt = fminf(c.cfl_h / sqrtf(mcs), c.p.CFL * sqrtf(c.h / ma));
+    const bool hg = c.p.hourglass_alpha > 0.0f;
+    int s = 0;
+    if (!c.p.hourglass_sts) {
+        if (hg) dt = fminf(dt, (float)(1.6 / (double)c.p.hg_rate));
+        P.sc->hg_work += (double)dt * P.ac->hg_power;
+        P.ac->hg_power = 0.0;
+    } else if (hg) {
+        s = 1;
+        if (c.p.hg_rate > 0.0f) {
+            double want = (double)c.p.hg_rate * (double)dt;
+            s = c.p.hg_sts_fixed > 0 ? c.p.hg_sts_fixed : max(1, (int)ceil(want / 1.6));
+            if (s > kStsMaxStages) { s = kStsMaxStages; atomicOr(&P.sc->err, SPH_EW_STS_CAP); }
+            double cap = s * 1.6 / (double)c.p.hg_rate;
+            if ((double)dt > cap) dt = (float)cap;
+        }
+    }
+    P.sc->dt = dt;
+    P.sc->sts_stages = s;
+    for (int k = 0; k < 8; ++k)
+        for (int d = 0; d < 3; ++d) { P.sc->constraint_force[k][d] = 0.0; P.sc->constraint_disp[k][d] = 0.0; }
+}
+
+// ------------------------------------------------------------------ sub-cycled damper
+// y lives in aux slot 0 (even stages read it) and slot 2 (odd stages read it); v_sync in
+// slot 4.zw + 5.x.  The history in slots 0..2 has been committed by then.
+__device__ __forceinline__ F3 y_load(const Ptr& P, int i, int buf) {
+    return f3(P.aux[6 * i + (buf ? 2 : 0)]);
+}
+__device__ __forceinline__ void y_store(const Ptr& P, int i, int buf, F3 y) {
+    P.aux[6 * i + (buf ? 2 : 0)] = make_float4(y.x, y.y, y.z, 0.0f);
+}
+
+__global__ void __launch_bounds__(kBlock) k_half_kick(Cst c, Ptr P) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    double ke = 0.0;
+    if (i < c.n) {
+        const float h = 0.5f * P.sc->dt;
+        float4* vel = as4(P.cur.vel);
+        float4 v = vel[i];
+        float4 a = P.acc[i];
+        v.x += h * a.x; v.y += h * a.y; v.z += h * a.z;
+        vel[i] = v;
+        float4 b4 = P.aux[6 * i + 4];
+        b4.z = v.x; b4.w = v.y;
+        P.aux[6 * i + 4] = b4;
+        float4 b5 = P.aux[6 * i + 5];
+        b5.x = v.z;
+        P.aux[6 * i + 5] = b5;
+        y_store(P, i, 0, f3(v));
+        ke = (double)(0.5f * v.w * (v.x * v.x + v.y * v.y + v.z * v.z));
+    }
+    block_sum_atomic(ke, &P.sc->hg_work);   // + KE before the damper
+}
+
+__global__ void __launch_bounds__(kBlock) k_hg_stage(Cst c, Ptr P, int stage) {
+    const int s = P.sc->sts_stages;
+    if (stage >= s) return;
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= c.n) return;
+    const int rb = stage & 1, wb = rb ^ 1;
+    const float4* __restrict__ pos = as4c(P.cur.pos);
+    const float4* __restrict__ vel = as4c(P.cur.vel);
+    float4 pi = pos[i];
+    F3 xi = f3(pi);
+    F3 yi = y_load(P, i, rb);
+    const float rho_i = __ldg(&vel[i].w) / pi.w;
+    const int ki = eos_of(P, i);
+    float Gi[3][3];
+    load_gradv(P, i, Gi);
+    const bool axc = c.p.axisymmetric && c.p.axi_conservative_x;
+    const float ri = r_axi_of(pi.y, c), inv_ri = 1.0f / ri;
+    const float hg_pre = c.p.hourglass_alpha * (c.p.mat_rho0[ki] / rho_i) * (c.p.mat_cp[ki] * c.inv_h)
+                         / (c.p.V0 * (float)c.p.hg_W_dx0);
+    F3 acc = {0, 0, 0};
+    for_each_neighbour(c, P, i, [&](int j, int mir) {
+        float4 pj = __ldg(pos + j);
+        F3 xj = f3(pj);
+        F3 yj = y_load(P, j, rb);
+        float Gj[3][3];
+        load_gradv(P, j, Gj);
+        if (mir) { xj = mirror3(mir, xj); yj = mirror3(mir, yj); mirror_mat3(mir, Gj); }
+        F3 r = xi - xj;
+        float rn2 = dot3(r, r);
+        float rn = rn2 > 0.0f ? rn2 * rsqrtf(rn2) : 0.0f;
+        if (!(rn > 1e-9f)) return;
+        float inv_rn = 1.0f / rn;
+        F3 rh = {-r.x * inv_rn, -r.y * inv_rn, -r.z * inv_rn};
+        F3 mr = -r;
+        F3 dvh = {(yj.x - yi.x) - 0.5f * ((Gi[0][0] + Gj[0][0]) * mr.x + (Gi[0][1] + Gj[0][1]) * mr.y + (Gi[0][2] + Gj[0][2]) * mr.z),
+                  (yj.y - yi.y) - 0.5f * ((Gi[1][0] + Gj[1][0]) * mr.x + (Gi[1][1] + Gj[1][1]) * mr.y + (Gi[1][2] + Gj[1][2]) * mr.z),
+                  (yj.z - yi.z) - 0.5f * ((Gi[2][0] + Gj[2][0]) * mr.x + (Gi[2][1] + Gj[2][1]) * mr.y + (Gi[2][2] + Gj[2][2]) * mr.z)};
+        float hg = dot3(dvh, rh);
+        float damp = hg_pre * w_of(pj, c) * wendland_W(rn, c) * hg;
+        F3 ah = damp * rh;
+        if (axc) ah.x *= 0.5f * (ri + r_axi_of(pj.y, c)) * inv_ri;
+        acc += ah;
+    });
+    const float sub = (float)((double)P.sc->dt / (double)s);
+    y_store(P, i, wb, yi + sub * acc);
+}
+
+__global__ void __launch_bounds__(kBlock) k_sts_finish(Cst c, Ptr P) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    double ke = 0.0, wl = 0.0;
+    if (i < c.n) {
+        const int s = P.sc->sts_stages;
+        const float dt = P.sc->dt, h = 0.5f * dt;
+        float4* vel = as4(P.cur.vel);
+        float4 v = vel[i];
+        F3 y = y_load(P, i, s & 1);
+        v.x = y.x; v.y = y.y; v.z = y.z;
+        ke = -(double)(0.5f * v.w * (v.x * v.x + v.y * v.y + v.z * v.z));   // - KE after
+        float4 b4 = P.aux[6 * i + 4], b5 = P.aux[6 * i + 5];
+        F3 dvv = {v.x - b4.z, v.y - b4.w, v.z - b5.x};
+        float4 a = P.acc[i];
+        F3 ha = {h * a.x, h * a.y, h * a.z};
+        wl = (double)(v.w * dot3(dvv, ha));
+        v.x += ha.x; v.y += ha.y; v.z += ha.z;
+        vel[i] = v;
+        float4* pos = as4(P.cur.pos);
+        float4 p = pos[i];
+        if (c.p.displacement_positions) {
+            float4* dsp = as4(P.cur.disp);
+            float4 u = dsp[i];
+            float4 x0 = as4(P.cur.x0)[i];
+            u.x += dt * v.x; u.y += dt * v.y; u.z += dt * v.z;
+            dsp[i] = u;
+            p.x = x0.x + u.x; p.y = x0.y + u.y; p.z = x0.z + u.z;
+        } else {
+            p.x += dt * v.x; p.y += dt * v.y; p.z += dt * v.z;
+        }
+        pos[i] = p;
+    }
+    block_sum_atomic(ke, &P.sc->hg_work);
+    block_sum_atomic(wl, &P.sc->leftover_work);
+}
+
+__global__ void __launch_bounds__(kBlock) k_solid_advect(Cst c, Ptr P) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= c.n) return;
+    const float dt = P.sc->dt;
+    float4* vel = as4(P.cur.vel);
+    float4 v = vel[i];
+    float4 a = P.acc[i];
+    v.x += dt * a.x; v.y += dt * a.y; v.z += dt * a.z;
+    vel[i] = v;
+    float4* pos = as4(P.cur.pos);
+    float4 p = pos[i];
+    if (c.p.displacement_positions) {
+        float4* dsp = as4(P.cur.disp);
+        float4 u = dsp[i];
+        float4 x0 = as4(P.cur.x0)[i];
+        u.x += dt * v.x; u.y += dt * v.y; u.z += dt * v.z;
+        dsp[i] = u;
+        p.x = x0.x + u.x; p.y = x0.y + u.y; p.z = x0.z + u.z;
+    } else {
+        p.x += dt * v.x; p.y += dt * v.y; p.z += dt * v.z;
+    }
+    pos[i] = p;
+}
+
+// ------------------------------------------------------------------ grips
+__global__ void __launch_bounds__(kBlock) k_constraints(Cst c, Ptr P) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= c.n) return;
+    int2 bc = reinterpret_cast<const int2*>(P.cur.bc)[i];
+    if (bc.x == 0) return;
+    const float s = P.sc->load_s, sd = P.sc->load_sdot;
+    const float scale = c.p.axisymmetric ? (float)(2.0 * M_PI) : 1.0f;
+    float4 bd = reinterpret_cast<const float4*>(P.cur.bcdisp)[i];
+    float4* pos = as4(P.cur.pos);
+    float4* vel = as4(P.cur.vel);
+    float4* dsp = as4(P.cur.disp);
+    float4 p = pos[i], v = vel[i], u = dsp[i], a = P.acc[i];
+    const float4 x0 = as4(P.cur.x0)[i];
+    const float m = v.w;
+    float* pc[3] = {&p.x, &p.y, &p.z};
+    float* vc[3] = {&v.x, &v.y, &v.z};
+    float* uc[3] = {&u.x, &u.y, &u.z};
+    float* ac[3] = {&a.x, &a.y, &a.z};
+    const float bdc[3] = {bd.x, bd.y, bd.z};
+    const float x0c[3] = {x0.x, x0.y, x0.z};
+#pragma unroll
+    for (int d = 0; d < 3; ++d) {
+        if (!(bc.x & (1 << d))) continue;
+        if (c.p.num_constraints > 0 && bc.y >= 0 && bc.y < 8) {
+            atomicAdd(&P.sc->constraint_force[bc.y][d], (double)(scale * m * *ac[d]));
+            P.sc->constraint_disp[bc.y][d] = (double)(bdc[d] * s);
+        }
+        *uc[d] = bdc[d] * s;
+        *pc[d] = x0c[d] + *uc[d];
+        *vc[d] = bdc[d] * sd;
+        *ac[d] = 0.0f;
+    }
+    pos[i] = p; vel[i] = v; dsp[i] = u; P.acc[i] = a;
+}
+
+__global__ void k_solid_time(Cst c, Ptr P) {
+    if (threadIdx.x == 0 && blockIdx.x == 0) P.sc->sim_time += (double)P.sc->dt;
+}
+
+// ------------------------------------------------------------------ host sequencing
+inline int grid_of(int n) { return n > 0 ? (n + kBlock - 1) / kBlock : 1; }
+
+// Launched before the rebuild of a solid step.
+inline int solid_pre_step(const Cst& c, const Ptr& P, SolidScratch&, cudaStream_t st) {
+    k_solid_load<<<1, 32, 0, st>>>(c, P);
+    return SPH_OK;
+}
+
+template <class Mark>
+inline int solid_substep_launch(const Cst& c, const Ptr& P, int n, cudaStream_t st, Mark&& mark,
+                                int first_stage = 0, int last_stage = 99) {
+    const int nb = grid_of(n);
+    auto in = [&](int s) { return s >= first_stage && s <= last_stage; };
+    if (in(SPH_STAGE_LAM)) {
+        k_lam<<<nb, kBlock, 0, st>>>(c, P); mark("k_lam");
+        if (c.p.kernel_correction) { k_kc_inverse<<<nb, kBlock, 0, st>>>(c, P); mark("k_kc_inverse"); }
+        k_solid_a<<<nb, kBlock, 0, st>>>(c, P); mark("k_solid_a");
+        k_solid_b<<<nb, kBlock, 0, st>>>(c, P); mark("k_solid_b");
+    }
+    if (in(SPH_STAGE_CONTINUITY)) { k_solid_commit<<<nb, kBlock, 0, st>>>(c, P); mark("k_solid_commit"); }
+    if (in(SPH_STAGE_FORCES)) { k_solid_force<<<nb, kBlock, 0, st>>>(c, P); mark("k_solid_force"); }
+    if (in(SPH_STAGE_DT)) { k_solid_dt<<<1, 32, 0, st>>>(c, P); mark("k_solid_dt"); }
+    if (in(SPH_STAGE_ADVECT)) {
+        if (c.p.hourglass_sts && c.p.hourglass_alpha > 0.0f) {
+            k_half_kick<<<nb, kBlock, 0, st>>>(c, P); mark("k_half_kick");
+            if (c.p.hg_sts_refresh) { k_gradv<<<nb, kBlock, 0, st>>>(c, P); mark("k_gradv"); }
+            for (int s = 0; s < kStsMaxStages; ++s) { k_hg_stage<<<nb, kBlock, 0, st>>>(c, P, s); mark("k_hg_stage"); }
+            k_sts_finish<<<nb, kBlock, 0, st>>>(c, P); mark("k_sts_finish");
+        } else {
+            k_solid_advect<<<nb, kBlock, 0, st>>>(c, P); mark("k_solid_advect");
+        }
+        k_constraints<<<nb, kBlock, 0, st>>>(c, P); mark("k_constraints");
+    }
+    if (in(SPH_STAGE_PST) && c.p.pst_enabled) {
+        k_pst_search<<<nb, kBlock, 0, st>>>(c, P); mark("k_pst_search");
+        k_pst<<<nb, kBlock, 0, st>>>(c, P); mark("k_pst");
+        k_finish<<<nb, kBlock, 0, st>>>(c, P, last_stage >= SPH_STAGE_BOUNDARY ? 3 : 1); mark("k_finish");
+    } else if (in(SPH_STAGE_BOUNDARY)) {
+        k_finish<<<nb, kBlock, 0, st>>>(c, P, 2); mark("k_finish");
+    }
+    if (in(SPH_STAGE_BOUNDARY)) { k_solid_time<<<1, 32, 0, st>>>(c, P); mark("k_solid_time"); }
+    return SPH_OK;
+}
+
 inline void solid_reduce_extra(const Cst&, const Ptr&, int, cudaStream_t) {}
 
 }  // namespace sph

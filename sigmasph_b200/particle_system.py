@@ -253,12 +253,15 @@ class ParticleSystem:
                 s["sdev"] = z(n, 8)
                 s["bc"] = z(n, 2, dtype=i32)
                 s["bcdisp"] = z(n, 4)
+                s["acc"] = z(n, 4)     # acceleration + de_int, carried across the sort
             self._sets.append(s)
         self._derived = {"acc": z(n, 4), "lam": z(n, 1), "lsym": z(n, 8), "lgrad": z(n, 4),
                          "div": z(n, 4)}
         if self.is_solid:
             self._derived["gradv"] = z(n, 12)
-            self._derived["aux"] = z(n, 16)
+            self._derived["aux"] = z(n, 24)
+            # the solid's acceleration is persistent: it lives in the buffer sets
+            del self._derived["acc"]
         s0 = self._sets[0]
         pos = np.zeros((n, 4), dtype=np.float32)
         pos[:, :3] = x
@@ -275,6 +278,11 @@ class ParticleSystem:
         if self.is_solid:
             bcd = np.zeros((n, 4), dtype=np.float32)
             bcd[:, 3] = self._eos_id.astype(np.float32)
+            # reference temperature per material (materials.py:429-435); e_int starts at 0
+            mats = sorted(config.get_materials().values(), key=lambda mm: mm.index)
+            t0 = np.array([mm.jc["T0"] if mm.jc is not None else 293.0 for mm in mats],
+                          dtype=np.float32)
+            s0["sdev"][:, 7].copy_(torch.from_numpy(t0[self._eos_id]))
             s0["bcdisp"].copy_(torch.from_numpy(bcd))
         self._parity_fn = lambda: 0
         self._on_write = None

@@ -125,7 +125,7 @@ class _SolverBase:
         b = abi.SphBuffers()
         for k, s in enumerate(ps.buffer_sets()):
             fs = b.set[k]
-            for key in ("pos", "vel", "x0", "disp", "shift", "pid", "sdev", "bc", "bcdisp"):
+            for key in ("pos", "vel", "x0", "disp", "shift", "pid", "sdev", "bc", "bcdisp", "acc"):
                 t = s.get(key)
                 setattr(fs, key, t.data_ptr() if t is not None else None)
         d = ps.derived()

@@ -1,0 +1,116 @@
+"""The solid half of the CPU oracle against the reference's known answers (no GPU):
+the J2 and Johnson-Cook return maps against the reference's own float64 mirrors
+(tests/golden/make_golden.py), the hourglass lattice constant, and conservation
+properties of the oracle's solid step."""
+import json
+import os
+
+import numpy as np
+import pytest
+
+from sigmasph_b200 import abi
+from sigmasph_b200.config import SimConfig
+from sigmasph_b200.particle_system import ParticleSystem
+from sigmasph_b200.scenes import scene_path
+from sigmasph_b200.solid_params import reference_kernel_sum
+from sigmasph_b200.solver import build_params
+from oracle.oracle import Oracle, state_from_sets, j2_return, jc_return
+
+GOLD = json.load(open(os.path.join(os.path.dirname(__file__), "golden", "reference_host.json")))
+
+
+def vm(s):
+    s = np.asarray(s)
+    return float(np.sqrt(1.5 * np.sum(s * s)))
+
+
+@pytest.mark.parametrize("k", range(len(GOLD["plasticity"]["j2"])))
+def test_j2_return_matches_reference(k):
+    """MAT001_linear_plasticity.py:65-81 (j2_radial_return_py)."""
+    e = GOLD["plasticity"]["j2"][k]
+    s_new, d = j2_return(e["s"], e["G"], e["sy0"], e["H"], e["eps_p"])
+    s_ref, d_ref = np.array(e["out"][0]), e["out"][1]
+    assert d == pytest.approx(d_ref, rel=1e-12, abs=1e-15)
+    assert np.abs(s_new - s_ref).max() <= 1e-12 * np.abs(s_ref).max()
+    if d > 0:   # consistency: the returned state sits on the hardened yield surface
+        assert vm(s_new) == pytest.approx(e["sy0"] + e["H"] * (e["eps_p"] + d), rel=1e-12)
+
+
+@pytest.mark.parametrize("k", range(len(GOLD["plasticity"]["jc"])))
+def test_jc_return_matches_reference(k):
+    """MAT002_johnson_cook.py:172-250 (jc_radial_return_py): bracketed Newton-bisection,
+    40 iterations at most, T* frozen at the step start."""
+    e = GOLD["plasticity"]["jc"][k]
+    (s, G, rho0, A, B, n, C, e0d, T0, Tm, m, Cp, chi, ep, temp, dt) = e["args"]
+    s_new, d, it = jc_return(s, G, A, B, n, C, e0d, T0, Tm, m, ep, temp, dt)
+    s_ref, d_ref = np.array(e["out"][0]), e["out"][1]
+    assert it < 40
+    assert d == pytest.approx(d_ref, rel=1e-12, abs=1e-15)
+    assert np.abs(s_new - s_ref).max() <= 1e-12 * max(np.abs(s_ref).max(), 1e-30)
+
+
+def test_jc_return_is_elastic_below_yield():
+    s = np.diag([0.1, -0.05, -0.05])
+    s_new, d, _ = jc_return(s, 76.92, 0.31, 1.0, 0.65, 0.02, 1.0, 293.0, 1720.0, 1.0, 0.0, 293.0, 1e-5)
+    assert d == 0.0 and np.array_equal(s_new, s)
+
+
+@pytest.mark.parametrize("two_d,expect", [(True, 6.639), (False, 15.413)])
+def test_hourglass_lattice_sum(two_d, expect):
+    """SOLID.py:1632-1657: S = sum_j W(|r_j|) / W(dx0) at support 3 dx0 (6.6 in plane
+    strain, SOLID.py:763); scale-free in dx0."""
+    assert reference_kernel_sum(0.1, 0.3, two_d) == pytest.approx(expect, abs=1e-3)
+    assert reference_kernel_sum(2.0, 6.0, two_d) == pytest.approx(expect, abs=1e-3)
+
+
+def test_dogbone_params():
+    ps = ParticleSystem(SimConfig(scene_path("tensile_axi_dogbone_dx0.1.json")), device="cpu")
+    p = build_params(ps)
+    assert p.is_solid and p.axisymmetric and p.hourglass_sts
+    assert p.hg_S == pytest.approx(6.639, abs=2e-3)
+    assert p.num_constraints == 2
+    # the signal speed is the dilatational speed of stainless steel (E 193 GPa, nu 0.3)
+    E, nu, rho = 193.0, 0.3, 7.9e-6
+    K, G = E / (3 * (1 - 2 * nu)), E / (2 * (1 + nu))
+    assert p.c_signal == pytest.approx(np.sqrt((K + 4 * G / 3) / rho), rel=1e-6)
+
+
+def free_block(dx=0.5):
+    """A free 3D elastic-plastic block (no grips, no gravity) with a random velocity
+    field: the pair forces are antisymmetric, so linear momentum is conserved."""
+    return {
+        "Domain": {"particleRadius": 0.5 * dx, "supportRadiusFactor": 6.0, "boundary": "open"},
+        "Time": {"CFL": 0.3},
+        "Solver": {"type": "hypoElastic", "viscosity": 0.02, "allowNegativePressure": True},
+        "Materials": [{"name": "steel", "density0": 7.9e-6, "eos": {"type": "linear"},
+                       "strength": {"type": "hypoElastic", "youngsModulus": 200.0,
+                                    "poissonRatio": 0.3,
+                                    "plasticity": {"model": "linear", "yieldStress": 0.03,
+                                                   "hardeningModulus": 1.0}}}],
+        "Load": {"gravitation": [0.0, 0.0, 0.0]},
+        "Diffusion": {"delta": 0.1},
+        "Shifting": {"enabled": False},
+        "Hourglass": {"alpha": 4.0},
+        "SolidBlocks": [{"objectId": 0, "start": [0.0, 0.0, 0.0], "end": [6.0, 6.0, 6.0],
+                         "material": "steel", "density": 7.9e-6}],
+    }
+
+
+def test_free_block_conserves_momentum():
+    ps = ParticleSystem(SimConfig(free_block()), device="cpu")
+    rng = np.random.default_rng(3)
+    n = ps.particle_max_num
+    ps.v.from_numpy(rng.uniform(-2.0, 2.0, (n, 3)).astype(np.float32))
+    p = build_params(ps)
+    o = Oracle(p, n, fp64=True)
+    st = state_from_sets(ps.state_numpy())
+    o.set_state(st, p.CFL * p.support_radius / p.c_signal)
+    m = st["m"].astype(np.float64)
+    P0 = (m[:, None] * st["v"].astype(np.float64)).sum(0)
+    o.stage(abi.STAGE_SORT)
+    o.step(20)
+    r = o.get_state()
+    P1 = (r["m"][:, None] * r["v"]).sum(0)
+    gross = (r["m"][:, None] * np.abs(r["v"])).sum(0)
+    assert np.abs(P1 - P0).max() <= 1e-10 * gross.max()
+    assert r["eps_p"].max() > 0.0       # the random field yields somewhere
