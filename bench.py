@@ -9,6 +9,10 @@ with the neighbour lists) is far larger than the 126 MB L2, so no flush is neede
 between steps.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference]
+                    [--workload dambreak3d|tensile_bar3d|tensile_bar3d_jc] [--dx DX]
+
+`--workload tensile_bar3d` times the hypoelastic solid step instead: the 3D round-bar
+tensile test (sigmasph_b200.scenes.tensile_bar3d), about 2.3M particles at dx = 0.113 mm.
 
 Under torchrun (N > 1) every rank runs an independent replica of the workload (the
 path does not shard at one-GPU scale: replicas only); the time is the max over ranks.
@@ -31,13 +35,16 @@ if ROOT not in sys.path:
     sys.path.insert(0, ROOT)
 
 METRIC = "particle-steps/s on 1 B200 (3D delta+-SPH dam break)"
+METRIC_BAR = "particle-steps/s on 1 B200 (3D round-bar tensile test)"
 UNIT = "particle-steps/s"
 DX_1M = 0.004762
+DX_BAR = 0.113
 
 # Algorithmic (compulsory, own-particle) bytes per particle of each kernel: the fields it
 # must read and write once in float32; neighbour data is assumed served on chip.
 ALGO_BYTES = {
     "k_nbr_build": 16 + 16 + 4,        # pos + cell read, count write (list entries: design)
+    "k_pst_search": 16 + 4,            # live pos read, count write (list entries: design)
     "k_lam": 16 + 4 + 32,              # pos read; lam + L (8 floats) write
     "k_lamgrad_cont": 16 + 16 + 16 + 32 + 4 + 16 + 16,  # pos vel shift L lam read; lgrad, div write
     "k_eos": 16 + 4 + 4 + 16 + 4 + 16,  # pos, div, V_lo, vel.m read; pos.V, V_lo, p, acc write
@@ -46,7 +53,20 @@ ALGO_BYTES = {
     "k_pst": 16 + 16 + 4 + 16 + 16,   # pos vel lam lgrad read; shift write
     "k_finish": 16 * 6 + 16 * 4,
     "k_gather": 2 * (16 * 5 + 4) + 16 + 4,
+    # solid passes: the survey's compulsory own-particle figures of the passes they fuse
+    "k_solid_a": 56 + 64,              # grad lambda + grad v
+    "k_solid_b": 144,                  # Jaumann + ALE(s, eps_p, e) + return map + e update
+    "k_solid_force": 132,              # EOS + stress force + in-loop hourglass + dt pairs
+    "k_solid_commit": 64,              # continuity (V) + commit of the returned state
 }
+# Compulsory own-particle bytes of a whole delta+-SPH particle-step (sort/reorder 168,
+# lambda/L 44, grad lambda 56, continuity 64, EOS + force + dt 60, advect 84, PST 60,
+# displace 60), neighbour gathers assumed served on chip.
+STEP_ALGO_BYTES = 600
+# The hypoelastic solid step without the sub-cycled damper: sort 340, lambda/L 44, grad
+# lambda 56, grad v 64, Jaumann + ALE + return + energy 144, continuity 64, EOS + force +
+# in-loop hourglass + dt 132, advect + grips 88, PST 64, displace 60.
+STEP_ALGO_BYTES_SOLID = 1060
 
 
 def load_peaks():
@@ -58,16 +78,22 @@ def load_peaks():
     return 6650.0, "fallback"
 
 
-def read_traffic(kernel):
-    """dram bytes per launch at the bench size from the committed ncu summary, if any."""
-    p = os.path.join(ROOT, "profiles", f"{kernel}_dambreak3d.md")
+def read_traffic(kernel, tag, n):
+    """DRAM bytes per launch of `kernel` from the committed ncu summary of the workload
+    (profiles/<tag>.md, the "DRAM B/particle" column of the --set full table), scaled to
+    n particles: the traffic of these kernels grows in proportion to the particles."""
+    p = os.path.join(ROOT, "profiles", f"{tag}.md")
     if not os.path.exists(p):
         return None
+    col = None
     with open(p) as f:
         for line in f:
-            if line.strip().startswith("dram_bytes_per_launch_at_bench_size:"):
+            cells = [c.strip() for c in line.strip().strip("|").split("|")]
+            if "DRAM B/particle" in cells:
+                col = cells.index("DRAM B/particle")
+            elif col is not None and cells and cells[0] == kernel and len(cells) > col:
                 try:
-                    return float(line.split(":", 1)[1].split()[0])
+                    return float(cells[col]) * n
                 except ValueError:
                     return None
     return None
@@ -137,6 +163,22 @@ def dist_setup():
     return ws, rank, local
 
 
+def workload(args):
+    """(scene, config description, profile tag) of the selected workload."""
+    from sigmasph_b200.scenes import dambreak3d, tensile_bar3d
+    if args.workload == "dambreak3d":
+        dx = args.dx or DX_1M
+        return (dambreak3d(dx=dx),
+                {"workload": "3D dam break, delta+-SPH, reflecting walls", "dx_m": dx,
+                 "support_dx": 2.6}, "dambreak3d")
+    dx = args.dx or DX_BAR
+    plast = "jc" if args.workload == "tensile_bar3d_jc" else "j2"
+    return (tensile_bar3d(dx=dx, plasticity=plast),
+            {"workload": "3D round-bar tensile test, hypoelastic %s, ALE + hourglass, grips"
+                         % ("Johnson-Cook" if plast == "jc" else "J2 linear hardening"),
+             "dx_mm": dx, "support_dx": 3.0}, "tensile_bar3d")
+
+
 def cpu_baseline(ps, steps_target_s=15.0, max_steps=6, threads=None):
     """The CPU restatement (float32, all host threads) on the same workload."""
     from oracle.oracle import Oracle, state_from_sets
@@ -167,35 +209,37 @@ def run_reference(args):
         return 0
     from sigmasph_b200.config import SimConfig
     from sigmasph_b200.particle_system import ParticleSystem
-    from sigmasph_b200.scenes import dambreak3d
     from oracle.oracle import Oracle, state_from_sets
     from sigmasph_b200.solver import build_params
-    cfg = SimConfig(dambreak3d(dx=args.dx))
-    ps = ParticleSystem(cfg, device="cpu")
+    scene, desc, _ = workload(args)
+    ps = ParticleSystem(SimConfig(scene), device="cpu")
     nt = Oracle.threads(os.cpu_count())
     p = build_params(ps)
     orc = Oracle(p, ps.particle_max_num, fp64=False)
     orc.set_state(state_from_sets(ps.state_numpy()), p.CFL * p.support_radius / p.c_signal)
     orc.stage(0)
+    # A bounded sample: one warm-up step, then as many of the K steps as fit in about
+    # 90 s of host time (a step of the 1M-particle workload takes about a second).
     t0 = time.perf_counter()
-    orc.step(args.warmup)
+    orc.step(1)
     t_w = time.perf_counter() - t0
+    k = max(1, min(args.steps, int(90.0 / max(t_w, 1e-3))))
     t0 = time.perf_counter()
-    orc.step(args.steps)
+    orc.step(k)
     el = time.perf_counter() - t0
     n = ps.particle_max_num
-    val = n * args.steps / el
-    line = {"impl": "reference", "metric": METRIC, "value": val, "unit": UNIT,
+    val = n * k / el
+    metric = METRIC if args.workload == "dambreak3d" else METRIC_BAR
+    line = {"impl": "reference", "metric": metric, "value": val, "unit": UNIT,
             "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
-            "ms_per_step": 1000.0 * el / args.steps, "higher_is_better": True,
+            "ms_per_step": 1000.0 * el / k, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-            "config": {"workload": "3D dam break, delta+-SPH, reflecting walls",
-                       "particles": n, "dx_m": args.dx, "support_dx": 2.6,
-                       "parallelism": "host threads"},
+            "config": dict(desc, particles=n, parallelism="host threads"),
             "cpu_baseline": {"value": val, "unit": UNIT, "cores": nt, "kind": "port",
-                             "sample": f"the full workload, {args.warmup} warm-up + {args.steps} "
-                                       "timed steps; CPU restatement of the reference kernels "
-                                       "(the reference's Taichi is not installable here)"},
+                             "sample": f"the full {n}-particle workload, 1 warm-up + {k} timed "
+                                       f"step(s) (of the {args.steps} asked, bounded to ~90 s); "
+                                       "CPU restatement of the reference kernels, float32, "
+                                       "OpenMP (the reference's Taichi is not installable here)"},
             "e2e": {"value": val, "unit": UNIT, "h2d_bytes_per_step": 0,
                     "d2h_bytes_per_step": 0}}
     print(json.dumps(line))
@@ -205,10 +249,12 @@ def run_reference(args):
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=40)
+    ap.add_argument("--steps", type=int, default=400)
     ap.add_argument("--warmup", type=int, default=6)
     ap.add_argument("--impl", default="b200", choices=("b200", "reference"))
-    ap.add_argument("--dx", type=float, default=DX_1M)
+    ap.add_argument("--workload", default="dambreak3d",
+                    choices=("dambreak3d", "tensile_bar3d", "tensile_bar3d_jc"))
+    ap.add_argument("--dx", type=float, default=None)
     ap.add_argument("--e2e-steps", type=int, default=None)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--profile-steps", type=int, default=4)
@@ -229,14 +275,12 @@ def main():
     from sigmasph_b200 import abi
     from sigmasph_b200.config import SimConfig
     from sigmasph_b200.particle_system import ParticleSystem
-    from sigmasph_b200.scenes import dambreak3d
-
-    cfg = SimConfig(dambreak3d(dx=args.dx))
-    ps = ParticleSystem(cfg, device=f"cuda:{local}")
+    scene, desc, tag = workload(args)
+    ps = ParticleSystem(SimConfig(scene), device=f"cuda:{local}")
     n = ps.particle_max_num
     cpu_ps = None
     if rank == 0 and ws == 1 and not args.no_cpu_baseline:
-        cpu_ps = ParticleSystem(SimConfig(dambreak3d(dx=args.dx)), device="cpu")
+        cpu_ps = ParticleSystem(SimConfig(scene), device="cpu")
     solver = ps.build_solver()
     solver.initialize()
     stream = torch.cuda.current_stream()
@@ -300,27 +344,36 @@ def main():
     solver.profile(False)
     launches_per_step = sum(c for _, c in prof.values()) / max(args.profile_steps, 1)
     per_step_ms = {k: v[0] / args.profile_steps for k, v in prof.items()}
-    dom = max((k for k in prof if k in ALGO_BYTES), key=lambda k: per_step_ms[k])
+    dom = max(prof, key=lambda k: per_step_ms[k])
+    if dom not in ALGO_BYTES:
+        dom = max((k for k in prof if k in ALGO_BYTES), key=lambda k: per_step_ms[k])
     dom_ms = prof[dom][0] / prof[dom][1]
     peak, peak_kind = load_peaks()
     achieved = ALGO_BYTES[dom] * n / (dom_ms / 1000.0) / 1e9
-    traffic = read_traffic(dom)
+    traffic = read_traffic(dom, tag, n)
     roofline = {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peak,
                 "unit": "GB/s", "frac": achieved / peak, "peak_source": peak_kind,
                 "algorithmic_bytes_per_particle": ALGO_BYTES[dom],
-                "launch_ms": dom_ms, "traffic": traffic}
+                "launch_ms": dom_ms, "traffic": traffic,
+                "traffic_source": ("ncu dram__bytes_read.sum + dram__bytes_write.sum per launch, "
+                                   "profiles/%s.md" % tag) if traffic else None}
+    step_bytes = STEP_ALGO_BYTES if tag == "dambreak3d" else STEP_ALGO_BYTES_SOLID
+    step_gbs = step_bytes * value / 1e9
+    step_roofline = {"bound": "hbm", "algorithmic_bytes_per_particle_step": step_bytes,
+                     "achieved": step_gbs, "peak": peak, "unit": "GB/s", "frac": step_gbs / peak,
+                     "peak_source": peak_kind}
 
     if rank == 0:
-        line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": ws, "steps": K,
+        metric = METRIC if args.workload == "dambreak3d" else METRIC_BAR
+        line = {"metric": metric, "value": value, "unit": UNIT, "n_gpus": ws, "steps": K,
                 "warmup": args.warmup, "ms_per_step": ms / K, "higher_is_better": True,
                 "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-                "config": {"workload": "3D dam break, delta+-SPH, reflecting walls",
-                           "particles": n, "dx_m": args.dx, "support_dx": 2.6,
-                           "parallelism": "replicas" if ws > 1 else "single GPU",
-                           "l2": "inputs larger than L2 (state + neighbour lists ~1 GB)",
-                           "graph": "two-step CUDA graph replayed"},
+                "config": dict(desc, particles=n,
+                               parallelism="replicas" if ws > 1 else "single GPU",
+                               l2="inputs larger than L2 (state + neighbour lists > 0.5 GB)",
+                               graph="two-step CUDA graph replayed"),
                 "e2e": e2e, "gpu_launches": int(round(launches_per_step * K)),
-                "roofline": roofline,
+                "roofline": roofline, "step_roofline": step_roofline,
                 "kernel_ms_per_step": {k: round(v, 5) for k, v in sorted(per_step_ms.items(),
                                                                        key=lambda t: -t[1])},
                 "error_word": err}

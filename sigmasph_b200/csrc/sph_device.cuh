@@ -9,6 +9,11 @@
 namespace sph {
 
 constexpr int kBlock = 256;          // threads per block of the particle-parallel kernels
+// Pair-loop kernels whose live state fits 64 registers with little spilling run four
+// 256-thread blocks per SM (50% occupancy): their gathers are latency-bound, so the extra
+// resident warps pay more than the spills cost.  Kernels that keep a 3x3 stress and
+// velocity gradient per pair live keep the compiler's default budget.
+#define SPH_PAIR_BOUNDS_OCC4 __launch_bounds__(kBlock, 4)
 constexpr int kMirShift = 30;        // neighbour entry = j | (mirror code << 30)
 constexpr int kIdxMask = (1 << kMirShift) - 1;
 

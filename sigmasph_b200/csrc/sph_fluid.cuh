@@ -24,7 +24,7 @@ __device__ __forceinline__ float4* as4(float* p) { return reinterpret_cast<float
 __device__ __forceinline__ const float4* as4c(const float* p) { return reinterpret_cast<const float4*>(p); }
 
 // ------------------------------------------------------------------ compute_lam pass 1
-__global__ void __launch_bounds__(kBlock) k_lam(Cst c, Ptr P) {
+__global__ void SPH_PAIR_BOUNDS_OCC4 k_lam(Cst c, Ptr P) {
     int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= c.n) return;
     const float4* __restrict__ pos = as4c(P.cur.pos);
@@ -101,7 +101,7 @@ __global__ void __launch_bounds__(kBlock) k_lam(Cst c, Ptr P) {
 }
 
 // ------------------------------------------------------------------ grad lambda + continuity
-__global__ void __launch_bounds__(kBlock) k_lamgrad_cont(Cst c, Ptr P) {
+__global__ void SPH_PAIR_BOUNDS_OCC4 k_lamgrad_cont(Cst c, Ptr P) {
     int i = blockIdx.x * blockDim.x + threadIdx.x;
     double wdiff = 0.0;
     if (i < c.n) {
@@ -213,7 +213,7 @@ __global__ void __launch_bounds__(kBlock) k_eos(Cst c, Ptr P) {
 }
 
 // ------------------------------------------------------------------ pressure + viscosity + dt pairs
-__global__ void __launch_bounds__(kBlock) k_force(Cst c, Ptr P) {
+__global__ void SPH_PAIR_BOUNDS_OCC4 k_force(Cst c, Ptr P) {
     int i = blockIdx.x * blockDim.x + threadIdx.x;
     float amag = 0.0f, csq = 0.0f;
     if (i < c.n) {
@@ -357,13 +357,13 @@ __global__ void __launch_bounds__(kBlock) k_advect(Cst c, Ptr P) {
 // evaluation below runs warp-coherent over ~80 pairs instead of inside the divergent
 // candidate loop.
 __global__ void __launch_bounds__(kBlock) k_pst_search(Cst c, Ptr P) {
-    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= c.n) return;
-    F3 xi = f3(as4c(P.cur.pos)[i]);
+    const F3 xi = f3(as4c(P.cur.pos)[i]);
     int cnt = 0;
     if (!(isnan(xi.x) || isnan(xi.y) || isnan(xi.z))) {
         const GridLayout L = *P.layout;
-        int cx = cell_of(xi.x, c.h), cy = cell_of(xi.y, c.h), cz = cell_of(xi.z, c.h);
+        const int cx = cell_of(xi.x, c.h), cy = cell_of(xi.y, c.h), cz = cell_of(xi.z, c.h);
         const int n = c.n, K = c.K;
         int* __restrict__ nb = P.nbr;
         enumerate_neighbours(c, P, L, i, xi, cx, cy, cz, [&](int j, int mir, float4) {
@@ -381,13 +381,7 @@ template <class F>
 __device__ __forceinline__ void for_each_live_neighbour(const Cst& c, const Ptr& P, int i, F3 xi, F&& f) {
     const int cnt = __ldg(P.nbr_cnt + i);
     const int m = cnt < c.K ? cnt : c.K;
-    const int* __restrict__ nb = P.nbr + i;
-    const size_t n = (size_t)c.n;
-#pragma unroll 4
-    for (int k = 0; k < m; ++k) {
-        int e = __ldg(nb + (size_t)k * n);
-        f(e & kIdxMask, (int)((unsigned)e >> kMirShift));
-    }
+    list_pairs(P.nbr + i, (size_t)c.n, m, f);
     if (cnt > c.K) {
         const GridLayout L = *P.layout;
         int cx = cell_of(xi.x, c.h), cy = cell_of(xi.y, c.h), cz = cell_of(xi.z, c.h);

@@ -263,7 +263,75 @@ __global__ void __launch_bounds__(kBlock) k_gather(Cst c, Ptr P) {
 }
 
 // ------------------------------------------------------------------ neighbour enumeration
-// Calls f(j, mirror) for every neighbour of a particle at xi whose centre cell is
+// Candidates of cell (nx, ny, nz) in bucket b: the bucket's range, filtered on the cell
+// id when the table is hashed (collisions share buckets).
+template <class F>
+__device__ __forceinline__ void bucket_candidates(const Ptr& P, bool hashed, int b, int nx, int ny,
+                                                  int nz, F&& f) {
+    const int s = __ldg(P.start + b), e = __ldg(P.start + b + 1);
+    for (int j = s; j < e; ++j) {
+        if (hashed) {
+            const int4 cj = __ldg(P.cell + j);
+            if (cj.x != nx || cj.y != ny || cj.z != nz) continue;
+        }
+        f(j);
+    }
+}
+
+// The y, z and corner mirror sweeps of a particle at xi in cell (cx, cy, cz)
+// (particle_system.py:1442-1490): the image of xi against the cells of the y = 0 row,
+// the z = 0 row and the corner column; a particle pairs with its own image too.
+template <class F>
+__device__ __forceinline__ void enumerate_mirrors(const Cst& c, const Ptr& P, const GridLayout& L,
+                                                  F3 xi, int cx, int cy, int cz, F&& f) {
+    const float4* __restrict__ pos = reinterpret_cast<const float4*>(P.cur.pos);
+    const bool hashed = L.mode != 0;
+    if (c.mirror_y && xi.y < c.h) {
+        const F3 xm = mirror3(1, xi);
+#pragma unroll 1
+        for (int o0 = -1; o0 <= 1; ++o0)
+#pragma unroll 1
+            for (int o1 = -1; o1 <= 1; ++o1) {
+                const int nx = cx + o0, ny = 0, nz = cz + o1;
+                const int b = bucket_of(nx, ny, nz, L, c.mcap);
+                if (b < 0) continue;
+                bucket_candidates(P, hashed, b, nx, ny, nz, [&](int j) {
+                    const float4 pj = __ldg(pos + j);
+                    if (dist2_rn(xm, f3(pj)) < c.d2_lt) f(j, 1, pj);
+                });
+            }
+    }
+    if (c.mirror_z && xi.z < c.h) {
+        const F3 xm = mirror3(2, xi);
+#pragma unroll 1
+        for (int o0 = -1; o0 <= 1; ++o0)
+#pragma unroll 1
+            for (int o1 = -1; o1 <= 1; ++o1) {
+                const int nx = cx + o0, ny = cy + o1, nz = 0;
+                const int b = bucket_of(nx, ny, nz, L, c.mcap);
+                if (b < 0) continue;
+                bucket_candidates(P, hashed, b, nx, ny, nz, [&](int j) {
+                    const float4 pj = __ldg(pos + j);
+                    if (dist2_rn(xm, f3(pj)) < c.d2_lt) f(j, 2, pj);
+                });
+            }
+    }
+    if (c.mirror_y && c.mirror_z && xi.y < c.h && xi.z < c.h) {
+        const F3 xm = mirror3(3, xi);
+#pragma unroll 1
+        for (int o0 = -1; o0 <= 1; ++o0) {
+            const int nx = cx + o0, ny = 0, nz = 0;
+            const int b = bucket_of(nx, ny, nz, L, c.mcap);
+            if (b < 0) continue;
+            bucket_candidates(P, hashed, b, nx, ny, nz, [&](int j) {
+                const float4 pj = __ldg(pos + j);
+                if (dist2_rn(xm, f3(pj)) < c.d2_lt) f(j, 3, pj);
+            });
+        }
+    }
+}
+
+// Calls f(j, mirror, pos_j) for every neighbour of a particle at xi whose centre cell is
 // (cx, cy, cz), in the reference's order: the 27 offsets with the last index fastest,
 // then the y, z and corner mirror sweeps (particle_system.py:1393-1490).  `self_idx` is
 // excluded from the real sweep only.  Positions are read from `pos` (live positions).
@@ -279,78 +347,16 @@ __device__ __forceinline__ void enumerate_neighbours(const Cst& c, const Ptr& P,
         for (int o1 = -1; o1 <= 1; ++o1)
 #pragma unroll 1
             for (int o2 = -1; o2 <= 1; ++o2) {
-                int nx = cx + o0, ny = cy + o1, nz = cz + o2;
-                int b = bucket_of(nx, ny, nz, L, c.mcap);
+                const int nx = cx + o0, ny = cy + o1, nz = cz + o2;
+                const int b = bucket_of(nx, ny, nz, L, c.mcap);
                 if (b < 0) continue;
-                int s = __ldg(P.start + b), e = __ldg(P.start + b + 1);
-                for (int j = s; j < e; ++j) {
-                    if (hashed) {
-                        int4 cj = __ldg(P.cell + j);
-                        if (cj.x != nx || cj.y != ny || cj.z != nz) continue;
-                    }
-                    if (j == self_idx) continue;
-                    float4 pj = __ldg(pos + j);
+                bucket_candidates(P, hashed, b, nx, ny, nz, [&](int j) {
+                    if (j == self_idx) return;
+                    const float4 pj = __ldg(pos + j);
                     if (dist2_rn(xi, f3(pj)) < c.d2_lt) f(j, 0, pj);
-                }
+                });
             }
-    if (c.mirror_y && xi.y < c.h) {
-        F3 xm = mirror3(1, xi);
-#pragma unroll 1
-        for (int o0 = -1; o0 <= 1; ++o0)
-#pragma unroll 1
-            for (int o1 = -1; o1 <= 1; ++o1) {
-                int nx = cx + o0, ny = 0, nz = cz + o1;
-                int b = bucket_of(nx, ny, nz, L, c.mcap);
-                if (b < 0) continue;
-                int s = __ldg(P.start + b), e = __ldg(P.start + b + 1);
-                for (int j = s; j < e; ++j) {
-                    if (hashed) {
-                        int4 cj = __ldg(P.cell + j);
-                        if (cj.x != nx || cj.y != ny || cj.z != nz) continue;
-                    }
-                    float4 pj = __ldg(pos + j);
-                    if (dist2_rn(xm, f3(pj)) < c.d2_lt) f(j, 1, pj);
-                }
-            }
-    }
-    if (c.mirror_z && xi.z < c.h) {
-        F3 xm = mirror3(2, xi);
-#pragma unroll 1
-        for (int o0 = -1; o0 <= 1; ++o0)
-#pragma unroll 1
-            for (int o1 = -1; o1 <= 1; ++o1) {
-                int nx = cx + o0, ny = cy + o1, nz = 0;
-                int b = bucket_of(nx, ny, nz, L, c.mcap);
-                if (b < 0) continue;
-                int s = __ldg(P.start + b), e = __ldg(P.start + b + 1);
-                for (int j = s; j < e; ++j) {
-                    if (hashed) {
-                        int4 cj = __ldg(P.cell + j);
-                        if (cj.x != nx || cj.y != ny || cj.z != nz) continue;
-                    }
-                    float4 pj = __ldg(pos + j);
-                    if (dist2_rn(xm, f3(pj)) < c.d2_lt) f(j, 2, pj);
-                }
-            }
-    }
-    if (c.mirror_y && c.mirror_z && xi.y < c.h && xi.z < c.h) {
-        F3 xm = mirror3(3, xi);
-#pragma unroll 1
-        for (int o0 = -1; o0 <= 1; ++o0) {
-            int nx = cx + o0, ny = 0, nz = 0;
-            int b = bucket_of(nx, ny, nz, L, c.mcap);
-            if (b < 0) continue;
-            int s = __ldg(P.start + b), e = __ldg(P.start + b + 1);
-            for (int j = s; j < e; ++j) {
-                if (hashed) {
-                    int4 cj = __ldg(P.cell + j);
-                    if (cj.x != nx || cj.y != ny || cj.z != nz) continue;
-                }
-                float4 pj = __ldg(pos + j);
-                if (dist2_rn(xm, f3(pj)) < c.d2_lt) f(j, 3, pj);
-            }
-        }
-    }
+    enumerate_mirrors(c, P, L, xi, cx, cy, cz, f);
 }
 
 // Builds the neighbour list of every particle from the positions the cells were binned
@@ -358,12 +364,12 @@ __device__ __forceinline__ void enumerate_neighbours(const Cst& c, const Ptr& P,
 // stored; the count is the true count and the pair passes recover the rest by a direct
 // search (for_each_neighbour below).
 __global__ void __launch_bounds__(kBlock) k_nbr_build(Cst c, Ptr P) {
-    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= c.n) return;
     const GridLayout L = *P.layout;
-    int4 ci = P.cell[i];
+    const int4 ci = P.cell[i];
     if (ci.w < 0) { P.nbr_cnt[i] = 0; return; }
-    F3 xi = f3(reinterpret_cast<const float4*>(P.cur.pos)[i]);
+    const F3 xi = f3(reinterpret_cast<const float4*>(P.cur.pos)[i]);
     int cnt = 0;
     const int n = c.n, K = c.K;
     int* __restrict__ nb = P.nbr;
@@ -375,19 +381,29 @@ __global__ void __launch_bounds__(kBlock) k_nbr_build(Cst c, Ptr P) {
     P.nbr_cnt[i] = cnt;
 }
 
+// The m stored entries of one particle's k-major list, with the next two entries in
+// flight while the current pair is evaluated (the pair passes are bound by the latency
+// of the dependent list -> particle gathers).
+template <class F>
+__device__ __forceinline__ void list_pairs(const int* __restrict__ nb, size_t n, int m, F&& f) {
+    int e0 = m > 0 ? __ldg(nb) : 0;
+    int e1 = m > 1 ? __ldg(nb + n) : 0;
+#pragma unroll 2
+    for (int k = 0; k < m; ++k) {
+        const int e = e0;
+        e0 = e1;
+        if (k + 2 < m) e1 = __ldg(nb + (size_t)(k + 2) * n);
+        f(e & kIdxMask, (int)((unsigned)e >> kMirShift));
+    }
+}
+
 // Calls f(j, mirror) for the stored neighbours of i, then for any beyond the list's
 // capacity by re-running the search (same order, first K skipped).
 template <class F>
 __device__ __forceinline__ void for_each_neighbour(const Cst& c, const Ptr& P, int i, F&& f) {
     const int cnt = __ldg(P.nbr_cnt + i);
     const int m = cnt < c.K ? cnt : c.K;
-    const int* __restrict__ nb = P.nbr + i;
-    const size_t n = (size_t)c.n;
-#pragma unroll 4
-    for (int k = 0; k < m; ++k) {
-        int e = __ldg(nb + (size_t)k * n);
-        f(e & kIdxMask, (int)((unsigned)e >> kMirShift));
-    }
+    list_pairs(P.nbr + i, (size_t)c.n, m, f);
     if (cnt > c.K) {
         const GridLayout L = *P.layout;
         int4 ci = P.cell[i];

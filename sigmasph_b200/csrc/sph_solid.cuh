@@ -207,7 +207,7 @@ __global__ void __launch_bounds__(kBlock) k_kc_inverse(Cst c, Ptr P) {
 }
 
 // ------------------------------------------------------------------ pass A
-__global__ void __launch_bounds__(kBlock) k_solid_a(Cst c, Ptr P) {
+__global__ void SPH_PAIR_BOUNDS_OCC4 k_solid_a(Cst c, Ptr P) {
     int i = blockIdx.x * blockDim.x + threadIdx.x;
     double wdiff = 0.0;
     if (i < c.n) {
@@ -282,7 +282,7 @@ __global__ void __launch_bounds__(kBlock) k_solid_a(Cst c, Ptr P) {
 }
 
 // ------------------------------------------------------------------ grad v alone (damper refresh)
-__global__ void __launch_bounds__(kBlock) k_gradv(Cst c, Ptr P) {
+__global__ void SPH_PAIR_BOUNDS_OCC4 k_gradv(Cst c, Ptr P) {
     int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= c.n) return;
     const float4* __restrict__ pos = as4c(P.cur.pos);
@@ -845,39 +845,59 @@ __global__ void __launch_bounds__(kBlock) k_solid_advect(Cst c, Ptr P) {
 }
 
 // ------------------------------------------------------------------ grips
+// The grip force is summed per block in shared memory (FP64) and pushed with one global
+// atomic per block, grip and axis: gripped particles are contiguous in the Morton order,
+// so a per-particle global atomic would serialise thousands of adds on a few addresses.
 __global__ void __launch_bounds__(kBlock) k_constraints(Cst c, Ptr P) {
-    int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= c.n) return;
-    int2 bc = reinterpret_cast<const int2*>(P.cur.bc)[i];
-    if (bc.x == 0) return;
-    const float s = P.sc->load_s, sd = P.sc->load_sdot;
-    const float scale = c.p.axisymmetric ? (float)(2.0 * M_PI) : 1.0f;
-    float4 bd = reinterpret_cast<const float4*>(P.cur.bcdisp)[i];
-    float4* pos = as4(P.cur.pos);
-    float4* vel = as4(P.cur.vel);
-    float4* dsp = as4(P.cur.disp);
-    float4 p = pos[i], v = vel[i], u = dsp[i], a = P.acc[i];
-    const float4 x0 = as4(P.cur.x0)[i];
-    const float m = v.w;
-    float* pc[3] = {&p.x, &p.y, &p.z};
-    float* vc[3] = {&v.x, &v.y, &v.z};
-    float* uc[3] = {&u.x, &u.y, &u.z};
-    float* ac[3] = {&a.x, &a.y, &a.z};
-    const float bdc[3] = {bd.x, bd.y, bd.z};
-    const float x0c[3] = {x0.x, x0.y, x0.z};
+    __shared__ double s_force[8][3];
+    __shared__ float s_disp[8][3];
+    __shared__ int s_axes[8];
+    if (threadIdx.x < 24) (&s_force[0][0])[threadIdx.x] = 0.0;
+    if (threadIdx.x < 8) s_axes[threadIdx.x] = 0;
+    __syncthreads();
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    int2 bc = make_int2(0, -1);
+    if (i < c.n) bc = reinterpret_cast<const int2*>(P.cur.bc)[i];
+    if (bc.x != 0) {
+        const float s = P.sc->load_s, sd = P.sc->load_sdot;
+        const float scale = c.p.axisymmetric ? (float)(2.0 * M_PI) : 1.0f;
+        float4 bd = reinterpret_cast<const float4*>(P.cur.bcdisp)[i];
+        float4* pos = as4(P.cur.pos);
+        float4* vel = as4(P.cur.vel);
+        float4* dsp = as4(P.cur.disp);
+        float4 p = pos[i], v = vel[i], u = dsp[i], a = P.acc[i];
+        const float4 x0 = as4(P.cur.x0)[i];
+        const float m = v.w;
+        float* pc[3] = {&p.x, &p.y, &p.z};
+        float* vc[3] = {&v.x, &v.y, &v.z};
+        float* uc[3] = {&u.x, &u.y, &u.z};
+        float* ac[3] = {&a.x, &a.y, &a.z};
+        const float bdc[3] = {bd.x, bd.y, bd.z};
+        const float x0c[3] = {x0.x, x0.y, x0.z};
+        const bool record = c.p.num_constraints > 0 && bc.y >= 0 && bc.y < 8;
+        if (record) atomicOr(&s_axes[bc.y], bc.x & 7);
 #pragma unroll
-    for (int d = 0; d < 3; ++d) {
-        if (!(bc.x & (1 << d))) continue;
-        if (c.p.num_constraints > 0 && bc.y >= 0 && bc.y < 8) {
-            atomicAdd(&P.sc->constraint_force[bc.y][d], (double)(scale * m * *ac[d]));
-            P.sc->constraint_disp[bc.y][d] = (double)(bdc[d] * s);
+        for (int d = 0; d < 3; ++d) {
+            if (!(bc.x & (1 << d))) continue;
+            if (record) {
+                atomicAdd(&s_force[bc.y][d], (double)(scale * m * *ac[d]));
+                s_disp[bc.y][d] = bdc[d] * s;     // one value per grip: a benign race
+            }
+            *uc[d] = bdc[d] * s;
+            *pc[d] = x0c[d] + *uc[d];
+            *vc[d] = bdc[d] * sd;
+            *ac[d] = 0.0f;
         }
-        *uc[d] = bdc[d] * s;
-        *pc[d] = x0c[d] + *uc[d];
-        *vc[d] = bdc[d] * sd;
-        *ac[d] = 0.0f;
+        pos[i] = p; vel[i] = v; dsp[i] = u; P.acc[i] = a;
     }
-    pos[i] = p; vel[i] = v; dsp[i] = u; P.acc[i] = a;
+    __syncthreads();
+    if (threadIdx.x < 24) {
+        const int k = threadIdx.x / 3, d = threadIdx.x % 3;
+        if (s_axes[k] & (1 << d)) {
+            atomicAdd(&P.sc->constraint_force[k][d], s_force[k][d]);
+            P.sc->constraint_disp[k][d] = (double)s_disp[k][d];
+        }
+    }
 }
 
 __global__ void k_solid_time(Cst c, Ptr P) {

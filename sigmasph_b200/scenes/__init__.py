@@ -9,6 +9,15 @@ so the domain is the tank grown by that radius.  dx = 4.762 mm gives 126 x 126 x
 1,000,188 particles; dx = 9.449 mm about 128k.
 
 `dambreak3d_1M.json` is the dx = 4.762 mm deck written out.
+
+`tensile_bar3d(dx, plasticity)` is the 3D round-bar tensile test: a parallel-gauge
+dogbone revolved about y (gauge diameter 6 mm x 30 mm, heads 10 mm x 15 mm, 3 mm
+fillets), steel (rho 7.9e-6 kg/mm^3, E 200 GPa, nu 0.3, linear EOS) with J2 linear
+hardening (sigma_y 0.3 GPa, H 1 GPa) or Johnson-Cook hardening (A 0.31, B 1.0 GPa,
+n 0.65, C 0.02, reference rate 1/ms), hourglass damper alpha 4, Colle shifting with a
+fixed Mach 0.05 and ALE transport, delta 0.1, viscosity 0.02.  The grips are the
+outer 10 mm of each head, pulled apart by 1 mm each over a 1 ms smoothstep ramp
+(1 m/s on average).  Units mm, GPa, ms.  dx = 0.113 mm lays about 2.3M particles.
 """
 from __future__ import annotations
 
@@ -53,6 +62,51 @@ def dambreak3d(dx=0.004762, support_factor_dx=2.6, cfl=0.25, column=(0.6, 0.6, 0
 def dx_for_particles(n, column=(0.6, 0.6, 0.3)):
     """The lattice spacing that lays about n particles in the column."""
     return (column[0] * column[1] * column[2] / float(n)) ** (1.0 / 3.0)
+
+
+def tensile_bar3d(dx=0.113, plasticity="j2", hourglass_subcycle=False, cfl=0.3):
+    gauge_d, gauge_l, head_d, head_l, fillet = 6.0, 30.0, 10.0, 15.0, 3.0
+    red = 0.5 * (head_d - gauge_d)
+    shoulder = math.sqrt(red * (2.0 * fillet - red))
+    half = 0.5 * gauge_l + shoulder + head_l
+    grip = half - 10.0
+    r = 0.5 * head_d
+    if plasticity == "j2":
+        plast = {"model": "linear", "yieldStress": 0.3, "hardeningModulus": 1.0}
+    elif plasticity == "jc":
+        plast = {"model": "johnson_cook", "A": 0.31, "B": 1.0, "n": 0.65, "C": 0.02,
+                 "eps0_dot": 1.0, "T0": 293.0, "Tm": 0.0}
+    else:
+        raise ValueError("plasticity must be 'j2' or 'jc'")
+    hg = {"alpha": 4.0}
+    if hourglass_subcycle:
+        hg["superTimeStepping"] = {"mode": "subcycle"}
+    # lattice sites span [start, end) from start + dx/2: the box is the bar's bounding box
+    return {
+        "Domain": {"particleRadius": 0.5 * dx, "supportRadiusFactor": 6.0, "boundary": "open"},
+        "Time": {"CFL": cfl},
+        "Solver": {"type": "hypoElastic", "viscosity": 0.02, "allowNegativePressure": True},
+        "Materials": [{"name": "steel", "density0": 7.9e-6, "eos": {"type": "linear"},
+                       "strength": {"type": "hypoElastic", "youngsModulus": 200.0,
+                                    "poissonRatio": 0.3, "plasticity": plast}}],
+        "Load": {"gravitation": [0.0, 0.0, 0.0], "rampTime": 1.0},
+        "Diffusion": {"delta": 0.1},
+        "Shifting": {"enabled": True, "mode": "colle", "maMode": "fixed", "maFixed": 0.05,
+                     "aleMomentum": True, "aleHistory": True},
+        "Hourglass": hg,
+        "SolidBlocks": [{"objectId": 0, "start": [-r, -half, -r], "end": [r, half, r],
+                         "translation": [0, 0, 0], "scale": [1, 1, 1], "velocity": [0, 0, 0],
+                         "density": 7.9e-6, "color": [200, 120, 60], "material": "steel",
+                         "shape": {"type": "gaugedogbone3d", "tabWidth": head_d,
+                                   "tabHeight": head_l, "gaugeWidth": gauge_d,
+                                   "radius": fillet, "gaugeLength": gauge_l,
+                                   "center": [0.0, 0.0, 0.0]}}],
+        "Constraints": [
+            {"name": "low", "region": [[-r - 1, -half - 1, -r - 1], [r + 1, -grip, r + 1]],
+             "components": "xyz", "displacement": [0.0, -1.0, 0.0]},
+            {"name": "high", "region": [[-r - 1, grip, -r - 1], [r + 1, half + 1, r + 1]],
+             "components": "xyz", "displacement": [0.0, 1.0, 0.0]}],
+    }
 
 
 def scene_path(name):
