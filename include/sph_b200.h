@@ -51,6 +51,8 @@ extern "C" {
                                       table; the step ran on the hashed fallback table   */
 #define SPH_EW_JC_NO_CONVERGE 0x4  /* a Johnson-Cook return map hit its iteration cap     */
 #define SPH_EW_STS_CAP        0x8  /* the hourglass sub-cycle count hit its cap          */
+#define SPH_EW_MLP_TIMEOUT    0x10 /* a tensor-core surrogate pass gave up waiting for its
+                                      MMAs; its returns fell back to the exact Newton      */
 
 /* ------------------------------------------------------------------ parameters */
 /* Flattened, resolved scene configuration.  Field meanings follow the reference's
@@ -280,6 +282,44 @@ int  sph_profile_read(SphHandle* h, char* names, int names_cap, double* ms, int*
 #define SPH_NOALLOC_MAX_PARTICLES 4194304
 int  sph_reduce_noalloc(const SphParams* p, const float* pos, const float* vel,
                         const float* shift, int64_t n, double* out, void* stream);
+
+/* ---- Johnson-Cook return-map surrogate (no counterpart in the reference; its return
+ * map is the Newton-bisection of MAT002_johnson_cook.py:251-354, called from
+ * SOLID.py:2889-2913).  A 4 -> 64 -> 64 -> 64 -> 1 SiLU MLP of sph_mlp_param_count()
+ * float32 parameters (W1[64][4], b1, W2[64][64], b2, W3[64][64], b3, W4[64], b4) maps the
+ * features of a yielding return, f0 = vm/sigma_y0 - 1, f1 = eps_p,
+ * f2 = ln(max(eps_dot_eq/eps0_dot, 1))/10, f3 = ln(max(d_hi/(dt eps0_dot), 1))/10, to
+ * u = 10 (1 - d/d_hi), with d_hi = (vm - sigma_y0)/(3G).  Every pointer is device memory; X rows are
+ * float4 (16-byte aligned), Y and T one float per row.  Calls are asynchronous on stream. */
+int     sph_mlp_param_count(void);
+int64_t sph_mlp_packed_bytes(void);
+/* Float32 forward on CUDA cores (the training reference). */
+int  sph_mlp_forward(const float* W, const float* X, int64_t n, float* Y, void* stream);
+/* Mean-squared-error gradient over n rows into G[param_count] (overwritten) and the loss
+ * into *loss (one double, overwritten). */
+int  sph_mlp_grad(const float* W, const float* X, const float* T, int64_t n, float* G,
+                  double* loss, void* stream);
+/* One Adam step (beta 0.9 / 0.999, eps 1e-8, bias-corrected; step counts from 1). */
+int  sph_mlp_adam(float* W, const float* G, float* M, float* V, int64_t step, float lr,
+                  void* stream);
+/* BF16 copy of W2 and W3 in the tensor cores' operand layout (sph_mlp_packed_bytes(),
+ * 16-byte aligned). */
+int  sph_mlp_pack(const float* W, void* packed, void* stream);
+/* BF16 tensor-core (tcgen05) inference with FP32 accumulation; *err gets
+ * SPH_EW_MLP_TIMEOUT if a bounded wait gave up. */
+int  sph_mlp_infer_tc(const float* W, const void* packed, const float* X, int64_t n, float* Y,
+                      int* err, void* stream);
+/* Enables (enable = 1, W = the parameters, tol = the |g|/sigma_y acceptance) or disables
+ * the surrogate in a solid handle's Johnson-Cook returns: yielding returns are queued,
+ * the network proposes d, and the exact Newton runs wherever the residual exceeds tol. */
+int  sph_jc_surrogate(SphHandle* h, const float* W, float tol, int enable, void* stream);
+/* Attaches (rows != NULL) or detaches a sample log: every exact Johnson-Cook return of the
+ * plain path appends {f0, f1, f2, f3, d/d_hi, d_hi, vm, sigma_y0} to rows[capacity][8];
+ * *count (device, zeroed by the caller) counts every return, logged or not. */
+int  sph_jc_log(SphHandle* h, float* rows, int64_t capacity, unsigned long long* count);
+/* Counters since the last reset: {Newton solves, Newton iterations, surrogate proposals,
+ * proposals accepted}; reset != 0 zeroes them after the read (synchronises stream). */
+int  sph_jc_stats(SphHandle* h, uint64_t* out, int reset, void* stream);
 
 /* Stage ids for sph_run_stage. */
 enum {

@@ -24,6 +24,7 @@ EW_NBR_OVERFLOW = 0x1
 EW_HASHED_GRID = 0x2
 EW_JC_NO_CONVERGE = 0x4
 EW_STS_CAP = 0x8
+EW_MLP_TIMEOUT = 0x10
 
 # Stage ids of sph_run_stage (include/sph_b200.h).
 STAGE_SORT, STAGE_LAM, STAGE_CONTINUITY, STAGE_FORCES, STAGE_DT, STAGE_ADVECT, \
@@ -154,6 +155,16 @@ def lib():
         "sph_profile_enable": (C.c_int, [vp, C.c_int]),
         "sph_profile_read": (C.c_int, [vp, C.c_char_p, C.c_int, C.POINTER(C.c_double),
                                        C.POINTER(C.c_int), C.c_int, C.POINTER(C.c_int)]),
+        "sph_mlp_param_count": (C.c_int, []),
+        "sph_mlp_packed_bytes": (i64, []),
+        "sph_mlp_forward": (C.c_int, [vp, vp, i64, vp, vp]),
+        "sph_mlp_grad": (C.c_int, [vp, vp, vp, i64, vp, vp, vp]),
+        "sph_mlp_adam": (C.c_int, [vp, vp, vp, vp, i64, C.c_float, vp]),
+        "sph_mlp_pack": (C.c_int, [vp, vp, vp]),
+        "sph_mlp_infer_tc": (C.c_int, [vp, vp, vp, i64, vp, vp, vp]),
+        "sph_jc_surrogate": (C.c_int, [vp, vp, C.c_float, C.c_int, vp]),
+        "sph_jc_log": (C.c_int, [vp, vp, i64, vp]),
+        "sph_jc_stats": (C.c_int, [vp, C.POINTER(C.c_uint64), C.c_int, vp]),
     }
     for name, (res, args) in sig.items():
         f = getattr(L, name)

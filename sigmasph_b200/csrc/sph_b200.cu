@@ -118,6 +118,7 @@ Ptr make_ptr(SphHandle* h) {
     P.nbr_cnt = h->nbr_cnt;
     P.sc = h->sc;
     P.ac = h->ac;
+    P.jc = solid_jc_ptr(h->solid);
     return P;
 }
 
@@ -626,3 +627,102 @@ extern "C" int sph_profile_read(SphHandle* h, char* names, int names_cap, double
     h->prof_used = 0;
     return SPH_OK;
 }
+
+// ------------------------------------------------------------------ Johnson-Cook surrogate
+extern "C" {
+
+int sph_mlp_param_count(void) { return kMlpParams; }
+int64_t sph_mlp_packed_bytes(void) { return (int64_t)kMlpPackedBytes; }
+
+int sph_mlp_forward(const float* W, const float* X, int64_t n, float* Y, void* stream) {
+    if (!W || (n > 0 && (!X || !Y)) || n < 0 || n > INT32_MAX) return SPH_ERR_ARG;
+    if (n == 0) return SPH_OK;
+    k_mlp_forward<<<(int)((n + 127) / 128), 128, 0, S(stream)>>>(W, reinterpret_cast<const float4*>(X), (int)n, Y);
+    CK(cudaGetLastError());
+    return SPH_OK;
+}
+
+int sph_mlp_grad(const float* W, const float* X, const float* T, int64_t n, float* G, double* loss,
+                 void* stream) {
+    if (!W || !G || !loss || n <= 0 || n > INT32_MAX || !X || !T) return SPH_ERR_ARG;
+    cudaStream_t st = S(stream);
+    CK(cudaMemsetAsync(G, 0, sizeof(float) * kMlpParams, st));
+    CK(cudaMemsetAsync(loss, 0, sizeof(double), st));
+    k_mlp_grad<<<(int)((n + kMlpGradThreads - 1) / kMlpGradThreads), kMlpGradThreads,
+                 sizeof(float) * kMlpParams, st>>>(W, reinterpret_cast<const float4*>(X), T, (int)n,
+                                                    1.0f / (float)n, G, loss);
+    CK(cudaGetLastError());
+    return SPH_OK;
+}
+
+int sph_mlp_adam(float* W, const float* G, float* M, float* V, int64_t step, float lr, void* stream) {
+    if (!W || !G || !M || !V || step < 1 || !(lr > 0.0f)) return SPH_ERR_ARG;
+    const double b1 = 0.9, b2 = 0.999;
+    const float c1 = (float)(1.0 / (1.0 - std::pow(b1, (double)step)));
+    const float c2 = (float)(1.0 / (1.0 - std::pow(b2, (double)step)));
+    k_mlp_adam<<<(kMlpParams + 255) / 256, 256, 0, S(stream)>>>(W, G, M, V, kMlpParams, lr, (float)b1,
+                                                                (float)b2, 1e-8f, c1, c2);
+    CK(cudaGetLastError());
+    return SPH_OK;
+}
+
+int sph_mlp_pack(const float* W, void* packed, void* stream) {
+    if (!W || !packed) return SPH_ERR_ARG;
+    if (reinterpret_cast<uintptr_t>(packed) % 16) return SPH_ERR_ARG;
+    k_mlp_pack<<<(2 * kMlpPackedHalf + 255) / 256, 256, 0, S(stream)>>>(W, static_cast<__nv_bfloat16*>(packed));
+    CK(cudaGetLastError());
+    return SPH_OK;
+}
+
+int sph_mlp_infer_tc(const float* W, const void* packed, const float* X, int64_t n, float* Y, int* err,
+                     void* stream) {
+    if (!W || !packed || !err || n < 0 || n > INT32_MAX || (n > 0 && (!X || !Y))) return SPH_ERR_ARG;
+    if (reinterpret_cast<uintptr_t>(packed) % 16 || reinterpret_cast<uintptr_t>(X) % 16) return SPH_ERR_ARG;
+    if (n == 0) return SPH_OK;
+    const int tiles = (int)((n + kMlpTileRows - 1) / kMlpTileRows);
+    k_mlp_tc<<<std::min(2 * 148, tiles), kMlpTcThreads, 0, S(stream)>>>(
+        W, static_cast<const __nv_bfloat16*>(packed), reinterpret_cast<const float4*>(X), (int)n, nullptr, Y, err);
+    CK(cudaGetLastError());
+    return SPH_OK;
+}
+
+int sph_jc_surrogate(SphHandle* h, const float* W, float tol, int enable, void* stream) {
+    if (!h || !h->p.is_solid) return SPH_ERR_ARG;
+    if (enable && (!W || !(tol > 0.0f))) return SPH_ERR_ARG;
+    cudaStream_t st = S(stream);
+    if (enable) {
+        int r = solid_jc_alloc(h->solid, h->n_max);
+        if (r) return r;
+        CK(cudaMemcpyAsync(h->solid.W, W, sizeof(float) * kMlpParams, cudaMemcpyDeviceToDevice, st));
+        k_mlp_pack<<<(2 * kMlpPackedHalf + 255) / 256, 256, 0, st>>>(h->solid.W,
+                                                                    static_cast<__nv_bfloat16*>(h->solid.packed));
+        CK(cudaGetLastError());
+        h->p.jc_surrogate_tol = h->c.p.jc_surrogate_tol = tol;
+    }
+    h->p.jc_surrogate = h->c.p.jc_surrogate = enable ? 1 : 0;
+    drop_graph(h);
+    return SPH_OK;
+}
+
+int sph_jc_log(SphHandle* h, float* rows, int64_t capacity, unsigned long long* count) {
+    if (!h || !h->p.is_solid) return SPH_ERR_ARG;
+    if (rows && (!count || capacity <= 0 || reinterpret_cast<uintptr_t>(rows) % 16)) return SPH_ERR_ARG;
+    h->solid.log = rows;
+    h->solid.log_count = rows ? count : nullptr;
+    h->solid.log_cap = rows ? capacity : 0;
+    drop_graph(h);
+    return SPH_OK;
+}
+
+int sph_jc_stats(SphHandle* h, uint64_t* out, int reset, void* stream) {
+    if (!h || !out || !h->p.is_solid || !h->solid.stats) return SPH_ERR_ARG;
+    cudaStream_t st = S(stream);
+    unsigned long long v[4];
+    CK(cudaMemcpyAsync(v, h->solid.stats, sizeof(v), cudaMemcpyDeviceToHost, st));
+    CK(cudaStreamSynchronize(st));
+    for (int k = 0; k < 4; ++k) out[k] = v[k];
+    if (reset) CK(cudaMemsetAsync(h->solid.stats, 0, sizeof(v), st));
+    return SPH_OK;
+}
+
+}  // extern "C"

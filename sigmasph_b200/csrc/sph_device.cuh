@@ -67,6 +67,20 @@ struct Cst {
     int mirror_y, mirror_z;
 };
 
+// Johnson-Cook return-map surrogate and sample log (solid only; null when unused).
+struct JcPtr {
+    int* count;                    // queued returns this step
+    int* idx;                      // [n] particle of each queued return
+    float4* feat;                  // [n] its features
+    float* fpred;                  // [n] network output u = 10 (1 - d / d_hi)
+    const float* W;                // [8705] float32 parameters
+    const void* packed;            // BF16 hidden-layer weights, tensor-core layout
+    unsigned long long* stats;     // Newton solves, Newton iterations, queued, accepted
+    float* log;                    // [log_cap][8] exact returns of the plain path
+    unsigned long long* log_count;
+    long long log_cap;
+};
+
 // Device pointers of one launch.
 struct Ptr {
     SphFieldSet cur, nxt;
@@ -92,6 +106,7 @@ struct Ptr {
     int* nbr_cnt;        // [n]
     DevScalars* sc;
     DevAccum* ac;
+    JcPtr jc;
 };
 
 // ------------------------------------------------------------------ small vector ops

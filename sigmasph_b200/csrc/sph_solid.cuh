@@ -28,18 +28,63 @@
 // has been committed.
 #pragma once
 #include "sph_fluid.cuh"
+#include "sph_mlp.cuh"
 
 namespace sph {
 
 constexpr int kStsMaxStages = 32;
 
+// Library-owned buffers of the Johnson-Cook surrogate, allocated on its first use
+// (sph_jc_surrogate); the sample log is caller-owned (sph_jc_log).
 struct SolidScratch {
-    int unused = 0;
+    int* q_count = nullptr;
+    int* q_idx = nullptr;
+    float4* q_feat = nullptr;
+    float* q_pred = nullptr;
+    float* W = nullptr;
+    void* packed = nullptr;
+    unsigned long long* stats = nullptr;
+    int* mlp_err = nullptr;
+    float* log = nullptr;
+    unsigned long long* log_count = nullptr;
+    long long log_cap = 0;
 };
 
 inline void solid_fill_constants(Cst&) {}
-inline int solid_alloc(SolidScratch&, const SphParams&, int64_t) { return SPH_OK; }
-inline void solid_free(SolidScratch&) {}
+inline int solid_alloc(SolidScratch& s, const SphParams& p, int64_t) {
+    if (!p.is_solid) return SPH_OK;
+    if (cudaMalloc(&s.stats, 4 * sizeof(unsigned long long)) != cudaSuccess) return SPH_ERR_NOMEM;
+    if (cudaMemset(s.stats, 0, 4 * sizeof(unsigned long long)) != cudaSuccess) return SPH_ERR_CUDA;
+    return SPH_OK;
+}
+inline int solid_jc_alloc(SolidScratch& s, int64_t n) {
+    if (s.q_count) return SPH_OK;
+    const size_t m = (size_t)(n > 0 ? n : 1);
+    if (cudaMalloc(&s.q_count, sizeof(int)) != cudaSuccess ||
+        cudaMalloc(&s.q_idx, m * sizeof(int)) != cudaSuccess ||
+        cudaMalloc(&s.q_feat, m * sizeof(float4)) != cudaSuccess ||
+        cudaMalloc(&s.q_pred, m * sizeof(float)) != cudaSuccess ||
+        cudaMalloc(&s.W, kMlpParams * sizeof(float)) != cudaSuccess ||
+        cudaMalloc(&s.packed, kMlpPackedBytes) != cudaSuccess ||
+        cudaMalloc(&s.mlp_err, sizeof(int)) != cudaSuccess)
+        return SPH_ERR_NOMEM;
+    if (cudaMemset(s.q_count, 0, sizeof(int)) != cudaSuccess ||
+        cudaMemset(s.mlp_err, 0, sizeof(int)) != cudaSuccess)
+        return SPH_ERR_CUDA;
+    return SPH_OK;
+}
+inline void solid_free(SolidScratch& s) {
+    void* ps[] = {s.q_count, s.q_idx, s.q_feat, s.q_pred, s.W, s.packed, s.stats, s.mlp_err};
+    for (void* q : ps) if (q) cudaFree(q);
+    s = SolidScratch();
+}
+inline JcPtr solid_jc_ptr(const SolidScratch& s) {
+    JcPtr j;
+    j.count = s.q_count; j.idx = s.q_idx; j.feat = s.q_feat; j.fpred = s.q_pred;
+    j.W = s.W; j.packed = s.packed; j.stats = s.stats;
+    j.log = s.log; j.log_count = s.log_count; j.log_cap = s.log_cap;
+    return j;
+}
 
 // ------------------------------------------------------------------ helpers
 struct Sym { float xx, yy, zz, xy, xz, yz; };
@@ -76,6 +121,7 @@ __device__ __forceinline__ float solid_pressure(const Cst& c, int k, float rho) 
 // ------------------------------------------------------------------ load factor
 __global__ void k_solid_load(Cst c, Ptr P) {
     if (threadIdx.x != 0 || blockIdx.x != 0) return;
+    if (P.jc.count) *P.jc.count = 0;            // the surrogate queue of this step
     double T = c.p.ramp_time;
     if (T <= 0.0) { P.sc->load_s = 1.0f; P.sc->load_sdot = 0.0f; return; }
     double u = fmin(1.0, fmax(0.0, P.sc->sim_time / T));
@@ -339,55 +385,100 @@ __device__ __forceinline__ void jc_residual(float d, float vm, float G, float A,
     g = vm - 3.0f * G * d - sy;
     dg = -3.0f * G - dsy;
 }
-// MAT002_johnson_cook.py:277-354: bracketed Newton-bisection, at most 40 iterations.
-__device__ __forceinline__ float jc_return(Sym& s, const Cst& c, int k, float ep, float temp, float dt,
-                                           bool& capped) {
-    const float G = c.p.mat_G[k], A = c.p.jc_A[k], B = c.p.jc_B[k], nn = c.p.jc_n[k];
-    const float C = c.p.jc_C[k], e0d = c.p.jc_eps0_dot[k], T0 = c.p.jc_T0[k], Tm = c.p.jc_Tm[k];
-    capped = false;
-    if (!(G > 0.0f && A > 0.0f)) return 0.0f;
-    float vm = vm_sym(s);
-    float mt = 1.0f;
+// The frozen part of a Johnson-Cook return: von Mises of the trial deviator, the thermal
+// softening factor at the step-start temperature, the yield stress at d = 0 and the
+// upper bracket d_hi = (vm - sigma_y0) / (3 G) (MAT002_johnson_cook.py:251-300).
+struct JcTrial {
+    float vm, G, A, B, nn, C, e0d, mt, sy0;
+    bool active;                 // material has G, A > 0
+    bool yields;                 // vm > sigma_y0 > 0
+};
+__device__ __forceinline__ JcTrial jc_trial(const Sym& s, const Cst& c, int k, float ep, float temp) {
+    JcTrial q;
+    q.G = c.p.mat_G[k]; q.A = c.p.jc_A[k]; q.B = c.p.jc_B[k]; q.nn = c.p.jc_n[k];
+    q.C = c.p.jc_C[k]; q.e0d = c.p.jc_eps0_dot[k];
+    const float T0 = c.p.jc_T0[k], Tm = c.p.jc_Tm[k];
+    q.active = q.G > 0.0f && q.A > 0.0f;
+    q.vm = vm_sym(s);
+    q.mt = 1.0f;
     if (Tm > T0 && temp > T0) {
         float ts = fminf(1.0f, fmaxf(0.0f, (temp - T0) / (Tm - T0)));
-        mt = fmaxf(0.0f, 1.0f - powf(ts, c.p.jc_m[k]));
+        q.mt = fmaxf(0.0f, 1.0f - powf(ts, c.p.jc_m[k]));
     }
-    float s0 = A;
-    if (ep > 0.0f && B > 0.0f && nn > 0.0f) s0 += B * powf(ep, nn);
-    float sy0 = s0 * mt;
-    if (!(vm > sy0 && sy0 > 0.0f)) return 0.0f;
-    float lo = 0.0f, hi = (vm - sy0) / (3.0f * G);
+    float s0 = q.A;
+    if (ep > 0.0f && q.B > 0.0f && q.nn > 0.0f) s0 += q.B * powf(ep, q.nn);
+    q.sy0 = s0 * q.mt;
+    q.yields = q.active && q.vm > q.sy0 && q.sy0 > 0.0f;
+    return q;
+}
+// MAT002_johnson_cook.py:277-354: bracketed Newton-bisection, at most 40 iterations.
+__device__ __forceinline__ float jc_newton(const JcTrial& q, float ep, float dt, int& iters) {
+    float lo = 0.0f, hi = (q.vm - q.sy0) / (3.0f * q.G);
     float dref = 0.0f;
-    if (dt > 0.0f && e0d > 0.0f && C > 0.0f) dref = dt * e0d;
+    if (dt > 0.0f && q.e0d > 0.0f && q.C > 0.0f) dref = dt * q.e0d;
     if (dref > 0.0f && dref < hi) {
         float g, dg;
-        jc_residual(dref, vm, G, A, B, nn, C, e0d, mt, ep, dt, g, dg);
+        jc_residual(dref, q.vm, q.G, q.A, q.B, q.nn, q.C, q.e0d, q.mt, ep, dt, g, dg);
         if (g > 0.0f) lo = dref; else hi = dref;
     }
     float d = lo > 0.0f ? lo : hi;
     int it = 0;
     for (; it < 40; ++it) {
         float g, dg;
-        jc_residual(d, vm, G, A, B, nn, C, e0d, mt, ep, dt, g, dg);
+        jc_residual(d, q.vm, q.G, q.A, q.B, q.nn, q.C, q.e0d, q.mt, ep, dt, g, dg);
         if (g > 0.0f) lo = d; else hi = d;
-        if (fabsf(g) <= 1e-6f * vm || hi - lo <= 1e-6f * hi) break;
+        if (fabsf(g) <= 1e-6f * q.vm || hi - lo <= 1e-6f * hi) break;
         float dn = d - g / dg;
         if (!(dn > lo && dn < hi)) dn = lo > 0.0f ? sqrtf(lo * hi) : 0.5f * hi;
         if (fabsf(dn - d) <= 1e-6f * d) { d = dn; break; }
         d = dn;
     }
-    capped = it >= 40;
-    float syf = fmaxf(0.0f, vm - 3.0f * G * d);
-    float sc = syf / vm;
-    s = {s.xx * sc, s.yy * sc, s.zz * sc, s.xy * sc, s.xz * sc, s.yz * sc};
+    iters = it;
     return d;
+}
+// Radial scaling of the deviator onto the yield surface after an increment d.
+__device__ __forceinline__ void jc_scale(Sym& s, const JcTrial& q, float d) {
+    float syf = fmaxf(0.0f, q.vm - 3.0f * q.G * d);
+    float sc = syf / q.vm;
+    s = {s.xx * sc, s.yy * sc, s.zz * sc, s.xy * sc, s.xz * sc, s.yz * sc};
+}
+__device__ __forceinline__ float jc_return(Sym& s, const Cst& c, int k, float ep, float temp, float dt,
+                                           bool& capped, int& iters) {
+    capped = false;
+    iters = 0;
+    const JcTrial q = jc_trial(s, c, k, ep, temp);
+    if (!q.active || !q.yields) return 0.0f;
+    const float d = jc_newton(q, ep, dt, iters);
+    capped = iters >= 40;
+    jc_scale(s, q, d);
+    return d;
+}
+// Surrogate inputs of a yielding return (features documented in sph_mlp.cuh); eq_rate is
+// the equivalent deviatoric strain rate sqrt(2/3 e':e').
+__device__ __forceinline__ float4 jc_features(const JcTrial& q, float ep, float dt, float eq_rate) {
+    const float d_hi = (q.vm - q.sy0) / (3.0f * q.G);
+    const float r0 = q.e0d > 0.0f ? eq_rate / q.e0d : 0.0f;
+    const float r1 = (q.e0d > 0.0f && dt > 0.0f) ? d_hi / (dt * q.e0d) : 0.0f;
+    return make_float4(q.vm / q.sy0 - 1.0f, ep, 0.1f * logf(fmaxf(r0, 1.0f)), 0.1f * logf(fmaxf(r1, 1.0f)));
 }
 
 // ------------------------------------------------------------------ pass B
+// Adds a per-thread count, summed over the block, to *dst (one atomic per block).
+__device__ __forceinline__ void block_count_add(unsigned v, unsigned long long* dst) {
+    __shared__ unsigned s_cnt;
+    if (threadIdx.x == 0) s_cnt = 0u;
+    __syncthreads();
+    v = warp_sum(v);
+    if ((threadIdx.x & 31) == 0 && v) atomicAdd(&s_cnt, v);
+    __syncthreads();
+    if (threadIdx.x == 0 && s_cnt && dst) atomicAdd(dst, (unsigned long long)s_cnt);
+}
+
 __global__ void __launch_bounds__(kBlock) k_solid_b(Cst c, Ptr P) {
     int i = blockIdx.x * blockDim.x + threadIdx.x;
     double pw = 0.0, wl = 0.0;
     bool capped_any = false;
+    unsigned newton_solves = 0u, newton_iters = 0u;
     if (i < c.n) {
         const float4* __restrict__ pos = as4c(P.cur.pos);
         const float4* __restrict__ vel = as4c(P.cur.vel);
@@ -483,9 +574,49 @@ __global__ void __launch_bounds__(kBlock) k_solid_b(Cst c, Ptr P) {
         float dprod = 0.0f;
         if (plastic_any) {
             if (c.p.plastic_kind[ki] == 2) {
-                bool capped;
-                dprod = jc_return(sn, c, ki, ep, T_old, dt, capped);
-                capped_any = capped;
+                const bool want_mlp = c.p.jc_surrogate != 0 && P.jc.count != nullptr;
+                const bool want_log = P.jc.log != nullptr;
+                if (want_mlp || want_log) {
+                    const JcTrial q = jc_trial(sn, c, ki, ep, T_old);
+                    if (q.yields) {
+                        float dd = 0.0f;
+#pragma unroll
+                        for (int a = 0; a < 3; ++a)
+#pragma unroll
+                            for (int b = 0; b < 3; ++b) {
+                                const float dv = ed[a][b] - ((a == b) ? tr / 3.0f : 0.0f);
+                                dd += dv * dv;
+                            }
+                        const float4 f = jc_features(q, ep, dt, sqrtf((2.0f / 3.0f) * dd));
+                        if (want_mlp) {
+                            // deferred: k_mlp_tc proposes d, k_jc_finish checks it
+                            const int slot = atomicAdd(P.jc.count, 1);
+                            P.jc.idx[slot] = i;
+                            P.jc.feat[slot] = f;
+                        } else {
+                            int it;
+                            dprod = jc_newton(q, ep, dt, it);
+                            capped_any = it >= 40;
+                            newton_solves = 1;
+                            newton_iters = (unsigned)it;
+                            jc_scale(sn, q, dprod);
+                            const unsigned long long row = atomicAdd(P.jc.log_count, 1ull);
+                            if ((long long)row < P.jc.log_cap) {
+                                const float d_hi = (q.vm - q.sy0) / (3.0f * q.G);
+                                float4* out = reinterpret_cast<float4*>(P.jc.log + 8 * row);
+                                out[0] = f;
+                                out[1] = make_float4(dprod / d_hi, d_hi, q.vm, q.sy0);
+                            }
+                        }
+                    }
+                } else {
+                    bool capped;
+                    int it;
+                    dprod = jc_return(sn, c, ki, ep, T_old, dt, capped, it);
+                    capped_any = capped;
+                    newton_solves = dprod > 0.0f ? 1u : 0u;
+                    newton_iters = (unsigned)it;
+                }
             } else {
                 dprod = j2_return(sn, c.p.mat_G[ki], c.p.plastic_sy0[ki], c.p.plastic_H[ki], ep);
             }
@@ -525,6 +656,67 @@ __global__ void __launch_bounds__(kBlock) k_solid_b(Cst c, Ptr P) {
     if (__syncthreads_or(capped_any) && threadIdx.x == 0) atomicOr(&P.sc->err, SPH_EW_JC_NO_CONVERGE);
     block_sum_atomic(pw, &P.sc->plastic_work);
     block_sum_atomic(wl, &P.sc->leftover_work);
+    if (P.jc.stats) {
+        block_count_add(newton_solves, P.jc.stats + 0);
+        block_count_add(newton_iters, P.jc.stats + 1);
+    }
+}
+
+// Completes the returns deferred to the surrogate: the prediction d = f d_hi is kept when
+// the Johnson-Cook residual |g(d)| is within jc_surrogate_tol of sigma_y(d); otherwise the
+// exact bracketed Newton-bisection runs, as on the plain path.
+__global__ void __launch_bounds__(kBlock) k_jc_finish(Cst c, Ptr P) {
+    const int qi = blockIdx.x * blockDim.x + threadIdx.x;
+    const int cnt = *P.jc.count;
+    double pw = 0.0;
+    bool capped = false;
+    unsigned solved = 0u, iters = 0u, queued = 0u, accepted = 0u;
+    if (qi < cnt) {
+        queued = 1u;
+        const int i = P.jc.idx[qi];
+        const float4 a0 = P.aux[6 * i + 0];
+        float4 a1 = P.aux[6 * i + 1];
+        Sym sn = {a0.x, a0.y, a0.z, a0.w, a1.x, a1.y};
+        float ep = a1.z;
+        const int k = eos_of(P, i);
+        const float T_old = P.cur.sdev[8 * i + 7];
+        const float dt = P.sc->dt;
+        const JcTrial q = jc_trial(sn, c, k, ep, T_old);
+        if (q.yields) {
+            const float d_hi = (q.vm - q.sy0) / (3.0f * q.G);
+            const float f = 1.0f - 0.1f * P.jc.fpred[qi];    // the network's u = 10 (1 - d / d_hi)
+            float d = 0.0f;
+            bool ok = false;
+            if (f > 0.0f && f <= 1.0f) {              // false for NaN
+                d = f * d_hi;
+                float g, dg;
+                jc_residual(d, q.vm, q.G, q.A, q.B, q.nn, q.C, q.e0d, q.mt, ep, dt, g, dg);
+                const float sy = q.vm - 3.0f * q.G * d - g;
+                ok = sy > 0.0f && fabsf(g) <= c.p.jc_surrogate_tol * sy;
+            }
+            if (ok) {
+                accepted = 1u;
+            } else {
+                int it;
+                d = jc_newton(q, ep, dt, it);
+                capped = it >= 40;
+                solved = 1u;
+                iters = (unsigned)it;
+            }
+            jc_scale(sn, q, d);
+            ep += d;
+            pw = (double)(P.cur.pos[4 * i + 3] * vm_sym(sn) * d);
+            P.aux[6 * i + 0] = make_float4(sn.xx, sn.yy, sn.zz, sn.xy);
+            a1.x = sn.xz; a1.y = sn.yz; a1.z = ep;
+            P.aux[6 * i + 1] = a1;
+        }
+    }
+    if (__syncthreads_or(capped) && threadIdx.x == 0) atomicOr(&P.sc->err, SPH_EW_JC_NO_CONVERGE);
+    block_sum_atomic(pw, &P.sc->plastic_work);
+    block_count_add(solved, P.jc.stats + 0);
+    block_count_add(iters, P.jc.stats + 1);
+    block_count_add(queued, P.jc.stats + 2);
+    block_count_add(accepted, P.jc.stats + 3);
 }
 
 // ------------------------------------------------------------------ commit + volume + EOS
@@ -923,6 +1115,14 @@ inline int solid_substep_launch(const Cst& c, const Ptr& P, int n, cudaStream_t 
         if (c.p.kernel_correction) { k_kc_inverse<<<nb, kBlock, 0, st>>>(c, P); mark("k_kc_inverse"); }
         k_solid_a<<<nb, kBlock, 0, st>>>(c, P); mark("k_solid_a");
         k_solid_b<<<nb, kBlock, 0, st>>>(c, P); mark("k_solid_b");
+        if (c.p.jc_surrogate && P.jc.count) {
+            const int tiles = (n + kMlpTileRows - 1) / kMlpTileRows;
+            const int g = std::min(2 * 148, std::max(tiles, 1));
+            k_mlp_tc<<<g, kMlpTcThreads, 0, st>>>(P.jc.W, static_cast<const __nv_bfloat16*>(P.jc.packed),
+                                                 P.jc.feat, n, P.jc.count, P.jc.fpred, &P.sc->err);
+            mark("k_mlp_tc");
+            k_jc_finish<<<nb, kBlock, 0, st>>>(c, P); mark("k_jc_finish");
+        }
     }
     if (in(SPH_STAGE_CONTINUITY)) { k_solid_commit<<<nb, kBlock, 0, st>>>(c, P); mark("k_solid_commit"); }
     if (in(SPH_STAGE_FORCES)) { k_solid_force<<<nb, kBlock, 0, st>>>(c, P); mark("k_solid_force"); }
@@ -949,6 +1149,33 @@ inline int solid_substep_launch(const Cst& c, const Ptr& P, int n, cudaStream_t 
     return SPH_OK;
 }
 
-inline void solid_reduce_extra(const Cst&, const Ptr&, int, cudaStream_t) {}
+// HypoElasticSolver.compute_elastic_energy (SOLID.py:2296-2322): per particle of a
+// material with G > 0, 0.5 K theta^2 V + 0.25 (s:s) V / G with theta = rho / rho0 - 1,
+// in float32 as the reference evaluates it, summed in FP64.
+__global__ void __launch_bounds__(kBlock) k_solid_elastic(Cst c, Ptr P) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    double e = 0.0;
+    if (i < c.n) {
+        const int k = eos_of(P, i);
+        const float G = (k >= 0 && k < 4) ? c.p.mat_G[k] : 0.0f;
+        if (G > 0.0f) {
+            const float K = c.p.mat_K[k], rho0 = c.p.mat_rho0[k];
+            const float V = P.cur.pos[4 * i + 3];
+            const float rho = P.cur.vel[4 * i + 3] / V;
+            const float theta = (rho - rho0) / rho0;
+            const float u_vol = 0.5f * K * theta * theta * V;
+            const Sym sd = load_s(P.cur.sdev, i);
+            const float ss = sd.xx * sd.xx + sd.yy * sd.yy + sd.zz * sd.zz +
+                             2.0f * (sd.xy * sd.xy + sd.xz * sd.xz + sd.yz * sd.yz);
+            const float u_dev = 0.25f * ss / G * V;
+            e = (double)(u_vol + u_dev);
+        }
+    }
+    block_sum_atomic(e, &P.ac->red[SPH_RED_ELASTIC]);
+}
+
+inline void solid_reduce_extra(const Cst& c, const Ptr& P, int n, cudaStream_t st) {
+    k_solid_elastic<<<grid_of(n), kBlock, 0, st>>>(c, P);
+}
 
 }  // namespace sph

@@ -313,6 +313,34 @@ class HypoElasticSolver(_SolverBase):
                         "force": np.array([s.constraint_force[k][d] for d in range(3)])})
         return out
 
+    # ------------------------------------------------------------------ JC surrogate
+    def enable_jc_surrogate(self, surrogate, tol=1e-3):
+        """Johnson-Cook returns proposed by `surrogate` (a JCSurrogate) on the tensor
+        cores and kept where |g| / sigma_y <= tol; the exact Newton elsewhere."""
+        self._jc_surrogate = surrogate          # keeps its parameters alive
+        abi.check(self.L.sph_jc_surrogate(self.h, C.c_void_p(surrogate.W.data_ptr()), C.c_float(tol),
+                                          1, _stream_ptr()), "sph_jc_surrogate")
+
+    def disable_jc_surrogate(self):
+        abi.check(self.L.sph_jc_surrogate(self.h, None, C.c_float(1.0), 0, _stream_ptr()),
+                  "sph_jc_surrogate")
+
+    def attach_jc_log(self, rows, count):
+        """Log every exact Johnson-Cook return into rows [cap][8] (float32 CUDA tensor),
+        counting into count (one int64 CUDA tensor); None detaches."""
+        self._jc_log = (rows, count)
+        if rows is None:
+            abi.check(self.L.sph_jc_log(self.h, None, 0, None), "sph_jc_log")
+            return
+        abi.check(self.L.sph_jc_log(self.h, C.c_void_p(rows.data_ptr()), rows.shape[0],
+                                    C.c_void_p(count.data_ptr())), "sph_jc_log")
+
+    def jc_stats(self, reset=False):
+        """{newton_solves, newton_iterations, proposals, accepted} since the last reset."""
+        out = (C.c_uint64 * 4)()
+        abi.check(self.L.sph_jc_stats(self.h, out, int(bool(reset)), _stream_ptr()), "sph_jc_stats")
+        return dict(zip(("newton_solves", "newton_iterations", "proposals", "accepted"), list(out)))
+
     def energy_budget(self):
         r = self._reduce()
         s = self._scalars()

@@ -223,3 +223,29 @@ def test_grip_force_and_time_bookkeeping(cuda):
     F0, F1 = d[0]["force"][0], d[1]["force"][0]
     assert F0 > 0 and F1 < 0 and abs(F0 + F1) <= 0.05 * abs(F0)
     assert d[1]["displacement"][0] == pytest.approx(10.0 * sv.load_s[None], rel=1e-5)
+
+
+def test_solid_reductions_match_numpy(cuda):
+    """HypoElasticSolver energy reductions (SOLID.py:2296-2322, sph_base.py:451-507) on a
+    perturbed plastic state against float64 numpy sums of the same fields."""
+    ps = ParticleSystem(SimConfig(bar3d_deck()), device="cuda")
+    perturb_solid(ps)
+    sv = ps.build_solver()
+    st = ps.state_numpy()
+    V = st["pos"][:, 3].astype(np.float64)
+    m = st["vel"][:, 3].astype(np.float64)
+    v = st["vel"][:, :3].astype(np.float64)
+    s = st["sdev"][:, :6].astype(np.float64)
+    p = build_params(ps)
+    K, G, rho0 = float(p.mat_K[0]), float(p.mat_G[0]), float(p.mat_rho0[0])
+    theta = (m / V - rho0) / rho0
+    ss = (s[:, :3] ** 2).sum(1) + 2.0 * (s[:, 3:] ** 2).sum(1)
+    elastic = (0.5 * K * theta ** 2 * V + 0.25 * ss / G * V).sum()
+    ke = (0.5 * m * (v ** 2).sum(1)).sum()
+    ie = (m * st["shift"][:, 3].astype(np.float64)).sum()
+    assert sv.compute_elastic_energy() == pytest.approx(elastic, rel=1e-5)
+    assert sv.compute_kinetic_energy() == pytest.approx(ke, rel=1e-5)
+    assert sv.compute_internal_energy() == pytest.approx(ie, rel=1e-5)
+    assert sv.compute_total_mass() == pytest.approx(m.sum(), rel=1e-6)
+    P = sv.compute_momentum()
+    assert np.abs(P - (m[:, None] * v).sum(0)).max() <= 1e-5 * (m[:, None] * np.abs(v)).sum()

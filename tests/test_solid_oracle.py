@@ -114,3 +114,20 @@ def test_free_block_conserves_momentum():
     gross = (r["m"][:, None] * np.abs(r["v"])).sum(0)
     assert np.abs(P1 - P0).max() <= 1e-10 * gross.max()
     assert r["eps_p"].max() > 0.0       # the random field yields somewhere
+
+
+def test_mlp_oracle_gradient_matches_finite_differences():
+    """The float64 surrogate-MLP oracle (the checker of the GPU training kernels):
+    analytic gradient against central differences."""
+    from oracle import mlp
+    rng = np.random.default_rng(5)
+    w = rng.normal(0.0, 0.3, mlp.N_PARAMS)
+    X = rng.uniform(0.0, 1.0, (7, 4))
+    T = rng.uniform(0.5, 1.0, 7)
+    _, g = mlp.loss_and_grad(w, X, T)
+    idx = rng.choice(mlp.N_PARAMS, 40, replace=False)
+    for q in idx:
+        e = np.zeros_like(w)
+        e[q] = 1e-6
+        fd = (mlp.loss_and_grad(w + e, X, T)[0] - mlp.loss_and_grad(w - e, X, T)[0]) / 2e-6
+        assert fd == pytest.approx(g[q], rel=1e-5, abs=1e-9)
