@@ -255,6 +255,9 @@ def main():
     ap.add_argument("--workload", default="dambreak3d",
                     choices=("dambreak3d", "tensile_bar3d", "tensile_bar3d_jc"))
     ap.add_argument("--dx", type=float, default=None)
+    ap.add_argument("--jc-surrogate", default=None,
+                    help="tensile_bar3d_jc only: surrogate parameters (.npy), e.g. "
+                         "sigmasph_b200/data/jc_surrogate_config0.npy")
     ap.add_argument("--e2e-steps", type=int, default=None)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--profile-steps", type=int, default=4)
@@ -282,6 +285,12 @@ def main():
     if rank == 0 and ws == 1 and not args.no_cpu_baseline:
         cpu_ps = ParticleSystem(SimConfig(scene), device="cpu")
     solver = ps.build_solver()
+    if args.jc_surrogate:
+        if args.workload != "tensile_bar3d_jc":
+            raise SystemExit("--jc-surrogate applies to --workload tensile_bar3d_jc")
+        from sigmasph_b200.surrogate import JCSurrogate
+        solver.enable_jc_surrogate(JCSurrogate.load(args.jc_surrogate), tol=1e-3)
+        desc = dict(desc, jc_surrogate=os.path.basename(args.jc_surrogate), jc_surrogate_tol=1e-3)
     solver.initialize()
     stream = torch.cuda.current_stream()
 

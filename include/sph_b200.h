@@ -287,7 +287,7 @@ int  sph_reduce_noalloc(const SphParams* p, const float* pos, const float* vel,
  * map is the Newton-bisection of MAT002_johnson_cook.py:251-354, called from
  * SOLID.py:2889-2913).  A 4 -> 64 -> 64 -> 64 -> 1 SiLU MLP of sph_mlp_param_count()
  * float32 parameters (W1[64][4], b1, W2[64][64], b2, W3[64][64], b3, W4[64], b4) maps the
- * features of a yielding return, f0 = vm/sigma_y0 - 1, f1 = eps_p,
+ * features of a yielding return, f0 = ln(max(vm/sigma_y0 - 1, 1e-8))/10, f1 = eps_p,
  * f2 = ln(max(eps_dot_eq/eps0_dot, 1))/10, f3 = ln(max(d_hi/(dt eps0_dot), 1))/10, to
  * u = 10 (1 - d/d_hi), with d_hi = (vm - sigma_y0)/(3G).  Every pointer is device memory; X rows are
  * float4 (16-byte aligned), Y and T one float per row.  Calls are asynchronous on stream. */

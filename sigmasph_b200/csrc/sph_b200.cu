@@ -680,7 +680,7 @@ int sph_mlp_infer_tc(const float* W, const void* packed, const float* X, int64_t
     if (reinterpret_cast<uintptr_t>(packed) % 16 || reinterpret_cast<uintptr_t>(X) % 16) return SPH_ERR_ARG;
     if (n == 0) return SPH_OK;
     const int tiles = (int)((n + kMlpTileRows - 1) / kMlpTileRows);
-    k_mlp_tc<<<std::min(2 * 148, tiles), kMlpTcThreads, 0, S(stream)>>>(
+    k_mlp_tc<<<std::min(kMlpCtasPerSm * 148, tiles), kMlpTcThreads, 0, S(stream)>>>(
         W, static_cast<const __nv_bfloat16*>(packed), reinterpret_cast<const float4*>(X), (int)n, nullptr, Y, err);
     CK(cudaGetLastError());
     return SPH_OK;

@@ -459,7 +459,8 @@ __device__ __forceinline__ float4 jc_features(const JcTrial& q, float ep, float 
     const float d_hi = (q.vm - q.sy0) / (3.0f * q.G);
     const float r0 = q.e0d > 0.0f ? eq_rate / q.e0d : 0.0f;
     const float r1 = (q.e0d > 0.0f && dt > 0.0f) ? d_hi / (dt * q.e0d) : 0.0f;
-    return make_float4(q.vm / q.sy0 - 1.0f, ep, 0.1f * logf(fmaxf(r0, 1.0f)), 0.1f * logf(fmaxf(r1, 1.0f)));
+    return make_float4(0.1f * logf(fmaxf(q.vm / q.sy0 - 1.0f, 1e-8f)), ep, 0.1f * logf(fmaxf(r0, 1.0f)),
+                       0.1f * logf(fmaxf(r1, 1.0f)));
 }
 
 // ------------------------------------------------------------------ pass B
@@ -1117,7 +1118,7 @@ inline int solid_substep_launch(const Cst& c, const Ptr& P, int n, cudaStream_t 
         k_solid_b<<<nb, kBlock, 0, st>>>(c, P); mark("k_solid_b");
         if (c.p.jc_surrogate && P.jc.count) {
             const int tiles = (n + kMlpTileRows - 1) / kMlpTileRows;
-            const int g = std::min(2 * 148, std::max(tiles, 1));
+            const int g = std::min(kMlpCtasPerSm * 148, std::max(tiles, 1));
             k_mlp_tc<<<g, kMlpTcThreads, 0, st>>>(P.jc.W, static_cast<const __nv_bfloat16*>(P.jc.packed),
                                                  P.jc.feat, n, P.jc.count, P.jc.fpred, &P.sc->err);
             mark("k_mlp_tc");

@@ -18,6 +18,12 @@ n 0.65, C 0.02, reference rate 1/ms), hourglass damper alpha 4, Colle shifting w
 fixed Mach 0.05 and ALE transport, delta 0.1, viscosity 0.02.  The grips are the
 outer 10 mm of each head, pulled apart by 1 mm each over a 1 ms smoothstep ramp
 (1 m/s on average).  Units mm, GPa, ms.  dx = 0.113 mm lays about 2.3M particles.
+
+`tensile_axi_gauge(dx, speed)` is the same bar as an axisymmetric (x axial, y = r from
+dx/2) half-section: about 26k particles at dx = 0.1 mm, Johnson-Cook steel (A 0.31,
+B 1.0 GPa, n 0.65; C and the reference rate selectable), hourglass damper sub-cycled,
+the outer 10 mm of each head pulled apart by 1 mm over a smoothstep ramp lasting
+1 mm / speed (speed in m/s = mm/ms).
 """
 from __future__ import annotations
 
@@ -106,6 +112,44 @@ def tensile_bar3d(dx=0.113, plasticity="j2", hourglass_subcycle=False, cfl=0.3):
              "components": "xyz", "displacement": [0.0, -1.0, 0.0]},
             {"name": "high", "region": [[-r - 1, grip, -r - 1], [r + 1, half + 1, r + 1]],
              "components": "xyz", "displacement": [0.0, 1.0, 0.0]}],
+    }
+
+
+def tensile_axi_gauge(dx=0.1, speed=1.0, C=0.0, eps0_dot=1.0, cfl=0.3, disp=1.0):
+    gauge_d, gauge_l, head_d, head_l, fillet = 6.0, 30.0, 10.0, 15.0, 3.0
+    red = 0.5 * (head_d - gauge_d)
+    shoulder = math.sqrt(red * (2.0 * fillet - red))
+    half = 0.5 * gauge_l + shoulder + head_l
+    grip = half - 10.0
+    r = 0.5 * head_d
+    return {
+        "Domain": {"particleRadius": 0.5 * dx, "supportRadiusFactor": 6.0, "axisymmetric": True,
+                   "boundary": "open"},
+        "Time": {"CFL": cfl},
+        "Solver": {"type": "hypoElastic", "viscosity": 0.02, "allowNegativePressure": True},
+        "Materials": [{"name": "steel", "density0": 7.9e-6, "eos": {"type": "linear"},
+                       "strength": {"type": "hypoElastic", "youngsModulus": 200.0,
+                                    "poissonRatio": 0.3,
+                                    "plasticity": {"model": "johnson_cook", "A": 0.31, "B": 1.0,
+                                                   "n": 0.65, "C": C, "eps0_dot": eps0_dot,
+                                                   "T0": 293.0, "Tm": 0.0}}}],
+        "Load": {"gravitation": [0.0, 0.0, 0.0], "rampTime": disp / speed},
+        "Diffusion": {"delta": 0.1},
+        "Shifting": {"enabled": True, "mode": "colle", "maMode": "fixed", "maFixed": 0.05,
+                     "aleMomentum": True, "aleHistory": True},
+        "Hourglass": {"alpha": 4.0, "superTimeStepping": {"mode": "subcycle"}},
+        "SolidBlocks": [{"objectId": 0, "start": [-half, 0.5 * dx, 0.0], "end": [half, r, 0.5 * dx],
+                         "translation": [0, 0, 0], "scale": [1, 1, 1], "velocity": [0, 0, 0],
+                         "density": 7.9e-6, "color": [200, 120, 60], "material": "steel",
+                         "shape": {"type": "gaugedogboneaxi", "tabWidth": head_d,
+                                   "tabHeight": head_l, "gaugeWidth": gauge_d,
+                                   "radius": fillet, "gaugeLength": gauge_l,
+                                   "center": [0.0, 0.0, 0.0]}}],
+        "Constraints": [
+            {"name": "left", "region": [[-half - 1, -1, -1], [-grip, r + 1, 1]],
+             "components": "xy", "displacement": [-disp, 0.0, 0.0]},
+            {"name": "right", "region": [[grip, -1, -1], [half + 1, r + 1, 1]],
+             "components": "xy", "displacement": [disp, 0.0, 0.0]}],
     }
 
 

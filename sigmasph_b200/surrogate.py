@@ -25,7 +25,7 @@ from . import abi
 from .config import SimConfig
 from .particle_system import ParticleSystem
 
-FEATURES = ("vm / sigma_y0 - 1", "eps_p", "ln(max(eps_dot_eq / eps0_dot, 1)) / 10",
+FEATURES = ("ln(max(vm / sigma_y0 - 1, 1e-8)) / 10", "eps_p", "ln(max(eps_dot_eq / eps0_dot, 1)) / 10",
             "ln(max(d_hi / (dt eps0_dot), 1)) / 10")
 LOG_COLUMNS = FEATURES + ("d / d_hi", "d_hi", "vm", "sigma_y0")
 
@@ -159,3 +159,128 @@ def collect_returns(scene, steps, capacity, perturb=None, device="cuda"):
     sv.attach_jc_log(None, None)
     data = rows[:m].clone()
     return data[:, :4].contiguous(), data[:, 4].contiguous(), data
+
+
+def config0_samples(total=5_000_000, rates=None, seed=20260101, dx=0.1, C=0.02, eps0_dot=1.0,
+                    chunk=2000, max_steps=200_000, device="cuda"):
+    """Exact returns logged from the axisymmetric parallel-gauge bar (scenes.tensile_axi_gauge)
+    pulled at grip speeds drawn log-uniformly from [0.1, 10] m/s, an equal quota per run.
+    Returns (X, F, speeds)."""
+    from .scenes import tensile_axi_gauge
+    rng = np.random.default_rng(seed)
+    if rates is None:
+        rates = np.exp(rng.uniform(np.log(0.1), np.log(10.0), 8))
+    quota = int(total // len(rates))
+    Xs, Fs = [], []
+    for v in rates:
+        ps = ParticleSystem(SimConfig(tensile_axi_gauge(dx=dx, speed=float(v), C=C, eps0_dot=eps0_dot)),
+                            device=device)
+        sv = ps.build_solver()
+        rows = torch.zeros((quota, 8), dtype=torch.float32, device=device)
+        count = torch.zeros(1, dtype=torch.int64, device=device)
+        sv.attach_jc_log(rows, count)
+        sv.initialize()
+        done = 0
+        while done < max_steps:
+            sv.step_many(chunk)
+            done += chunk
+            if int(count.item()) >= quota:
+                break
+        sv.attach_jc_log(None, None)
+        m = min(int(count.item()), quota)
+        Xs.append(rows[:m, :4].clone())
+        Fs.append(rows[:m, 4].clone())
+        del sv, ps
+    return torch.cat(Xs), torch.cat(Fs), list(map(float, rates))
+
+
+def force_displacement(scene, surrogate=None, tol=1e-3, record_every=50, t_end=None, device="cuda"):
+    """Runs a solid scene to t_end (default: its load ramp) recording the right grip's
+    force and displacement along the pull axis every `record_every` steps; returns
+    (disp, force, ms_per_step, stats)."""
+    ps = ParticleSystem(SimConfig(scene), device=device)
+    sv = ps.build_solver()
+    if surrogate is not None:
+        sv.enable_jc_surrogate(surrogate, tol=tol)
+    sv.initialize()
+    t_end = t_end if t_end is not None else float(ps.cfg.get_cfg("rampTime"))
+    axis = int(np.argmax(np.abs(np.array(ps.cfg.get_constraints()[-1]["displacement"]))))
+    sv.jc_stats(reset=True)
+    disp, force = [], []
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    steps = 0
+    e0.record()
+    while sv.sim_time < t_end:
+        sv.step_many(record_every)
+        steps += record_every
+        d = sv.get_constraint_data()[-1]
+        disp.append(float(d["displacement"][axis]))
+        force.append(float(d["force"][axis]))
+    e1.record()
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1) / max(steps, 1)
+    return np.array(disp), np.array(force), ms, sv.jc_stats()
+
+
+def compare_bar(surrogate, dx=0.4, tol=1e-3, record_every=50, device="cuda"):
+    """Plain vs surrogate on the Johnson-Cook 3D round bar (scenes.tensile_bar3d, grips
+    +-1 mm over 1 ms): peak-force error and L2 error of the force-displacement curve."""
+    from .scenes import tensile_bar3d
+    sc = tensile_bar3d(dx=dx, plasticity="jc", hourglass_subcycle=True)
+    dp, fp, msp, sp = force_displacement(sc, None, tol, record_every, device=device)
+    ds, fs, mss, ss = force_displacement(sc, surrogate, tol, record_every, device=device)
+    m = min(len(fp), len(fs))
+    peak_p, peak_s = float(np.max(np.abs(fp))), float(np.max(np.abs(fs)))
+    return {"dx_mm": dx, "records": m,
+            "peak_force_plain": peak_p, "peak_force_surrogate": peak_s,
+            "peak_force_rel_err": abs(peak_s - peak_p) / peak_p,
+            "curve_l2_rel_err": float(np.linalg.norm(fs[:m] - fp[:m]) / np.linalg.norm(fp[:m])),
+            "ms_per_step_plain": msp, "ms_per_step_surrogate": mss,
+            "stats_plain": sp, "stats_surrogate": ss,
+            "curve_plain": [[float(a), float(b)] for a, b in zip(dp[:m], fp[:m])],
+            "curve_surrogate": [[float(a), float(b)] for a, b in zip(ds[:m], fs[:m])]}
+
+
+def main(argv=None):
+    import argparse
+    import json
+    import time
+    ap = argparse.ArgumentParser(description="Train / evaluate the Johnson-Cook return-map surrogate")
+    sub = ap.add_subparsers(dest="cmd", required=True)
+    t = sub.add_parser("train", help="log config-0 returns, train, save the parameters")
+    t.add_argument("--out", required=True)
+    t.add_argument("--samples", type=int, default=5_000_000)
+    t.add_argument("--steps", type=int, default=20000)
+    t.add_argument("--batch", type=int, default=8192)
+    c = sub.add_parser("compare", help="plain vs surrogate force-displacement on the 3D JC bar")
+    c.add_argument("--weights", required=True)
+    c.add_argument("--dx", type=float, default=0.4)
+    c.add_argument("--out", default=None)
+    a = ap.parse_args(argv)
+    if a.cmd == "train":
+        t0 = time.time()
+        X, F, rates = config0_samples(total=a.samples)
+        t1 = time.time()
+        sur = JCSurrogate()
+        hist = sur.fit(X, F, steps=a.steps, batch=a.batch, lr=3e-3, lr_final=3e-5,
+                       log_every=max(a.steps // 10, 1))
+        t2 = time.time()
+        sur.save(a.out)
+        u = sur.predict(X[:200000])
+        err = (u - JCSurrogate.target(F[:200000])).abs()
+        print(json.dumps({"samples": int(X.shape[0]), "speeds_mps": rates, "loss": hist,
+                          "collect_s": t1 - t0, "train_s": t2 - t1,
+                          "abs_err_u_tc_p50": float(err.median()),
+                          "abs_err_u_tc_p99": float(err.quantile(0.99))}))
+    else:
+        res = compare_bar(JCSurrogate.load(a.weights), dx=a.dx)
+        line = {k: v for k, v in res.items() if not k.startswith("curve")}
+        print(json.dumps(line))
+        if a.out:
+            with open(a.out, "w") as f:
+                json.dump(res, f)
+    return 0
+
+
+if __name__ == "__main__":
+    raise SystemExit(main())

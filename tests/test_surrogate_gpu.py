@@ -99,7 +99,7 @@ def test_logged_returns_are_exact_fractions(cuda, trained):
 
 def test_surrogate_in_solver_matches_plain_and_saves_newton(cuda, trained):
     sur, X, T, hist = trained
-    assert hist[-1] < 0.1 * hist[0]
+    assert hist[-1] < 0.2 * hist[0]
     deck = scene_path("tensile_axi_dogbone_dx0.1.json")
     runs = {}
     for mode in ("plain", "surrogate"):
