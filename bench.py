@@ -246,6 +246,69 @@ def run_reference(args):
     return 0
 
 
+def run_strips(args):
+    """256 plane-strain Johnson-Cook strips (2k-60k particles each, ~6M in all) as packed
+    size buckets with autotuned block sizes; a step is one step of every strip (each with
+    its own dt), two steps per CUDA-graph launch."""
+    import torch
+    from sigmasph_b200.ensemble import Ensemble, strip_specs
+    ws, rank, local = dist_setup()
+    torch.cuda.set_device(local)
+    specs = strip_specs(256)
+    ens = Ensemble(specs, buckets=args.buckets)
+    tune = ens.autotune(candidates=(64, 128, 256), steps=4)
+    ens.capture()
+    for _ in range(max(args.warmup // 2, 2)):
+        ens.step2()
+    torch.cuda.synchronize()
+    n = ens.particles
+    K2 = max(args.steps // 2, 1)
+    clocks = ClockSampler(local)
+    clocks.start()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(K2):
+        ens.step2()
+    e1.record()
+    torch.cuda.synchronize()
+    ck = clocks.stop()
+    ms = e0.elapsed_time(e1)
+    value = n * 2 * K2 / (ms / 1000.0)
+    # end to end: after every launch read every strip's state (clock, dt, grip forces)
+    t0 = time.perf_counter()
+    nread = 0
+    for _ in range(K2):
+        ens.step2()
+        for b in ens.buckets:
+            nread += len(b.state())
+    el = time.perf_counter() - t0
+    from sigmasph_b200 import abi
+    import ctypes as C
+    d2h = C.sizeof(abi.SphInstState) * len(specs) // 2
+    launches = 0
+    for b in ens.buckets:                     # kernels of one step, counted on an eager step
+        b.solver.profile(True)
+        b.solver.profile_read()
+        b.solver.step()
+        launches += sum(cnt for _, cnt in b.solver.profile_read().values())
+        b.solver.profile(False)
+    line = {"metric": "particle-steps/s on 1 B200 (256 plane-strain strip ensemble)", "value": value,
+            "unit": UNIT, "n_gpus": ws, "steps": 2 * K2, "warmup": args.warmup,
+            "ms_per_step": ms / (2 * K2), "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": {"workload": "256 plane-strain JC strips, packed size buckets, one graph launch per 2 steps",
+                       "particles": n, "strips": len(specs), "buckets": tune,
+                       "l2": "inputs larger than L2 (state + neighbour lists > 1 GB)"},
+            "e2e": {"value": n * 2 * K2 / el, "unit": UNIT, "h2d_bytes_per_step": 0,
+                    "d2h_bytes_per_step": d2h},
+            "gpu_launches": launches * 2 * K2}
+    if ck is not None:
+        line["clocks"] = ck
+    if rank == 0:
+        print(json.dumps(line))
+    return 0
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -253,7 +316,8 @@ def main():
     ap.add_argument("--warmup", type=int, default=6)
     ap.add_argument("--impl", default="b200", choices=("b200", "reference"))
     ap.add_argument("--workload", default="dambreak3d",
-                    choices=("dambreak3d", "tensile_bar3d", "tensile_bar3d_jc"))
+                    choices=("dambreak3d", "tensile_bar3d", "tensile_bar3d_jc", "strips256"))
+    ap.add_argument("--buckets", type=int, default=4, help="strips256: size buckets")
     ap.add_argument("--dx", type=float, default=None)
     ap.add_argument("--jc-surrogate", default=None,
                     help="tensile_bar3d_jc only: surrogate parameters (.npy), e.g. "
@@ -266,6 +330,8 @@ def main():
         args.warmup = 3
     if args.impl == "reference":
         return run_reference(args)
+    if args.workload == "strips256":
+        return run_strips(args)
 
     import torch
     ws, rank, local = dist_setup()

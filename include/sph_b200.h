@@ -200,6 +200,39 @@ typedef struct SphScalars {
     double  constraint_disp[8][3];
 } SphScalars;
 
+/* ---- Solid material rows and ensemble instances (no counterpart in the reference,
+ * which runs one scene per process: run_simulation.py:649-708).  A solid handle keeps
+ * its material rows in device memory (built from SphParams for an ordinary scene).  An
+ * ensemble packs many independent scenes into one handle: instance k's particles carry
+ * material row k, each instance has its own time step, clock, load ramp, damper stage
+ * count and two grips, and the instances are placed far enough apart that no pair
+ * crosses between them. */
+typedef struct SphMatRow {
+    float   rho0, K, G, cp, c0, delta;   /* as SphParams mat_*                              */
+    int32_t plastic_kind;                /* 0 none, 1 J2, 2 Johnson-Cook                    */
+    float   sy0, H;                      /* J2 / JC: yield stress at zero plastic strain, H */
+    float   jc_A, jc_B, jc_n, jc_C, jc_eps0_dot, jc_T0, jc_Tm, jc_m, jc_chi;
+    float   cv, stiff, gamma, T0;        /* specific heat, EOS stiffness / exponent, T ref   */
+} SphMatRow;
+
+typedef struct SphInstRow {              /* constants of one ensemble instance               */
+    float   c_signal;                    /* CFL floor speed                                  */
+    float   hg_rate;                     /* hourglass damper rate (sub-cycle count)          */
+    float   ramp_time;                   /* load ramp                                        */
+    float   c0;                          /* speed c0 of delta-SPH and the Colle shift        */
+    float   visc_coef;                   /* Morris viscosity coefficient 10 nu               */
+    float   reserved[3];
+} SphInstRow;
+
+typedef struct SphInstState {            /* per-instance device state (sph_ensemble_state)  */
+    double  sim_time;
+    float   dt, load_s, load_sdot;
+    int32_t sts_stages;
+    uint32_t max_c_sq_bits, max_accel_bits;  /* internal: the step's dt maxima           */
+    double  constraint_force[2][3];      /* grips 0 and 1 (FP64, x 2 pi if axisymmetric)    */
+    double  constraint_disp[2][3];
+} SphInstState;
+
 /* Reduction indices of sph_reduce(). */
 enum {
     SPH_RED_KE = 0, SPH_RED_KE_OFFGRID, SPH_RED_PE, SPH_RED_SE, SPH_RED_IE,
@@ -320,6 +353,18 @@ int  sph_jc_log(SphHandle* h, float* rows, int64_t capacity, unsigned long long*
 /* Counters since the last reset: {Newton solves, Newton iterations, surrogate proposals,
  * proposals accepted}; reset != 0 zeroes them after the read (synchronises stream). */
 int  sph_jc_stats(SphHandle* h, uint64_t* out, int reset, void* stream);
+
+/* Turns a solid handle into an ensemble of n_inst instances (1 <= n_inst <= 1024):
+ * mat[k] and inst[k] are instance k's material row and constants (host arrays, copied),
+ * every particle's material id (bcdisp.w) must be its instance, constraint ids (bc.y)
+ * 0 or 1 within the instance; dt0[k] (host) is the first step of instance k.  n_inst = 0
+ * returns the handle to single-scene mode. */
+int  sph_ensemble_set(SphHandle* h, const SphMatRow* mat, const SphInstRow* inst, int n_inst,
+                      const float* dt0, void* stream);
+/* Copies the per-instance state into out[n_inst] (host; synchronises stream). */
+int  sph_ensemble_state(SphHandle* h, SphInstState* out, int n_inst, void* stream);
+/* Threads per block of the particle kernels (a multiple of 32, 64..256; 0 = 256). */
+int  sph_set_block(SphHandle* h, int threads);
 
 /* Stage ids for sph_run_stage. */
 enum {

@@ -117,6 +117,26 @@ class SphError(RuntimeError):
         super().__init__(msg)
 
 
+class SphMatRow(C.Structure):
+    _fields_ = [(k, C.c_float) for k in ("rho0", "K", "G", "cp", "c0", "delta")] + \
+               [("plastic_kind", C.c_int32)] + \
+               [(k, C.c_float) for k in ("sy0", "H", "jc_A", "jc_B", "jc_n", "jc_C", "jc_eps0_dot",
+                                         "jc_T0", "jc_Tm", "jc_m", "jc_chi", "cv", "stiff", "gamma",
+                                         "T0")]
+
+
+class SphInstRow(C.Structure):
+    _fields_ = [("c_signal", C.c_float), ("hg_rate", C.c_float), ("ramp_time", C.c_float),
+                ("c0", C.c_float), ("visc_coef", C.c_float), ("reserved", C.c_float * 3)]
+
+
+class SphInstState(C.Structure):
+    _fields_ = [("sim_time", C.c_double), ("dt", C.c_float), ("load_s", C.c_float),
+                ("load_sdot", C.c_float), ("sts_stages", C.c_int32), ("max_c_sq_bits", C.c_uint32),
+                ("max_accel_bits", C.c_uint32), ("constraint_force", (C.c_double * 3) * 2),
+                ("constraint_disp", (C.c_double * 3) * 2)]
+
+
 _LIB = None
 
 
@@ -165,6 +185,9 @@ def lib():
         "sph_jc_surrogate": (C.c_int, [vp, vp, C.c_float, C.c_int, vp]),
         "sph_jc_log": (C.c_int, [vp, vp, i64, vp]),
         "sph_jc_stats": (C.c_int, [vp, C.POINTER(C.c_uint64), C.c_int, vp]),
+        "sph_ensemble_set": (C.c_int, [vp, vp, vp, C.c_int, vp, vp]),
+        "sph_ensemble_state": (C.c_int, [vp, vp, C.c_int, vp]),
+        "sph_set_block": (C.c_int, [vp, C.c_int]),
     }
     for name, (res, args) in sig.items():
         f = getattr(L, name)

@@ -119,6 +119,9 @@ Ptr make_ptr(SphHandle* h) {
     P.sc = h->sc;
     P.ac = h->ac;
     P.jc = solid_jc_ptr(h->solid);
+    P.mat = h->solid.mat;
+    P.irow = h->solid.irow;
+    P.inst = h->solid.inst;
     return P;
 }
 
@@ -306,7 +309,8 @@ int sph_create(const SphParams* p, int64_t n_max, SphHandle** out) {
         delete h;
         return r;
     }
-    if (p->is_solid && (r = solid_alloc(h->solid, *p, n_max)) != SPH_OK) {
+    if (p->is_solid && ((r = solid_alloc(h->solid, *p, n_max)) != SPH_OK ||
+                        (r = solid_sync_rows(h->solid, h->p, h->c)) != SPH_OK)) {
         free_all(h);
         delete h;
         return r;
@@ -354,12 +358,14 @@ int sph_parity(const SphHandle* h) { return h ? h->parity : -1; }
 int sph_set_params(SphHandle* h, const SphParams* p) {
     if (!h || !p || p->struct_size != (int32_t)sizeof(SphParams)) return SPH_ERR_ARG;
     if (p->is_solid != h->p.is_solid) return SPH_ERR_ARG;
-    int K = h->c.K, mcap = h->c.mcap, lg = h->c.mcap_log2;
+    if (p->is_solid && (p->n_materials < 1 || p->n_materials > 4)) return SPH_ERR_ARG;
+    int K = h->c.K, mcap = h->c.mcap, lg = h->c.mcap_log2, bs = h->c.block;
     h->p = *p;
     fill_constants(h);
-    h->c.K = K; h->c.mcap = mcap; h->c.mcap_log2 = lg; h->c.n = (int)h->n;
+    h->c.K = K; h->c.mcap = mcap; h->c.mcap_log2 = lg; h->c.n = (int)h->n; h->c.block = bs;
+    int r = solid_sync_rows(h->solid, h->p, h->c);
     drop_graph(h);
-    return SPH_OK;
+    return r;
 }
 
 int sph_initialize(SphHandle* h, void* stream) {
@@ -722,6 +728,60 @@ int sph_jc_stats(SphHandle* h, uint64_t* out, int reset, void* stream) {
     CK(cudaStreamSynchronize(st));
     for (int k = 0; k < 4; ++k) out[k] = v[k];
     if (reset) CK(cudaMemsetAsync(h->solid.stats, 0, sizeof(v), st));
+    return SPH_OK;
+}
+
+}  // extern "C"
+
+// ------------------------------------------------------------------ ensembles and launch shape
+extern "C" {
+
+int sph_ensemble_set(SphHandle* h, const SphMatRow* mat, const SphInstRow* inst, int n_inst,
+                     const float* dt0, void* stream) {
+    if (!h || !h->p.is_solid || n_inst < 0 || n_inst > kMaxInstances) return SPH_ERR_ARG;
+    if (n_inst > 0 && (!mat || !inst || !dt0)) return SPH_ERR_ARG;
+    cudaStream_t st = S(stream);
+    if (n_inst == 0) {
+        h->solid.n_inst = 0;
+        int r = solid_sync_rows(h->solid, h->p, h->c);
+        drop_graph(h);
+        return r;
+    }
+    for (int k = 0; k < n_inst; ++k)
+        if (!(dt0[k] > 0.0f) || !(mat[k].rho0 > 0.0f)) return SPH_ERR_ARG;
+    std::vector<SphInstState> s0((size_t)n_inst);
+    for (int k = 0; k < n_inst; ++k) {
+        memset(&s0[k], 0, sizeof(SphInstState));
+        s0[k].dt = dt0[k];
+        s0[k].sts_stages = 1;
+    }
+    CK(cudaMemcpyAsync(h->solid.mat, mat, sizeof(SphMatRow) * n_inst, cudaMemcpyHostToDevice, st));
+    CK(cudaMemcpyAsync(h->solid.irow, inst, sizeof(SphInstRow) * n_inst, cudaMemcpyHostToDevice, st));
+    CK(cudaMemcpyAsync(h->solid.inst, s0.data(), sizeof(SphInstState) * n_inst, cudaMemcpyHostToDevice, st));
+    CK(cudaStreamSynchronize(st));           // s0 is a host temporary
+    solid_row_flags(mat, n_inst, h->solid.any_plastic, h->solid.all_gamma_one);
+    h->solid.n_inst = n_inst;
+    h->c.n_inst = n_inst;
+    h->c.any_plastic = h->solid.any_plastic;
+    h->c.all_gamma_one = h->solid.all_gamma_one;
+    drop_graph(h);
+    return SPH_OK;
+}
+
+int sph_ensemble_state(SphHandle* h, SphInstState* out, int n_inst, void* stream) {
+    if (!h || !out || !h->p.is_solid || n_inst < 1 || n_inst > h->solid.n_inst) return SPH_ERR_ARG;
+    cudaStream_t st = S(stream);
+    CK(cudaMemcpyAsync(out, h->solid.inst, sizeof(SphInstState) * n_inst, cudaMemcpyDeviceToHost, st));
+    CK(cudaStreamSynchronize(st));
+    return SPH_OK;
+}
+
+int sph_set_block(SphHandle* h, int threads) {
+    if (!h) return SPH_ERR_ARG;
+    if (threads == 0) threads = kBlock;
+    if (threads < 64 || threads > kBlock || threads % 32) return SPH_ERR_ARG;
+    h->c.block = threads;
+    drop_graph(h);
     return SPH_OK;
 }
 

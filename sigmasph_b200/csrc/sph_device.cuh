@@ -65,6 +65,11 @@ struct Cst {
     float colle_coef;    // -2 h
     float sun_coef;      // -CFL
     int mirror_y, mirror_z;
+    // solid material table (device) and ensemble mode
+    int n_inst;          // 0: one scene; > 0: instances, instance = material row
+    int any_plastic;     // some material row has a yield stress
+    int all_gamma_one;   // every EOS is linear (exponent 1)
+    int block;           // threads per block of the solid particle kernels
 };
 
 // Johnson-Cook return-map surrogate and sample log (solid only; null when unused).
@@ -107,6 +112,9 @@ struct Ptr {
     DevScalars* sc;
     DevAccum* ac;
     JcPtr jc;
+    const SphMatRow* mat;      // [rows] solid material rows
+    const SphInstRow* irow;    // [n_inst] ensemble instance constants
+    SphInstState* inst;        // [n_inst] ensemble instance state
 };
 
 // ------------------------------------------------------------------ small vector ops

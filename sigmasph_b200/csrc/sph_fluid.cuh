@@ -432,22 +432,29 @@ __global__ void __launch_bounds__(kBlock) k_pst(Cst c, Ptr P) {
     }
     float4 vi4 = vel[i];
     F3 vi = f3(vi4);
+    // an ensemble instance (solid: material row = instance) has its own speed and dt
+    float c0 = c.p.c0, dt = P.sc->dt;
+    if (c.n_inst > 0) {
+        const int k = (int)__ldg(P.cur.bcdisp + 4 * i + 3);
+        c0 = P.irow[k].c0;
+        dt = P.inst[k].dt;
+    }
     float Ma;
     if (c.p.pst_ma_mode == 2) Ma = c.p.pst_ma_fixed;
     else {
         float vref = c.p.pst_ma_mode == 1 ? __uint_as_float(P.ac->max_v_bits) : norm3(vi);
-        Ma = vref / c.p.c0;
+        Ma = vref / c0;
     }
     F3 dr;
     if (c.p.pst_colle) {
-        float cc = c.colle_coef * c.p.c0 * Ma;
+        float cc = c.colle_coef * c0 * Ma;
         F3 dvv = cc * sr;
         if (c.p.pst_clamp_vel) {
             float cap = c.p.pst_m_delta * norm3(vi);
             float dn = norm3(dvv);
             if (dn > cap) dvv = (cap / fmaxf(dn, 1e-30f)) * dvv;
         }
-        dr = P.sc->dt * dvv;
+        dr = dt * dvv;
     } else {
         float cc = c.sun_coef * Ma * c.h * c.h;
         dr = cc * sr;

@@ -21,6 +21,10 @@ inline float d2_threshold(float h) {
 inline void fill_constants_from(const SphParams& p, int64_t n, Cst& c) {
     c.p = p;
     c.n = (int)n;
+    c.n_inst = 0;
+    c.any_plastic = 0;
+    c.all_gamma_one = 1;
+    c.block = kBlock;
     double hd = p.support_radius;
     double al = p.two_d ? 7.0 / (M_PI * hd * hd) : 21.0 / (2.0 * M_PI * hd * hd * hd);
     c.h = (float)hd;

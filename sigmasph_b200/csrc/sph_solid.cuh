@@ -48,13 +48,63 @@ struct SolidScratch {
     float* log = nullptr;
     unsigned long long* log_count = nullptr;
     long long log_cap = 0;
+    // material rows (ordinary scene: from SphParams) and ensemble instances
+    SphMatRow* mat = nullptr;
+    SphInstRow* irow = nullptr;
+    SphInstState* inst = nullptr;
+    int n_inst = 0;
+    bool any_plastic = false, all_gamma_one = true;
 };
+constexpr int kMaxInstances = 1024;
 
 inline void solid_fill_constants(Cst&) {}
 inline int solid_alloc(SolidScratch& s, const SphParams& p, int64_t) {
     if (!p.is_solid) return SPH_OK;
-    if (cudaMalloc(&s.stats, 4 * sizeof(unsigned long long)) != cudaSuccess) return SPH_ERR_NOMEM;
+    if (cudaMalloc(&s.stats, 4 * sizeof(unsigned long long)) != cudaSuccess ||
+        cudaMalloc(&s.mat, kMaxInstances * sizeof(SphMatRow)) != cudaSuccess ||
+        cudaMalloc(&s.irow, kMaxInstances * sizeof(SphInstRow)) != cudaSuccess ||
+        cudaMalloc(&s.inst, kMaxInstances * sizeof(SphInstState)) != cudaSuccess)
+        return SPH_ERR_NOMEM;
     if (cudaMemset(s.stats, 0, 4 * sizeof(unsigned long long)) != cudaSuccess) return SPH_ERR_CUDA;
+    return SPH_OK;
+}
+// The rows of an ordinary scene, from SphParams' per-material tables.
+inline void solid_rows_from_params(const SphParams& p, SphMatRow* rows) {
+    for (int k = 0; k < p.n_materials && k < 4; ++k) {
+        SphMatRow& r = rows[k];
+        r.rho0 = p.mat_rho0[k]; r.K = p.mat_K[k]; r.G = p.mat_G[k]; r.cp = p.mat_cp[k];
+        r.c0 = p.mat_c0[k]; r.delta = p.mat_delta[k];
+        r.plastic_kind = p.plastic_kind[k]; r.sy0 = p.plastic_sy0[k]; r.H = p.plastic_H[k];
+        r.jc_A = p.jc_A[k]; r.jc_B = p.jc_B[k]; r.jc_n = p.jc_n[k]; r.jc_C = p.jc_C[k];
+        r.jc_eps0_dot = p.jc_eps0_dot[k]; r.jc_T0 = p.jc_T0[k]; r.jc_Tm = p.jc_Tm[k];
+        r.jc_m = p.jc_m[k]; r.jc_chi = p.jc_chi[k];
+        r.cv = p.mat_cv[k]; r.stiff = p.mat_stiff[k]; r.gamma = p.mat_gamma[k]; r.T0 = p.mat_T0[k];
+    }
+}
+inline void solid_row_flags(const SphMatRow* rows, int n, bool& any_plastic, bool& all_gamma_one) {
+    any_plastic = false;
+    all_gamma_one = true;
+    for (int k = 0; k < n; ++k) {
+        any_plastic = any_plastic || rows[k].sy0 > 0.0f;
+        all_gamma_one = all_gamma_one && rows[k].gamma == 1.0f;
+    }
+}
+// Uploads the scene's own rows (single-scene mode) and sets the table flags in c.
+inline int solid_sync_rows(SolidScratch& s, const SphParams& p, Cst& c) {
+    if (!p.is_solid || !s.mat) return SPH_OK;
+    if (s.n_inst > 0) {                      // an ensemble keeps its rows
+        c.n_inst = s.n_inst;
+        c.any_plastic = s.any_plastic;
+        c.all_gamma_one = s.all_gamma_one;
+        return SPH_OK;
+    }
+    SphMatRow rows[4] = {};
+    solid_rows_from_params(p, rows);
+    solid_row_flags(rows, p.n_materials, s.any_plastic, s.all_gamma_one);
+    c.n_inst = 0;
+    c.any_plastic = s.any_plastic;
+    c.all_gamma_one = s.all_gamma_one;
+    if (cudaMemcpy(s.mat, rows, sizeof(rows), cudaMemcpyHostToDevice) != cudaSuccess) return SPH_ERR_CUDA;
     return SPH_OK;
 }
 inline int solid_jc_alloc(SolidScratch& s, int64_t n) {
@@ -74,7 +124,8 @@ inline int solid_jc_alloc(SolidScratch& s, int64_t n) {
     return SPH_OK;
 }
 inline void solid_free(SolidScratch& s) {
-    void* ps[] = {s.q_count, s.q_idx, s.q_feat, s.q_pred, s.W, s.packed, s.stats, s.mlp_err};
+    void* ps[] = {s.q_count, s.q_idx, s.q_feat, s.q_pred, s.W, s.packed, s.stats, s.mlp_err,
+                  s.mat, s.irow, s.inst};
     for (void* q : ps) if (q) cudaFree(q);
     s = SolidScratch();
 }
@@ -105,21 +156,77 @@ __device__ __forceinline__ float vm_sym(const Sym& s) {
 __device__ __forceinline__ int eos_of(const Ptr& P, int i) {
     return (int)__ldg(P.cur.bcdisp + 4 * i + 3);
 }
+// Ensemble mode: a particle's material row is its instance, whose step state is
+// per instance; an ordinary scene keeps one state in the device scalars.
+__device__ __forceinline__ float dt_at(const Cst& c, const Ptr& P, int k) {
+    return c.n_inst > 0 ? P.inst[k].dt : P.sc->dt;
+}
+__device__ __forceinline__ float visc_at(const Cst& c, const Ptr& P, int k) {
+    return c.n_inst > 0 ? P.irow[k].visc_coef : c.visc_coef;
+}
+// atomicMax of a non-negative float (as its bits) into a field of each lane's instance:
+// one pass per distinct instance in the warp (usually one), all lanes reducing together.
+__device__ __forceinline__ void inst_max_atomic(float v, int k, bool on, unsigned int SphInstState::*field,
+                                                SphInstState* inst) {
+    const unsigned full = 0xffffffffu;
+    unsigned pending = __ballot_sync(full, on);
+    while (pending) {
+        const int leader = __ffs(pending) - 1;
+        const int kl = __shfl_sync(full, k, leader);
+        const bool mine = on && k == kl;
+        const unsigned bits = __reduce_max_sync(full, mine ? __float_as_uint(v) : 0u);
+        if ((int)(threadIdx.x & 31) == leader) atomicMax(&(inst[kl].*field), bits);
+        pending &= ~__ballot_sync(full, mine);
+    }
+}
+// atomicAdd of v into *addr, one atomic per distinct address in the warp.
+__device__ __forceinline__ void addr_add_atomic(double v, double* addr, bool on) {
+    const unsigned full = 0xffffffffu;
+    const unsigned long long a = (unsigned long long)addr;
+    unsigned pending = __ballot_sync(full, on);
+    while (pending) {
+        const int leader = __ffs(pending) - 1;
+        const unsigned long long al = __shfl_sync(full, a, leader);
+        const bool mine = on && a == al;
+        double t = mine ? v : 0.0;
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) t += __shfl_xor_sync(full, t, o);
+        if ((int)(threadIdx.x & 31) == leader) atomicAdd(reinterpret_cast<double*>(al), t);
+        pending &= ~__ballot_sync(full, mine);
+    }
+}
 __device__ __forceinline__ float r_axi_of(float y, const Cst& c) { return fmaxf(y, c.p.axi_r_min); }
 
 // Per-material pressure: S((rho/rho0)^gamma - 1), exactly linear when every material's
 // gamma is 1 (SOLID.py:3009-3038).
-__device__ __forceinline__ float solid_pressure(const Cst& c, int k, float rho) {
-    bool all_one = true;
-    for (int q = 0; q < c.p.n_materials; ++q) all_one = all_one && (c.p.mat_gamma[q] == 1.0f);
-    float rho0 = c.p.mat_rho0[k], S = c.p.mat_stiff[k];
-    float p = all_one ? S * (rho / rho0 - 1.0f) : S * (powf(rho / rho0, c.p.mat_gamma[k]) - 1.0f);
+__device__ __forceinline__ float solid_pressure(const Cst& c, const Ptr& P, int k, float rho) {
+    const SphMatRow& M = P.mat[k];
+    float rho0 = M.rho0, S = M.stiff;
+    float p = c.all_gamma_one ? S * (rho / rho0 - 1.0f) : S * (powf(rho / rho0, M.gamma) - 1.0f);
     if (!c.p.allow_negative_pressure) p = fmaxf(p, 0.0f);
     return p;
 }
 
 // ------------------------------------------------------------------ load factor
 __global__ void k_solid_load(Cst c, Ptr P) {
+    if (c.n_inst > 0) {
+        // per instance: its smoothstep from its own clock, and a fresh dt maximum
+        for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < c.n_inst; k += gridDim.x * blockDim.x) {
+            SphInstState& S = P.inst[k];
+            const double T = P.irow[k].ramp_time;
+            if (T <= 0.0) { S.load_s = 1.0f; S.load_sdot = 0.0f; }
+            else {
+                const double u = fmin(1.0, fmax(0.0, S.sim_time / T));
+                S.load_s = (float)(u * u * (3.0 - 2.0 * u));
+                S.load_sdot = (float)(6.0 * u * (1.0 - u) / T);
+            }
+            const float cs = P.irow[k].c_signal;
+            S.max_c_sq_bits = __float_as_uint(cs * cs);
+            S.max_accel_bits = __float_as_uint(1e-10f);
+        }
+        if (blockIdx.x == 0 && threadIdx.x == 0 && P.jc.count) *P.jc.count = 0;
+        return;
+    }
     if (threadIdx.x != 0 || blockIdx.x != 0) return;
     if (P.jc.count) *P.jc.count = 0;            // the surrogate queue of this step
     double T = c.p.ramp_time;
@@ -267,10 +374,11 @@ __global__ void SPH_PAIR_BOUNDS_OCC4 k_solid_a(Cst c, Ptr P) {
         const float L00 = l0.x, L11 = l0.y, L22 = l0.z, L01 = l0.w, L02 = l1.x, L12 = l1.y;
         const float lam_i = lam[i];
         const float rho_i = vi4.w / pi.w, inv_rho_i = 1.0f / rho_i;
-        const float dt = P.sc->dt, inv_dt = 1.0f / dt;
         const bool pst = c.p.pst_enabled;
         const int ki = eos_of(P, i);
-        const float di = c.p.mat_delta[ki];
+        const float dt = dt_at(c, P, ki), inv_dt = 1.0f / dt;
+        const float di = P.mat[ki].delta;
+        const float c0i = c.n_inst > 0 ? P.irow[ki].c0 : c.p.c0;
         F3 du_i = {0, 0, 0};
         if (pst) { float4 s = shf[i]; du_i = {s.x * inv_dt, s.y * inv_dt, s.z * inv_dt}; }
         const F3 vhat_i = vi + du_i;
@@ -305,12 +413,12 @@ __global__ void SPH_PAIR_BOUNDS_OCC4 k_solid_a(Cst c, Ptr P) {
             r0 += Vj * dot3(vhat_i - vh_j, g);
             int kj = eos_of(P, j);
             if (kj == ki) {   // pair_delta (SOLID.py:4103-4114) on same-material pairs
-                float dj = c.p.mat_delta[kj];
+                float dj = P.mat[kj].delta;
                 float den = di + dj;
                 float dl = den > 1e-12f ? 2.0f * di * dj / den : 0.0f;
                 if (dl > 0.0f) {
                     float psig = __fdividef(2.0f * (rho_j - rho_i) * (-dot3(r, g)), rn2 + c.eta2);
-                    float rate = dl * c.h * c.p.c0 * Vj * psig * inv_rho_i;
+                    float rate = dl * c.h * c0i * Vj * psig * inv_rho_i;
                     r0 += rate;
                     r1 += rate;
                 }
@@ -393,17 +501,18 @@ struct JcTrial {
     bool active;                 // material has G, A > 0
     bool yields;                 // vm > sigma_y0 > 0
 };
-__device__ __forceinline__ JcTrial jc_trial(const Sym& s, const Cst& c, int k, float ep, float temp) {
+__device__ __forceinline__ JcTrial jc_trial(const Sym& s, const Ptr& P, int k, float ep, float temp) {
     JcTrial q;
-    q.G = c.p.mat_G[k]; q.A = c.p.jc_A[k]; q.B = c.p.jc_B[k]; q.nn = c.p.jc_n[k];
-    q.C = c.p.jc_C[k]; q.e0d = c.p.jc_eps0_dot[k];
-    const float T0 = c.p.jc_T0[k], Tm = c.p.jc_Tm[k];
+    const SphMatRow& M = P.mat[k];
+    q.G = M.G; q.A = M.jc_A; q.B = M.jc_B; q.nn = M.jc_n;
+    q.C = M.jc_C; q.e0d = M.jc_eps0_dot;
+    const float T0 = M.jc_T0, Tm = M.jc_Tm;
     q.active = q.G > 0.0f && q.A > 0.0f;
     q.vm = vm_sym(s);
     q.mt = 1.0f;
     if (Tm > T0 && temp > T0) {
         float ts = fminf(1.0f, fmaxf(0.0f, (temp - T0) / (Tm - T0)));
-        q.mt = fmaxf(0.0f, 1.0f - powf(ts, c.p.jc_m[k]));
+        q.mt = fmaxf(0.0f, 1.0f - powf(ts, M.jc_m));
     }
     float s0 = q.A;
     if (ep > 0.0f && q.B > 0.0f && q.nn > 0.0f) s0 += q.B * powf(ep, q.nn);
@@ -442,11 +551,11 @@ __device__ __forceinline__ void jc_scale(Sym& s, const JcTrial& q, float d) {
     float sc = syf / q.vm;
     s = {s.xx * sc, s.yy * sc, s.zz * sc, s.xy * sc, s.xz * sc, s.yz * sc};
 }
-__device__ __forceinline__ float jc_return(Sym& s, const Cst& c, int k, float ep, float temp, float dt,
+__device__ __forceinline__ float jc_return(Sym& s, const Ptr& P, int k, float ep, float temp, float dt,
                                            bool& capped, int& iters) {
     capped = false;
     iters = 0;
-    const JcTrial q = jc_trial(s, c, k, ep, temp);
+    const JcTrial q = jc_trial(s, P, k, ep, temp);
     if (!q.active || !q.yields) return 0.0f;
     const float d = jc_newton(q, ep, dt, iters);
     capped = iters >= 40;
@@ -488,16 +597,15 @@ __global__ void __launch_bounds__(kBlock) k_solid_b(Cst c, Ptr P) {
         float4 pi = pos[i], vi4 = vel[i], shi = shf[i];
         F3 xi = f3(pi);
         const float rho_i = vi4.w / pi.w, inv_rho_i = 1.0f / rho_i;
-        const float dt = P.sc->dt, inv_dt = 1.0f / dt;
         const int ki = eos_of(P, i);
+        const float dt = dt_at(c, P, ki), inv_dt = 1.0f / dt;
         const Sym s = load_s(sdev, i);
         const float4 sd1 = __ldg(reinterpret_cast<const float4*>(sdev) + 2 * i + 1);
         float ep = sd1.z;
         const float T_old = sd1.w;
         const float e_i = shi.w;
         const bool ale = c.p.ale_history != 0;
-        bool plastic_any = false;
-        for (int q = 0; q < c.p.n_materials; ++q) plastic_any = plastic_any || (c.p.plastic_sy0[q] > 0.0f);
+        const bool plastic_any = c.any_plastic != 0;
         const F3 du_i = {shi.x * inv_dt, shi.y * inv_dt, shi.z * inv_dt};
         Sym A = {0, 0, 0, 0, 0, 0};
         float dep = 0.0f, adv = 0.0f, dif = 0.0f;
@@ -549,7 +657,8 @@ __global__ void __launch_bounds__(kBlock) k_solid_b(Cst c, Ptr P) {
             for (int b = 0; b < 3; ++b) { ed[a][b] = 0.5f * (Lg[a][b] + Lg[b][a]); sp[a][b] = 0.5f * (Lg[a][b] - Lg[b][a]); }
         float tr = ed[0][0] + ed[1][1] + ed[2][2];
         float S[3][3] = {{s.xx, s.xy, s.xz}, {s.xy, s.yy, s.yz}, {s.xz, s.yz, s.zz}};
-        const float G2 = 2.0f * c.p.mat_G[ki];
+        const SphMatRow& Mi = P.mat[ki];
+        const float G2 = 2.0f * Mi.G;
         float Sn[3][3];
 #pragma unroll
         for (int a = 0; a < 3; ++a)
@@ -570,15 +679,15 @@ __global__ void __launch_bounds__(kBlock) k_solid_b(Cst c, Ptr P) {
                   0.5f * (Sn[1][2] + Sn[2][1])};
         float tr3 = (sn.xx + sn.yy + sn.zz) / 3.0f;
         sn.xx -= tr3; sn.yy -= tr3; sn.zz -= tr3;
-        if (c.p.mat_G[ki] <= 0.0f) sn = {0, 0, 0, 0, 0, 0};
+        if (Mi.G <= 0.0f) sn = {0, 0, 0, 0, 0, 0};
         if (ale && plastic_any) ep = fmaxf(0.0f, ep + dt * dep);
         float dprod = 0.0f;
         if (plastic_any) {
-            if (c.p.plastic_kind[ki] == 2) {
+            if (Mi.plastic_kind == 2) {
                 const bool want_mlp = c.p.jc_surrogate != 0 && P.jc.count != nullptr;
                 const bool want_log = P.jc.log != nullptr;
                 if (want_mlp || want_log) {
-                    const JcTrial q = jc_trial(sn, c, ki, ep, T_old);
+                    const JcTrial q = jc_trial(sn, P, ki, ep, T_old);
                     if (q.yields) {
                         float dd = 0.0f;
 #pragma unroll
@@ -613,13 +722,13 @@ __global__ void __launch_bounds__(kBlock) k_solid_b(Cst c, Ptr P) {
                 } else {
                     bool capped;
                     int it;
-                    dprod = jc_return(sn, c, ki, ep, T_old, dt, capped, it);
+                    dprod = jc_return(sn, P, ki, ep, T_old, dt, capped, it);
                     capped_any = capped;
                     newton_solves = dprod > 0.0f ? 1u : 0u;
                     newton_iters = (unsigned)it;
                 }
             } else {
-                dprod = j2_return(sn, c.p.mat_G[ki], c.p.plastic_sy0[ki], c.p.plastic_H[ki], ep);
+                dprod = j2_return(sn, Mi.G, Mi.sy0, Mi.H, ep);
             }
             ep += dprod;
             if (dprod > 0.0f) pw = (double)(pi.w * vm_sym(sn) * dprod);
@@ -637,16 +746,16 @@ __global__ void __launch_bounds__(kBlock) k_solid_b(Cst c, Ptr P) {
         }
         // update_temperature (SOLID.py:2239-2293) from the new energy and the current V
         float T_new = T_old;
-        const float cv = c.p.mat_cv[ki];
+        const float cv = Mi.cv;
         if (cv > 0.0f) {
-            double rho = (double)vi4.w / (double)pi.w, rho0 = (double)c.p.mat_rho0[ki];
-            double St = (double)c.p.mat_stiff[ki], gam = (double)c.p.mat_gamma[ki];
+            double rho = (double)vi4.w / (double)pi.w, rho0 = (double)Mi.rho0;
+            double St = (double)Mi.stiff, gam = (double)Mi.gamma;
             double xx = rho / rho0, ec;
             if (fabs(gam - 1.0) < 1.0e-6) ec = (St / rho0) * (log(xx) + 1.0 / xx - 1.0);
             else ec = (St / rho0) * ((pow(xx, gam - 1.0) - 1.0) / (gam - 1.0) + 1.0 / xx - 1.0);
             if (!c.p.allow_negative_pressure && rho < rho0) ec = 0.0;
             double eth = (double)e_new - ec;
-            T_new = c.p.mat_T0[ki] + (float)(eth / (double)cv);
+            T_new = Mi.T0 + (float)(eth / (double)cv);
         }
         P.aux[6 * i + 0] = make_float4(sn.xx, sn.yy, sn.zz, sn.xy);
         P.aux[6 * i + 1] = make_float4(sn.xz, sn.yz, ep, e_new);
@@ -681,8 +790,8 @@ __global__ void __launch_bounds__(kBlock) k_jc_finish(Cst c, Ptr P) {
         float ep = a1.z;
         const int k = eos_of(P, i);
         const float T_old = P.cur.sdev[8 * i + 7];
-        const float dt = P.sc->dt;
-        const JcTrial q = jc_trial(sn, c, k, ep, T_old);
+        const float dt = dt_at(c, P, k);
+        const JcTrial q = jc_trial(sn, P, k, ep, T_old);
         if (q.yields) {
             const float d_hi = (q.vm - q.sy0) / (3.0f * q.G);
             const float f = 1.0f - 0.1f * P.jc.fpred[qi];    // the network's u = 10 (1 - d / d_hi)
@@ -723,14 +832,16 @@ __global__ void __launch_bounds__(kBlock) k_jc_finish(Cst c, Ptr P) {
 // ------------------------------------------------------------------ commit + volume + EOS
 __global__ void __launch_bounds__(kBlock) k_solid_commit(Cst c, Ptr P) {
     int i = blockIdx.x * blockDim.x + threadIdx.x;
-    const float dt = P.sc->dt;
     if (i == 0) {
-        P.sc->diff_work += (double)dt * P.ac->w_diff_step;
+        // ensembles keep their dt maxima per instance (reset in k_solid_load) and no
+        // scene-wide diffusion work
+        if (c.n_inst == 0) P.sc->diff_work += (double)P.sc->dt * P.ac->w_diff_step;
         P.ac->w_diff_step = 0.0;
         P.ac->max_c_sq_bits = __float_as_uint(c.p.c_signal * c.p.c_signal);
         P.ac->max_accel_bits = __float_as_uint(1e-10f);
     }
     if (i >= c.n) return;
+    const float dt = dt_at(c, P, eos_of(P, i));
     float4 a0 = P.aux[6 * i + 0], a1 = P.aux[6 * i + 1], a2 = P.aux[6 * i + 2];
     float4* sd = reinterpret_cast<float4*>(P.cur.sdev) + 2 * i;
     sd[0] = a0;
@@ -755,7 +866,7 @@ __global__ void __launch_bounds__(kBlock) k_solid_commit(Cst c, Ptr P) {
     pi.w = V;
     pos[i] = pi;
     float m = P.cur.vel[4 * i + 3];
-    P.cur.disp[4 * i + 3] = solid_pressure(c, eos_of(P, i), m / V);
+    P.cur.disp[4 * i + 3] = solid_pressure(c, P, eos_of(P, i), m / V);
     // gravity; de_int restarts for this step's force pass
     P.acc[i] = make_float4(c.p.gravity[0], c.p.gravity[1], c.p.gravity[2], 0.0f);
 }
@@ -765,6 +876,8 @@ __global__ void __launch_bounds__(kBlock) k_solid_force(Cst c, Ptr P) {
     int i = blockIdx.x * blockDim.x + threadIdx.x;
     float amag = 0.0f, csq = 0.0f;
     double hgp = 0.0;
+    int kinst = 0;
+    bool on = false;
     if (i < c.n) {
         const float4* __restrict__ pos = as4c(P.cur.pos);
         const float4* __restrict__ vel = as4c(P.cur.vel);
@@ -776,8 +889,8 @@ __global__ void __launch_bounds__(kBlock) k_solid_force(Cst c, Ptr P) {
         const float p_i = dsp[i].w;
         const float rho_i = vi4.w / pi.w, inv_rho_i = 1.0f / rho_i;
         const float w_i = w_of(pi, c), mw_i = mw_of(vi4.w, pi, c), inv_mw = 1.0f / mw_i;
-        const float dt = P.sc->dt, inv_dt = 1.0f / dt;
         const int ki = eos_of(P, i);
+        const float dt = dt_at(c, P, ki), inv_dt = 1.0f / dt;
         const Sym s = load_s(sdev, i);
         const bool ale = c.p.pst_enabled && c.p.pst_ale_momentum;
         const bool hg_inloop = c.p.hourglass_alpha > 0.0f && !c.p.hourglass_sts;
@@ -785,12 +898,16 @@ __global__ void __launch_bounds__(kBlock) k_solid_force(Cst c, Ptr P) {
         const float ri = r_axi_of(pi.y, c), inv_ri = 1.0f / ri;
         float Gi[3][3];
         if (hg_inloop) load_gradv(P, i, Gi);
-        const float hg_pre = c.p.hourglass_alpha * (c.p.mat_rho0[ki] * inv_rho_i) * (c.p.mat_cp[ki] * c.inv_h)
+        const float hg_pre = c.p.hourglass_alpha * (P.mat[ki].rho0 * inv_rho_i) * (P.mat[ki].cp * c.inv_h)
                              / (c.p.V0 * (float)c.p.hg_W_dx0);
+        const float visc = visc_at(c, P, ki);
+        kinst = ki;
+        on = true;
         F3 du_i = {0, 0, 0};
         if (ale) { float4 q = shf[i]; du_i = {q.x * inv_dt, q.y * inv_dt, q.z * inv_dt}; }
         const float eps_rho = 1e-3f * c.p.density0;
-        float cl = c.p.c_signal * c.p.c_signal;
+        const float csig = c.n_inst > 0 ? P.irow[ki].c_signal : c.p.c_signal;
+        float cl = csig * csig;
         F3 a = {0, 0, 0};
         float dei = 0.0f, dhg = 0.0f;
         for_each_neighbour(c, P, i, [&](int j, int mir) {
@@ -816,7 +933,7 @@ __global__ void __launch_bounds__(kBlock) k_solid_force(Cst c, Ptr P) {
             F3 vij = vi - vj;
             dei += -0.5f * dot3(f, vij) * inv_mw;
             float vxy = dot3(vij, r);
-            F3 am = __fdividef(c.visc_coef * w_j * vxy, rn * rn + c.eta2) * g;
+            F3 am = __fdividef(visc * w_j * vxy, rn * rn + c.eta2) * g;
             a += am;
             if (c.p.viscosity > 0.0f) dei += -0.5f * dot3(am, vij);
             if (hg_inloop && rn > 1e-9f) {
@@ -863,6 +980,11 @@ __global__ void __launch_bounds__(kBlock) k_solid_force(Cst c, Ptr P) {
         if (c.p.dt_pair_mode != 0) csq = cl;
         hgp = (double)(mw_i * dhg);
     }
+    if (c.n_inst > 0) {
+        inst_max_atomic(amag, kinst, on, &SphInstState::max_accel_bits, P.inst);
+        inst_max_atomic(csq, kinst, on, &SphInstState::max_c_sq_bits, P.inst);
+        return;
+    }
     block_max_atomic(amag, &P.ac->max_accel_bits);
     block_max_atomic(csq, &P.ac->max_c_sq_bits);
     if (c.p.hourglass_alpha > 0.0f && !c.p.hourglass_sts) block_sum_atomic(hgp, &P.ac->hg_power);
@@ -870,6 +992,33 @@ __global__ void __launch_bounds__(kBlock) k_solid_force(Cst c, Ptr P) {
 
 // ------------------------------------------------------------------ dt, damper cap / stage count
 __global__ void k_solid_dt(Cst c, Ptr P) {
+    if (c.n_inst > 0) {
+        // per instance: its own CFL dt, damper cap or stage count; grips cleared
+        for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < c.n_inst; k += gridDim.x * blockDim.x) {
+            SphInstState& S = P.inst[k];
+            const float mcs = __uint_as_float(S.max_c_sq_bits), ma = __uint_as_float(S.max_accel_bits);
+            float dt = fminf(c.cfl_h / sqrtf(mcs), c.p.CFL * sqrtf(c.h / ma));
+            const double rate = (double)P.irow[k].hg_rate;
+            int s = 0;
+            if (c.p.hourglass_alpha > 0.0f && rate > 0.0) {
+                if (!c.p.hourglass_sts) {
+                    dt = fminf(dt, (float)(1.6 / rate));
+                } else {
+                    s = c.p.hg_sts_fixed > 0 ? c.p.hg_sts_fixed : max(1, (int)ceil(rate * (double)dt / 1.6));
+                    if (s > kStsMaxStages) { s = kStsMaxStages; atomicOr(&P.sc->err, SPH_EW_STS_CAP); }
+                    const double cap = s * 1.6 / rate;
+                    if ((double)dt > cap) dt = (float)cap;
+                }
+            } else if (c.p.hourglass_alpha > 0.0f && c.p.hourglass_sts) {
+                s = 1;
+            }
+            S.dt = dt;
+            S.sts_stages = s;
+            for (int g = 0; g < 2; ++g)
+                for (int d = 0; d < 3; ++d) { S.constraint_force[g][d] = 0.0; S.constraint_disp[g][d] = 0.0; }
+        }
+        return;
+    }
     if (threadIdx.x != 0 || blockIdx.x != 0) return;
     float mcs = __uint_as_float(P.ac->max_c_sq_bits);
     float ma = __uint_as_float(P.ac->max_accel_bits);
@@ -912,7 +1061,7 @@ __global__ void __launch_bounds__(kBlock) k_half_kick(Cst c, Ptr P) {
     int i = blockIdx.x * blockDim.x + threadIdx.x;
     double ke = 0.0;
     if (i < c.n) {
-        const float h = 0.5f * P.sc->dt;
+        const float h = 0.5f * dt_at(c, P, eos_of(P, i));
         float4* vel = as4(P.cur.vel);
         float4 v = vel[i];
         float4 a = P.acc[i];
@@ -931,10 +1080,12 @@ __global__ void __launch_bounds__(kBlock) k_half_kick(Cst c, Ptr P) {
 }
 
 __global__ void __launch_bounds__(kBlock) k_hg_stage(Cst c, Ptr P, int stage) {
-    const int s = P.sc->sts_stages;
-    if (stage >= s) return;
+    if (c.n_inst == 0 && stage >= P.sc->sts_stages) return;
     int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= c.n) return;
+    const int ki = eos_of(P, i);
+    const int s = c.n_inst > 0 ? P.inst[ki].sts_stages : P.sc->sts_stages;
+    if (stage >= s) return;
     const int rb = stage & 1, wb = rb ^ 1;
     const float4* __restrict__ pos = as4c(P.cur.pos);
     const float4* __restrict__ vel = as4c(P.cur.vel);
@@ -942,12 +1093,11 @@ __global__ void __launch_bounds__(kBlock) k_hg_stage(Cst c, Ptr P, int stage) {
     F3 xi = f3(pi);
     F3 yi = y_load(P, i, rb);
     const float rho_i = __ldg(&vel[i].w) / pi.w;
-    const int ki = eos_of(P, i);
     float Gi[3][3];
     load_gradv(P, i, Gi);
     const bool axc = c.p.axisymmetric && c.p.axi_conservative_x;
     const float ri = r_axi_of(pi.y, c), inv_ri = 1.0f / ri;
-    const float hg_pre = c.p.hourglass_alpha * (c.p.mat_rho0[ki] / rho_i) * (c.p.mat_cp[ki] * c.inv_h)
+    const float hg_pre = c.p.hourglass_alpha * (P.mat[ki].rho0 / rho_i) * (P.mat[ki].cp * c.inv_h)
                          / (c.p.V0 * (float)c.p.hg_W_dx0);
     F3 acc = {0, 0, 0};
     for_each_neighbour(c, P, i, [&](int j, int mir) {
@@ -973,7 +1123,7 @@ __global__ void __launch_bounds__(kBlock) k_hg_stage(Cst c, Ptr P, int stage) {
         if (axc) ah.x *= 0.5f * (ri + r_axi_of(pj.y, c)) * inv_ri;
         acc += ah;
     });
-    const float sub = (float)((double)P.sc->dt / (double)s);
+    const float sub = (float)((double)dt_at(c, P, ki) / (double)s);
     y_store(P, i, wb, yi + sub * acc);
 }
 
@@ -981,8 +1131,9 @@ __global__ void __launch_bounds__(kBlock) k_sts_finish(Cst c, Ptr P) {
     int i = blockIdx.x * blockDim.x + threadIdx.x;
     double ke = 0.0, wl = 0.0;
     if (i < c.n) {
-        const int s = P.sc->sts_stages;
-        const float dt = P.sc->dt, h = 0.5f * dt;
+        const int ki = eos_of(P, i);
+        const int s = c.n_inst > 0 ? P.inst[ki].sts_stages : P.sc->sts_stages;
+        const float dt = dt_at(c, P, ki), h = 0.5f * dt;
         float4* vel = as4(P.cur.vel);
         float4 v = vel[i];
         F3 y = y_load(P, i, s & 1);
@@ -1016,7 +1167,7 @@ __global__ void __launch_bounds__(kBlock) k_sts_finish(Cst c, Ptr P) {
 __global__ void __launch_bounds__(kBlock) k_solid_advect(Cst c, Ptr P) {
     int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= c.n) return;
-    const float dt = P.sc->dt;
+    const float dt = dt_at(c, P, eos_of(P, i));
     float4* vel = as4(P.cur.vel);
     float4 v = vel[i];
     float4 a = P.acc[i];
@@ -1041,7 +1192,55 @@ __global__ void __launch_bounds__(kBlock) k_solid_advect(Cst c, Ptr P) {
 // The grip force is summed per block in shared memory (FP64) and pushed with one global
 // atomic per block, grip and axis: gripped particles are contiguous in the Morton order,
 // so a per-particle global atomic would serialise thousands of adds on a few addresses.
+// Ensemble form: each gripped particle uses its instance's load factor and adds to its
+// instance's grip (bc.y = 0 or 1), one FP64 atomic per warp and distinct grip.
+__device__ __forceinline__ void constraints_ensemble(const Cst& c, const Ptr& P) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    int2 bc = make_int2(0, -1);
+    if (i < c.n) bc = reinterpret_cast<const int2*>(P.cur.bc)[i];
+    int k = 0, g = 0;
+    double fd[3] = {0.0, 0.0, 0.0};
+    bool rec[3] = {false, false, false};
+    if (bc.x != 0) {
+        k = eos_of(P, i);
+        SphInstState& S = P.inst[k];
+        const float s = S.load_s, sd = S.load_sdot;
+        const float scale = c.p.axisymmetric ? (float)(2.0 * M_PI) : 1.0f;
+        const float4 bd = reinterpret_cast<const float4*>(P.cur.bcdisp)[i];
+        float4* pos = as4(P.cur.pos);
+        float4* vel = as4(P.cur.vel);
+        float4* dsp = as4(P.cur.disp);
+        float4 p = pos[i], v = vel[i], u = dsp[i], a = P.acc[i];
+        const float4 x0 = as4(P.cur.x0)[i];
+        float* pc[3] = {&p.x, &p.y, &p.z};
+        float* vc[3] = {&v.x, &v.y, &v.z};
+        float* uc[3] = {&u.x, &u.y, &u.z};
+        float* ac[3] = {&a.x, &a.y, &a.z};
+        const float bdc[3] = {bd.x, bd.y, bd.z};
+        const float x0c[3] = {x0.x, x0.y, x0.z};
+        const bool record = bc.y == 0 || bc.y == 1;
+        g = record ? bc.y : 0;
+#pragma unroll
+        for (int d = 0; d < 3; ++d) {
+            if (!(bc.x & (1 << d))) continue;
+            if (record) {
+                fd[d] = (double)(scale * v.w * *ac[d]);
+                rec[d] = true;
+                S.constraint_disp[g][d] = (double)(bdc[d] * s);   // one value per grip
+            }
+            *uc[d] = bdc[d] * s;
+            *pc[d] = x0c[d] + *uc[d];
+            *vc[d] = bdc[d] * sd;
+            *ac[d] = 0.0f;
+        }
+        pos[i] = p; vel[i] = v; dsp[i] = u; P.acc[i] = a;
+    }
+#pragma unroll
+    for (int d = 0; d < 3; ++d) addr_add_atomic(fd[d], &P.inst[k].constraint_force[g][d], rec[d]);
+}
+
 __global__ void __launch_bounds__(kBlock) k_constraints(Cst c, Ptr P) {
+    if (c.n_inst > 0) { constraints_ensemble(c, P); return; }
     __shared__ double s_force[8][3];
     __shared__ float s_disp[8][3];
     __shared__ int s_axes[8];
@@ -1094,59 +1293,70 @@ __global__ void __launch_bounds__(kBlock) k_constraints(Cst c, Ptr P) {
 }
 
 __global__ void k_solid_time(Cst c, Ptr P) {
+    if (c.n_inst > 0) {
+        for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < c.n_inst; k += gridDim.x * blockDim.x)
+            P.inst[k].sim_time += (double)P.inst[k].dt;
+        return;
+    }
     if (threadIdx.x == 0 && blockIdx.x == 0) P.sc->sim_time += (double)P.sc->dt;
 }
 
 // ------------------------------------------------------------------ host sequencing
-inline int grid_of(int n) { return n > 0 ? (n + kBlock - 1) / kBlock : 1; }
+inline int grid_of(int n, int bs = kBlock) { return n > 0 ? (n + bs - 1) / bs : 1; }
+// Launch shape of the per-instance kernels (one thread per instance, or one thread).
+inline int inst_blocks(const Cst& c) { return c.n_inst > 0 ? (c.n_inst + 127) / 128 : 1; }
+inline int inst_threads(const Cst& c) { return c.n_inst > 0 ? 128 : 32; }
 
 // Launched before the rebuild of a solid step.
 inline int solid_pre_step(const Cst& c, const Ptr& P, SolidScratch&, cudaStream_t st) {
-    k_solid_load<<<1, 32, 0, st>>>(c, P);
+    k_solid_load<<<inst_blocks(c), inst_threads(c), 0, st>>>(c, P);
     return SPH_OK;
 }
 
 template <class Mark>
 inline int solid_substep_launch(const Cst& c, const Ptr& P, int n, cudaStream_t st, Mark&& mark,
                                 int first_stage = 0, int last_stage = 99) {
-    const int nb = grid_of(n);
+    // the particle kernels take the handle's block size (sph_set_block); the tensor-core
+    // and per-instance kernels have their own shapes
+    const int bs = c.block > 0 ? c.block : kBlock;
+    const int nb = grid_of(n, bs);
     auto in = [&](int s) { return s >= first_stage && s <= last_stage; };
     if (in(SPH_STAGE_LAM)) {
-        k_lam<<<nb, kBlock, 0, st>>>(c, P); mark("k_lam");
-        if (c.p.kernel_correction) { k_kc_inverse<<<nb, kBlock, 0, st>>>(c, P); mark("k_kc_inverse"); }
-        k_solid_a<<<nb, kBlock, 0, st>>>(c, P); mark("k_solid_a");
-        k_solid_b<<<nb, kBlock, 0, st>>>(c, P); mark("k_solid_b");
+        k_lam<<<nb, bs, 0, st>>>(c, P); mark("k_lam");
+        if (c.p.kernel_correction) { k_kc_inverse<<<nb, bs, 0, st>>>(c, P); mark("k_kc_inverse"); }
+        k_solid_a<<<nb, bs, 0, st>>>(c, P); mark("k_solid_a");
+        k_solid_b<<<nb, bs, 0, st>>>(c, P); mark("k_solid_b");
         if (c.p.jc_surrogate && P.jc.count) {
             const int tiles = (n + kMlpTileRows - 1) / kMlpTileRows;
             const int g = std::min(kMlpCtasPerSm * 148, std::max(tiles, 1));
             k_mlp_tc<<<g, kMlpTcThreads, 0, st>>>(P.jc.W, static_cast<const __nv_bfloat16*>(P.jc.packed),
                                                  P.jc.feat, n, P.jc.count, P.jc.fpred, &P.sc->err);
             mark("k_mlp_tc");
-            k_jc_finish<<<nb, kBlock, 0, st>>>(c, P); mark("k_jc_finish");
+            k_jc_finish<<<grid_of(n), kBlock, 0, st>>>(c, P); mark("k_jc_finish");
         }
     }
-    if (in(SPH_STAGE_CONTINUITY)) { k_solid_commit<<<nb, kBlock, 0, st>>>(c, P); mark("k_solid_commit"); }
-    if (in(SPH_STAGE_FORCES)) { k_solid_force<<<nb, kBlock, 0, st>>>(c, P); mark("k_solid_force"); }
-    if (in(SPH_STAGE_DT)) { k_solid_dt<<<1, 32, 0, st>>>(c, P); mark("k_solid_dt"); }
+    if (in(SPH_STAGE_CONTINUITY)) { k_solid_commit<<<nb, bs, 0, st>>>(c, P); mark("k_solid_commit"); }
+    if (in(SPH_STAGE_FORCES)) { k_solid_force<<<nb, bs, 0, st>>>(c, P); mark("k_solid_force"); }
+    if (in(SPH_STAGE_DT)) { k_solid_dt<<<inst_blocks(c), inst_threads(c), 0, st>>>(c, P); mark("k_solid_dt"); }
     if (in(SPH_STAGE_ADVECT)) {
         if (c.p.hourglass_sts && c.p.hourglass_alpha > 0.0f) {
-            k_half_kick<<<nb, kBlock, 0, st>>>(c, P); mark("k_half_kick");
-            if (c.p.hg_sts_refresh) { k_gradv<<<nb, kBlock, 0, st>>>(c, P); mark("k_gradv"); }
-            for (int s = 0; s < kStsMaxStages; ++s) { k_hg_stage<<<nb, kBlock, 0, st>>>(c, P, s); mark("k_hg_stage"); }
-            k_sts_finish<<<nb, kBlock, 0, st>>>(c, P); mark("k_sts_finish");
+            k_half_kick<<<nb, bs, 0, st>>>(c, P); mark("k_half_kick");
+            if (c.p.hg_sts_refresh) { k_gradv<<<nb, bs, 0, st>>>(c, P); mark("k_gradv"); }
+            for (int s = 0; s < kStsMaxStages; ++s) { k_hg_stage<<<nb, bs, 0, st>>>(c, P, s); mark("k_hg_stage"); }
+            k_sts_finish<<<nb, bs, 0, st>>>(c, P); mark("k_sts_finish");
         } else {
-            k_solid_advect<<<nb, kBlock, 0, st>>>(c, P); mark("k_solid_advect");
+            k_solid_advect<<<nb, bs, 0, st>>>(c, P); mark("k_solid_advect");
         }
-        k_constraints<<<nb, kBlock, 0, st>>>(c, P); mark("k_constraints");
+        k_constraints<<<nb, bs, 0, st>>>(c, P); mark("k_constraints");
     }
     if (in(SPH_STAGE_PST) && c.p.pst_enabled) {
-        k_pst_search<<<nb, kBlock, 0, st>>>(c, P); mark("k_pst_search");
-        k_pst<<<nb, kBlock, 0, st>>>(c, P); mark("k_pst");
-        k_finish<<<nb, kBlock, 0, st>>>(c, P, last_stage >= SPH_STAGE_BOUNDARY ? 3 : 1); mark("k_finish");
+        k_pst_search<<<nb, bs, 0, st>>>(c, P); mark("k_pst_search");
+        k_pst<<<nb, bs, 0, st>>>(c, P); mark("k_pst");
+        k_finish<<<nb, bs, 0, st>>>(c, P, last_stage >= SPH_STAGE_BOUNDARY ? 3 : 1); mark("k_finish");
     } else if (in(SPH_STAGE_BOUNDARY)) {
-        k_finish<<<nb, kBlock, 0, st>>>(c, P, 2); mark("k_finish");
+        k_finish<<<nb, bs, 0, st>>>(c, P, 2); mark("k_finish");
     }
-    if (in(SPH_STAGE_BOUNDARY)) { k_solid_time<<<1, 32, 0, st>>>(c, P); mark("k_solid_time"); }
+    if (in(SPH_STAGE_BOUNDARY)) { k_solid_time<<<inst_blocks(c), inst_threads(c), 0, st>>>(c, P); mark("k_solid_time"); }
     return SPH_OK;
 }
 
@@ -1158,9 +1368,10 @@ __global__ void __launch_bounds__(kBlock) k_solid_elastic(Cst c, Ptr P) {
     double e = 0.0;
     if (i < c.n) {
         const int k = eos_of(P, i);
-        const float G = (k >= 0 && k < 4) ? c.p.mat_G[k] : 0.0f;
+        const int rows = c.n_inst > 0 ? c.n_inst : c.p.n_materials;
+        const float G = (k >= 0 && k < rows) ? P.mat[k].G : 0.0f;
         if (G > 0.0f) {
-            const float K = c.p.mat_K[k], rho0 = c.p.mat_rho0[k];
+            const float K = P.mat[k].K, rho0 = P.mat[k].rho0;
             const float V = P.cur.pos[4 * i + 3];
             const float rho = P.cur.vel[4 * i + 3] / V;
             const float theta = (rho - rho0) / rho0;
