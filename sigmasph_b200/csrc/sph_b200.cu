@@ -39,6 +39,8 @@ struct SphHandle {
     GridLayout* layout = nullptr;
     int* nbr = nullptr;
     int* nbr_cnt = nullptr;
+    int* shell = nullptr;
+    int* shell_cnt = nullptr;
     DevScalars* sc = nullptr;
     DevAccum* ac = nullptr;
     SphScalars* pinned = nullptr;   // page-locked staging of the scalar copies
@@ -116,6 +118,8 @@ Ptr make_ptr(SphHandle* h) {
     P.layout = h->layout;
     P.nbr = h->nbr;
     P.nbr_cnt = h->nbr_cnt;
+    P.shell = h->shell;
+    P.shell_cnt = h->shell_cnt;
     P.sc = h->sc;
     P.ac = h->ac;
     P.jc = solid_jc_ptr(h->solid);
@@ -168,7 +172,8 @@ int fluid_substep_and_boundary(SphHandle* h, cudaStream_t st) {
     LAUNCH("k_dt", k_dt<<<1, 32, 0, st>>>(c, P));
     LAUNCH("k_advect", k_advect<<<nb, kBlock, 0, st>>>(c, P));
     if (h->p.pst_enabled) {
-        LAUNCH("k_pst_search", k_pst_search<<<nb, kBlock, 0, st>>>(c, P));
+        // the fluid's shift reads the lists of the sort (k_pst, for_each_pst_neighbour)
+        if (!c.pst_skin) LAUNCH("k_pst_search", k_pst_search<<<nb, kBlock, 0, st>>>(c, P));
         LAUNCH("k_pst", k_pst<<<nb, kBlock, 0, st>>>(c, P));
         LAUNCH("k_finish", k_finish<<<nb, kBlock, 0, st>>>(c, P, 3));
     } else {
@@ -201,7 +206,7 @@ void free_all(SphHandle* h) {
     h->prof_pool.clear();
     if (h->cap_stream) cudaStreamDestroy(h->cap_stream);
     void* ptrs[] = {h->cell, h->cell_tmp, h->key, h->rank, h->perm, h->hist, h->start, h->bsum,
-                    h->bbox, h->layout, h->nbr, h->nbr_cnt, h->sc, h->ac};
+                    h->bbox, h->layout, h->nbr, h->nbr_cnt, h->shell, h->shell_cnt, h->sc, h->ac};
     for (void* q : ptrs) if (q) cudaFree(q);
     if (h->pinned) cudaFreeHost(h->pinned);
     solid_free(h->solid);
@@ -285,12 +290,17 @@ int sph_create(const SphParams* p, int64_t n_max, SphHandle** out) {
     double est = p->two_d ? M_PI * ratio * ratio * 1.5 : (4.0 / 3.0) * M_PI * ratio * ratio * ratio;
     int K = (int)std::ceil((1.5 * est + 16.0) / 32.0) * 32;
     K = std::max(32, std::min(K, 512));
+    // the shift's shell h <= |r| < 1.1 h: (1.1^d - 1) of the neighbour count, with headroom
+    const double shell_est = est * (p->two_d ? 0.21 : 0.331);
+    int Ks = (int)std::ceil((1.5 * shell_est + 16.0) / 32.0) * 32;
+    Ks = std::max(32, std::min(Ks, 256));
     int64_t mcap = 131072;
     while (mcap < 4 * n_max) mcap <<= 1;
     int lg = 0;
     while ((1ll << lg) < mcap) ++lg;
     h->n = 0;
     fill_constants(h);
+    h->c.Ks = Ks;
     h->c.K = K;
     h->c.mcap = (int)mcap;
     h->c.mcap_log2 = lg;
@@ -303,6 +313,7 @@ int sph_create(const SphParams* p, int64_t n_max, SphHandle** out) {
         (r = dalloc(&h->bsum, tiles)) || (r = dalloc(&h->bbox, 8)) ||
         (r = dalloc(&h->layout, 1)) || (r = dalloc(&h->nbr, N * (size_t)K)) ||
         (r = dalloc(&h->nbr_cnt, N)) || (r = dalloc(&h->sc, 1)) || (r = dalloc(&h->ac, 1)) ||
+        (!p->is_solid && ((r = dalloc(&h->shell, N * (size_t)Ks)) || (r = dalloc(&h->shell_cnt, N)))) ||
         cudaMallocHost((void**)&h->pinned, sizeof(SphScalars)) != cudaSuccess) {
         if (!r) r = SPH_ERR_NOMEM;
         free_all(h);
@@ -359,10 +370,11 @@ int sph_set_params(SphHandle* h, const SphParams* p) {
     if (!h || !p || p->struct_size != (int32_t)sizeof(SphParams)) return SPH_ERR_ARG;
     if (p->is_solid != h->p.is_solid) return SPH_ERR_ARG;
     if (p->is_solid && (p->n_materials < 1 || p->n_materials > 4)) return SPH_ERR_ARG;
-    int K = h->c.K, mcap = h->c.mcap, lg = h->c.mcap_log2, bs = h->c.block;
+    int K = h->c.K, mcap = h->c.mcap, lg = h->c.mcap_log2, bs = h->c.block, Ks = h->c.Ks;
     h->p = *p;
     fill_constants(h);
     h->c.K = K; h->c.mcap = mcap; h->c.mcap_log2 = lg; h->c.n = (int)h->n; h->c.block = bs;
+    h->c.Ks = Ks;
     int r = solid_sync_rows(h->solid, h->p, h->c);
     drop_graph(h);
     return r;
@@ -448,7 +460,7 @@ int sph_run_stage(SphHandle* h, int stage, void* stream) {
         case SPH_STAGE_ADVECT: k_advect<<<nb, kBlock, 0, st>>>(c, P); break;
         case SPH_STAGE_PST:
             if (h->p.pst_enabled) {
-                k_pst_search<<<nb, kBlock, 0, st>>>(c, P);
+                if (!c.pst_skin) k_pst_search<<<nb, kBlock, 0, st>>>(c, P);
                 k_pst<<<nb, kBlock, 0, st>>>(c, P);
                 k_finish<<<nb, kBlock, 0, st>>>(c, P, 1);
             }

@@ -37,7 +37,7 @@ struct DevAccum {
     unsigned int max_c_sq_bits;
     unsigned int max_accel_bits;
     unsigned int max_v_bits;
-    int pad;
+    unsigned int max_disp_bits;  // max |x - x_sort| of this step's advect (float bits)
     double hg_power;         // sum_i mw_i de_hg_i of the in-loop damper (solid)
 };
 
@@ -70,6 +70,11 @@ struct Cst {
     int any_plastic;     // some material row has a yield stress
     int all_gamma_one;   // every EOS is linear (exponent 1)
     int block;           // threads per block of the solid particle kernels
+    // the shift's candidate shell: pairs binned within h + skin at the sort
+    int pst_skin;        // 1: the shift pass reads the lists instead of searching again
+    int Ks;              // shell-list capacity per particle
+    float skin;          // skin width
+    float d2_skin;       // |r| < h + skin (conservative) in dist2_rn units
 };
 
 // Johnson-Cook return-map surrogate and sample log (solid only; null when unused).
@@ -109,6 +114,8 @@ struct Ptr {
     GridLayout* layout;
     int* nbr;            // [K][n] neighbour entries, k-major
     int* nbr_cnt;        // [n]
+    int* shell;          // [Ks][n] entries with h <= |r| < h + skin at the sort, k-major
+    int* shell_cnt;      // [n]
     DevScalars* sc;
     DevAccum* ac;
     JcPtr jc;

@@ -190,6 +190,7 @@ __global__ void __launch_bounds__(kBlock) k_eos(Cst c, Ptr P) {
         P.ac->w_diff_step = 0.0;
         P.ac->max_c_sq_bits = __float_as_uint(c.p.c_signal * c.p.c_signal);
         P.ac->max_accel_bits = __float_as_uint(1e-10f);
+        P.ac->max_disp_bits = 0u;
     }
     if (i >= c.n) return;
     float4* pos = as4(P.cur.pos);
@@ -303,7 +304,7 @@ __global__ void __launch_bounds__(kBlock) k_advect(Cst c, Ptr P) {
     int i = blockIdx.x * blockDim.x + threadIdx.x;
     const float dt = P.sc->dt;
     double wl = 0.0, wv = 0.0;
-    float vmag = 0.0f;
+    float vmag = 0.0f, disp = 0.0f;
     if (i < c.n) {
         float4 a4 = P.acc[i];
         float4* vel = as4(P.cur.vel);
@@ -327,6 +328,12 @@ __global__ void __launch_bounds__(kBlock) k_advect(Cst c, Ptr P) {
         } else {
             p.x += dt * v4.x; p.y += dt * v4.y; p.z += dt * v4.z;
         }
+        if (c.pst_skin) {
+            // how far this particle moved since the sort, rounded up (fmaxf drops NaN)
+            const float4 po = pos[i];
+            const F3 d = {p.x - po.x, p.y - po.y, p.z - po.z};
+            disp = norm3(d) * (1.0f + 1e-5f);
+        }
         pos[i] = p;
         if (c.p.pst_enabled && c.p.pst_ma_mode == 1 && !(isnan(p.x) || isnan(p.y) || isnan(p.z)))
             vmag = sqrtf(v4.x * v4.x + v4.y * v4.y + v4.z * v4.z);
@@ -348,6 +355,7 @@ __global__ void __launch_bounds__(kBlock) k_advect(Cst c, Ptr P) {
         }
     }
     if (c.p.pst_enabled && c.p.pst_ma_mode == 1) block_max_atomic(vmag, &P.ac->max_v_bits);
+    if (c.pst_skin) block_max_atomic(disp, &P.ac->max_disp_bits);
 }
 
 // ------------------------------------------------------------------ apply_pst (DSPH.py:725-1046)
@@ -393,6 +401,39 @@ __device__ __forceinline__ void for_each_live_neighbour(const Cst& c, const Ptr&
     }
 }
 
+// Pairs of the shift from the lists of the sort (fluid step): the neighbours proper and
+// the shell out to h + skin, each re-tested at the live positions.  That is the
+// reference's stale-bin live search exactly when this particle is still in its binned
+// cell (same 27-cell window) and no particle moved more than skin / 2 since the sort (so
+// every live pair within h was within h + skin then); otherwise -- or past either list's
+// capacity -- the live search runs for this particle.  Mirror entries keep the live
+// plane test of their sweep.
+template <class F>
+__device__ __forceinline__ void for_each_pst_neighbour(const Cst& c, const Ptr& P, int i, F3 xi, F&& f) {
+    const int4 ci = P.cell[i];
+    const int cnt = __ldg(P.nbr_cnt + i), scnt = __ldg(P.shell_cnt + i);
+    const float dmax = __uint_as_float(P.ac->max_disp_bits);
+    const int lx = cell_of(xi.x, c.h), ly = cell_of(xi.y, c.h), lz = cell_of(xi.z, c.h);
+    const bool fast = ci.w >= 0 && 2.0f * dmax <= c.skin && cnt <= c.K && scnt <= c.Ks &&
+                      lx == ci.x && ly == ci.y && lz == ci.z;
+    if (!fast) {
+        if (isnan(xi.x) || isnan(xi.y) || isnan(xi.z)) return;
+        const GridLayout L = *P.layout;
+        enumerate_neighbours(c, P, L, i, xi, lx, ly, lz, [&](int j, int mir, float4) { f(j, mir); });
+        return;
+    }
+    const float4* __restrict__ pos = as4c(P.cur.pos);
+    const bool py = xi.y < c.h, pz = xi.z < c.h;
+    auto take = [&](int j, int mir) {
+        if (mir && (((mir & 1) && !py) || ((mir & 2) && !pz))) return;
+        F3 xj = f3(__ldg(pos + j));
+        if (mir) xj = mirror3(mir, xj);
+        if (dist2_rn(xi, xj) < c.d2_lt) f(j, mir);
+    };
+    list_pairs(P.nbr + i, (size_t)c.n, cnt, take);
+    list_pairs(P.shell + i, (size_t)c.n, scnt, take);
+}
+
 __global__ void __launch_bounds__(kBlock) k_pst(Cst c, Ptr P) {
     int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= c.n) return;
@@ -406,7 +447,7 @@ __global__ void __launch_bounds__(kBlock) k_pst(Cst c, Ptr P) {
     {
         const float Wd = c.W_dx0;
         const float inv_Wd = Wd > 0.0f ? 1.0f / Wd : 0.0f;
-        for_each_live_neighbour(c, P, i, xi, [&](int j, int mir) {
+        auto pair = [&](int j, int mir) {
             float4 pj = __ldg(pos + j);
             F3 xj = f3(pj);
             if (mir) xj = mirror3(mir, xj);
@@ -428,7 +469,9 @@ __global__ void __launch_bounds__(kBlock) k_pst(Cst c, Ptr P) {
                     if (ra > 1e-10f) sr += ((1.0f + f) * (mj / ra)) * g;
                 }
             }
-        });
+        };
+        if (c.pst_skin) for_each_pst_neighbour(c, P, i, xi, pair);
+        else for_each_live_neighbour(c, P, i, xi, pair);
     }
     float4 vi4 = vel[i];
     F3 vi = f3(vi4);

@@ -280,13 +280,16 @@ __device__ __forceinline__ void bucket_candidates(const Ptr& P, bool hashed, int
 
 // The y, z and corner mirror sweeps of a particle at xi in cell (cx, cy, cz)
 // (particle_system.py:1442-1490): the image of xi against the cells of the y = 0 row,
-// the z = 0 row and the corner column; a particle pairs with its own image too.
+// the z = 0 row and the corner column; a particle pairs with its own image too.  A sweep
+// runs when xi is within hcut of its plane; f(j, mirror, pos_j, d2) gets every candidate
+// with d2 < d2cut (the neighbour test uses hcut = h, d2cut = the |r| < h threshold).
 template <class F>
-__device__ __forceinline__ void enumerate_mirrors(const Cst& c, const Ptr& P, const GridLayout& L,
-                                                  F3 xi, int cx, int cy, int cz, F&& f) {
+__device__ __forceinline__ void enumerate_mirrors_cut(const Cst& c, const Ptr& P, const GridLayout& L,
+                                                      F3 xi, int cx, int cy, int cz, float d2cut,
+                                                      float hcut, F&& f) {
     const float4* __restrict__ pos = reinterpret_cast<const float4*>(P.cur.pos);
     const bool hashed = L.mode != 0;
-    if (c.mirror_y && xi.y < c.h) {
+    if (c.mirror_y && xi.y < hcut) {
         const F3 xm = mirror3(1, xi);
 #pragma unroll 1
         for (int o0 = -1; o0 <= 1; ++o0)
@@ -297,11 +300,12 @@ __device__ __forceinline__ void enumerate_mirrors(const Cst& c, const Ptr& P, co
                 if (b < 0) continue;
                 bucket_candidates(P, hashed, b, nx, ny, nz, [&](int j) {
                     const float4 pj = __ldg(pos + j);
-                    if (dist2_rn(xm, f3(pj)) < c.d2_lt) f(j, 1, pj);
+                    const float d2 = dist2_rn(xm, f3(pj));
+                    if (d2 < d2cut) f(j, 1, pj, d2);
                 });
             }
     }
-    if (c.mirror_z && xi.z < c.h) {
+    if (c.mirror_z && xi.z < hcut) {
         const F3 xm = mirror3(2, xi);
 #pragma unroll 1
         for (int o0 = -1; o0 <= 1; ++o0)
@@ -312,11 +316,12 @@ __device__ __forceinline__ void enumerate_mirrors(const Cst& c, const Ptr& P, co
                 if (b < 0) continue;
                 bucket_candidates(P, hashed, b, nx, ny, nz, [&](int j) {
                     const float4 pj = __ldg(pos + j);
-                    if (dist2_rn(xm, f3(pj)) < c.d2_lt) f(j, 2, pj);
+                    const float d2 = dist2_rn(xm, f3(pj));
+                    if (d2 < d2cut) f(j, 2, pj, d2);
                 });
             }
     }
-    if (c.mirror_y && c.mirror_z && xi.y < c.h && xi.z < c.h) {
+    if (c.mirror_y && c.mirror_z && xi.y < hcut && xi.z < hcut) {
         const F3 xm = mirror3(3, xi);
 #pragma unroll 1
         for (int o0 = -1; o0 <= 1; ++o0) {
@@ -325,20 +330,21 @@ __device__ __forceinline__ void enumerate_mirrors(const Cst& c, const Ptr& P, co
             if (b < 0) continue;
             bucket_candidates(P, hashed, b, nx, ny, nz, [&](int j) {
                 const float4 pj = __ldg(pos + j);
-                if (dist2_rn(xm, f3(pj)) < c.d2_lt) f(j, 3, pj);
+                const float d2 = dist2_rn(xm, f3(pj));
+                if (d2 < d2cut) f(j, 3, pj, d2);
             });
         }
     }
 }
 
-// Calls f(j, mirror, pos_j) for every neighbour of a particle at xi whose centre cell is
-// (cx, cy, cz), in the reference's order: the 27 offsets with the last index fastest,
-// then the y, z and corner mirror sweeps (particle_system.py:1393-1490).  `self_idx` is
-// excluded from the real sweep only.  Positions are read from `pos` (live positions).
+// Every candidate of a particle at xi whose centre cell is (cx, cy, cz) with d2 < d2cut,
+// in the reference's order: the 27 offsets with the last index fastest, then the y, z and
+// corner mirror sweeps (particle_system.py:1393-1490).  `self_idx` is excluded from the
+// real sweep only.  Positions are read from `pos` (live positions).
 template <class F>
-__device__ __forceinline__ void enumerate_neighbours(const Cst& c, const Ptr& P, const GridLayout& L,
-                                                     int self_idx, F3 xi, int cx, int cy, int cz,
-                                                     F&& f) {
+__device__ __forceinline__ void enumerate_cut(const Cst& c, const Ptr& P, const GridLayout& L, int self_idx,
+                                              F3 xi, int cx, int cy, int cz, float d2cut, float hcut,
+                                              F&& f) {
     const float4* __restrict__ pos = reinterpret_cast<const float4*>(P.cur.pos);
     const bool hashed = L.mode != 0;
 #pragma unroll 1
@@ -353,10 +359,20 @@ __device__ __forceinline__ void enumerate_neighbours(const Cst& c, const Ptr& P,
                 bucket_candidates(P, hashed, b, nx, ny, nz, [&](int j) {
                     if (j == self_idx) return;
                     const float4 pj = __ldg(pos + j);
-                    if (dist2_rn(xi, f3(pj)) < c.d2_lt) f(j, 0, pj);
+                    const float d2 = dist2_rn(xi, f3(pj));
+                    if (d2 < d2cut) f(j, 0, pj, d2);
                 });
             }
-    enumerate_mirrors(c, P, L, xi, cx, cy, cz, f);
+    enumerate_mirrors_cut(c, P, L, xi, cx, cy, cz, d2cut, hcut, f);
+}
+
+// The neighbours proper: f(j, mirror, pos_j) for |r| < h (bit-exact against the reference).
+template <class F>
+__device__ __forceinline__ void enumerate_neighbours(const Cst& c, const Ptr& P, const GridLayout& L,
+                                                     int self_idx, F3 xi, int cx, int cy, int cz,
+                                                     F&& f) {
+    enumerate_cut(c, P, L, self_idx, xi, cx, cy, cz, c.d2_lt, c.h,
+                  [&](int j, int mir, float4 pj, float) { f(j, mir, pj); });
 }
 
 // Builds the neighbour list of every particle from the positions the cells were binned
@@ -368,15 +384,40 @@ __global__ void __launch_bounds__(kBlock) k_nbr_build(Cst c, Ptr P) {
     if (i >= c.n) return;
     const GridLayout L = *P.layout;
     const int4 ci = P.cell[i];
-    if (ci.w < 0) { P.nbr_cnt[i] = 0; return; }
+    if (ci.w < 0) {
+        P.nbr_cnt[i] = 0;
+        if (c.pst_skin) P.shell_cnt[i] = 0;
+        return;
+    }
     const F3 xi = f3(reinterpret_cast<const float4*>(P.cur.pos)[i]);
     int cnt = 0;
     const int n = c.n, K = c.K;
     int* __restrict__ nb = P.nbr;
-    enumerate_neighbours(c, P, L, i, xi, ci.x, ci.y, ci.z, [&](int j, int mir, float4) {
-        if (cnt < K) nb[(size_t)cnt * n + i] = j | (mir << kMirShift);
-        ++cnt;
-    });
+    if (c.pst_skin) {
+        // the same sweep out to h + skin: neighbours proper go to the list (in the same
+        // order as without the shell), the rest of the shell to the shift's candidates
+        int scnt = 0;
+        const int Ks = c.Ks;
+        int* __restrict__ sb = P.shell;
+        enumerate_cut(c, P, L, i, xi, ci.x, ci.y, ci.z, c.d2_skin, c.h + c.skin,
+                      [&](int j, int mir, float4, float d2) {
+            const bool plane = mir == 0 || (((mir & 1) == 0 || xi.y < c.h) && ((mir & 2) == 0 || xi.z < c.h));
+            const int e = j | (mir << kMirShift);
+            if (d2 < c.d2_lt && plane) {
+                if (cnt < K) nb[(size_t)cnt * n + i] = e;
+                ++cnt;
+            } else {
+                if (scnt < Ks) sb[(size_t)scnt * n + i] = e;
+                ++scnt;
+            }
+        });
+        P.shell_cnt[i] = scnt;
+    } else {
+        enumerate_neighbours(c, P, L, i, xi, ci.x, ci.y, ci.z, [&](int j, int mir, float4) {
+            if (cnt < K) nb[(size_t)cnt * n + i] = j | (mir << kMirShift);
+            ++cnt;
+        });
+    }
     if (cnt > K) atomicOr(&P.sc->err, SPH_EW_NBR_OVERFLOW);
     P.nbr_cnt[i] = cnt;
 }

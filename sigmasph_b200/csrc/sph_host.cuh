@@ -25,6 +25,15 @@ inline void fill_constants_from(const SphParams& p, int64_t n, Cst& c) {
     c.any_plastic = 0;
     c.all_gamma_one = 1;
     c.block = kBlock;
+    // skin of the shift's candidate shell: a tenth of the support; the squared cut is
+    // rounded up so that it contains every pair a float32 distance test could place
+    // within h + skin
+    {
+        const double hs = p.support_radius;
+        c.skin = (float)(0.1 * hs);
+        c.d2_skin = (float)((1.1 * hs) * (1.1 * hs) * (1.0 + 1e-5));
+    }
+    c.pst_skin = p.is_solid ? 0 : 1;
     double hd = p.support_radius;
     double al = p.two_d ? 7.0 / (M_PI * hd * hd) : 21.0 / (2.0 * M_PI * hd * hd * hd);
     c.h = (float)hd;
