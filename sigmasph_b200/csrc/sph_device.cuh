@@ -14,8 +14,9 @@ constexpr int kBlock = 256;          // threads per block of the particle-parall
 // resident warps pay more than the spills cost.  Kernels that keep a 3x3 stress and
 // velocity gradient per pair live keep the compiler's default budget.
 #define SPH_PAIR_BOUNDS_OCC4 __launch_bounds__(kBlock, 4)
-constexpr int kMirShift = 30;        // neighbour entry = j | (mirror code << 30)
-constexpr int kIdxMask = (1 << kMirShift) - 1;
+constexpr int kMirShift = 30;        // neighbour entry = j | rim << 29 | mirror code << 30
+constexpr int kRimBit = 1 << 29;     // the pair may leave the support before the shift pass
+constexpr int kIdxMask = kRimBit - 1;
 
 // Cell layout of the current rebuild, written by k_layout on the device.
 struct GridLayout {
@@ -38,6 +39,8 @@ struct DevAccum {
     unsigned int max_accel_bits;
     unsigned int max_v_bits;
     unsigned int max_disp_bits;  // max |x - x_sort| of this step's advect (float bits)
+    unsigned int max_grip_disp_bits;  // max position change of the grips' overwrite
+    int pad2;
     double hg_power;         // sum_i mw_i de_hg_i of the in-loop damper (solid)
 };
 
@@ -75,6 +78,7 @@ struct Cst {
     int Ks;              // shell-list capacity per particle
     float skin;          // skin width
     float d2_skin;       // |r| < h + skin (conservative) in dist2_rn units
+    float d2_deep;       // |r| < h - skin (conservative): stays within h under the bound
 };
 
 // Johnson-Cook return-map surrogate and sample log (solid only; null when unused).

@@ -191,6 +191,7 @@ __global__ void __launch_bounds__(kBlock) k_eos(Cst c, Ptr P) {
         P.ac->max_c_sq_bits = __float_as_uint(c.p.c_signal * c.p.c_signal);
         P.ac->max_accel_bits = __float_as_uint(1e-10f);
         P.ac->max_disp_bits = 0u;
+        P.ac->max_grip_disp_bits = 0u;
     }
     if (i >= c.n) return;
     float4* pos = as4(P.cur.pos);
@@ -412,7 +413,7 @@ template <class F>
 __device__ __forceinline__ void for_each_pst_neighbour(const Cst& c, const Ptr& P, int i, F3 xi, F&& f) {
     const int4 ci = P.cell[i];
     const int cnt = __ldg(P.nbr_cnt + i), scnt = __ldg(P.shell_cnt + i);
-    const float dmax = __uint_as_float(P.ac->max_disp_bits);
+    const float dmax = __uint_as_float(P.ac->max_disp_bits) + __uint_as_float(P.ac->max_grip_disp_bits);
     const int lx = cell_of(xi.x, c.h), ly = cell_of(xi.y, c.h), lz = cell_of(xi.z, c.h);
     const bool fast = ci.w >= 0 && 2.0f * dmax <= c.skin && cnt <= c.K && scnt <= c.Ks &&
                       lx == ci.x && ly == ci.y && lz == ci.z;
@@ -424,17 +425,22 @@ __device__ __forceinline__ void for_each_pst_neighbour(const Cst& c, const Ptr& 
     }
     const float4* __restrict__ pos = as4c(P.cur.pos);
     const bool py = xi.y < c.h, pz = xi.z < c.h;
-    auto take = [&](int j, int mir) {
+    // entries deeper than h - skin at the sort are still within h: no live test
+    auto take = [&](int e) {
+        const int j = e & kIdxMask, mir = (int)((unsigned)e >> kMirShift);
         if (mir && (((mir & 1) && !py) || ((mir & 2) && !pz))) return;
-        F3 xj = f3(__ldg(pos + j));
-        if (mir) xj = mirror3(mir, xj);
-        if (dist2_rn(xi, xj) < c.d2_lt) f(j, mir);
+        if (e & kRimBit) {
+            F3 xj = f3(__ldg(pos + j));
+            if (mir) xj = mirror3(mir, xj);
+            if (!(dist2_rn(xi, xj) < c.d2_lt)) return;
+        }
+        f(j, mir);
     };
-    list_pairs(P.nbr + i, (size_t)c.n, cnt, take);
-    list_pairs(P.shell + i, (size_t)c.n, scnt, take);
+    list_entries(P.nbr + i, (size_t)c.n, cnt, take);
+    list_entries(P.shell + i, (size_t)c.n, scnt, take);
 }
 
-__global__ void __launch_bounds__(kBlock) k_pst(Cst c, Ptr P) {
+__global__ void __launch_bounds__(kBlock, 5) k_pst(Cst c, Ptr P) {
     int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= c.n) return;
     const float4* __restrict__ pos = as4c(P.cur.pos);

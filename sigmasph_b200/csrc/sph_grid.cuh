@@ -402,7 +402,7 @@ __global__ void __launch_bounds__(kBlock) k_nbr_build(Cst c, Ptr P) {
         enumerate_cut(c, P, L, i, xi, ci.x, ci.y, ci.z, c.d2_skin, c.h + c.skin,
                       [&](int j, int mir, float4, float d2) {
             const bool plane = mir == 0 || (((mir & 1) == 0 || xi.y < c.h) && ((mir & 2) == 0 || xi.z < c.h));
-            const int e = j | (mir << kMirShift);
+            const int e = j | (d2 < c.d2_deep ? 0 : kRimBit) | (mir << kMirShift);
             if (d2 < c.d2_lt && plane) {
                 if (cnt < K) nb[(size_t)cnt * n + i] = e;
                 ++cnt;
@@ -426,7 +426,7 @@ __global__ void __launch_bounds__(kBlock) k_nbr_build(Cst c, Ptr P) {
 // flight while the current pair is evaluated (the pair passes are bound by the latency
 // of the dependent list -> particle gathers).
 template <class F>
-__device__ __forceinline__ void list_pairs(const int* __restrict__ nb, size_t n, int m, F&& f) {
+__device__ __forceinline__ void list_entries(const int* __restrict__ nb, size_t n, int m, F&& f) {
     int e0 = m > 0 ? __ldg(nb) : 0;
     int e1 = m > 1 ? __ldg(nb + n) : 0;
 #pragma unroll 2
@@ -434,8 +434,12 @@ __device__ __forceinline__ void list_pairs(const int* __restrict__ nb, size_t n,
         const int e = e0;
         e0 = e1;
         if (k + 2 < m) e1 = __ldg(nb + (size_t)(k + 2) * n);
-        f(e & kIdxMask, (int)((unsigned)e >> kMirShift));
+        f(e);
     }
+}
+template <class F>
+__device__ __forceinline__ void list_pairs(const int* __restrict__ nb, size_t n, int m, F&& f) {
+    list_entries(nb, n, m, [&](int e) { f(e & kIdxMask, (int)((unsigned)e >> kMirShift)); });
 }
 
 // Calls f(j, mirror) for the stored neighbours of i, then for any beyond the list's

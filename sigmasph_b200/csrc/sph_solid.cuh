@@ -209,6 +209,10 @@ __device__ __forceinline__ float solid_pressure(const Cst& c, const Ptr& P, int 
 
 // ------------------------------------------------------------------ load factor
 __global__ void k_solid_load(Cst c, Ptr P) {
+    if (blockIdx.x == 0 && threadIdx.x == 0) {   // this step's displacement bounds
+        P.ac->max_disp_bits = 0u;
+        P.ac->max_grip_disp_bits = 0u;
+    }
     if (c.n_inst > 0) {
         // per instance: its smoothstep from its own clock, and a fresh dt maximum
         for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < c.n_inst; k += gridDim.x * blockDim.x) {
@@ -1130,6 +1134,7 @@ __global__ void __launch_bounds__(kBlock) k_hg_stage(Cst c, Ptr P, int stage) {
 __global__ void __launch_bounds__(kBlock) k_sts_finish(Cst c, Ptr P) {
     int i = blockIdx.x * blockDim.x + threadIdx.x;
     double ke = 0.0, wl = 0.0;
+    float disp = 0.0f;
     if (i < c.n) {
         const int ki = eos_of(P, i);
         const int s = c.n_inst > 0 ? P.inst[ki].sts_stages : P.sc->sts_stages;
@@ -1158,15 +1163,21 @@ __global__ void __launch_bounds__(kBlock) k_sts_finish(Cst c, Ptr P) {
         } else {
             p.x += dt * v.x; p.y += dt * v.y; p.z += dt * v.z;
         }
+        if (c.pst_skin) {
+            const float4 po = pos[i];
+            disp = norm3(F3{p.x - po.x, p.y - po.y, p.z - po.z}) * (1.0f + 1e-5f);
+        }
         pos[i] = p;
     }
     block_sum_atomic(ke, &P.sc->hg_work);
     block_sum_atomic(wl, &P.sc->leftover_work);
+    if (c.pst_skin) block_max_atomic(disp, &P.ac->max_disp_bits);
 }
 
 __global__ void __launch_bounds__(kBlock) k_solid_advect(Cst c, Ptr P) {
     int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= c.n) return;
+    float disp = 0.0f;
+    if (i < c.n) {
     const float dt = dt_at(c, P, eos_of(P, i));
     float4* vel = as4(P.cur.vel);
     float4 v = vel[i];
@@ -1185,7 +1196,13 @@ __global__ void __launch_bounds__(kBlock) k_solid_advect(Cst c, Ptr P) {
     } else {
         p.x += dt * v.x; p.y += dt * v.y; p.z += dt * v.z;
     }
+    if (c.pst_skin) {
+        const float4 po = pos[i];
+        disp = norm3(F3{p.x - po.x, p.y - po.y, p.z - po.z}) * (1.0f + 1e-5f);
+    }
     pos[i] = p;
+    }
+    if (c.pst_skin) block_max_atomic(disp, &P.ac->max_disp_bits);
 }
 
 // ------------------------------------------------------------------ grips
@@ -1199,6 +1216,7 @@ __device__ __forceinline__ void constraints_ensemble(const Cst& c, const Ptr& P)
     int2 bc = make_int2(0, -1);
     if (i < c.n) bc = reinterpret_cast<const int2*>(P.cur.bc)[i];
     int k = 0, g = 0;
+    float gdisp = 0.0f;
     double fd[3] = {0.0, 0.0, 0.0};
     bool rec[3] = {false, false, false};
     if (bc.x != 0) {
@@ -1220,6 +1238,7 @@ __device__ __forceinline__ void constraints_ensemble(const Cst& c, const Ptr& P)
         const float x0c[3] = {x0.x, x0.y, x0.z};
         const bool record = bc.y == 0 || bc.y == 1;
         g = record ? bc.y : 0;
+        const float4 po = p;
 #pragma unroll
         for (int d = 0; d < 3; ++d) {
             if (!(bc.x & (1 << d))) continue;
@@ -1234,13 +1253,17 @@ __device__ __forceinline__ void constraints_ensemble(const Cst& c, const Ptr& P)
             *ac[d] = 0.0f;
         }
         pos[i] = p; vel[i] = v; dsp[i] = u; P.acc[i] = a;
+        gdisp = norm3(F3{p.x - po.x, p.y - po.y, p.z - po.z}) * (1.0f + 1e-5f);
     }
 #pragma unroll
     for (int d = 0; d < 3; ++d) addr_add_atomic(fd[d], &P.inst[k].constraint_force[g][d], rec[d]);
+    const float wm = warp_max(gdisp);
+    if ((threadIdx.x & 31) == 0 && wm > 0.0f) atomicMax(&P.ac->max_grip_disp_bits, __float_as_uint(wm));
 }
 
 __global__ void __launch_bounds__(kBlock) k_constraints(Cst c, Ptr P) {
     if (c.n_inst > 0) { constraints_ensemble(c, P); return; }
+    float gdisp = 0.0f;
     __shared__ double s_force[8][3];
     __shared__ float s_disp[8][3];
     __shared__ int s_axes[8];
@@ -1268,6 +1291,7 @@ __global__ void __launch_bounds__(kBlock) k_constraints(Cst c, Ptr P) {
         const float x0c[3] = {x0.x, x0.y, x0.z};
         const bool record = c.p.num_constraints > 0 && bc.y >= 0 && bc.y < 8;
         if (record) atomicOr(&s_axes[bc.y], bc.x & 7);
+        const float4 po = p;
 #pragma unroll
         for (int d = 0; d < 3; ++d) {
             if (!(bc.x & (1 << d))) continue;
@@ -1281,8 +1305,10 @@ __global__ void __launch_bounds__(kBlock) k_constraints(Cst c, Ptr P) {
             *ac[d] = 0.0f;
         }
         pos[i] = p; vel[i] = v; dsp[i] = u; P.acc[i] = a;
+        gdisp = norm3(F3{p.x - po.x, p.y - po.y, p.z - po.z}) * (1.0f + 1e-5f);
     }
-    __syncthreads();
+    if (c.pst_skin) block_max_atomic(gdisp, &P.ac->max_grip_disp_bits);
+    else __syncthreads();
     if (threadIdx.x < 24) {
         const int k = threadIdx.x / 3, d = threadIdx.x % 3;
         if (s_axes[k] & (1 << d)) {
@@ -1350,7 +1376,7 @@ inline int solid_substep_launch(const Cst& c, const Ptr& P, int n, cudaStream_t 
         k_constraints<<<nb, bs, 0, st>>>(c, P); mark("k_constraints");
     }
     if (in(SPH_STAGE_PST) && c.p.pst_enabled) {
-        k_pst_search<<<nb, bs, 0, st>>>(c, P); mark("k_pst_search");
+        if (!c.pst_skin) { k_pst_search<<<nb, bs, 0, st>>>(c, P); mark("k_pst_search"); }
         k_pst<<<nb, bs, 0, st>>>(c, P); mark("k_pst");
         k_finish<<<nb, bs, 0, st>>>(c, P, last_stage >= SPH_STAGE_BOUNDARY ? 3 : 1); mark("k_finish");
     } else if (in(SPH_STAGE_BOUNDARY)) {
