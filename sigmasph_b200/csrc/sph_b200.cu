@@ -771,11 +771,12 @@ int sph_ensemble_set(SphHandle* h, const SphMatRow* mat, const SphInstRow* inst,
     CK(cudaMemcpyAsync(h->solid.irow, inst, sizeof(SphInstRow) * n_inst, cudaMemcpyHostToDevice, st));
     CK(cudaMemcpyAsync(h->solid.inst, s0.data(), sizeof(SphInstState) * n_inst, cudaMemcpyHostToDevice, st));
     CK(cudaStreamSynchronize(st));           // s0 is a host temporary
-    solid_row_flags(mat, n_inst, h->solid.any_plastic, h->solid.all_gamma_one);
+    solid_row_flags(mat, n_inst, h->solid.any_plastic, h->solid.all_gamma_one, h->solid.any_jc);
     h->solid.n_inst = n_inst;
     h->c.n_inst = n_inst;
     h->c.any_plastic = h->solid.any_plastic;
     h->c.all_gamma_one = h->solid.all_gamma_one;
+    h->c.any_jc = h->solid.any_jc;
     drop_graph(h);
     return SPH_OK;
 }

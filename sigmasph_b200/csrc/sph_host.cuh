@@ -24,6 +24,7 @@ inline void fill_constants_from(const SphParams& p, int64_t n, Cst& c) {
     c.n_inst = 0;
     c.any_plastic = 0;
     c.all_gamma_one = 1;
+    c.any_jc = 0;
     c.block = kBlock;
     // skin of the shift's candidate shell: a tenth of the support; the squared cut is
     // rounded up so that it contains every pair a float32 distance test could place

@@ -53,7 +53,7 @@ struct SolidScratch {
     SphInstRow* irow = nullptr;
     SphInstState* inst = nullptr;
     int n_inst = 0;
-    bool any_plastic = false, all_gamma_one = true;
+    bool any_plastic = false, all_gamma_one = true, any_jc = false;
 };
 constexpr int kMaxInstances = 1024;
 
@@ -81,12 +81,15 @@ inline void solid_rows_from_params(const SphParams& p, SphMatRow* rows) {
         r.cv = p.mat_cv[k]; r.stiff = p.mat_stiff[k]; r.gamma = p.mat_gamma[k]; r.T0 = p.mat_T0[k];
     }
 }
-inline void solid_row_flags(const SphMatRow* rows, int n, bool& any_plastic, bool& all_gamma_one) {
+inline void solid_row_flags(const SphMatRow* rows, int n, bool& any_plastic, bool& all_gamma_one,
+                            bool& any_jc) {
     any_plastic = false;
     all_gamma_one = true;
+    any_jc = false;
     for (int k = 0; k < n; ++k) {
         any_plastic = any_plastic || rows[k].sy0 > 0.0f;
         all_gamma_one = all_gamma_one && rows[k].gamma == 1.0f;
+        any_jc = any_jc || rows[k].plastic_kind == 2;
     }
 }
 // Uploads the scene's own rows (single-scene mode) and sets the table flags in c.
@@ -96,14 +99,16 @@ inline int solid_sync_rows(SolidScratch& s, const SphParams& p, Cst& c) {
         c.n_inst = s.n_inst;
         c.any_plastic = s.any_plastic;
         c.all_gamma_one = s.all_gamma_one;
+        c.any_jc = s.any_jc;
         return SPH_OK;
     }
     SphMatRow rows[4] = {};
     solid_rows_from_params(p, rows);
-    solid_row_flags(rows, p.n_materials, s.any_plastic, s.all_gamma_one);
+    solid_row_flags(rows, p.n_materials, s.any_plastic, s.all_gamma_one, s.any_jc);
     c.n_inst = 0;
     c.any_plastic = s.any_plastic;
     c.all_gamma_one = s.all_gamma_one;
+    c.any_jc = s.any_jc;
     if (cudaMemcpy(s.mat, rows, sizeof(rows), cudaMemcpyHostToDevice) != cudaSuccess) return SPH_ERR_CUDA;
     return SPH_OK;
 }
@@ -364,7 +369,7 @@ __global__ void __launch_bounds__(kBlock) k_kc_inverse(Cst c, Ptr P) {
 }
 
 // ------------------------------------------------------------------ pass A
-__global__ void SPH_PAIR_BOUNDS_OCC4 k_solid_a(Cst c, Ptr P) {
+__global__ void SPH_PAIR_BOUNDS_OCC3 k_solid_a(Cst c, Ptr P) {
     int i = blockIdx.x * blockDim.x + threadIdx.x;
     double wdiff = 0.0;
     if (i < c.n) {
@@ -417,7 +422,7 @@ __global__ void SPH_PAIR_BOUNDS_OCC4 k_solid_a(Cst c, Ptr P) {
             r0 += Vj * dot3(vhat_i - vh_j, g);
             int kj = eos_of(P, j);
             if (kj == ki) {   // pair_delta (SOLID.py:4103-4114) on same-material pairs
-                float dj = P.mat[kj].delta;
+                const float dj = di;          // same material row
                 float den = di + dj;
                 float dl = den > 1e-12f ? 2.0f * di * dj / den : 0.0f;
                 if (dl > 0.0f) {
@@ -588,7 +593,7 @@ __device__ __forceinline__ void block_count_add(unsigned v, unsigned long long* 
     if (threadIdx.x == 0 && s_cnt && dst) atomicAdd(dst, (unsigned long long)s_cnt);
 }
 
-__global__ void __launch_bounds__(kBlock) k_solid_b(Cst c, Ptr P) {
+__global__ void SPH_PAIR_BOUNDS_OCC3 k_solid_b(Cst c, Ptr P) {
     int i = blockIdx.x * blockDim.x + threadIdx.x;
     double pw = 0.0, wl = 0.0;
     bool capped_any = false;
@@ -770,7 +775,7 @@ __global__ void __launch_bounds__(kBlock) k_solid_b(Cst c, Ptr P) {
     if (__syncthreads_or(capped_any) && threadIdx.x == 0) atomicOr(&P.sc->err, SPH_EW_JC_NO_CONVERGE);
     block_sum_atomic(pw, &P.sc->plastic_work);
     block_sum_atomic(wl, &P.sc->leftover_work);
-    if (P.jc.stats) {
+    if (c.any_jc && P.jc.stats) {
         block_count_add(newton_solves, P.jc.stats + 0);
         block_count_add(newton_iters, P.jc.stats + 1);
     }
@@ -876,7 +881,7 @@ __global__ void __launch_bounds__(kBlock) k_solid_commit(Cst c, Ptr P) {
 }
 
 // ------------------------------------------------------------------ stress force
-__global__ void __launch_bounds__(kBlock) k_solid_force(Cst c, Ptr P) {
+__global__ void SPH_PAIR_BOUNDS_OCC3 k_solid_force(Cst c, Ptr P) {
     int i = blockIdx.x * blockDim.x + threadIdx.x;
     float amag = 0.0f, csq = 0.0f;
     double hgp = 0.0;
