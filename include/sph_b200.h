@@ -287,6 +287,14 @@ int  sph_reduce(SphHandle* h, double* out, void* stream);
  * (i, j, mirror) triples as current-order indices and the total into *count. */
 int  sph_pairs(SphHandle* h, int mode, int32_t* pi, int32_t* pj, int32_t* mir,
                int64_t cap, int64_t* count, void* stream);
+/* The pairs the shift pass evaluates at the current positions (the PST sweep,
+ * DSPH.py:771-886): the lists of the last rebuild re-tested at the live positions, with
+ * the live search for the particles the lists cannot serve.  disp_bound >= 0 stands for
+ * the largest distance a particle moved since the last rebuild (the caller vouches for
+ * it); < 0 uses the bound the step's advect and grips recorded.  As a set, equal to
+ * sph_pairs mode 1 whenever the bound holds.  Output as sph_pairs. */
+int  sph_shift_pairs(SphHandle* h, float disp_bound, int32_t* pi, int32_t* pj, int32_t* mir,
+                     int64_t cap, int64_t* count, void* stream);
 
 /* Per-kernel timing with CUDA events recorded on the launching stream around every
  * kernel of eagerly launched steps (sph_step with nsteps == 1, sph_run_stage).  Off by

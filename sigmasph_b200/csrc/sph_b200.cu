@@ -313,7 +313,7 @@ int sph_create(const SphParams* p, int64_t n_max, SphHandle** out) {
         (r = dalloc(&h->bsum, tiles)) || (r = dalloc(&h->bbox, 8)) ||
         (r = dalloc(&h->layout, 1)) || (r = dalloc(&h->nbr, N * (size_t)K)) ||
         (r = dalloc(&h->nbr_cnt, N)) || (r = dalloc(&h->sc, 1)) || (r = dalloc(&h->ac, 1)) ||
-        (!p->is_solid && ((r = dalloc(&h->shell, N * (size_t)Ks)) || (r = dalloc(&h->shell_cnt, N)))) ||
+        (r = dalloc(&h->shell, N * (size_t)Ks)) || (r = dalloc(&h->shell_cnt, N)) ||
         cudaMallocHost((void**)&h->pinned, sizeof(SphScalars)) != cudaSuccess) {
         if (!r) r = SPH_ERR_NOMEM;
         free_all(h);
@@ -521,22 +521,68 @@ int sph_reduce(SphHandle* h, double* out, void* stream) {
 }  // extern "C"
 
 namespace {
-__global__ void k_pairs_live(Cst c, Ptr P, const int* off, int* out_i, int* out_j, int* out_m, int write) {
+// Pair export: one thread per particle counts (off == nullptr, counts to cnt_out) or
+// writes its pairs at off[i].  kShift 0: the live search against the current bins;
+// kShift 1: the pairs the shift pass evaluates (for_each_pst_neighbour).
+template <int kShift>
+__global__ void k_pairs_export(Cst c, Ptr P, const int* off, int* cnt_out, int* out_i, int* out_j,
+                               int* out_m) {
     int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= c.n) return;
-    float4 pi = reinterpret_cast<const float4*>(P.cur.pos)[i];
-    F3 xi = f3(pi);
+    const F3 xi = f3(reinterpret_cast<const float4*>(P.cur.pos)[i]);
     int cnt = 0;
-    if (!(isnan(xi.x) || isnan(xi.y) || isnan(xi.z))) {
+    const int base = off ? off[i] : 0;
+    auto emit = [&](int j, int mir) {
+        if (off) { out_i[base + cnt] = i; out_j[base + cnt] = j; out_m[base + cnt] = mir; }
+        ++cnt;
+    };
+    if (kShift) {
+        for_each_pst_neighbour(c, P, i, xi, emit);
+    } else if (!(isnan(xi.x) || isnan(xi.y) || isnan(xi.z))) {
         const GridLayout L = *P.layout;
         int cx = cell_of(xi.x, c.h), cy = cell_of(xi.y, c.h), cz = cell_of(xi.z, c.h);
-        int base = write ? off[i] : 0;
-        enumerate_neighbours(c, P, L, i, xi, cx, cy, cz, [&](int j, int mir, float4) {
-            if (write) { out_i[base + cnt] = i; out_j[base + cnt] = j; out_m[base + cnt] = mir; }
-            ++cnt;
-        });
+        enumerate_neighbours(c, P, L, i, xi, cx, cy, cz, [&](int j, int mir, float4) { emit(j, mir); });
     }
-    if (!write) P.nbr_cnt[i] = cnt;  // reused as a count buffer; restored by the caller
+    if (!off) cnt_out[i] = cnt;
+}
+
+// Counts, then writes, the pairs of one export kernel into host arrays.
+template <int kShift>
+int export_pairs(SphHandle* h, int32_t* pi, int32_t* pj, int32_t* mir, int64_t cap, int64_t* count,
+                 cudaStream_t st) {
+    const int n = (int)h->n;
+    Ptr P = make_ptr(h);
+    int* dcnt = nullptr;
+    int r = dalloc(&dcnt, n);
+    if (r) return r;
+    std::vector<int> cnt(n);
+    k_pairs_export<kShift><<<blocks_for(n), kBlock, 0, st>>>(h->c, P, nullptr, dcnt, nullptr, nullptr, nullptr);
+    cudaMemcpyAsync(cnt.data(), dcnt, n * sizeof(int), cudaMemcpyDeviceToHost, st);
+    cudaError_t e = cudaStreamSynchronize(st);
+    if (e != cudaSuccess) { cudaFree(dcnt); CK(e); }
+    std::vector<int> off(n);
+    int64_t tot = 0;
+    for (int i = 0; i < n; ++i) { off[i] = (int)tot; tot += cnt[i]; }
+    *count = tot;
+    int *di = nullptr, *dj = nullptr, *dm = nullptr;
+    if ((r = dalloc(&di, (size_t)std::max<int64_t>(tot, 1))) || (r = dalloc(&dj, (size_t)std::max<int64_t>(tot, 1))) ||
+        (r = dalloc(&dm, (size_t)std::max<int64_t>(tot, 1)))) {
+        cudaFree(dcnt); cudaFree(di); cudaFree(dj); cudaFree(dm);
+        return r;
+    }
+    cudaMemcpyAsync(dcnt, off.data(), n * sizeof(int), cudaMemcpyHostToDevice, st);
+    k_pairs_export<kShift><<<blocks_for(n), kBlock, 0, st>>>(h->c, P, dcnt, nullptr, di, dj, dm);
+    int64_t m = std::min<int64_t>(cap, tot);
+    if (pi && m > 0) {
+        cudaMemcpyAsync(pi, di, m * sizeof(int), cudaMemcpyDeviceToHost, st);
+        cudaMemcpyAsync(pj, dj, m * sizeof(int), cudaMemcpyDeviceToHost, st);
+        cudaMemcpyAsync(mir, dm, m * sizeof(int), cudaMemcpyDeviceToHost, st);
+    }
+    e = cudaStreamSynchronize(st);
+    cudaFree(dcnt); cudaFree(di); cudaFree(dj); cudaFree(dm);
+    CK(e);
+    CK(cudaGetLastError());
+    return SPH_OK;
 }
 }  // namespace
 
@@ -548,56 +594,51 @@ extern "C" int sph_pairs(SphHandle* h, int mode, int32_t* pi, int32_t* pj, int32
     const int n = (int)h->n;
     *count = 0;
     if (n == 0) return SPH_OK;
+    if (mode == 1) return export_pairs<0>(h, pi, pj, mir, cap, count, st);
     std::vector<int> cnt(n);
-    if (mode == 0) {
-        CK(cudaMemcpyAsync(cnt.data(), h->nbr_cnt, n * sizeof(int), cudaMemcpyDeviceToHost, st));
-        std::vector<int> lst((size_t)n * h->c.K);
-        CK(cudaMemcpyAsync(lst.data(), h->nbr, lst.size() * sizeof(int), cudaMemcpyDeviceToHost, st));
-        CK(cudaStreamSynchronize(st));
-        int64_t k = 0;
-        for (int i = 0; i < n; ++i) {
-            if (cnt[i] > h->c.K) return SPH_ERR_NEIGHBOUR_CAP;
-            for (int t = 0; t < cnt[i]; ++t) {
-                int e = lst[(size_t)t * n + i];
-                if (k < cap && pi) { pi[k] = i; pj[k] = e & kIdxMask; mir[k] = (int)((unsigned)e >> kMirShift); }
-                ++k;
-            }
-        }
-        *count = k;
-        return SPH_OK;
-    }
-    // mode 1: live search; nbr_cnt is borrowed as the count buffer and restored after.
-    std::vector<int> saved(n);
-    CK(cudaMemcpyAsync(saved.data(), h->nbr_cnt, n * sizeof(int), cudaMemcpyDeviceToHost, st));
-    Ptr P = make_ptr(h);
-    k_pairs_live<<<blocks_for(n), kBlock, 0, st>>>(h->c, P, nullptr, nullptr, nullptr, nullptr, 0);
     CK(cudaMemcpyAsync(cnt.data(), h->nbr_cnt, n * sizeof(int), cudaMemcpyDeviceToHost, st));
+    std::vector<int> lst((size_t)n * h->c.K);
+    CK(cudaMemcpyAsync(lst.data(), h->nbr, lst.size() * sizeof(int), cudaMemcpyDeviceToHost, st));
     CK(cudaStreamSynchronize(st));
-    std::vector<int> off(n);
-    int64_t tot = 0;
-    for (int i = 0; i < n; ++i) { off[i] = (int)tot; tot += cnt[i]; }
-    *count = tot;
-    int *doff = nullptr, *di = nullptr, *dj = nullptr, *dm = nullptr;
-    int r = SPH_OK;
-    if ((r = dalloc(&doff, n)) || (r = dalloc(&di, (size_t)tot)) || (r = dalloc(&dj, (size_t)tot)) ||
-        (r = dalloc(&dm, (size_t)tot))) {
-        cudaFree(doff); cudaFree(di); cudaFree(dj); cudaFree(dm);
-        return r;
+    int64_t k = 0;
+    for (int i = 0; i < n; ++i) {
+        if (cnt[i] > h->c.K) return SPH_ERR_NEIGHBOUR_CAP;
+        for (int t = 0; t < cnt[i]; ++t) {
+            int e = lst[(size_t)t * n + i];
+            if (k < cap && pi) { pi[k] = i; pj[k] = e & kIdxMask; mir[k] = (int)((unsigned)e >> kMirShift); }
+            ++k;
+        }
     }
-    cudaMemcpyAsync(doff, off.data(), n * sizeof(int), cudaMemcpyHostToDevice, st);
-    k_pairs_live<<<blocks_for(n), kBlock, 0, st>>>(h->c, P, doff, di, dj, dm, 1);
-    int64_t m = std::min<int64_t>(cap, tot);
-    if (pi && m > 0) {
-        cudaMemcpyAsync(pi, di, m * sizeof(int), cudaMemcpyDeviceToHost, st);
-        cudaMemcpyAsync(pj, dj, m * sizeof(int), cudaMemcpyDeviceToHost, st);
-        cudaMemcpyAsync(mir, dm, m * sizeof(int), cudaMemcpyDeviceToHost, st);
-    }
-    cudaMemcpyAsync(h->nbr_cnt, saved.data(), n * sizeof(int), cudaMemcpyHostToDevice, st);
-    cudaError_t e = cudaStreamSynchronize(st);
-    cudaFree(doff); cudaFree(di); cudaFree(dj); cudaFree(dm);
-    CK(e);
-    CK(cudaGetLastError());
+    *count = k;
     return SPH_OK;
+}
+
+extern "C" int sph_shift_pairs(SphHandle* h, float disp_bound, int32_t* pi, int32_t* pj, int32_t* mir,
+                               int64_t cap, int64_t* count, void* stream) {
+    if (!h || !count || std::isnan(disp_bound)) return SPH_ERR_ARG;
+    if (!h->bound) return SPH_ERR_NOT_BOUND;
+    cudaStream_t st = S(stream);
+    *count = 0;
+    if (h->n == 0) return SPH_OK;
+    // the step's displacement bounds, replaced for this call when a bound is given
+    unsigned int* dbits = &h->ac->max_disp_bits;
+    unsigned int* gbits = &h->ac->max_grip_disp_bits;
+    unsigned int saved[2];
+    CK(cudaMemcpyAsync(&saved[0], dbits, sizeof(unsigned int), cudaMemcpyDeviceToHost, st));
+    CK(cudaMemcpyAsync(&saved[1], gbits, sizeof(unsigned int), cudaMemcpyDeviceToHost, st));
+    CK(cudaStreamSynchronize(st));
+    if (disp_bound >= 0.0f) {
+        unsigned int set[2];
+        std::memcpy(&set[0], &disp_bound, sizeof(float));
+        set[1] = 0u;
+        CK(cudaMemcpyAsync(dbits, &set[0], sizeof(unsigned int), cudaMemcpyHostToDevice, st));
+        CK(cudaMemcpyAsync(gbits, &set[1], sizeof(unsigned int), cudaMemcpyHostToDevice, st));
+    }
+    const int r = export_pairs<1>(h, pi, pj, mir, cap, count, st);
+    CK(cudaMemcpyAsync(dbits, &saved[0], sizeof(unsigned int), cudaMemcpyHostToDevice, st));
+    CK(cudaMemcpyAsync(gbits, &saved[1], sizeof(unsigned int), cudaMemcpyHostToDevice, st));
+    CK(cudaStreamSynchronize(st));
+    return r;
 }
 
 extern "C" int sph_profile_enable(SphHandle* h, int on) {

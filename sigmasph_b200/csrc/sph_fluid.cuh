@@ -402,33 +402,87 @@ __device__ __forceinline__ void for_each_live_neighbour(const Cst& c, const Ptr&
     }
 }
 
-// Pairs of the shift from the lists of the sort (fluid step): the neighbours proper and
-// the shell out to h + skin, each re-tested at the live positions.  That is the
-// reference's stale-bin live search exactly when this particle is still in its binned
-// cell (same 27-cell window) and no particle moved more than skin / 2 since the sort (so
-// every live pair within h was within h + skin then); otherwise -- or past either list's
-// capacity -- the live search runs for this particle.  Mirror entries keep the live
-// plane test of their sweep.
+// The stale-bin cells a particle's live window (lx, ly, lz) +- 1 holds and its binned
+// window (lx - ex, ly - ey, lz - ez) +- 1 does not: for each sweep (real, y, z and corner
+// mirror, particle_system.py:1393-1490) the cells whose offset along a moved axis a is
+// e_a.  f(j, mirror) gets every candidate there within h of the live position.
+template <class F>
+__device__ __forceinline__ void pst_far_slab(const Cst& c, const Ptr& P, F3 xi, int lx, int ly, int lz,
+                                             int ex, int ey, int ez, F&& f) {
+    const GridLayout L = *P.layout;
+    const bool hashed = L.mode != 0;
+    const float4* __restrict__ pos = as4c(P.cur.pos);
+    auto sweep = [&](int mir, F3 xs, int nx, int ny, int nz) {
+        const int b = bucket_of(nx, ny, nz, L, c.mcap);
+        if (b < 0) return;
+        bucket_candidates(P, hashed, b, nx, ny, nz, [&](int j) {
+            if (dist2_rn(xs, f3(__ldg(pos + j))) < c.d2_lt) f(j, mir);
+        });
+    };
+    auto far = [](int e, int o) { return e != 0 && o == e; };
+#pragma unroll 1
+    for (int o0 = -1; o0 <= 1; ++o0)
+#pragma unroll 1
+        for (int o1 = -1; o1 <= 1; ++o1)
+#pragma unroll 1
+            for (int o2 = -1; o2 <= 1; ++o2)
+                if (far(ex, o0) || far(ey, o1) || far(ez, o2)) sweep(0, xi, lx + o0, ly + o1, lz + o2);
+    const bool my = c.mirror_y && xi.y < c.h, mz = c.mirror_z && xi.z < c.h;
+    if (my) {
+#pragma unroll 1
+        for (int o0 = -1; o0 <= 1; ++o0)
+#pragma unroll 1
+            for (int o1 = -1; o1 <= 1; ++o1)
+                if (far(ex, o0) || far(ez, o1)) sweep(1, mirror3(1, xi), lx + o0, 0, lz + o1);
+    }
+    if (mz) {
+#pragma unroll 1
+        for (int o0 = -1; o0 <= 1; ++o0)
+#pragma unroll 1
+            for (int o1 = -1; o1 <= 1; ++o1)
+                if (far(ex, o0) || far(ey, o1)) sweep(2, mirror3(2, xi), lx + o0, ly + o1, 0);
+    }
+    if (my && mz && ex != 0) sweep(3, mirror3(3, xi), lx + ex, 0, 0);
+}
+
+// Pairs of the shift from the lists of the sort: the neighbours proper and the shell out
+// to h + skin, each re-tested at the live positions.  While no particle moved more than
+// skin / 2 since the sort, every live pair within h was within h + skin then, so the
+// lists hold every candidate of the particle's binned 27-cell window.  The reference
+// searches the stale bins around the LIVE cell instead (particle_system.py:1377-1411):
+// a particle that changed cells keeps only the entries binned inside its live window
+// (their binned cell is read back) and adds the candidates of the cells the live window
+// gained.  Past either list's capacity, or when the bound fails, the live search runs
+// for this particle.  Mirror entries keep the live plane test of their sweep.
 template <class F>
 __device__ __forceinline__ void for_each_pst_neighbour(const Cst& c, const Ptr& P, int i, F3 xi, F&& f) {
     const int4 ci = P.cell[i];
     const int cnt = __ldg(P.nbr_cnt + i), scnt = __ldg(P.shell_cnt + i);
     const float dmax = __uint_as_float(P.ac->max_disp_bits) + __uint_as_float(P.ac->max_grip_disp_bits);
     const int lx = cell_of(xi.x, c.h), ly = cell_of(xi.y, c.h), lz = cell_of(xi.z, c.h);
-    const bool fast = ci.w >= 0 && 2.0f * dmax <= c.skin && cnt <= c.K && scnt <= c.Ks &&
-                      lx == ci.x && ly == ci.y && lz == ci.z;
-    if (!fast) {
+    const int ex = lx - ci.x, ey = ly - ci.y, ez = lz - ci.z;
+    const bool lists = ci.w >= 0 && 2.0f * dmax <= c.skin && cnt <= c.K && scnt <= c.Ks &&
+                       abs(ex) <= 1 && abs(ey) <= 1 && abs(ez) <= 1;
+    if (!lists) {
         if (isnan(xi.x) || isnan(xi.y) || isnan(xi.z)) return;
         const GridLayout L = *P.layout;
         enumerate_neighbours(c, P, L, i, xi, lx, ly, lz, [&](int j, int mir, float4) { f(j, mir); });
         return;
     }
+    const bool moved = (ex | ey | ez) != 0;
     const float4* __restrict__ pos = as4c(P.cur.pos);
     const bool py = xi.y < c.h, pz = xi.z < c.h;
     // entries deeper than h - skin at the sort are still within h: no live test
     auto take = [&](int e) {
         const int j = e & kIdxMask, mir = (int)((unsigned)e >> kMirShift);
         if (mir && (((mir & 1) && !py) || ((mir & 2) && !pz))) return;
+        if (moved) {
+            // a mirror sweep fixes the cell index across its plane (y = 0, z = 0 rows)
+            const int4 cj = __ldg(P.cell + j);
+            if (abs(cj.x - lx) > 1 || (!(mir & 1) && abs(cj.y - ly) > 1) ||
+                (!(mir & 2) && abs(cj.z - lz) > 1))
+                return;
+        }
         if (e & kRimBit) {
             F3 xj = f3(__ldg(pos + j));
             if (mir) xj = mirror3(mir, xj);
@@ -438,6 +492,7 @@ __device__ __forceinline__ void for_each_pst_neighbour(const Cst& c, const Ptr& 
     };
     list_entries(P.nbr + i, (size_t)c.n, cnt, take);
     list_entries(P.shell + i, (size_t)c.n, scnt, take);
+    if (moved) pst_far_slab(c, P, xi, lx, ly, lz, ex, ey, ez, f);
 }
 
 __global__ void __launch_bounds__(kBlock, 5) k_pst(Cst c, Ptr P) {

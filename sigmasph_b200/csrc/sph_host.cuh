@@ -35,10 +35,7 @@ inline void fill_constants_from(const SphParams& p, int64_t n, Cst& c) {
         c.d2_skin = (float)((1.1 * hs) * (1.1 * hs) * (1.0 + 1e-5));
         c.d2_deep = (float)((0.9 * hs) * (0.9 * hs) * (1.0 - 1e-5));
     }
-    // solids keep the separate live search: their lattices sit on the cell boundaries
-    // (support a whole number of spacings from a grid-aligned origin), so most particles
-    // would leave their binned cell and take the fallback
-    c.pst_skin = p.is_solid ? 0 : 1;
+    c.pst_skin = 1;
     double hd = p.support_radius;
     double al = p.two_d ? 7.0 / (M_PI * hd * hd) : 21.0 / (2.0 * M_PI * hd * hd * hd);
     c.h = (float)hd;

@@ -210,6 +210,21 @@ class _SolverBase:
                                        n, C.byref(cnt), _stream_ptr()))
         return pi, pj, pm
 
+    def shift_pairs(self, disp_bound=-1.0):
+        """(i, j, mirror) triples the shift pass evaluates at the current positions;
+        disp_bound >= 0 is the caller's bound on every particle's move since the sort."""
+        cnt = C.c_int64()
+        f = self.L.sph_shift_pairs
+        abi.check(f(self.h, disp_bound, None, None, None, 0, C.byref(cnt), _stream_ptr()))
+        n = cnt.value
+        pi = np.zeros(n, dtype=np.int32)
+        pj = np.zeros(n, dtype=np.int32)
+        pm = np.zeros(n, dtype=np.int32)
+        if n:
+            abi.check(f(self.h, disp_bound, pi.ctypes.data, pj.ctypes.data, pm.ctypes.data, n,
+                        C.byref(cnt), _stream_ptr()))
+        return pi, pj, pm
+
     # ------------------------------------------------------------------ reductions
     def _reduce(self):
         out = (C.c_double * abi.RED_COUNT)()

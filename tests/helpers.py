@@ -49,6 +49,46 @@ def pair_set(pi, pj, pm, pid):
     return set(zip(pid[pi].tolist(), pid[pj].tolist(), pm.tolist()))
 
 
+def check_shift_pairs(ps, solver, seed, reach):
+    """After the sort, moves every particle by at most reach * h (random direction and
+    length), then checks that the pairs the shift pass takes from the sort's lists equal,
+    as a set, the live search against the stale bins (particle_system.py:1377-1411).
+    Returns how many particles changed cells along 0, 1, 2 and 3 axes."""
+    h = float(ps.support_radius)
+    x = ps.x.to_numpy()
+    rng = np.random.default_rng(seed)
+    d = rng.normal(size=x.shape)
+    if ps.two_d:
+        d[:, 2] = 0.0
+    d /= np.linalg.norm(d, axis=1, keepdims=True)
+    d *= rng.uniform(0.0, reach * h, (len(x), 1))
+    # half of the particles that can reach a cell corner (3 axes) or edge (2 axes) within
+    # the bound step just past it, so multi-axis cell changes are always covered
+    ax = 2 if ps.two_d else 3
+    xd = x[:, :ax].astype(np.float64)
+    o = np.round(xd / h) * h - xd
+    o += np.where(o < 0, -1e-3, 1e-3) * h + np.where(o == 0, -2e-3, 0.0) * h
+    order = np.argsort(np.abs(o), axis=1)
+    for k in (ax, 2):
+        t = np.zeros_like(o)
+        rows = np.arange(len(x))[:, None]
+        t[rows, order[:, :k]] = o[rows, order[:, :k]]
+        ok = (np.linalg.norm(t, axis=1) < reach * h) & (rng.uniform(size=len(x)) < 0.5)
+        d[ok] = 0.0
+        d[ok, :ax] = t[ok]
+    x1 = (x + d).astype(np.float32)
+    moved = np.linalg.norm(x1.astype(np.float64) - x.astype(np.float64), axis=1).max()
+    ps.x.from_numpy(x1)
+    pid = ps.pid.to_numpy()
+    A = solver.shift_pairs(float(moved) * (1.0 + 1e-5))
+    B = solver.pairs(1)
+    SA, SB = pair_set(*A, pid), pair_set(*B, pid)
+    assert len(SA) == len(A[0]), "duplicate pairs in the shift's enumeration"
+    assert SA == SB, (len(SA - SB), len(SB - SA))
+    axes = (np.floor(x1.astype(np.float64) / h) != np.floor(x.astype(np.float64) / h)).sum(axis=1)
+    return np.bincount(axes, minlength=4)
+
+
 def rel_err(a, b, floor):
     return np.abs(a - b).max() / max(np.abs(b).max(), floor)
 

@@ -21,7 +21,7 @@ from sigmasph_b200.scenes import dambreak3d, dx_for_particles
 from sigmasph_b200.solver import build_params
 from oracle.oracle import Oracle, state_from_sets
 from tests.helpers import (make_pair, pair_set, gpu_fields, oracle_fields, field_errors,
-                           perturb)
+                           perturb, check_shift_pairs)
 
 pytestmark = pytest.mark.gpu
 
@@ -115,6 +115,28 @@ def test_live_search_uses_stale_bins(cuda):
     orc.set_state(st, solver.dt[None])
     A, B = _pairs_equal(ps, solver, orc, mode=1)
     assert A == B
+
+
+@pytest.mark.parametrize("reach", [0.045, 0.08], ids=["lists", "fallback"])
+@pytest.mark.parametrize("scene_fn", [lambda: small_scene(5000), axi_fluid_scene, quarter_scene],
+                         ids=["3d", "axisymmetric", "quarter_yz"])
+def test_shift_pairs_from_lists(cuda, scene_fn, reach):
+    """The shift pass serves its pairs from the sort's lists (neighbours + the shell out to
+    1.1 h) while every particle moved less than 0.05 h; particles that changed cells keep
+    the entries binned in their live window and add the cells it gained.  Beyond 0.05 h
+    it searches again.  Either way the pair set is the stale-bin live search's."""
+    ps, solver, _ = make_pair(scene_fn(), fp64=False)
+    # off the lattice by up to half a spacing, so that particles sit near cell edges too
+    x = ps.x.to_numpy()
+    j = np.random.default_rng(3).uniform(-0.5, 0.5, x.shape) * ps.particle_diameter
+    if ps.two_d:
+        j[:, 2] = 0.0
+    ps.x.from_numpy((x + j).astype(np.float32))
+    solver.initialize()
+    crossed = check_shift_pairs(ps, solver, seed=5, reach=reach)
+    assert crossed[1:].sum() > 0
+    if not ps.two_d:   # 3D: ~50 of these decks' particles change cells along 2 axes
+        assert crossed[2:].sum() > 0
 
 
 @pytest.mark.parametrize("scene_fn", [lambda: small_scene(), axi_fluid_scene, quarter_scene],

@@ -12,7 +12,7 @@ from sigmasph_b200.particle_system import ParticleSystem
 from sigmasph_b200.scenes import scene_path
 from sigmasph_b200.solver import build_params
 from oracle.oracle import Oracle, state_from_sets
-from tests.helpers import pair_set, perturb
+from tests.helpers import pair_set, perturb, check_shift_pairs
 
 pytestmark = pytest.mark.gpu
 
@@ -178,6 +178,24 @@ def test_solid_stages_match_oracle(cuda, deck):
     fo = s32["constraint_force"][:nc]
     assert np.abs(fg - fo).max() <= 1e-4 * np.abs(fo).max()
     assert abs(sg.plastic_work - s32["plastic_work"]) <= 1e-4 * abs(s32["plastic_work"]) + 1e-12
+
+
+@pytest.mark.parametrize("deck", [bar3d_deck, strip_ps_deck], ids=["bar3d", "plane_strain"])
+def test_solid_shift_pairs_from_lists(cuda, deck):
+    """A solid lattice starts on the cell boundaries, so small moves change many
+    particles' cells: the shift's list path must still give the stale-bin pair set, for
+    host-made moves under a given bound and after the real step's advect and grips."""
+    ps, solver, _, _ = make_solid(deck())
+    solver.initialize()
+    crossed = check_shift_pairs(ps, solver, seed=9, reach=0.045)
+    assert crossed[1:].sum() > 0.05 * crossed.sum()
+    ps, solver, _, _ = make_solid(deck())
+    for s in range(abi.STAGE_ADVECT + 1):
+        solver.run_stage(s)
+    pid = ps.pid.to_numpy()
+    A = pair_set(*solver.shift_pairs(), pid)
+    B = pair_set(*solver.pairs(1), pid)
+    assert A == B
 
 
 @pytest.mark.parametrize("deck", [axi_deck, bar3d_deck], ids=["axi_dogbone", "bar3d"])
