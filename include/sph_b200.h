@@ -45,14 +45,21 @@ extern "C" {
 #define SPH_ERR_SCRATCH_CAP   -8   /* request exceeds the fixed static scratch capacity    */
 
 /* Device error-word bits (SphScalars.err).  Set by kernels, never by a trap. */
-#define SPH_EW_NBR_OVERFLOW   0x1  /* a particle had more neighbours than the list holds;
-                                      its extra pairs were found by a direct search      */
+#define SPH_EW_NBR_OVERFLOW   0x1  /* a particle had more neighbours within h than its
+                                      list holds (twice the lattice count within 1.1 h);
+                                      the extra pairs went to the overflow pool          */
 #define SPH_EW_HASHED_GRID    0x2  /* the occupied cell box did not fit the dense Morton
                                       table; the step ran on the hashed fallback table   */
 #define SPH_EW_JC_NO_CONVERGE 0x4  /* a Johnson-Cook return map hit its iteration cap     */
 #define SPH_EW_STS_CAP        0x8  /* the hourglass sub-cycle count hit its cap          */
 #define SPH_EW_MLP_TIMEOUT    0x10 /* a tensor-core surrogate pass gave up waiting for its
                                       MMAs; its returns fell back to the exact Newton      */
+#define SPH_EW_CAND_OVERFLOW  0x20 /* a particle had more candidates within h + skin than
+                                      its candidate list holds; its pairs came from a
+                                      direct search of the coarse cell table              */
+#define SPH_EW_NBR_DROPPED    0x40 /* the overflow pool (as many entries as the lists of
+                                      all particles) ran out: pairs were dropped and the
+                                      step is not exact                                    */
 
 /* ------------------------------------------------------------------ parameters */
 /* Flattened, resolved scene configuration.  Field meanings follow the reference's
@@ -281,20 +288,24 @@ int  sph_clear_error(SphHandle* h, void* stream);
  * internal / total_mass (sph_base.py:425-557, DSPH.py:1670-1712) and compute_momentum /
  * compute_gross_momentum (sph_base.py:560-620), into out[SPH_RED_COUNT]. */
 int  sph_reduce(SphHandle* h, double* out, void* stream);
-/* Neighbour pairs of the current bins (for_all_neighbors, particle_system.py:1348-1490):
- * mode 0 = the list built at the last rebuild; mode 1 = a fresh search from the live
- * positions against the stale bins (the PST sweep, DSPH.py:771-886).  Writes up to cap
- * (i, j, mirror) triples as current-order indices and the total into *count. */
+/* Neighbour pairs (for_all_neighbors, particle_system.py:1348-1490): mode 0 = this
+ * step's list (the sweep against the bins of the step's start); mode 1 = a fresh search
+ * from the current positions against those bins (the PST sweep, DSPH.py:771-886).  Writes
+ * up to cap (i, j, mirror) triples as current-order indices and the total into *count. */
 int  sph_pairs(SphHandle* h, int mode, int32_t* pi, int32_t* pj, int32_t* mir,
                int64_t cap, int64_t* count, void* stream);
 /* The pairs the shift pass evaluates at the current positions (the PST sweep,
- * DSPH.py:771-886): the lists of the last rebuild re-tested at the live positions, with
- * the live search for the particles the lists cannot serve.  disp_bound >= 0 stands for
- * the largest distance a particle moved since the last rebuild (the caller vouches for
- * it); < 0 uses the bound the step's advect and grips recorded.  As a set, equal to
+ * DSPH.py:771-886): the candidate lists of the last build re-tested at the current
+ * positions, or the coarse-table search when the displacement bound does not hold.
+ * disp_bound >= 0 stands for the largest distance a particle moved since the lists were
+ * built (the caller vouches for it); < 0 uses what the step recorded.  As a set, equal to
  * sph_pairs mode 1 whenever the bound holds.  Output as sph_pairs. */
 int  sph_shift_pairs(SphHandle* h, float disp_bound, int32_t* pi, int32_t* pj, int32_t* mir,
                      int64_t cap, int64_t* count, void* stream);
+/* Candidate-list statistics since creation or the last reset: out[0] steps, out[1] steps
+ * that built the candidate lists, out[2] shift passes that searched the coarse table
+ * instead of reading the lists.  reset != 0 zeroes them after reading. */
+int  sph_list_stats(SphHandle* h, uint64_t* out, int reset, void* stream);
 
 /* Per-kernel timing with CUDA events recorded on the launching stream around every
  * kernel of eagerly launched steps (sph_step with nsteps == 1, sph_run_stage).  Off by

@@ -25,6 +25,8 @@ EW_HASHED_GRID = 0x2
 EW_JC_NO_CONVERGE = 0x4
 EW_STS_CAP = 0x8
 EW_MLP_TIMEOUT = 0x10
+EW_CAND_OVERFLOW = 0x20
+EW_NBR_DROPPED = 0x40
 
 # Stage ids of sph_run_stage (include/sph_b200.h).
 STAGE_SORT, STAGE_LAM, STAGE_CONTINUITY, STAGE_FORCES, STAGE_DT, STAGE_ADVECT, \
@@ -173,6 +175,7 @@ def lib():
         "sph_reduce": (C.c_int, [vp, C.POINTER(C.c_double), vp]),
         "sph_pairs": (C.c_int, [vp, C.c_int, vp, vp, vp, i64, C.POINTER(i64), vp]),
         "sph_shift_pairs": (C.c_int, [vp, C.c_float, vp, vp, vp, i64, C.POINTER(i64), vp]),
+        "sph_list_stats": (C.c_int, [vp, vp, C.c_int, vp]),
         "sph_profile_enable": (C.c_int, [vp, C.c_int]),
         "sph_profile_read": (C.c_int, [vp, C.c_char_p, C.c_int, C.POINTER(C.c_double),
                                        C.POINTER(C.c_int), C.c_int, C.POINTER(C.c_int)]),

@@ -39,8 +39,13 @@ struct SphHandle {
     GridLayout* layout = nullptr;
     int* nbr = nullptr;
     int* nbr_cnt = nullptr;
-    int* shell = nullptr;
-    int* shell_cnt = nullptr;
+    int* vl = nullptr;
+    int* vl_cnt = nullptr;
+    int* ovf = nullptr;
+    int* ovf_off = nullptr;
+    int4* fcell = nullptr;
+    float4* xb = nullptr;
+    bool force_pending = true;      // the next step builds the candidate lists
     DevScalars* sc = nullptr;
     DevAccum* ac = nullptr;
     SphScalars* pinned = nullptr;   // page-locked staging of the scalar copies
@@ -118,8 +123,12 @@ Ptr make_ptr(SphHandle* h) {
     P.layout = h->layout;
     P.nbr = h->nbr;
     P.nbr_cnt = h->nbr_cnt;
-    P.shell = h->shell;
-    P.shell_cnt = h->shell_cnt;
+    P.vl = h->vl;
+    P.vl_cnt = h->vl_cnt;
+    P.ovf = h->ovf;
+    P.ovf_off = h->ovf_off;
+    P.fcell = h->fcell;
+    P.xb = h->xb;
     P.sc = h->sc;
     P.ac = h->ac;
     P.jc = solid_jc_ptr(h->solid);
@@ -135,7 +144,20 @@ void drop_graph(SphHandle* h) {
 
 int scan_tiles(const SphHandle* h) { return (int)((h->c.mcap + 1 + kScanTile - 1) / kScanTile); }
 
-// initialize_particle_system + the neighbour-list rebuild.
+// Hands a pending build request to the device (outside any capture: the next step's
+// k_layout reads it).
+int apply_force(SphHandle* h, cudaStream_t st) {
+    if (!h->force_pending) return SPH_OK;
+    static const int one = 1;
+    CK(cudaMemcpyAsync(&h->ac->force_build, &one, sizeof(int), cudaMemcpyHostToDevice, st));
+    h->force_pending = false;
+    return SPH_OK;
+}
+
+// update_grid_id / counting_sort / the neighbour search of every step
+// (particle_system.py:1300-1490): the step-start bins, the candidate lists when the
+// displacement bound asks for a build (the sort kernels return at once otherwise), and
+// this step's neighbour list.
 int rebuild(SphHandle* h, cudaStream_t st) {
     const int nb = blocks_for(h->n);
     Ptr P = make_ptr(h);
@@ -157,7 +179,8 @@ int rebuild(SphHandle* h, cudaStream_t st) {
     LAUNCH("k_gather", k_gather<<<nb, kBlock, 0, st>>>(c, P));
     h->parity ^= 1;
     P = make_ptr(h);
-    LAUNCH("k_nbr_build", k_nbr_build<<<nb, kBlock, 0, st>>>(c, P));
+    LAUNCH("k_vlist_build", k_vlist_build<<<nb, kBlock, 0, st>>>(c, P));
+    LAUNCH("k_nbr_filter", k_nbr_filter<<<nb, kBlock, 0, st>>>(c, P));
     return SPH_OK;
 }
 
@@ -172,8 +195,6 @@ int fluid_substep_and_boundary(SphHandle* h, cudaStream_t st) {
     LAUNCH("k_dt", k_dt<<<1, 32, 0, st>>>(c, P));
     LAUNCH("k_advect", k_advect<<<nb, kBlock, 0, st>>>(c, P));
     if (h->p.pst_enabled) {
-        // the fluid's shift reads the lists of the sort (k_pst, for_each_pst_neighbour)
-        if (!c.pst_skin) LAUNCH("k_pst_search", k_pst_search<<<nb, kBlock, 0, st>>>(c, P));
         LAUNCH("k_pst", k_pst<<<nb, kBlock, 0, st>>>(c, P));
         LAUNCH("k_finish", k_finish<<<nb, kBlock, 0, st>>>(c, P, 3));
     } else {
@@ -206,7 +227,8 @@ void free_all(SphHandle* h) {
     h->prof_pool.clear();
     if (h->cap_stream) cudaStreamDestroy(h->cap_stream);
     void* ptrs[] = {h->cell, h->cell_tmp, h->key, h->rank, h->perm, h->hist, h->start, h->bsum,
-                    h->bbox, h->layout, h->nbr, h->nbr_cnt, h->shell, h->shell_cnt, h->sc, h->ac};
+                    h->bbox, h->layout, h->nbr, h->nbr_cnt, h->vl, h->vl_cnt, h->ovf, h->ovf_off, h->fcell, h->xb,
+                    h->sc, h->ac};
     for (void* q : ptrs) if (q) cudaFree(q);
     if (h->pinned) cudaFreeHost(h->pinned);
     solid_free(h->solid);
@@ -285,23 +307,27 @@ int sph_create(const SphParams* p, int64_t n_max, SphHandle** out) {
     h->p = *p;
     h->n_max = n_max;
     cudaGetDevice(&h->device);
-    // neighbour-list capacity from the lattice count at this support, with headroom
+    // list capacities from the lattice count at this support: the candidates within
+    // 1.1 h (1.1^d of the neighbours) with room for twice the lattice density; the
+    // neighbour list holds as many, so it cannot overflow while the candidates fit
     double ratio = (double)p->support_radius / (double)p->particle_diameter;
     double est = p->two_d ? M_PI * ratio * ratio * 1.5 : (4.0 / 3.0) * M_PI * ratio * ratio * ratio;
-    int K = (int)std::ceil((1.5 * est + 16.0) / 32.0) * 32;
-    K = std::max(32, std::min(K, 512));
-    // the shift's shell h <= |r| < 1.1 h: (1.1^d - 1) of the neighbour count, with headroom
-    const double shell_est = est * (p->two_d ? 0.21 : 0.331);
-    int Ks = (int)std::ceil((1.5 * shell_est + 16.0) / 32.0) * 32;
-    Ks = std::max(32, std::min(Ks, 256));
+    const double cand_est = est * (p->two_d ? 1.21 : 1.331);
+    int Kv = (int)std::ceil((2.0 * cand_est + 16.0) / 32.0) * 32;
+    Kv = std::max(64, std::min(Kv, 1024));
+    const int K = Kv;
     int64_t mcap = 131072;
     while (mcap < 4 * n_max) mcap <<= 1;
     int lg = 0;
     while ((1ll << lg) < mcap) ++lg;
     h->n = 0;
     fill_constants(h);
-    h->c.Ks = Ks;
+    h->c.Kv = Kv;
     h->c.K = K;
+    // the overflow pool: as many entries as all lists (a uniform 2x compression beyond
+    // the lists' own headroom)
+    const size_t ovf_cap = std::min<size_t>((size_t)std::max<int64_t>(n_max, 1) * (size_t)K, 0x7fffffffu);
+    h->c.ovf_cap = (unsigned int)ovf_cap;
     h->c.mcap = (int)mcap;
     h->c.mcap_log2 = lg;
     int r = SPH_OK;
@@ -313,7 +339,9 @@ int sph_create(const SphParams* p, int64_t n_max, SphHandle** out) {
         (r = dalloc(&h->bsum, tiles)) || (r = dalloc(&h->bbox, 8)) ||
         (r = dalloc(&h->layout, 1)) || (r = dalloc(&h->nbr, N * (size_t)K)) ||
         (r = dalloc(&h->nbr_cnt, N)) || (r = dalloc(&h->sc, 1)) || (r = dalloc(&h->ac, 1)) ||
-        (r = dalloc(&h->shell, N * (size_t)Ks)) || (r = dalloc(&h->shell_cnt, N)) ||
+        (r = dalloc(&h->vl, N * (size_t)Kv)) || (r = dalloc(&h->vl_cnt, N)) ||
+        (r = dalloc(&h->ovf, ovf_cap)) || (r = dalloc(&h->ovf_off, N)) ||
+        (r = dalloc(&h->fcell, N)) || (r = dalloc(&h->xb, N)) ||
         cudaMallocHost((void**)&h->pinned, sizeof(SphScalars)) != cudaSuccess) {
         if (!r) r = SPH_ERR_NOMEM;
         free_all(h);
@@ -334,7 +362,13 @@ int sph_create(const SphParams* p, int64_t n_max, SphHandle** out) {
     memset(&a0, 0, sizeof(a0));
     if (cudaMemcpy(h->sc, &s0, sizeof(s0), cudaMemcpyHostToDevice) != cudaSuccess ||
         cudaMemcpy(h->ac, &a0, sizeof(a0), cudaMemcpyHostToDevice) != cudaSuccess ||
-        cudaMemset(h->nbr_cnt, 0, N * sizeof(int)) != cudaSuccess) {
+        cudaMemset(h->nbr_cnt, 0, N * sizeof(int)) != cudaSuccess ||
+        // no lists and no cells until the first build: empty counts, off-grid cells, an
+        // empty layout
+        cudaMemset(h->vl_cnt, 0, N * sizeof(int)) != cudaSuccess ||
+        cudaMemset(h->cell, 0xff, N * sizeof(int4)) != cudaSuccess ||
+        cudaMemset(h->fcell, 0xff, N * sizeof(int4)) != cudaSuccess ||
+        cudaMemset(h->layout, 0, sizeof(GridLayout)) != cudaSuccess) {
         free_all(h);
         delete h;
         return SPH_ERR_CUDA;
@@ -361,6 +395,7 @@ int sph_bind(SphHandle* h, const SphBuffers* b, int64_t n) {
     h->c.n = (int)n;
     h->parity = 0;
     h->bound = true;
+    h->force_pending = true;
     return SPH_OK;
 }
 
@@ -370,11 +405,14 @@ int sph_set_params(SphHandle* h, const SphParams* p) {
     if (!h || !p || p->struct_size != (int32_t)sizeof(SphParams)) return SPH_ERR_ARG;
     if (p->is_solid != h->p.is_solid) return SPH_ERR_ARG;
     if (p->is_solid && (p->n_materials < 1 || p->n_materials > 4)) return SPH_ERR_ARG;
-    int K = h->c.K, mcap = h->c.mcap, lg = h->c.mcap_log2, bs = h->c.block, Ks = h->c.Ks;
+    int K = h->c.K, mcap = h->c.mcap, lg = h->c.mcap_log2, bs = h->c.block, Kv = h->c.Kv;
+    unsigned int cap = h->c.ovf_cap;
     h->p = *p;
     fill_constants(h);
     h->c.K = K; h->c.mcap = mcap; h->c.mcap_log2 = lg; h->c.n = (int)h->n; h->c.block = bs;
-    h->c.Ks = Ks;
+    h->c.Kv = Kv;
+    h->c.ovf_cap = cap;
+    h->force_pending = true;
     int r = solid_sync_rows(h->solid, h->p, h->c);
     drop_graph(h);
     return r;
@@ -384,7 +422,9 @@ int sph_initialize(SphHandle* h, void* stream) {
     if (!h) return SPH_ERR_ARG;
     if (!h->bound) return SPH_ERR_NOT_BOUND;
     if (h->n == 0) return SPH_OK;
-    int r = rebuild(h, S(stream));
+    h->force_pending = true;
+    int r = apply_force(h, S(stream));
+    if (!r) r = rebuild(h, S(stream));
     if (r) return r;
     CK(cudaGetLastError());
     return SPH_OK;
@@ -395,6 +435,7 @@ int sph_step(SphHandle* h, int nsteps, void* stream) {
     if (!h->bound) return SPH_ERR_NOT_BOUND;
     if (h->n == 0 || nsteps == 0) return SPH_OK;
     cudaStream_t st = S(stream);
+    if (int r = apply_force(h, st)) return r;
     int pairs = nsteps / 2;
     if (pairs > 0) {
         if (!h->graph2) {
@@ -431,6 +472,7 @@ int sph_run_stage(SphHandle* h, int stage, void* stream) {
     if (!h->bound) return SPH_ERR_NOT_BOUND;
     if (h->n == 0) return SPH_OK;
     cudaStream_t st = S(stream);
+    if (int r = apply_force(h, st)) return r;
     const int nb = blocks_for(h->n);
     if (h->p.is_solid) {
         if (stage < SPH_STAGE_SORT || stage > SPH_STAGE_BOUNDARY) return SPH_ERR_ARG;
@@ -460,7 +502,6 @@ int sph_run_stage(SphHandle* h, int stage, void* stream) {
         case SPH_STAGE_ADVECT: k_advect<<<nb, kBlock, 0, st>>>(c, P); break;
         case SPH_STAGE_PST:
             if (h->p.pst_enabled) {
-                if (!c.pst_skin) k_pst_search<<<nb, kBlock, 0, st>>>(c, P);
                 k_pst<<<nb, kBlock, 0, st>>>(c, P);
                 k_finish<<<nb, kBlock, 0, st>>>(c, P, 1);
             }
@@ -521,12 +562,28 @@ int sph_reduce(SphHandle* h, double* out, void* stream) {
 }  // extern "C"
 
 namespace {
+// Largest |x - x_build| over the particles, rounded up, into *dbits (float bits).
+__global__ void __launch_bounds__(kBlock) k_disp_since_build(Cst c, Ptr P, unsigned int* dbits) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    float d = 0.0f;
+    if (i < c.n) {
+        const float4 p = reinterpret_cast<const float4*>(P.cur.pos)[i];
+        if (!(isnan(p.x) || isnan(p.y) || isnan(p.z))) {
+            const float4 b = P.xb[i];
+            d = norm3(F3{p.x - b.x, p.y - b.y, p.z - b.z}) * (1.0f + 1e-5f);
+            if (isnan(d)) d = INFINITY;
+        }
+    }
+    block_max_atomic(d, dbits);
+}
+
 // Pair export: one thread per particle counts (off == nullptr, counts to cnt_out) or
-// writes its pairs at off[i].  kShift 0: the live search against the current bins;
+// writes its pairs at off[i].  kShift 0: the reference's sweep from the current positions
+// against this step's start bins, searched in the coarse table for displacement *dbits;
 // kShift 1: the pairs the shift pass evaluates (for_each_pst_neighbour).
 template <int kShift>
-__global__ void k_pairs_export(Cst c, Ptr P, const int* off, int* cnt_out, int* out_i, int* out_j,
-                               int* out_m) {
+__global__ void k_pairs_export(Cst c, Ptr P, const unsigned int* dbits, const int* off, int* cnt_out,
+                               int* out_i, int* out_j, int* out_m) {
     int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= c.n) return;
     const F3 xi = f3(reinterpret_cast<const float4*>(P.cur.pos)[i]);
@@ -539,9 +596,8 @@ __global__ void k_pairs_export(Cst c, Ptr P, const int* off, int* cnt_out, int* 
     if (kShift) {
         for_each_pst_neighbour(c, P, i, xi, emit);
     } else if (!(isnan(xi.x) || isnan(xi.y) || isnan(xi.z))) {
-        const GridLayout L = *P.layout;
-        int cx = cell_of(xi.x, c.h), cy = cell_of(xi.y, c.h), cz = cell_of(xi.z, c.h);
-        enumerate_neighbours(c, P, L, i, xi, cx, cy, cz, [&](int j, int mir, float4) { emit(j, mir); });
+        stale_search(c, P, i, xi, cell_of(xi.x, c.h), cell_of(xi.y, c.h), cell_of(xi.z, c.h),
+                     __uint_as_float(*dbits), emit);
     }
     if (!off) cnt_out[i] = cnt;
 }
@@ -553,25 +609,30 @@ int export_pairs(SphHandle* h, int32_t* pi, int32_t* pj, int32_t* mir, int64_t c
     const int n = (int)h->n;
     Ptr P = make_ptr(h);
     int* dcnt = nullptr;
+    unsigned int* dbits = nullptr;
     int r = dalloc(&dcnt, n);
-    if (r) return r;
+    if (!r) r = dalloc(&dbits, 1);
+    if (r) { cudaFree(dcnt); return r; }
     std::vector<int> cnt(n);
-    k_pairs_export<kShift><<<blocks_for(n), kBlock, 0, st>>>(h->c, P, nullptr, dcnt, nullptr, nullptr, nullptr);
+    cudaMemsetAsync(dbits, 0, sizeof(unsigned int), st);
+    k_disp_since_build<<<blocks_for(n), kBlock, 0, st>>>(h->c, P, dbits);
+    k_pairs_export<kShift><<<blocks_for(n), kBlock, 0, st>>>(h->c, P, dbits, nullptr, dcnt, nullptr, nullptr,
+                                                             nullptr);
     cudaMemcpyAsync(cnt.data(), dcnt, n * sizeof(int), cudaMemcpyDeviceToHost, st);
     cudaError_t e = cudaStreamSynchronize(st);
-    if (e != cudaSuccess) { cudaFree(dcnt); CK(e); }
+    if (e != cudaSuccess) { cudaFree(dcnt); cudaFree(dbits); CK(e); }
     std::vector<int> off(n);
     int64_t tot = 0;
     for (int i = 0; i < n; ++i) { off[i] = (int)tot; tot += cnt[i]; }
     *count = tot;
     int *di = nullptr, *dj = nullptr, *dm = nullptr;
-    if ((r = dalloc(&di, (size_t)std::max<int64_t>(tot, 1))) || (r = dalloc(&dj, (size_t)std::max<int64_t>(tot, 1))) ||
-        (r = dalloc(&dm, (size_t)std::max<int64_t>(tot, 1)))) {
-        cudaFree(dcnt); cudaFree(di); cudaFree(dj); cudaFree(dm);
+    const size_t m1 = (size_t)std::max<int64_t>(tot, 1);
+    if ((r = dalloc(&di, m1)) || (r = dalloc(&dj, m1)) || (r = dalloc(&dm, m1))) {
+        cudaFree(dcnt); cudaFree(dbits); cudaFree(di); cudaFree(dj); cudaFree(dm);
         return r;
     }
     cudaMemcpyAsync(dcnt, off.data(), n * sizeof(int), cudaMemcpyHostToDevice, st);
-    k_pairs_export<kShift><<<blocks_for(n), kBlock, 0, st>>>(h->c, P, dcnt, nullptr, di, dj, dm);
+    k_pairs_export<kShift><<<blocks_for(n), kBlock, 0, st>>>(h->c, P, dbits, dcnt, nullptr, di, dj, dm);
     int64_t m = std::min<int64_t>(cap, tot);
     if (pi && m > 0) {
         cudaMemcpyAsync(pi, di, m * sizeof(int), cudaMemcpyDeviceToHost, st);
@@ -579,7 +640,7 @@ int export_pairs(SphHandle* h, int32_t* pi, int32_t* pj, int32_t* mir, int64_t c
         cudaMemcpyAsync(mir, dm, m * sizeof(int), cudaMemcpyDeviceToHost, st);
     }
     e = cudaStreamSynchronize(st);
-    cudaFree(dcnt); cudaFree(di); cudaFree(dj); cudaFree(dm);
+    cudaFree(dcnt); cudaFree(dbits); cudaFree(di); cudaFree(dj); cudaFree(dm);
     CK(e);
     CK(cudaGetLastError());
     return SPH_OK;
@@ -620,25 +681,39 @@ extern "C" int sph_shift_pairs(SphHandle* h, float disp_bound, int32_t* pi, int3
     cudaStream_t st = S(stream);
     *count = 0;
     if (h->n == 0) return SPH_OK;
-    // the step's displacement bounds, replaced for this call when a bound is given
-    unsigned int* dbits = &h->ac->max_disp_bits;
-    unsigned int* gbits = &h->ac->max_grip_disp_bits;
-    unsigned int saved[2];
-    CK(cudaMemcpyAsync(&saved[0], dbits, sizeof(unsigned int), cudaMemcpyDeviceToHost, st));
-    CK(cudaMemcpyAsync(&saved[1], gbits, sizeof(unsigned int), cudaMemcpyDeviceToHost, st));
+    // the step's displacement record (since the build, this step's advect, the grips),
+    // replaced for this call when a bound is given
+    unsigned int* words[3] = {&h->ac->d_start_bits, &h->ac->max_disp_bits, &h->ac->max_grip_disp_bits};
+    unsigned int saved[3];
+    for (int k = 0; k < 3; ++k)
+        CK(cudaMemcpyAsync(&saved[k], words[k], sizeof(unsigned int), cudaMemcpyDeviceToHost, st));
     CK(cudaStreamSynchronize(st));
+    unsigned int set[3] = {0u, 0u, 0u};
     if (disp_bound >= 0.0f) {
-        unsigned int set[2];
         std::memcpy(&set[0], &disp_bound, sizeof(float));
-        set[1] = 0u;
-        CK(cudaMemcpyAsync(dbits, &set[0], sizeof(unsigned int), cudaMemcpyHostToDevice, st));
-        CK(cudaMemcpyAsync(gbits, &set[1], sizeof(unsigned int), cudaMemcpyHostToDevice, st));
+        for (int k = 0; k < 3; ++k)
+            CK(cudaMemcpyAsync(words[k], &set[k], sizeof(unsigned int), cudaMemcpyHostToDevice, st));
     }
     const int r = export_pairs<1>(h, pi, pj, mir, cap, count, st);
-    CK(cudaMemcpyAsync(dbits, &saved[0], sizeof(unsigned int), cudaMemcpyHostToDevice, st));
-    CK(cudaMemcpyAsync(gbits, &saved[1], sizeof(unsigned int), cudaMemcpyHostToDevice, st));
+    for (int k = 0; k < 3; ++k)
+        CK(cudaMemcpyAsync(words[k], &saved[k], sizeof(unsigned int), cudaMemcpyHostToDevice, st));
     CK(cudaStreamSynchronize(st));
     return r;
+}
+
+extern "C" int sph_list_stats(SphHandle* h, uint64_t* out, int reset, void* stream) {
+    if (!h || !out) return SPH_ERR_ARG;
+    cudaStream_t st = S(stream);
+    unsigned long long v[3];
+    CK(cudaMemcpyAsync(v, &h->ac->n_steps, sizeof(v), cudaMemcpyDeviceToHost, st));
+    CK(cudaStreamSynchronize(st));
+    for (int k = 0; k < 3; ++k) out[k] = (uint64_t)v[k];
+    if (reset) {
+        static const unsigned long long zero[3] = {0ull, 0ull, 0ull};
+        CK(cudaMemcpyAsync(&h->ac->n_steps, zero, sizeof(zero), cudaMemcpyHostToDevice, st));
+        CK(cudaStreamSynchronize(st));
+    }
+    return SPH_OK;
 }
 
 extern "C" int sph_profile_enable(SphHandle* h, int on) {
@@ -818,6 +893,7 @@ int sph_ensemble_set(SphHandle* h, const SphMatRow* mat, const SphInstRow* inst,
     h->c.any_plastic = h->solid.any_plastic;
     h->c.all_gamma_one = h->solid.all_gamma_one;
     h->c.any_jc = h->solid.any_jc;
+    h->force_pending = true;
     drop_graph(h);
     return SPH_OK;
 }

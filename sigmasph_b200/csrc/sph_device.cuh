@@ -42,10 +42,16 @@ struct DevAccum {
     unsigned int max_c_sq_bits;
     unsigned int max_accel_bits;
     unsigned int max_v_bits;
-    unsigned int max_disp_bits;  // max |x - x_sort| of this step's advect (float bits)
+    unsigned int max_disp_bits;  // max position change of this step's advect (float bits)
     unsigned int max_grip_disp_bits;  // max position change of the grips' overwrite
-    int pad2;
+    unsigned int d_start_bits;   // max |x - x_build| at this step's start (0 after a build)
+    int rebuild;                 // 1: this step builds the candidate lists
+    int force_build;             // set by the host: the next step builds
+    int off_grid_build;          // off-grid count at the last build
+    unsigned int ovf_used;       // overflow-pool entries taken this step
+    int pad3;
     double hg_power;         // sum_i mw_i de_hg_i of the in-loop damper (solid)
+    unsigned long long n_steps, n_builds, n_shift_search;   // list statistics
 };
 
 // Constants of one handle, passed by value to every kernel.
@@ -53,9 +59,9 @@ struct Cst {
     SphParams p;
     int n;               // active particles
     int K;               // neighbour-list capacity per particle
-    int mcap;            // bucket capacity of the cell table (power of two)
+    int mcap;            // bucket capacity of the coarse cell table (power of two)
     int mcap_log2;
-    float h;             // support radius == cell size
+    float h;             // support radius == cell size of the reference's bins
     float inv_h;         // 1 / h
     float alpha;         // Wendland prefactor
     float kgrad;         // 20 alpha / h
@@ -78,10 +84,13 @@ struct Cst {
     int all_gamma_one;   // every EOS is linear (exponent 1)
     int any_jc;          // some material row is Johnson-Cook (return statistics kept)
     int block;           // threads per block of the solid particle kernels
-    // the shift's candidate shell: pairs binned within h + skin at the sort
-    int pst_skin;        // 1: the shift pass reads the lists instead of searching again
-    int Ks;              // shell-list capacity per particle
-    float skin;          // skin width
+    // candidate lists with a skin: every pair within h + skin at the last build, binned
+    // in coarse cells of h + skin; complete while no particle moved more than dlim since
+    int Kv;              // candidate-list capacity per particle
+    unsigned int ovf_cap;  // overflow-pool capacity (entries)
+    float skin;          // skin width (h / 10)
+    float hc;            // coarse cell size h + skin
+    float dlim;          // displacement bound of the lists: skin / 2, less a margin
     float d2_skin;       // |r| < h + skin (conservative) in dist2_rn units
     float d2_deep;       // |r| < h - skin (conservative): stays within h under the bound
 };
@@ -111,8 +120,11 @@ struct Ptr {
     float* gradv;
     float4* aux;
     // scratch
-    int4* cell;          // binned cell of the current order: x, y, z, key (-1 off-grid)
-    int4* cell_tmp;      // binned cell of the pre-sort order
+    int4* cell;          // coarse cell at the last build, current order: x, y, z, bucket
+                         // (w = -1 off-grid)
+    int4* fcell;         // cell of size h at this step's start: x, y, z, 0 (w = -1 off-grid)
+    float4* xb;          // positions at the last build
+    int4* cell_tmp;      // coarse cell of the pre-sort order
     int* key;            // bucket of each pre-sort particle
     int* rank;           // slot within its bucket (arbitrary before the stabilise pass)
     int* perm;           // new index -> old index
@@ -121,10 +133,12 @@ struct Ptr {
     int* bsum;           // block sums of the scan
     int* bbox;           // [6] cell box min/max
     GridLayout* layout;
-    int* nbr;            // [K][n] neighbour entries, k-major
-    int* nbr_cnt;        // [n]
-    int* shell;          // [Ks][n] entries with h <= |r| < h + skin at the sort, k-major
-    int* shell_cnt;      // [n]
+    int* nbr;            // [K][n] this step's neighbours, k-major
+    int* nbr_cnt;        // [n] true count; entries past K sit in the overflow pool
+    int* ovf;            // [ovf_cap] overflow pool, one run per overflowing particle
+    int* ovf_off;        // [n] start of the particle's run
+    int* vl;             // [Kv][n] candidates within h + skin at the last build, k-major
+    int* vl_cnt;         // [n]
     DevScalars* sc;
     DevAccum* ac;
     JcPtr jc;
@@ -162,6 +176,15 @@ __device__ __forceinline__ int cell_of(float x, float h) {
     float q = floorf(__fdiv_rn(x, h));
     q = fminf(fmaxf(q, -1.0e9f), 1.0e9f);
     return (int)q;
+}
+
+// cell_of from a product with the rounded reciprocal when that cannot change the floor:
+// x * inv_h is within 2.5e-7 relative of x / h, so a quotient more than 1e-6 (relative)
+// from the nearest integer floors the same; otherwise the correctly rounded division.
+__device__ __forceinline__ int cell_of_fast(float x, float h, float inv_h) {
+    const float q = x * inv_h;
+    if (fabsf(q - rintf(q)) > 1.0e-6f * fmaxf(fabsf(q), 1.0f) && fabsf(q) < 1.0e9f) return (int)floorf(q);
+    return cell_of(x, h);
 }
 
 // Spatial hash of the reference (particle_system.py:1283-1293), the fallback table.

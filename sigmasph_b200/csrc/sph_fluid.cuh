@@ -190,8 +190,6 @@ __global__ void __launch_bounds__(kBlock) k_eos(Cst c, Ptr P) {
         P.ac->w_diff_step = 0.0;
         P.ac->max_c_sq_bits = __float_as_uint(c.p.c_signal * c.p.c_signal);
         P.ac->max_accel_bits = __float_as_uint(1e-10f);
-        P.ac->max_disp_bits = 0u;
-        P.ac->max_grip_disp_bits = 0u;
     }
     if (i >= c.n) return;
     float4* pos = as4(P.cur.pos);
@@ -329,11 +327,12 @@ __global__ void __launch_bounds__(kBlock) k_advect(Cst c, Ptr P) {
         } else {
             p.x += dt * v4.x; p.y += dt * v4.y; p.z += dt * v4.z;
         }
-        if (c.pst_skin) {
-            // how far this particle moved since the sort, rounded up (fmaxf drops NaN)
+        {
+            // how far this particle moved, rounded up (a NaN counts as infinitely far)
             const float4 po = pos[i];
             const F3 d = {p.x - po.x, p.y - po.y, p.z - po.z};
             disp = norm3(d) * (1.0f + 1e-5f);
+            if (isnan(disp)) disp = INFINITY;
         }
         pos[i] = p;
         if (c.p.pst_enabled && c.p.pst_ma_mode == 1 && !(isnan(p.x) || isnan(p.y) || isnan(p.z)))
@@ -356,147 +355,50 @@ __global__ void __launch_bounds__(kBlock) k_advect(Cst c, Ptr P) {
         }
     }
     if (c.p.pst_enabled && c.p.pst_ma_mode == 1) block_max_atomic(vmag, &P.ac->max_v_bits);
-    if (c.pst_skin) block_max_atomic(disp, &P.ac->max_disp_bits);
+    block_max_atomic(disp, &P.ac->max_disp_bits);
 }
 
 // ------------------------------------------------------------------ apply_pst (DSPH.py:725-1046)
-// First the neighbour search of the shift: live positions after advect against the bins
-// of the step's rebuild (particle_system.py:1377-1411).  The pairs are compacted into the
-// neighbour list, whose pre-advect content is dead once the force pass has run, so the
-// evaluation below runs warp-coherent over ~80 pairs instead of inside the divergent
-// candidate loop.
-__global__ void __launch_bounds__(kBlock) k_pst_search(Cst c, Ptr P) {
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= c.n) return;
-    const F3 xi = f3(as4c(P.cur.pos)[i]);
-    int cnt = 0;
-    if (!(isnan(xi.x) || isnan(xi.y) || isnan(xi.z))) {
-        const GridLayout L = *P.layout;
-        const int cx = cell_of(xi.x, c.h), cy = cell_of(xi.y, c.h), cz = cell_of(xi.z, c.h);
-        const int n = c.n, K = c.K;
-        int* __restrict__ nb = P.nbr;
-        enumerate_neighbours(c, P, L, i, xi, cx, cy, cz, [&](int j, int mir, float4) {
-            if (cnt < K) nb[(size_t)cnt * n + i] = j | (mir << kMirShift);
-            ++cnt;
-        });
-        if (cnt > K) atomicOr(&P.sc->err, SPH_EW_NBR_OVERFLOW);
-    }
-    P.nbr_cnt[i] = cnt;
-}
-
-// Pairs of the shift search: the stored list, then (past the list's capacity) the same
-// live search again with the first K skipped.
-template <class F>
-__device__ __forceinline__ void for_each_live_neighbour(const Cst& c, const Ptr& P, int i, F3 xi, F&& f) {
-    const int cnt = __ldg(P.nbr_cnt + i);
-    const int m = cnt < c.K ? cnt : c.K;
-    list_pairs(P.nbr + i, (size_t)c.n, m, f);
-    if (cnt > c.K) {
-        const GridLayout L = *P.layout;
-        int cx = cell_of(xi.x, c.h), cy = cell_of(xi.y, c.h), cz = cell_of(xi.z, c.h);
-        int k = 0;
-        enumerate_neighbours(c, P, L, i, xi, cx, cy, cz, [&](int j, int mir, float4) {
-            if (k >= c.K) f(j, mir);
-            ++k;
-        });
-    }
-}
-
-// The stale-bin cells a particle's live window (lx, ly, lz) +- 1 holds and its binned
-// window (lx - ex, ly - ey, lz - ez) +- 1 does not: for each sweep (real, y, z and corner
-// mirror, particle_system.py:1393-1490) the cells whose offset along a moved axis a is
-// e_a.  f(j, mirror) gets every candidate there within h of the live position.
-template <class F>
-__device__ __forceinline__ void pst_far_slab(const Cst& c, const Ptr& P, F3 xi, int lx, int ly, int lz,
-                                             int ex, int ey, int ez, F&& f) {
-    const GridLayout L = *P.layout;
-    const bool hashed = L.mode != 0;
-    const float4* __restrict__ pos = as4c(P.cur.pos);
-    auto sweep = [&](int mir, F3 xs, int nx, int ny, int nz) {
-        const int b = bucket_of(nx, ny, nz, L, c.mcap);
-        if (b < 0) return;
-        bucket_candidates(P, hashed, b, nx, ny, nz, [&](int j) {
-            if (dist2_rn(xs, f3(__ldg(pos + j))) < c.d2_lt) f(j, mir);
-        });
-    };
-    auto far = [](int e, int o) { return e != 0 && o == e; };
-#pragma unroll 1
-    for (int o0 = -1; o0 <= 1; ++o0)
-#pragma unroll 1
-        for (int o1 = -1; o1 <= 1; ++o1)
-#pragma unroll 1
-            for (int o2 = -1; o2 <= 1; ++o2)
-                if (far(ex, o0) || far(ey, o1) || far(ez, o2)) sweep(0, xi, lx + o0, ly + o1, lz + o2);
-    const bool my = c.mirror_y && xi.y < c.h, mz = c.mirror_z && xi.z < c.h;
-    if (my) {
-#pragma unroll 1
-        for (int o0 = -1; o0 <= 1; ++o0)
-#pragma unroll 1
-            for (int o1 = -1; o1 <= 1; ++o1)
-                if (far(ex, o0) || far(ez, o1)) sweep(1, mirror3(1, xi), lx + o0, 0, lz + o1);
-    }
-    if (mz) {
-#pragma unroll 1
-        for (int o0 = -1; o0 <= 1; ++o0)
-#pragma unroll 1
-            for (int o1 = -1; o1 <= 1; ++o1)
-                if (far(ex, o0) || far(ey, o1)) sweep(2, mirror3(2, xi), lx + o0, ly + o1, 0);
-    }
-    if (my && mz && ex != 0) sweep(3, mirror3(3, xi), lx + ex, 0, 0);
-}
-
-// Pairs of the shift from the lists of the sort: the neighbours proper and the shell out
-// to h + skin, each re-tested at the live positions.  While no particle moved more than
-// skin / 2 since the sort, every live pair within h was within h + skin then, so the
-// lists hold every candidate of the particle's binned 27-cell window.  The reference
-// searches the stale bins around the LIVE cell instead (particle_system.py:1377-1411):
-// a particle that changed cells keeps only the entries binned inside its live window
-// (their binned cell is read back) and adds the candidates of the cells the live window
-// gained.  Past either list's capacity, or when the bound fails, the live search runs
-// for this particle.  Mirror entries keep the live plane test of their sweep.
+// Pairs of the shift: the reference's sweep from the live positions after advect against
+// the bins of this step's start (particle_system.py:1377-1411).  While the particles'
+// displacement since the lists' build -- at the step's start plus this step's advect and
+// grips -- is within the bound, from the candidate lists: every entry tested for
+// distance at the live positions, all but the deep ones also for j's step-start cell
+// against i's live cell.  Otherwise (or past the list's capacity) the stale-bin search.
 template <class F>
 __device__ __forceinline__ void for_each_pst_neighbour(const Cst& c, const Ptr& P, int i, F3 xi, F&& f) {
-    const int4 ci = P.cell[i];
-    const int cnt = __ldg(P.nbr_cnt + i), scnt = __ldg(P.shell_cnt + i);
-    const float dmax = __uint_as_float(P.ac->max_disp_bits) + __uint_as_float(P.ac->max_grip_disp_bits);
+    if (isnan(xi.x) || isnan(xi.y) || isnan(xi.z)) return;
+    const float dtot = __uint_as_float(P.ac->d_start_bits) + __uint_as_float(P.ac->max_disp_bits) +
+                       __uint_as_float(P.ac->max_grip_disp_bits);
     const int lx = cell_of(xi.x, c.h), ly = cell_of(xi.y, c.h), lz = cell_of(xi.z, c.h);
-    const int ex = lx - ci.x, ey = ly - ci.y, ez = lz - ci.z;
-    const bool lists = ci.w >= 0 && 2.0f * dmax <= c.skin && cnt <= c.K && scnt <= c.Ks &&
-                       abs(ex) <= 1 && abs(ey) <= 1 && abs(ez) <= 1;
-    if (!lists) {
-        if (isnan(xi.x) || isnan(xi.y) || isnan(xi.z)) return;
-        const GridLayout L = *P.layout;
-        enumerate_neighbours(c, P, L, i, xi, lx, ly, lz, [&](int j, int mir, float4) { f(j, mir); });
+    const int vc = __ldg(P.vl_cnt + i);
+    if (!(dtot <= c.dlim) || vc > c.Kv) {
+        stale_search(c, P, i, xi, lx, ly, lz, dtot, f);
         return;
     }
-    const bool moved = (ex | ey | ez) != 0;
     const float4* __restrict__ pos = as4c(P.cur.pos);
     const bool py = xi.y < c.h, pz = xi.z < c.h;
-    // entries deeper than h - skin at the sort are still within h: no live test
-    auto take = [&](int e) {
+    list_entries(P.vl + i, (size_t)c.n, vc, [&](int e) {
         const int j = e & kIdxMask, mir = (int)((unsigned)e >> kMirShift);
         if (mir && (((mir & 1) && !py) || ((mir & 2) && !pz))) return;
-        if (moved) {
-            // a mirror sweep fixes the cell index across its plane (y = 0, z = 0 rows)
-            const int4 cj = __ldg(P.cell + j);
-            if (abs(cj.x - lx) > 1 || (!(mir & 1) && abs(cj.y - ly) > 1) ||
-                (!(mir & 2) && abs(cj.z - lz) > 1))
-                return;
-        }
+        F3 xj = f3(__ldg(pos + j));
+        if (mir) xj = mirror3(mir, xj);
+        if (!(dist2_rn(xi, xj) < c.d2_lt)) return;
         if (e & kRimBit) {
-            F3 xj = f3(__ldg(pos + j));
-            if (mir) xj = mirror3(mir, xj);
-            if (!(dist2_rn(xi, xj) < c.d2_lt)) return;
+            const int4 fj = __ldg(P.fcell + j);
+            if (!sweep_cell_ok(mir, fj.x, fj.y, fj.z, lx, ly, lz)) return;
         }
         f(j, mir);
-    };
-    list_entries(P.nbr + i, (size_t)c.n, cnt, take);
-    list_entries(P.shell + i, (size_t)c.n, scnt, take);
-    if (moved) pst_far_slab(c, P, xi, lx, ly, lz, ex, ey, ez, f);
+    });
 }
 
 __global__ void __launch_bounds__(kBlock, 5) k_pst(Cst c, Ptr P) {
     int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i == 0) {   // steps whose shift could not use the candidate lists
+        const float dtot = __uint_as_float(P.ac->d_start_bits) + __uint_as_float(P.ac->max_disp_bits) +
+                           __uint_as_float(P.ac->max_grip_disp_bits);
+        if (!(dtot <= c.dlim)) P.ac->n_shift_search += 1ull;
+    }
     if (i >= c.n) return;
     const float4* __restrict__ pos = as4c(P.cur.pos);
     const float4* __restrict__ vel = as4c(P.cur.vel);
@@ -531,8 +433,7 @@ __global__ void __launch_bounds__(kBlock, 5) k_pst(Cst c, Ptr P) {
                 }
             }
         };
-        if (c.pst_skin) for_each_pst_neighbour(c, P, i, xi, pair);
-        else for_each_live_neighbour(c, P, i, xi, pair);
+        for_each_pst_neighbour(c, P, i, xi, pair);
     }
     float4 vi4 = vel[i];
     F3 vi = f3(vi4);

@@ -22,24 +22,28 @@ __global__ void k_grid_reset(Ptr P) {
         P.bbox[3] = P.bbox[4] = P.bbox[5] = (int)0x80000000;
         P.sc->off_grid_num = 0;
         P.sc->off_grid_mass = 0.0;
+        P.ac->d_start_bits = 0u;
     }
 }
 
-// update_grid_id's first half: the cell of every particle, NaN quarantine
-// (particle_system.py:1224-1234, :1304-1316), and the box of occupied cells.
+// update_grid_id's first half (particle_system.py:1224-1234, :1304-1316): NaN
+// quarantine and the off-grid tally, the coarse cell of every particle and the box of
+// occupied coarse cells (used if this step builds), and how far the particles moved since
+// the last build.
 __global__ void __launch_bounds__(kBlock) k_cells(Cst c, Ptr P) {
     int i = blockIdx.x * blockDim.x + threadIdx.x;
     int mn[3] = {0x7fffffff, 0x7fffffff, 0x7fffffff};
     int mx[3] = {(int)0x80000000, (int)0x80000000, (int)0x80000000};
     int offg = 0;
     double offm = 0.0;
+    float dst = 0.0f;
     if (i < c.n) {
         float4 p = reinterpret_cast<const float4*>(P.cur.pos)[i];
         bool nan = isnan(p.x) || isnan(p.y) || isnan(p.z);
         int4 cl;
-        cl.x = cell_of(p.x, c.h);
-        cl.y = cell_of(p.y, c.h);
-        cl.z = cell_of(p.z, c.h);
+        cl.x = cell_of(p.x, c.hc);
+        cl.y = cell_of(p.y, c.hc);
+        cl.z = cell_of(p.z, c.hc);
         cl.w = nan ? -1 : 0;
         if (nan) { cl.x = cl.y = cl.z = 0; }
         P.cell_tmp[i] = cl;
@@ -48,8 +52,13 @@ __global__ void __launch_bounds__(kBlock) k_cells(Cst c, Ptr P) {
             offm = (double)P.cur.vel[4 * i + 3];
         } else {
             mn[0] = mx[0] = cl.x; mn[1] = mx[1] = cl.y; mn[2] = mx[2] = cl.z;
+            const float4 b = P.xb[i];
+            // rounded up; a NaN build position (never built) reads as infinitely far
+            const float d = norm3(F3{p.x - b.x, p.y - b.y, p.z - b.z}) * (1.0f + 1e-5f);
+            dst = isnan(d) ? INFINITY : d;
         }
     }
+    block_max_atomic(dst, &P.ac->d_start_bits);
 #pragma unroll
     for (int a = 0; a < 3; ++a) {
         int v0 = mn[a], v1 = mx[a];
@@ -74,10 +83,29 @@ __global__ void __launch_bounds__(kBlock) k_cells(Cst c, Ptr P) {
     }
 }
 
-// Chooses the table: dense Morton over the occupied box if its compact code fits the
+// Decides whether this step builds the candidate lists: when the host asked, when the
+// off-grid count changed (the lists hold no quarantined particle), or when the particles'
+// displacement since the last build plus the last step's could pass the lists' bound (so
+// that the shift pass, after this step's move, can still use them).  A build chooses the
+// table: dense Morton over the occupied coarse-cell box if its compact code fits the
 // capacity, else the hashed table.
 __global__ void k_layout(Cst c, Ptr P) {
     if (threadIdx.x != 0 || blockIdx.x != 0) return;
+    DevAccum& A = *P.ac;
+    const float dstart = __uint_as_float(A.d_start_bits);
+    const float pred = __uint_as_float(A.max_disp_bits) + __uint_as_float(A.max_grip_disp_bits);
+    A.max_disp_bits = 0u;       // this step's move accumulates from here
+    A.max_grip_disp_bits = 0u;
+    A.ovf_used = 0u;
+    const int offg = P.sc->off_grid_num;
+    const int build = A.force_build || offg != A.off_grid_build || !(dstart + pred <= c.dlim);
+    A.n_steps += 1ull;
+    A.rebuild = build;
+    if (!build) return;
+    A.force_build = 0;
+    A.off_grid_build = offg;
+    A.d_start_bits = 0u;
+    A.n_builds += 1ull;
     GridLayout L;
     int any = P.bbox[0] <= P.bbox[3];
     int tb = 0;
@@ -103,6 +131,7 @@ __global__ void k_layout(Cst c, Ptr P) {
 }
 
 __global__ void k_zero_hist(Cst c, Ptr P) {
+    if (!P.ac->rebuild) return;
     int nb = P.layout->nbuckets + 2;
     for (int b = blockIdx.x * blockDim.x + threadIdx.x; b < nb; b += gridDim.x * blockDim.x)
         P.hist[b] = 0;
@@ -111,7 +140,7 @@ __global__ void k_zero_hist(Cst c, Ptr P) {
 // Bucket of every particle and its arbitrary slot in the bucket.
 __global__ void __launch_bounds__(kBlock) k_keys(Cst c, Ptr P) {
     int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= c.n) return;
+    if (i >= c.n || !P.ac->rebuild) return;
     const GridLayout L = *P.layout;
     int4 cl = P.cell_tmp[i];
     int key = cl.w < 0 ? L.nbuckets : bucket_of(cl.x, cl.y, cl.z, L, c.mcap);
@@ -152,6 +181,7 @@ __device__ __forceinline__ int block_exclusive_scan(int v, int* total) {
 }
 
 __global__ void __launch_bounds__(kBlock) k_scan_reduce(Ptr P) {
+    if (!P.ac->rebuild) return;
     int nb = P.layout->nbuckets + 1;
     int ntiles = (nb + kScanTile - 1) / kScanTile;
     for (int t = blockIdx.x; t < ntiles; t += gridDim.x) {
@@ -173,6 +203,7 @@ __global__ void __launch_bounds__(kBlock) k_scan_reduce(Ptr P) {
 }
 
 __global__ void __launch_bounds__(1024) k_scan_bsum(Ptr P) {
+    if (!P.ac->rebuild) return;
     int nb = P.layout->nbuckets + 1;
     int ntiles = (nb + kScanTile - 1) / kScanTile;
     __shared__ int carry;
@@ -191,6 +222,7 @@ __global__ void __launch_bounds__(1024) k_scan_bsum(Ptr P) {
 }
 
 __global__ void __launch_bounds__(kBlock) k_scan_apply(Ptr P) {
+    if (!P.ac->rebuild) return;
     int nb = P.layout->nbuckets + 1;
     int ntiles = (nb + kScanTile - 1) / kScanTile;
     for (int t = blockIdx.x; t < ntiles; t += gridDim.x) {
@@ -216,7 +248,7 @@ __global__ void __launch_bounds__(kBlock) k_scan_apply(Ptr P) {
 
 __global__ void __launch_bounds__(kBlock) k_scatter(Cst c, Ptr P) {
     int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= c.n) return;
+    if (i >= c.n || !P.ac->rebuild) return;
     P.perm[P.start[P.key[i]] + P.rank[i]] = i;
 }
 
@@ -224,7 +256,7 @@ __global__ void __launch_bounds__(kBlock) k_scatter(Cst c, Ptr P) {
 // particle that drew slot 0 insertion-sorts its bucket's permutation entries.
 __global__ void __launch_bounds__(kBlock) k_stabilise(Cst c, Ptr P) {
     int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= c.n || P.rank[i] != 0) return;
+    if (i >= c.n || !P.ac->rebuild || P.rank[i] != 0) return;
     int k = P.key[i];
     int s = P.start[k], e = P.start[k + 1];
     for (int a = s + 1; a < e; ++a) {
@@ -235,11 +267,15 @@ __global__ void __launch_bounds__(kBlock) k_stabilise(Cst c, Ptr P) {
     }
 }
 
-// Gathers every persistent field into the other buffer set in the new order.
+// Gathers every persistent field into the other buffer set: in the new order when this
+// step builds, else as they are (the two sets alternate every step either way).  Writes
+// the step-start cell of size h (the reference's bins) of every particle; a build also
+// records each particle's coarse cell and position.
 __global__ void __launch_bounds__(kBlock) k_gather(Cst c, Ptr P) {
     int d = blockIdx.x * blockDim.x + threadIdx.x;
     if (d >= c.n) return;
-    int s = P.perm[d];
+    const bool build = P.ac->rebuild != 0;
+    const int s = build ? P.perm[d] : d;
     const SphFieldSet& A = P.cur;
     const SphFieldSet& B = P.nxt;
     reinterpret_cast<float4*>(B.pos)[d] = __ldg(reinterpret_cast<const float4*>(A.pos) + s);
@@ -257,14 +293,32 @@ __global__ void __launch_bounds__(kBlock) k_gather(Cst c, Ptr P) {
         reinterpret_cast<float4*>(B.bcdisp)[d] = __ldg(reinterpret_cast<const float4*>(A.bcdisp) + s);
         reinterpret_cast<float4*>(B.acc)[d] = __ldg(reinterpret_cast<const float4*>(A.acc) + s);
     }
-    int4 cl = P.cell_tmp[s];
-    cl.w = cl.w < 0 ? -1 : P.key[s];
-    P.cell[d] = cl;
+    const float4 p = __ldg(reinterpret_cast<const float4*>(A.pos) + s);
+    const bool nan = isnan(p.x) || isnan(p.y) || isnan(p.z);
+    P.fcell[d] = nan ? make_int4(0, 0, 0, -1)
+                     : make_int4(cell_of(p.x, c.h), cell_of(p.y, c.h), cell_of(p.z, c.h), 0);
+    if (build) {
+        int4 cl = P.cell_tmp[s];
+        cl.w = cl.w < 0 ? -1 : P.key[s];
+        P.cell[d] = cl;
+        P.xb[d] = p;
+    }
 }
 
 // ------------------------------------------------------------------ neighbour enumeration
-// Candidates of cell (nx, ny, nz) in bucket b: the bucket's range, filtered on the cell
-// id when the table is hashed (collisions share buckets).
+// The reference bins every step in cells of size h and pairs i with j when j is binned in
+// one of the 27 cells around i's cell, j != i and |x_i - x_j| < h; the y, z and corner
+// mirror sweeps pair i's image with the particles binned in the y = 0 row, the z = 0 row
+// and the corner column (particle_system.py:1348-1490).  Here the pairs come from
+// candidate lists: every pair within h + skin at the last build, found over coarse cells
+// of h + skin.  While no particle has moved more than dlim since the build, every pair of
+// the reference's sweep is in the list, and the list is filtered with the reference's own
+// tests: the distance, and the cells of size h (a pair whose axis separations all stay
+// well inside h always passes those; one that ends up 2 cells apart in floating point
+// does not).
+
+// Candidates of the coarse cell (nx, ny, nz) in bucket b: the bucket's range, filtered on
+// the cell id when the table is hashed (collisions share buckets).
 template <class F>
 __device__ __forceinline__ void bucket_candidates(const Ptr& P, bool hashed, int b, int nx, int ny,
                                                   int nz, F&& f) {
@@ -278,148 +332,95 @@ __device__ __forceinline__ void bucket_candidates(const Ptr& P, bool hashed, int
     }
 }
 
-// The y, z and corner mirror sweeps of a particle at xi in cell (cx, cy, cz)
-// (particle_system.py:1442-1490): the image of xi against the cells of the y = 0 row,
-// the z = 0 row and the corner column; a particle pairs with its own image too.  A sweep
-// runs when xi is within hcut of its plane; f(j, mirror, pos_j, d2) gets every candidate
-// with d2 < d2cut (the neighbour test uses hcut = h, d2cut = the |r| < h threshold).
+// Every candidate of the coarse table around coarse cell (bx, by, bz), radius w: the real
+// sweep (self excluded) with the query point xq, then -- when xq is within hcut of the
+// plane -- the mirror sweeps with xq's image over coarse rows rlo..rhi of the mirrored
+// axis.  f(j, mirror, pos_j, d2) for d2 < d2cut.
 template <class F>
-__device__ __forceinline__ void enumerate_mirrors_cut(const Cst& c, const Ptr& P, const GridLayout& L,
-                                                      F3 xi, int cx, int cy, int cz, float d2cut,
-                                                      float hcut, F&& f) {
+__device__ __forceinline__ void sweep_coarse(const Cst& c, const Ptr& P, const GridLayout& L, int self_idx,
+                                             F3 xq, int bx, int by, int bz, int w, int rlo, int rhi,
+                                             float d2cut, float hcut, F&& f) {
     const float4* __restrict__ pos = reinterpret_cast<const float4*>(P.cur.pos);
     const bool hashed = L.mode != 0;
-    if (c.mirror_y && xi.y < hcut) {
-        const F3 xm = mirror3(1, xi);
+    auto cell = [&](int mir, F3 xs, int nx, int ny, int nz) {
+        const int b = bucket_of(nx, ny, nz, L, c.mcap);
+        if (b < 0) return;
+        bucket_candidates(P, hashed, b, nx, ny, nz, [&](int j) {
+            if (mir == 0 && j == self_idx) return;
+            const float4 pj = __ldg(pos + j);
+            const float d2 = dist2_rn(xs, f3(pj));
+            if (d2 < d2cut) f(j, mir, pj, d2);
+        });
+    };
 #pragma unroll 1
-        for (int o0 = -1; o0 <= 1; ++o0)
+    for (int o0 = -w; o0 <= w; ++o0)
 #pragma unroll 1
-            for (int o1 = -1; o1 <= 1; ++o1) {
-                const int nx = cx + o0, ny = 0, nz = cz + o1;
-                const int b = bucket_of(nx, ny, nz, L, c.mcap);
-                if (b < 0) continue;
-                bucket_candidates(P, hashed, b, nx, ny, nz, [&](int j) {
-                    const float4 pj = __ldg(pos + j);
-                    const float d2 = dist2_rn(xm, f3(pj));
-                    if (d2 < d2cut) f(j, 1, pj, d2);
-                });
-            }
+        for (int o1 = -w; o1 <= w; ++o1)
+#pragma unroll 1
+            for (int o2 = -w; o2 <= w; ++o2) cell(0, xq, bx + o0, by + o1, bz + o2);
+    const bool my = c.mirror_y && xq.y < hcut, mz = c.mirror_z && xq.z < hcut;
+    if (my) {
+        const F3 xm = mirror3(1, xq);
+#pragma unroll 1
+        for (int o0 = -w; o0 <= w; ++o0)
+#pragma unroll 1
+            for (int ry = rlo; ry <= rhi; ++ry)
+#pragma unroll 1
+                for (int o1 = -w; o1 <= w; ++o1) cell(1, xm, bx + o0, ry, bz + o1);
     }
-    if (c.mirror_z && xi.z < hcut) {
-        const F3 xm = mirror3(2, xi);
+    if (mz) {
+        const F3 xm = mirror3(2, xq);
 #pragma unroll 1
-        for (int o0 = -1; o0 <= 1; ++o0)
+        for (int o0 = -w; o0 <= w; ++o0)
 #pragma unroll 1
-            for (int o1 = -1; o1 <= 1; ++o1) {
-                const int nx = cx + o0, ny = cy + o1, nz = 0;
-                const int b = bucket_of(nx, ny, nz, L, c.mcap);
-                if (b < 0) continue;
-                bucket_candidates(P, hashed, b, nx, ny, nz, [&](int j) {
-                    const float4 pj = __ldg(pos + j);
-                    const float d2 = dist2_rn(xm, f3(pj));
-                    if (d2 < d2cut) f(j, 2, pj, d2);
-                });
-            }
+            for (int o1 = -w; o1 <= w; ++o1)
+#pragma unroll 1
+                for (int rz = rlo; rz <= rhi; ++rz) cell(2, xm, bx + o0, by + o1, rz);
     }
-    if (c.mirror_y && c.mirror_z && xi.y < hcut && xi.z < hcut) {
-        const F3 xm = mirror3(3, xi);
+    if (my && mz) {
+        const F3 xm = mirror3(3, xq);
 #pragma unroll 1
-        for (int o0 = -1; o0 <= 1; ++o0) {
-            const int nx = cx + o0, ny = 0, nz = 0;
-            const int b = bucket_of(nx, ny, nz, L, c.mcap);
-            if (b < 0) continue;
-            bucket_candidates(P, hashed, b, nx, ny, nz, [&](int j) {
-                const float4 pj = __ldg(pos + j);
-                const float d2 = dist2_rn(xm, f3(pj));
-                if (d2 < d2cut) f(j, 3, pj, d2);
-            });
-        }
+        for (int o0 = -w; o0 <= w; ++o0)
+#pragma unroll 1
+            for (int ry = rlo; ry <= rhi; ++ry)
+#pragma unroll 1
+                for (int rz = rlo; rz <= rhi; ++rz) cell(3, xm, bx + o0, ry, rz);
     }
 }
 
-// Every candidate of a particle at xi whose centre cell is (cx, cy, cz) with d2 < d2cut,
-// in the reference's order: the 27 offsets with the last index fastest, then the y, z and
-// corner mirror sweeps (particle_system.py:1393-1490).  `self_idx` is excluded from the
-// real sweep only.  Positions are read from `pos` (live positions).
-template <class F>
-__device__ __forceinline__ void enumerate_cut(const Cst& c, const Ptr& P, const GridLayout& L, int self_idx,
-                                              F3 xi, int cx, int cy, int cz, float d2cut, float hcut,
-                                              F&& f) {
-    const float4* __restrict__ pos = reinterpret_cast<const float4*>(P.cur.pos);
-    const bool hashed = L.mode != 0;
-#pragma unroll 1
-    for (int o0 = -1; o0 <= 1; ++o0)
-#pragma unroll 1
-        for (int o1 = -1; o1 <= 1; ++o1)
-#pragma unroll 1
-            for (int o2 = -1; o2 <= 1; ++o2) {
-                const int nx = cx + o0, ny = cy + o1, nz = cz + o2;
-                const int b = bucket_of(nx, ny, nz, L, c.mcap);
-                if (b < 0) continue;
-                bucket_candidates(P, hashed, b, nx, ny, nz, [&](int j) {
-                    if (j == self_idx) return;
-                    const float4 pj = __ldg(pos + j);
-                    const float d2 = dist2_rn(xi, f3(pj));
-                    if (d2 < d2cut) f(j, 0, pj, d2);
-                });
-            }
-    enumerate_mirrors_cut(c, P, L, xi, cx, cy, cz, d2cut, hcut, f);
+// The cell test of the reference's sweeps for a pair that passed the distance test: j's
+// cell (jx, jy, jz) of size h against the query cell q.  A mirror sweep takes j from the
+// y = 0 row (y image), the z = 0 row (z image) or both (corner).
+__device__ __forceinline__ bool sweep_cell_ok(int mir, int jx, int jy, int jz, int qx, int qy, int qz) {
+    if (abs(jx - qx) > 1) return false;
+    if (mir & 1) { if (jy != 0) return false; } else if (abs(jy - qy) > 1) return false;
+    if (mir & 2) { if (jz != 0) return false; } else if (abs(jz - qz) > 1) return false;
+    return true;
 }
 
-// The neighbours proper: f(j, mirror, pos_j) for |r| < h (bit-exact against the reference).
-template <class F>
-__device__ __forceinline__ void enumerate_neighbours(const Cst& c, const Ptr& P, const GridLayout& L,
-                                                     int self_idx, F3 xi, int cx, int cy, int cz,
-                                                     F&& f) {
-    enumerate_cut(c, P, L, self_idx, xi, cx, cy, cz, c.d2_lt, c.h,
-                  [&](int j, int mir, float4 pj, float) { f(j, mir, pj); });
-}
-
-// Builds the neighbour list of every particle from the positions the cells were binned
-// at (before advect the live and the binned cell coincide).  Entries beyond K are not
-// stored; the count is the true count and the pair passes recover the rest by a direct
-// search (for_each_neighbour below).
-__global__ void __launch_bounds__(kBlock) k_nbr_build(Cst c, Ptr P) {
+// Builds every particle's candidate list at the build's positions: the coarse 27-cell
+// sweep out to h + skin, and the mirror sweeps over coarse rows -1 and 0 (a particle
+// that crosses the plane later is binned in row 0 or -1 of size h).  Entries within
+// h - skin are marked deep: under the bound they stay within h and their cells stay
+// adjacent, so the per-step filter takes them without a test.
+__global__ void __launch_bounds__(kBlock) k_vlist_build(Cst c, Ptr P) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= c.n) return;
-    const GridLayout L = *P.layout;
+    if (i >= c.n || !P.ac->rebuild) return;
     const int4 ci = P.cell[i];
-    if (ci.w < 0) {
-        P.nbr_cnt[i] = 0;
-        if (c.pst_skin) P.shell_cnt[i] = 0;
-        return;
-    }
+    if (ci.w < 0) { P.vl_cnt[i] = 0; return; }
+    const GridLayout L = *P.layout;
     const F3 xi = f3(reinterpret_cast<const float4*>(P.cur.pos)[i]);
     int cnt = 0;
-    const int n = c.n, K = c.K;
-    int* __restrict__ nb = P.nbr;
-    if (c.pst_skin) {
-        // the same sweep out to h + skin: neighbours proper go to the list (in the same
-        // order as without the shell), the rest of the shell to the shift's candidates
-        int scnt = 0;
-        const int Ks = c.Ks;
-        int* __restrict__ sb = P.shell;
-        enumerate_cut(c, P, L, i, xi, ci.x, ci.y, ci.z, c.d2_skin, c.h + c.skin,
-                      [&](int j, int mir, float4, float d2) {
-            const bool plane = mir == 0 || (((mir & 1) == 0 || xi.y < c.h) && ((mir & 2) == 0 || xi.z < c.h));
-            const int e = j | (d2 < c.d2_deep ? 0 : kRimBit) | (mir << kMirShift);
-            if (d2 < c.d2_lt && plane) {
-                if (cnt < K) nb[(size_t)cnt * n + i] = e;
-                ++cnt;
-            } else {
-                if (scnt < Ks) sb[(size_t)scnt * n + i] = e;
-                ++scnt;
-            }
-        });
-        P.shell_cnt[i] = scnt;
-    } else {
-        enumerate_neighbours(c, P, L, i, xi, ci.x, ci.y, ci.z, [&](int j, int mir, float4) {
-            if (cnt < K) nb[(size_t)cnt * n + i] = j | (mir << kMirShift);
-            ++cnt;
-        });
-    }
-    if (cnt > K) atomicOr(&P.sc->err, SPH_EW_NBR_OVERFLOW);
-    P.nbr_cnt[i] = cnt;
+    const int n = c.n, Kv = c.Kv;
+    int* __restrict__ vl = P.vl;
+    sweep_coarse(c, P, L, i, xi, ci.x, ci.y, ci.z, 1, -1, 0, c.d2_skin, c.h + c.skin,
+                 [&](int j, int mir, float4, float d2) {
+        const int e = j | ((mir == 0 && d2 < c.d2_deep) ? 0 : kRimBit) | (mir << kMirShift);
+        if (cnt < Kv) vl[(size_t)cnt * n + i] = e;
+        ++cnt;
+    });
+    if (cnt > Kv) atomicOr(&P.sc->err, SPH_EW_CAND_OVERFLOW);
+    P.vl_cnt[i] = cnt;
 }
 
 // The m stored entries of one particle's k-major list, with the next two entries in
@@ -442,23 +443,101 @@ __device__ __forceinline__ void list_pairs(const int* __restrict__ nb, size_t n,
     list_entries(nb, n, m, [&](int e) { f(e & kIdxMask, (int)((unsigned)e >> kMirShift)); });
 }
 
-// Calls f(j, mirror) for the stored neighbours of i, then for any beyond the list's
-// capacity by re-running the search (same order, first K skipped).
+// The reference's sweep against the bins of this step's start (particle_system.py:
+// 1348-1490) for query point xq in cell q of size h, without the candidate lists: the
+// coarse table of the last build searched wide enough for displacement D since it, each
+// candidate tested for distance at the current positions and for its step-start cell.
+template <class F>
+__device__ __forceinline__ void stale_search(const Cst& c, const Ptr& P, int i, F3 xq, int qx, int qy, int qz,
+                                             float D, F&& f) {
+    const int4 bi = P.cell[i];
+    if (bi.w < 0) return;
+    const GridLayout L = *P.layout;
+    // |r| < h now => |r| < h + 2 D at the build => coarse cells at most w apart; a row of
+    // size h at the plane (y in [0, h)) lies in coarse rows floor(-D / hc) .. w - 1
+    const float wf = ceilf((c.h + 2.0f * D) / c.hc);
+    const int w = wf <= 8.0f ? max((int)wf, 1) : 8;
+    if (!(wf <= 8.0f)) atomicOr(&P.sc->err, SPH_EW_NBR_OVERFLOW);
+    const float rf = ceilf(D / c.hc);
+    const int rlo = -(rf <= 8.0f ? max((int)rf, 1) : 8);
+    sweep_coarse(c, P, L, i, xq, bi.x, bi.y, bi.z, w, rlo, w - 1, c.d2_lt, c.h,
+                 [&](int j, int mir, float4, float) {
+        const int4 fj = __ldg(P.fcell + j);
+        if (fj.w >= 0 && sweep_cell_ok(mir, fj.x, fj.y, fj.z, qx, qy, qz)) f(j, mir);
+    });
+}
+
+// The neighbours of i at this step's start (the reference's sweep against fresh bins):
+// the candidate list filtered -- deep entries as they are, the others by distance and
+// cell at the current positions -- or, past the list's capacity, the stale-bin search.
+template <class F>
+__device__ __forceinline__ void for_each_start_neighbour(const Cst& c, const Ptr& P, int i, F&& f) {
+    const int4 fi = P.fcell[i];
+    if (fi.w < 0) return;
+    const float4* __restrict__ pos = reinterpret_cast<const float4*>(P.cur.pos);
+    const F3 xi = f3(pos[i]);
+    const int vc = __ldg(P.vl_cnt + i);
+    if (vc > c.Kv) {
+        stale_search(c, P, i, xi, fi.x, fi.y, fi.z, __uint_as_float(P.ac->d_start_bits), f);
+        return;
+    }
+    const bool py = xi.y < c.h, pz = xi.z < c.h;
+    list_entries(P.vl + i, (size_t)c.n, vc, [&](int e) {
+        const int j = e & kIdxMask, mir = (int)((unsigned)e >> kMirShift);
+        if (mir && (((mir & 1) && !py) || ((mir & 2) && !pz))) return;
+        if (e & kRimBit) {
+            const float4 pj = __ldg(pos + j);
+            F3 xj = f3(pj);
+            if (mir) xj = mirror3(mir, xj);
+            if (!(dist2_rn(xi, xj) < c.d2_lt)) return;
+            if (!sweep_cell_ok(mir, cell_of_fast(pj.x, c.h, c.inv_h), cell_of_fast(pj.y, c.h, c.inv_h),
+                               cell_of_fast(pj.z, c.h, c.inv_h), fi.x, fi.y, fi.z))
+                return;
+        }
+        f(j, mir);
+    });
+}
+
+// This step's neighbour list from the candidate lists (every step; the pair passes read
+// it).  It holds as many entries as the candidate list, so it overflows only when the
+// candidate list did and more than K pairs lie within h: the pairs past K then go, in
+// order, to a run of the overflow pool (the enumeration runs a second time to write it).
+__global__ void __launch_bounds__(kBlock) k_nbr_filter(Cst c, Ptr P) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= c.n) return;
+    int cnt = 0;
+    const int n = c.n, K = c.K;
+    int* __restrict__ nb = P.nbr;
+    for_each_start_neighbour(c, P, i, [&](int j, int mir) {
+        if (cnt < K) nb[(size_t)cnt * n + i] = j | (mir << kMirShift);
+        ++cnt;
+    });
+    if (cnt > K) {
+        atomicOr(&P.sc->err, SPH_EW_NBR_OVERFLOW);
+        const unsigned extra = (unsigned)(cnt - K);
+        const unsigned base = atomicAdd(&P.ac->ovf_used, extra);
+        if (base <= c.ovf_cap && extra <= c.ovf_cap - base) {
+            P.ovf_off[i] = (int)base;
+            int* __restrict__ run = P.ovf + base;
+            int k = 0;
+            for_each_start_neighbour(c, P, i, [&](int j, int mir) {
+                if (k >= K) run[k - K] = j | (mir << kMirShift);
+                ++k;
+            });
+        } else {
+            atomicOr(&P.sc->err, SPH_EW_NBR_DROPPED);
+            cnt = K;
+        }
+    }
+    P.nbr_cnt[i] = cnt;
+}
+
+// Calls f(j, mirror) for this step's neighbours of i: the list, then any overflow run.
 template <class F>
 __device__ __forceinline__ void for_each_neighbour(const Cst& c, const Ptr& P, int i, F&& f) {
     const int cnt = __ldg(P.nbr_cnt + i);
-    const int m = cnt < c.K ? cnt : c.K;
-    list_pairs(P.nbr + i, (size_t)c.n, m, f);
-    if (cnt > c.K) {
-        const GridLayout L = *P.layout;
-        int4 ci = P.cell[i];
-        F3 xi = f3(reinterpret_cast<const float4*>(P.cur.pos)[i]);
-        int k = 0;
-        enumerate_neighbours(c, P, L, i, xi, ci.x, ci.y, ci.z, [&](int j, int mir, float4) {
-            if (k >= c.K) f(j, mir);
-            ++k;
-        });
-    }
+    list_pairs(P.nbr + i, (size_t)c.n, cnt < c.K ? cnt : c.K, f);
+    if (cnt > c.K) list_pairs(P.ovf + __ldg(P.ovf_off + i), 1, cnt - c.K, f);
 }
 
 }  // namespace sph

@@ -26,16 +26,18 @@ inline void fill_constants_from(const SphParams& p, int64_t n, Cst& c) {
     c.all_gamma_one = 1;
     c.any_jc = 0;
     c.block = kBlock;
-    // skin of the shift's candidate shell: a tenth of the support; the squared cut is
-    // rounded up so that it contains every pair a float32 distance test could place
-    // within h + skin
+    // skin of the candidate lists: a tenth of the support.  The squared cut is rounded up
+    // so that it holds every pair a float32 distance test could place within h + skin;
+    // the bound keeps 2 dlim a thousandth of the skin short of it, far beyond the
+    // rounding of the displacement, distance and coarse-cell computations.
     {
         const double hs = p.support_radius;
         c.skin = (float)(0.1 * hs);
+        c.hc = (float)(1.1 * hs);
+        c.dlim = (float)(0.05 * hs * (1.0 - 1e-3));
         c.d2_skin = (float)((1.1 * hs) * (1.1 * hs) * (1.0 + 1e-5));
         c.d2_deep = (float)((0.9 * hs) * (0.9 * hs) * (1.0 - 1e-5));
     }
-    c.pst_skin = 1;
     double hd = p.support_radius;
     double al = p.two_d ? 7.0 / (M_PI * hd * hd) : 21.0 / (2.0 * M_PI * hd * hd * hd);
     c.h = (float)hd;

@@ -17,7 +17,7 @@
 //                    the half kicks, with a device-side stage count (SOLID.py:4485-4615)
 //   k_solid_advect   plain advect when the damper is in-loop
 //   k_constraints    grip kinematics and FP64 grip force          (SOLID.py:5019-5055)
-//   (k_pst_search, k_pst, k_finish as for the fluid)
+//   (k_pst, k_finish as for the fluid)
 //
 // Per-step scratch in aux ([n][24] floats = 6 float4):
 //   aux[0]  s_new xx yy zz xy     aux[1]  s_new xz yz, eps_p_new, e_new
@@ -214,10 +214,6 @@ __device__ __forceinline__ float solid_pressure(const Cst& c, const Ptr& P, int 
 
 // ------------------------------------------------------------------ load factor
 __global__ void k_solid_load(Cst c, Ptr P) {
-    if (blockIdx.x == 0 && threadIdx.x == 0) {   // this step's displacement bounds
-        P.ac->max_disp_bits = 0u;
-        P.ac->max_grip_disp_bits = 0u;
-    }
     if (c.n_inst > 0) {
         // per instance: its smoothstep from its own clock, and a fresh dt maximum
         for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < c.n_inst; k += gridDim.x * blockDim.x) {
@@ -1168,15 +1164,16 @@ __global__ void __launch_bounds__(kBlock) k_sts_finish(Cst c, Ptr P) {
         } else {
             p.x += dt * v.x; p.y += dt * v.y; p.z += dt * v.z;
         }
-        if (c.pst_skin) {
+        {
             const float4 po = pos[i];
             disp = norm3(F3{p.x - po.x, p.y - po.y, p.z - po.z}) * (1.0f + 1e-5f);
+            if (isnan(disp)) disp = INFINITY;
         }
         pos[i] = p;
     }
     block_sum_atomic(ke, &P.sc->hg_work);
     block_sum_atomic(wl, &P.sc->leftover_work);
-    if (c.pst_skin) block_max_atomic(disp, &P.ac->max_disp_bits);
+    block_max_atomic(disp, &P.ac->max_disp_bits);
 }
 
 __global__ void __launch_bounds__(kBlock) k_solid_advect(Cst c, Ptr P) {
@@ -1201,13 +1198,14 @@ __global__ void __launch_bounds__(kBlock) k_solid_advect(Cst c, Ptr P) {
     } else {
         p.x += dt * v.x; p.y += dt * v.y; p.z += dt * v.z;
     }
-    if (c.pst_skin) {
+    {
         const float4 po = pos[i];
         disp = norm3(F3{p.x - po.x, p.y - po.y, p.z - po.z}) * (1.0f + 1e-5f);
+        if (isnan(disp)) disp = INFINITY;
     }
     pos[i] = p;
     }
-    if (c.pst_skin) block_max_atomic(disp, &P.ac->max_disp_bits);
+    block_max_atomic(disp, &P.ac->max_disp_bits);
 }
 
 // ------------------------------------------------------------------ grips
@@ -1259,6 +1257,7 @@ __device__ __forceinline__ void constraints_ensemble(const Cst& c, const Ptr& P)
         }
         pos[i] = p; vel[i] = v; dsp[i] = u; P.acc[i] = a;
         gdisp = norm3(F3{p.x - po.x, p.y - po.y, p.z - po.z}) * (1.0f + 1e-5f);
+        if (isnan(gdisp)) gdisp = INFINITY;
     }
 #pragma unroll
     for (int d = 0; d < 3; ++d) addr_add_atomic(fd[d], &P.inst[k].constraint_force[g][d], rec[d]);
@@ -1311,9 +1310,9 @@ __global__ void __launch_bounds__(kBlock) k_constraints(Cst c, Ptr P) {
         }
         pos[i] = p; vel[i] = v; dsp[i] = u; P.acc[i] = a;
         gdisp = norm3(F3{p.x - po.x, p.y - po.y, p.z - po.z}) * (1.0f + 1e-5f);
+        if (isnan(gdisp)) gdisp = INFINITY;
     }
-    if (c.pst_skin) block_max_atomic(gdisp, &P.ac->max_grip_disp_bits);
-    else __syncthreads();
+    block_max_atomic(gdisp, &P.ac->max_grip_disp_bits);
     if (threadIdx.x < 24) {
         const int k = threadIdx.x / 3, d = threadIdx.x % 3;
         if (s_axes[k] & (1 << d)) {
@@ -1381,7 +1380,6 @@ inline int solid_substep_launch(const Cst& c, const Ptr& P, int n, cudaStream_t 
         k_constraints<<<nb, bs, 0, st>>>(c, P); mark("k_constraints");
     }
     if (in(SPH_STAGE_PST) && c.p.pst_enabled) {
-        if (!c.pst_skin) { k_pst_search<<<nb, bs, 0, st>>>(c, P); mark("k_pst_search"); }
         k_pst<<<nb, bs, 0, st>>>(c, P); mark("k_pst");
         k_finish<<<nb, bs, 0, st>>>(c, P, last_stage >= SPH_STAGE_BOUNDARY ? 3 : 1); mark("k_finish");
     } else if (in(SPH_STAGE_BOUNDARY)) {

@@ -225,6 +225,13 @@ class _SolverBase:
                         C.byref(cnt), _stream_ptr()))
         return pi, pj, pm
 
+    def list_stats(self, reset=False):
+        """Candidate-list statistics: steps, steps that built the lists, shift passes that
+        searched the coarse table."""
+        out = (C.c_uint64 * 3)()
+        abi.check(self.L.sph_list_stats(self.h, out, int(bool(reset)), _stream_ptr()), "sph_list_stats")
+        return {"steps": out[0], "builds": out[1], "shift_searches": out[2]}
+
     # ------------------------------------------------------------------ reductions
     def _reduce(self):
         out = (C.c_double * abi.RED_COUNT)()

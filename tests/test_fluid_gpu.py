@@ -121,10 +121,11 @@ def test_live_search_uses_stale_bins(cuda):
 @pytest.mark.parametrize("scene_fn", [lambda: small_scene(5000), axi_fluid_scene, quarter_scene],
                          ids=["3d", "axisymmetric", "quarter_yz"])
 def test_shift_pairs_from_lists(cuda, scene_fn, reach):
-    """The shift pass serves its pairs from the sort's lists (neighbours + the shell out to
-    1.1 h) while every particle moved less than 0.05 h; particles that changed cells keep
-    the entries binned in their live window and add the cells it gained.  Beyond 0.05 h
-    it searches again.  Either way the pair set is the stale-bin live search's."""
+    """The shift pass serves its pairs from the candidate lists (every pair within 1.1 h
+    at the build) while every particle moved less than 0.05 h since: entries re-tested for
+    distance at the live positions and for j's step-start cell against i's live cell.
+    Beyond 0.05 h it searches the coarse table.  Either way the pair set is the stale-bin
+    live search's."""
     ps, solver, _ = make_pair(scene_fn(), fp64=False)
     # off the lattice by up to half a spacing, so that particles sit near cell edges too
     x = ps.x.to_numpy()
@@ -137,6 +138,52 @@ def test_shift_pairs_from_lists(cuda, scene_fn, reach):
     assert crossed[1:].sum() > 0
     if not ps.two_d:   # 3D: ~50 of these decks' particles change cells along 2 axes
         assert crossed[2:].sum() > 0
+
+
+def _oracle_pairs_at(ps, solver):
+    """The oracle's neighbour pairs after its own sort of the GPU's current state."""
+    orc = Oracle(build_params(ps), ps.particle_max_num, fp64=False)
+    orc.set_state(state_from_sets(ps.state_numpy()), solver.dt[None])
+    orc.stage(abi.STAGE_SORT)
+    oi, oj, om = orc.pairs()
+    return pair_set(oi, oj, om, orc.get_state()["pid"])
+
+
+@pytest.mark.parametrize("scene_fn", [lambda: small_scene(6000), quarter_scene], ids=["3d", "quarter_yz"])
+def test_lists_between_builds_match_oracle(cuda, scene_fn):
+    """The candidate lists are built again only when the particles' displacement since
+    the last build could pass the bound; every step in between filters them, and that
+    step's neighbour list must be the reference's sweep against fresh bins."""
+    ps, solver, _ = make_pair(scene_fn(), fp64=False)
+    solver.initialize()
+    solver.list_stats(reset=True)
+    solver.step_many(7)
+    stats = solver.list_stats()
+    solver.run_stage(abi.STAGE_SORT)
+    after = solver.list_stats()
+    assert stats["steps"] == 7 and stats["builds"] < stats["steps"], stats
+    assert after["builds"] == stats["builds"], "the checked step should filter, not build"
+    A = pair_set(*solver.pairs(0), ps.pid.to_numpy())
+    assert A == _oracle_pairs_at(ps, solver)
+    assert solver.error_word() & ~abi.EW_HASHED_GRID == 0
+
+
+def test_large_move_forces_a_build(cuda):
+    """Positions written from the host are measured against the build: a move past the
+    bound makes the next step build the lists again, and its pairs stay exact."""
+    ps, solver, _ = make_pair(small_scene(5000), fp64=False)
+    solver.initialize()
+    solver.list_stats(reset=True)
+    x = ps.x.to_numpy()
+    rng = np.random.default_rng(11)
+    x[:, 0] += np.float32(0.2 * ps.support_radius)
+    x += rng.uniform(-0.02, 0.02, x.shape).astype(np.float32) * np.float32(ps.support_radius)
+    ps.x.from_numpy(x.astype(np.float32))
+    solver.run_stage(abi.STAGE_SORT)
+    st = solver.list_stats()
+    assert st["builds"] == 1 and st["steps"] == 1, st
+    A = pair_set(*solver.pairs(0), ps.pid.to_numpy())
+    assert A == _oracle_pairs_at(ps, solver)
 
 
 @pytest.mark.parametrize("scene_fn", [lambda: small_scene(), axi_fluid_scene, quarter_scene],
@@ -268,9 +315,10 @@ def test_hashed_fallback_table(cuda):
 
 
 def test_neighbour_overflow_path(cuda):
-    """Particles four times denser than the lattice the list was sized for: the counts
-    exceed the list capacity and the extra pairs come from the direct search; fields
-    still match the oracle."""
+    """Particles four times denser than the lattice the lists were sized for: the
+    candidates exceed their list (the neighbours then come from a direct search of the
+    coarse table) and the neighbours exceed theirs (the extra pairs go to the overflow
+    pool); fields still match the oracle."""
     sc = small_scene(3000)
     ps, solver, orc = make_pair(sc, fp64=False, perturbed=False)
     x = ps.x.to_numpy()
@@ -283,7 +331,8 @@ def test_neighbour_overflow_path(cuda):
     orc.set_state(st, solver.dt[None])
     solver.initialize()
     orc.stage(abi.STAGE_SORT)
-    assert solver.error_word() & abi.EW_NBR_OVERFLOW
+    ew = solver.error_word()
+    assert ew & abi.EW_NBR_OVERFLOW and ew & abi.EW_CAND_OVERFLOW and not ew & abi.EW_NBR_DROPPED
     solver.run_stage(abi.STAGE_LAM)
     orc.stage(abi.STAGE_LAM)
     e = field_errors(gpu_fields(ps), oracle_fields(orc), ["lam", "L_sym", "lam_grad"])

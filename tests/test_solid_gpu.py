@@ -198,6 +198,25 @@ def test_solid_shift_pairs_from_lists(cuda, deck):
     assert A == B
 
 
+@pytest.mark.parametrize("deck", [bar3d_deck, strip_ps_deck], ids=["bar3d", "plane_strain"])
+def test_solid_lists_between_builds_match_oracle(cuda, deck):
+    """Steps that filter the candidate lists instead of building them give the
+    reference's neighbour pairs (the oracle sorts the same state afresh)."""
+    ps, solver, _, _ = make_solid(deck())
+    solver.initialize()
+    solver.list_stats(reset=True)
+    solver.step_many(6)
+    stats = solver.list_stats()
+    solver.run_stage(abi.STAGE_SORT)
+    assert solver.list_stats()["builds"] == stats["builds"] < stats["steps"] == 6, stats
+    orc = Oracle(build_params(ps), ps.particle_max_num, fp64=False)
+    orc.set_state(state_from_sets(ps.state_numpy()), solver.dt[None])
+    orc.stage(abi.STAGE_SORT)
+    B = pair_set(*orc.pairs(), orc.get_state()["pid"])
+    A = pair_set(*solver.pairs(0), ps.pid.to_numpy())
+    assert A == B
+
+
 @pytest.mark.parametrize("deck", [axi_deck, bar3d_deck], ids=["axi_dogbone", "bar3d"])
 def test_solid_multistep_tracks_fp64(cuda, deck):
     ps, solver, o64, o32 = make_solid(deck())
