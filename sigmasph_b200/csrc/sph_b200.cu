@@ -43,6 +43,7 @@ struct SphHandle {
     int* vl_cnt = nullptr;
     int* ovf = nullptr;
     int* ovf_off = nullptr;
+    unsigned* xbits = nullptr;
     int4* fcell = nullptr;
     float4* xb = nullptr;
     bool force_pending = true;      // the next step builds the candidate lists
@@ -127,6 +128,7 @@ Ptr make_ptr(SphHandle* h) {
     P.vl_cnt = h->vl_cnt;
     P.ovf = h->ovf;
     P.ovf_off = h->ovf_off;
+    P.xbits = h->xbits;
     P.fcell = h->fcell;
     P.xb = h->xb;
     P.sc = h->sc;
@@ -195,6 +197,7 @@ int fluid_substep_and_boundary(SphHandle* h, cudaStream_t st) {
     LAUNCH("k_dt", k_dt<<<1, 32, 0, st>>>(c, P));
     LAUNCH("k_advect", k_advect<<<nb, kBlock, 0, st>>>(c, P));
     if (h->p.pst_enabled) {
+        LAUNCH("k_crossed", k_crossed<<<nb, kBlock, 0, st>>>(c, P));
         LAUNCH("k_pst", k_pst<<<nb, kBlock, 0, st>>>(c, P));
         LAUNCH("k_finish", k_finish<<<nb, kBlock, 0, st>>>(c, P, 3));
     } else {
@@ -227,7 +230,7 @@ void free_all(SphHandle* h) {
     h->prof_pool.clear();
     if (h->cap_stream) cudaStreamDestroy(h->cap_stream);
     void* ptrs[] = {h->cell, h->cell_tmp, h->key, h->rank, h->perm, h->hist, h->start, h->bsum,
-                    h->bbox, h->layout, h->nbr, h->nbr_cnt, h->vl, h->vl_cnt, h->ovf, h->ovf_off, h->fcell, h->xb,
+                    h->bbox, h->layout, h->nbr, h->nbr_cnt, h->vl, h->vl_cnt, h->ovf, h->ovf_off, h->xbits, h->fcell, h->xb,
                     h->sc, h->ac};
     for (void* q : ptrs) if (q) cudaFree(q);
     if (h->pinned) cudaFreeHost(h->pinned);
@@ -341,6 +344,7 @@ int sph_create(const SphParams* p, int64_t n_max, SphHandle** out) {
         (r = dalloc(&h->nbr_cnt, N)) || (r = dalloc(&h->sc, 1)) || (r = dalloc(&h->ac, 1)) ||
         (r = dalloc(&h->vl, N * (size_t)Kv)) || (r = dalloc(&h->vl_cnt, N)) ||
         (r = dalloc(&h->ovf, ovf_cap)) || (r = dalloc(&h->ovf_off, N)) ||
+        (r = dalloc(&h->xbits, N / 32 + 1)) ||
         (r = dalloc(&h->fcell, N)) || (r = dalloc(&h->xb, N)) ||
         cudaMallocHost((void**)&h->pinned, sizeof(SphScalars)) != cudaSuccess) {
         if (!r) r = SPH_ERR_NOMEM;
@@ -502,6 +506,7 @@ int sph_run_stage(SphHandle* h, int stage, void* stream) {
         case SPH_STAGE_ADVECT: k_advect<<<nb, kBlock, 0, st>>>(c, P); break;
         case SPH_STAGE_PST:
             if (h->p.pst_enabled) {
+                k_crossed<<<nb, kBlock, 0, st>>>(c, P);
                 k_pst<<<nb, kBlock, 0, st>>>(c, P);
                 k_finish<<<nb, kBlock, 0, st>>>(c, P, 1);
             }
@@ -580,7 +585,8 @@ __global__ void __launch_bounds__(kBlock) k_disp_since_build(Cst c, Ptr P, unsig
 // Pair export: one thread per particle counts (off == nullptr, counts to cnt_out) or
 // writes its pairs at off[i].  kShift 0: the reference's sweep from the current positions
 // against this step's start bins, searched in the coarse table for displacement *dbits;
-// kShift 1: the pairs the shift pass evaluates (for_each_pst_neighbour).
+// kShift 1: the pairs the shift pass evaluates (for_each_pst_neighbour); kShift 2: this
+// step's neighbour list as the pair passes read it (for_each_neighbour).
 template <int kShift>
 __global__ void k_pairs_export(Cst c, Ptr P, const unsigned int* dbits, const int* off, int* cnt_out,
                                int* out_i, int* out_j, int* out_m) {
@@ -593,7 +599,9 @@ __global__ void k_pairs_export(Cst c, Ptr P, const unsigned int* dbits, const in
         if (off) { out_i[base + cnt] = i; out_j[base + cnt] = j; out_m[base + cnt] = mir; }
         ++cnt;
     };
-    if (kShift) {
+    if (kShift == 2) {
+        for_each_neighbour(c, P, i, emit);
+    } else if (kShift == 1) {
         for_each_pst_neighbour(c, P, i, xi, emit);
     } else if (!(isnan(xi.x) || isnan(xi.y) || isnan(xi.z))) {
         stale_search(c, P, i, xi, cell_of(xi.x, c.h), cell_of(xi.y, c.h), cell_of(xi.z, c.h),
@@ -616,6 +624,7 @@ int export_pairs(SphHandle* h, int32_t* pi, int32_t* pj, int32_t* mir, int64_t c
     std::vector<int> cnt(n);
     cudaMemsetAsync(dbits, 0, sizeof(unsigned int), st);
     k_disp_since_build<<<blocks_for(n), kBlock, 0, st>>>(h->c, P, dbits);
+    if (kShift == 1) k_crossed<<<blocks_for(n), kBlock, 0, st>>>(h->c, P);
     k_pairs_export<kShift><<<blocks_for(n), kBlock, 0, st>>>(h->c, P, dbits, nullptr, dcnt, nullptr, nullptr,
                                                              nullptr);
     cudaMemcpyAsync(cnt.data(), dcnt, n * sizeof(int), cudaMemcpyDeviceToHost, st);
@@ -656,22 +665,7 @@ extern "C" int sph_pairs(SphHandle* h, int mode, int32_t* pi, int32_t* pj, int32
     *count = 0;
     if (n == 0) return SPH_OK;
     if (mode == 1) return export_pairs<0>(h, pi, pj, mir, cap, count, st);
-    std::vector<int> cnt(n);
-    CK(cudaMemcpyAsync(cnt.data(), h->nbr_cnt, n * sizeof(int), cudaMemcpyDeviceToHost, st));
-    std::vector<int> lst((size_t)n * h->c.K);
-    CK(cudaMemcpyAsync(lst.data(), h->nbr, lst.size() * sizeof(int), cudaMemcpyDeviceToHost, st));
-    CK(cudaStreamSynchronize(st));
-    int64_t k = 0;
-    for (int i = 0; i < n; ++i) {
-        if (cnt[i] > h->c.K) return SPH_ERR_NEIGHBOUR_CAP;
-        for (int t = 0; t < cnt[i]; ++t) {
-            int e = lst[(size_t)t * n + i];
-            if (k < cap && pi) { pi[k] = i; pj[k] = e & kIdxMask; mir[k] = (int)((unsigned)e >> kMirShift); }
-            ++k;
-        }
-    }
-    *count = k;
-    return SPH_OK;
+    return export_pairs<2>(h, pi, pj, mir, cap, count, st);
 }
 
 extern "C" int sph_shift_pairs(SphHandle* h, float disp_bound, int32_t* pi, int32_t* pj, int32_t* mir,

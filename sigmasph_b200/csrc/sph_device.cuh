@@ -18,9 +18,8 @@ constexpr int kBlock = 256;          // threads per block of the particle-parall
 // default budget) run three blocks per SM: 80 registers and a few spills measured 6%
 // faster per step than two blocks without spills.
 #define SPH_PAIR_BOUNDS_OCC3 __launch_bounds__(kBlock, 3)
-constexpr int kMirShift = 30;        // neighbour entry = j | rim << 29 | mirror code << 30
-constexpr int kRimBit = 1 << 29;     // the pair may leave the support before the shift pass
-constexpr int kIdxMask = kRimBit - 1;
+constexpr int kMirShift = 30;        // neighbour entry = j | mirror code << 30
+constexpr int kIdxMask = (1 << 29) - 1;
 
 // Cell layout of the current rebuild, written by k_layout on the device.
 struct GridLayout {
@@ -135,6 +134,7 @@ struct Ptr {
     GridLayout* layout;
     int* nbr;            // [K][n] this step's neighbours, k-major
     int* nbr_cnt;        // [n] true count; entries past K sit in the overflow pool
+    unsigned* xbits;     // [n / 32] bit per particle: its cell changed since the step's start
     int* ovf;            // [ovf_cap] overflow pool, one run per overflowing particle
     int* ovf_off;        // [n] start of the particle's run
     int* vl;             // [Kv][n] candidates within h + skin at the last build, k-major

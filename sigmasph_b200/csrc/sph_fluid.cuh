@@ -363,8 +363,9 @@ __global__ void __launch_bounds__(kBlock) k_advect(Cst c, Ptr P) {
 // the bins of this step's start (particle_system.py:1377-1411).  While the particles'
 // displacement since the lists' build -- at the step's start plus this step's advect and
 // grips -- is within the bound, from the candidate lists: every entry tested for
-// distance at the live positions, all but the deep ones also for j's step-start cell
-// against i's live cell.  Otherwise (or past the list's capacity) the stale-bin search.
+// distance at the live positions, the edge entries also for j's step-start cell (its
+// current cell unless its bit in xbits says it moved) against i's live cell.  Otherwise
+// (or when the candidate list overflowed) the stale-bin search.
 template <class F>
 __device__ __forceinline__ void for_each_pst_neighbour(const Cst& c, const Ptr& P, int i, F3 xi, F&& f) {
     if (isnan(xi.x) || isnan(xi.y) || isnan(xi.z)) return;
@@ -372,21 +373,36 @@ __device__ __forceinline__ void for_each_pst_neighbour(const Cst& c, const Ptr& 
                        __uint_as_float(P.ac->max_grip_disp_bits);
     const int lx = cell_of(xi.x, c.h), ly = cell_of(xi.y, c.h), lz = cell_of(xi.z, c.h);
     const int vc = __ldg(P.vl_cnt + i);
-    if (!(dtot <= c.dlim) || vc > c.Kv) {
+    if (!(dtot <= c.dlim) || vl_overflow(c, vc)) {
         stale_search(c, P, i, xi, lx, ly, lz, dtot, f);
         return;
     }
     const float4* __restrict__ pos = as4c(P.cur.pos);
     const bool py = xi.y < c.h, pz = xi.z < c.h;
-    list_entries(P.vl + i, (size_t)c.n, vc, [&](int e) {
+    const int d = vl_deep(vc);
+    const size_t n = (size_t)c.n;
+    const int* __restrict__ vl = P.vl + i;
+    const int* __restrict__ nb = P.nbr + i;
+    // the deep rows of the neighbour list, then the edge rows of the candidate list
+    split_entries(d + vl_edge(vc), [&](int k) { return k < d ? __ldg(nb + (size_t)k * n) : __ldg(vl + (size_t)(k - d) * n); },
+                  [&](int k, int e) {
         const int j = e & kIdxMask, mir = (int)((unsigned)e >> kMirShift);
         if (mir && (((mir & 1) && !py) || ((mir & 2) && !pz))) return;
-        F3 xj = f3(__ldg(pos + j));
+        const float4 pj = __ldg(pos + j);
+        F3 xj = f3(pj);
         if (mir) xj = mirror3(mir, xj);
         if (!(dist2_rn(xi, xj) < c.d2_lt)) return;
-        if (e & kRimBit) {
-            const int4 fj = __ldg(P.fcell + j);
-            if (!sweep_cell_ok(mir, fj.x, fj.y, fj.z, lx, ly, lz)) return;
+        if (k >= d) {
+            int jx, jy, jz;
+            if ((__ldg(P.xbits + (j >> 5)) >> (j & 31)) & 1u) {
+                const int4 fj = __ldg(P.fcell + j);
+                jx = fj.x; jy = fj.y; jz = fj.z;
+            } else {
+                jx = cell_of_fast(pj.x, c.h, c.inv_h);
+                jy = cell_of_fast(pj.y, c.h, c.inv_h);
+                jz = cell_of_fast(pj.z, c.h, c.inv_h);
+            }
+            if (!sweep_cell_ok(mir, jx, jy, jz, lx, ly, lz)) return;
         }
         f(j, mir);
     });

@@ -398,11 +398,21 @@ __device__ __forceinline__ bool sweep_cell_ok(int mir, int jx, int jy, int jz, i
     return true;
 }
 
+// Candidate counts, packed: deep entries in the low half, edge entries in the high half,
+// each saturated at 0xffff.  The deep entries sit in rows 0 .. deep-1 of the neighbour
+// list (untouched between builds; every step appends its accepted edge entries after
+// them), the edge entries in rows 0 .. edge-1 of the candidate list.  More than Kv in all
+// means the candidates overflowed and neither is used.
+__device__ __forceinline__ int vl_deep(int vc) { return vc & 0xffff; }
+__device__ __forceinline__ int vl_edge(int vc) { return (int)((unsigned)vc >> 16); }
+__device__ __forceinline__ bool vl_overflow(const Cst& c, int vc) { return vl_deep(vc) + vl_edge(vc) > c.Kv; }
+
 // Builds every particle's candidate list at the build's positions: the coarse 27-cell
 // sweep out to h + skin, and the mirror sweeps over coarse rows -1 and 0 (a particle
-// that crosses the plane later is binned in row 0 or -1 of size h).  Entries within
-// h - skin are marked deep: under the bound they stay within h and their cells stay
-// adjacent, so the per-step filter takes them without a test.
+// that crosses the plane later is binned in row 0 or -1 of size h).  Real entries within
+// h - skin are deep: under the bound they stay within h and their cells stay adjacent, so
+// every step takes them as they are (they go straight to the neighbour list).  The others
+// (edge entries) are tested every step.
 __global__ void __launch_bounds__(kBlock) k_vlist_build(Cst c, Ptr P) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= c.n || !P.ac->rebuild) return;
@@ -410,17 +420,18 @@ __global__ void __launch_bounds__(kBlock) k_vlist_build(Cst c, Ptr P) {
     if (ci.w < 0) { P.vl_cnt[i] = 0; return; }
     const GridLayout L = *P.layout;
     const F3 xi = f3(reinterpret_cast<const float4*>(P.cur.pos)[i]);
-    int cnt = 0;
+    int nd = 0, ne = 0;
     const int n = c.n, Kv = c.Kv;
     int* __restrict__ vl = P.vl;
+    int* __restrict__ nb = P.nbr;
     sweep_coarse(c, P, L, i, xi, ci.x, ci.y, ci.z, 1, -1, 0, c.d2_skin, c.h + c.skin,
                  [&](int j, int mir, float4, float d2) {
-        const int e = j | ((mir == 0 && d2 < c.d2_deep) ? 0 : kRimBit) | (mir << kMirShift);
-        if (cnt < Kv) vl[(size_t)cnt * n + i] = e;
-        ++cnt;
+        const bool deep = mir == 0 && d2 < c.d2_deep;
+        if (nd + ne < Kv) (deep ? nb + (size_t)nd * n : vl + (size_t)ne * n)[i] = j | (mir << kMirShift);
+        if (deep) ++nd; else ++ne;
     });
-    if (cnt > Kv) atomicOr(&P.sc->err, SPH_EW_CAND_OVERFLOW);
-    P.vl_cnt[i] = cnt;
+    if (nd + ne > Kv) atomicOr(&P.sc->err, SPH_EW_CAND_OVERFLOW);
+    P.vl_cnt[i] = min(nd, 0xffff) | (min(ne, 0xffff) << 16);
 }
 
 // The m stored entries of one particle's k-major list, with the next two entries in
@@ -443,6 +454,21 @@ __device__ __forceinline__ void list_pairs(const int* __restrict__ nb, size_t n,
     list_entries(nb, n, m, [&](int e) { f(e & kIdxMask, (int)((unsigned)e >> kMirShift)); });
 }
 
+// Entries 0 .. m-1 of a list made of pieces, with the same two-entry prefetch: at(k)
+// loads entry k; f(k, entry).
+template <class At, class F>
+__device__ __forceinline__ void split_entries(int m, At&& at, F&& f) {
+    int e0 = m > 0 ? at(0) : 0;
+    int e1 = m > 1 ? at(1) : 0;
+#pragma unroll 2
+    for (int k = 0; k < m; ++k) {
+        const int e = e0;
+        e0 = e1;
+        if (k + 2 < m) e1 = at(k + 2);
+        f(k, e);
+    }
+}
+
 // The reference's sweep against the bins of this step's start (particle_system.py:
 // 1348-1490) for query point xq in cell q of size h, without the candidate lists: the
 // coarse table of the last build searched wide enough for displacement D since it, each
@@ -457,7 +483,7 @@ __device__ __forceinline__ void stale_search(const Cst& c, const Ptr& P, int i, 
     // size h at the plane (y in [0, h)) lies in coarse rows floor(-D / hc) .. w - 1
     const float wf = ceilf((c.h + 2.0f * D) / c.hc);
     const int w = wf <= 8.0f ? max((int)wf, 1) : 8;
-    if (!(wf <= 8.0f)) atomicOr(&P.sc->err, SPH_EW_NBR_OVERFLOW);
+    if (!(wf <= 8.0f)) atomicOr(&P.sc->err, SPH_EW_NBR_DROPPED);
     const float rf = ceilf(D / c.hc);
     const int rlo = -(rf <= 8.0f ? max((int)rf, 1) : 8);
     sweep_coarse(c, P, L, i, xq, bi.x, bi.y, bi.z, w, rlo, w - 1, c.d2_lt, c.h,
@@ -467,25 +493,28 @@ __device__ __forceinline__ void stale_search(const Cst& c, const Ptr& P, int i, 
     });
 }
 
-// The neighbours of i at this step's start (the reference's sweep against fresh bins):
-// the candidate list filtered -- deep entries as they are, the others by distance and
-// cell at the current positions -- or, past the list's capacity, the stale-bin search.
-template <class F>
-__device__ __forceinline__ void for_each_start_neighbour(const Cst& c, const Ptr& P, int i, F&& f) {
+// This step's neighbour list (every step; the pair passes read it): after the deep rows,
+// the edge entries that pass the reference's own tests at the step-start positions --
+// distance, and cells of size h (from the positions, which are the bins).  A particle
+// whose candidates overflowed gets all its pairs from the stale-bin search instead; past
+// K of those, the rest go in order to a run of the overflow pool (the search runs a
+// second time to write it).
+__global__ void __launch_bounds__(kBlock) k_nbr_filter(Cst c, Ptr P) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= c.n) return;
     const int4 fi = P.fcell[i];
-    if (fi.w < 0) return;
-    const float4* __restrict__ pos = reinterpret_cast<const float4*>(P.cur.pos);
-    const F3 xi = f3(pos[i]);
+    int cnt = 0;
+    const int n = c.n, K = c.K;
+    int* __restrict__ nb = P.nbr;
     const int vc = __ldg(P.vl_cnt + i);
-    if (vc > c.Kv) {
-        stale_search(c, P, i, xi, fi.x, fi.y, fi.z, __uint_as_float(P.ac->d_start_bits), f);
-        return;
-    }
-    const bool py = xi.y < c.h, pz = xi.z < c.h;
-    list_entries(P.vl + i, (size_t)c.n, vc, [&](int e) {
-        const int j = e & kIdxMask, mir = (int)((unsigned)e >> kMirShift);
-        if (mir && (((mir & 1) && !py) || ((mir & 2) && !pz))) return;
-        if (e & kRimBit) {
+    const float4* __restrict__ pos = reinterpret_cast<const float4*>(P.cur.pos);
+    if (fi.w >= 0 && !vl_overflow(c, vc)) {
+        const F3 xi = f3(pos[i]);
+        const bool py = xi.y < c.h, pz = xi.z < c.h;
+        cnt = vl_deep(vc);
+        list_entries(P.vl + i, (size_t)n, vl_edge(vc), [&](int e) {
+            const int j = e & kIdxMask, mir = (int)((unsigned)e >> kMirShift);
+            if (mir && (((mir & 1) && !py) || ((mir & 2) && !pz))) return;
             const float4 pj = __ldg(pos + j);
             F3 xj = f3(pj);
             if (mir) xj = mirror3(mir, xj);
@@ -493,40 +522,32 @@ __device__ __forceinline__ void for_each_start_neighbour(const Cst& c, const Ptr
             if (!sweep_cell_ok(mir, cell_of_fast(pj.x, c.h, c.inv_h), cell_of_fast(pj.y, c.h, c.inv_h),
                                cell_of_fast(pj.z, c.h, c.inv_h), fi.x, fi.y, fi.z))
                 return;
-        }
-        f(j, mir);
-    });
-}
-
-// This step's neighbour list from the candidate lists (every step; the pair passes read
-// it).  It holds as many entries as the candidate list, so it overflows only when the
-// candidate list did and more than K pairs lie within h: the pairs past K then go, in
-// order, to a run of the overflow pool (the enumeration runs a second time to write it).
-__global__ void __launch_bounds__(kBlock) k_nbr_filter(Cst c, Ptr P) {
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= c.n) return;
-    int cnt = 0;
-    const int n = c.n, K = c.K;
-    int* __restrict__ nb = P.nbr;
-    for_each_start_neighbour(c, P, i, [&](int j, int mir) {
-        if (cnt < K) nb[(size_t)cnt * n + i] = j | (mir << kMirShift);
-        ++cnt;
-    });
-    if (cnt > K) {
-        atomicOr(&P.sc->err, SPH_EW_NBR_OVERFLOW);
-        const unsigned extra = (unsigned)(cnt - K);
-        const unsigned base = atomicAdd(&P.ac->ovf_used, extra);
-        if (base <= c.ovf_cap && extra <= c.ovf_cap - base) {
-            P.ovf_off[i] = (int)base;
-            int* __restrict__ run = P.ovf + base;
-            int k = 0;
-            for_each_start_neighbour(c, P, i, [&](int j, int mir) {
-                if (k >= K) run[k - K] = j | (mir << kMirShift);
-                ++k;
-            });
-        } else {
-            atomicOr(&P.sc->err, SPH_EW_NBR_DROPPED);
-            cnt = K;
+            nb[(size_t)cnt * n + i] = e;   // deep + edge <= Kv = K
+            ++cnt;
+        });
+    } else if (fi.w >= 0) {
+        const F3 xi = f3(pos[i]);
+        const float D = __uint_as_float(P.ac->d_start_bits);
+        stale_search(c, P, i, xi, fi.x, fi.y, fi.z, D, [&](int j, int mir) {
+            if (cnt < K) nb[(size_t)cnt * n + i] = j | (mir << kMirShift);
+            ++cnt;
+        });
+        if (cnt > K) {
+            atomicOr(&P.sc->err, SPH_EW_NBR_OVERFLOW);
+            const unsigned extra = (unsigned)(cnt - K);
+            const unsigned base = atomicAdd(&P.ac->ovf_used, extra);
+            if (base <= c.ovf_cap && extra <= c.ovf_cap - base) {
+                P.ovf_off[i] = (int)base;
+                int* __restrict__ run = P.ovf + base;
+                int k = 0;
+                stale_search(c, P, i, xi, fi.x, fi.y, fi.z, D, [&](int j, int mir) {
+                    if (k >= K) run[k - K] = j | (mir << kMirShift);
+                    ++k;
+                });
+            } else {
+                atomicOr(&P.sc->err, SPH_EW_NBR_DROPPED);
+                cnt = K;
+            }
         }
     }
     P.nbr_cnt[i] = cnt;
@@ -538,6 +559,22 @@ __device__ __forceinline__ void for_each_neighbour(const Cst& c, const Ptr& P, i
     const int cnt = __ldg(P.nbr_cnt + i);
     list_pairs(P.nbr + i, (size_t)c.n, cnt < c.K ? cnt : c.K, f);
     if (cnt > c.K) list_pairs(P.ovf + __ldg(P.ovf_off + i), 1, cnt - c.K, f);
+}
+
+// One bit per particle: its cell of size h changed since this step's start (the shift
+// pass needs a moved particle's step-start cell; the others' is their current cell).
+// NaN positions count as moved.
+__global__ void __launch_bounds__(kBlock) k_crossed(Cst c, Ptr P) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    bool x = false;
+    if (i < c.n) {
+        const float4 p = reinterpret_cast<const float4*>(P.cur.pos)[i];
+        const int4 f = P.fcell[i];
+        x = isnan(p.x) || isnan(p.y) || isnan(p.z) || cell_of_fast(p.x, c.h, c.inv_h) != f.x ||
+            cell_of_fast(p.y, c.h, c.inv_h) != f.y || cell_of_fast(p.z, c.h, c.inv_h) != f.z;
+    }
+    const unsigned b = __ballot_sync(0xffffffffu, x);
+    if ((threadIdx.x & 31) == 0 && i < c.n) P.xbits[i >> 5] = b;
 }
 
 }  // namespace sph

@@ -1380,6 +1380,7 @@ inline int solid_substep_launch(const Cst& c, const Ptr& P, int n, cudaStream_t 
         k_constraints<<<nb, bs, 0, st>>>(c, P); mark("k_constraints");
     }
     if (in(SPH_STAGE_PST) && c.p.pst_enabled) {
+        k_crossed<<<nb, bs, 0, st>>>(c, P); mark("k_crossed");
         k_pst<<<nb, bs, 0, st>>>(c, P); mark("k_pst");
         k_finish<<<nb, bs, 0, st>>>(c, P, last_stage >= SPH_STAGE_BOUNDARY ? 3 : 1); mark("k_finish");
     } else if (in(SPH_STAGE_BOUNDARY)) {
