@@ -17,9 +17,10 @@
  *  - The caller owns every per-particle buffer (PyTorch tensors in the Python host
  *    layer).  The library allocates only scratch: sort keys, permutation, cell table,
  *    neighbour lists, device scalars.
- *  - The persistent particle state lives in TWO buffer sets (A and B).  Every neighbour
- *    rebuild gathers the state from the current set into the other one in the new
- *    order and flips the parity; sph_parity() says which set is current.
+ *  - The persistent particle state lives in buffer set A; set B is the reorder's
+ *    scratch.  A build of the neighbour candidates gathers the state into B in the new
+ *    order and copies it back to A.  sph_parity() says which set is current (always A,
+ *    0, since the copy back; kept so that a host need not assume it).
  */
 #ifndef SPH_B200_H
 #define SPH_B200_H

@@ -28,7 +28,6 @@ struct SphHandle {
     int device = 0;
     // scratch
     int4* cell = nullptr;
-    int4* cell_tmp = nullptr;
     int* key = nullptr;
     int* rank = nullptr;
     int* perm = nullptr;
@@ -51,7 +50,7 @@ struct SphHandle {
     DevAccum* ac = nullptr;
     SphScalars* pinned = nullptr;   // page-locked staging of the scalar copies
     SolidScratch solid;
-    // CUDA graph of two consecutive steps (parity returns to where it started)
+    // CUDA graph of two consecutive steps
     cudaGraphExec_t graph2 = nullptr;
     cudaStream_t cap_stream = nullptr;
     // per-kernel event profile of eager launches
@@ -113,7 +112,6 @@ Ptr make_ptr(SphHandle* h) {
     P.gradv = h->buf.gradv;
     P.aux = reinterpret_cast<float4*>(h->buf.aux);
     P.cell = h->cell;
-    P.cell_tmp = h->cell_tmp;
     P.key = h->key;
     P.rank = h->rank;
     P.perm = h->perm;
@@ -179,8 +177,7 @@ int rebuild(SphHandle* h, cudaStream_t st) {
     LAUNCH("k_scatter", k_scatter<<<nb, kBlock, 0, st>>>(c, P));
     LAUNCH("k_stabilise", k_stabilise<<<nb, kBlock, 0, st>>>(c, P));
     LAUNCH("k_gather", k_gather<<<nb, kBlock, 0, st>>>(c, P));
-    h->parity ^= 1;
-    P = make_ptr(h);
+    LAUNCH("k_gather_back", k_gather_back<<<nb, kBlock, 0, st>>>(c, P));
     LAUNCH("k_vlist_build", k_vlist_build<<<nb, kBlock, 0, st>>>(c, P));
     LAUNCH("k_nbr_filter", k_nbr_filter<<<nb, kBlock, 0, st>>>(c, P));
     return SPH_OK;
@@ -229,7 +226,7 @@ void free_all(SphHandle* h) {
     for (cudaEvent_t e : h->prof_pool) cudaEventDestroy(e);
     h->prof_pool.clear();
     if (h->cap_stream) cudaStreamDestroy(h->cap_stream);
-    void* ptrs[] = {h->cell, h->cell_tmp, h->key, h->rank, h->perm, h->hist, h->start, h->bsum,
+    void* ptrs[] = {h->cell, h->key, h->rank, h->perm, h->hist, h->start, h->bsum,
                     h->bbox, h->layout, h->nbr, h->nbr_cnt, h->vl, h->vl_cnt, h->ovf, h->ovf_off, h->xbits, h->fcell, h->xb,
                     h->sc, h->ac};
     for (void* q : ptrs) if (q) cudaFree(q);
@@ -336,7 +333,7 @@ int sph_create(const SphParams* p, int64_t n_max, SphHandle** out) {
     int r = SPH_OK;
     const size_t N = (size_t)std::max<int64_t>(n_max, 1);
     const size_t tiles = (size_t)((mcap + 1 + kScanTile - 1) / kScanTile) + 1;
-    if ((r = dalloc(&h->cell, N)) || (r = dalloc(&h->cell_tmp, N)) || (r = dalloc(&h->key, N)) ||
+    if ((r = dalloc(&h->cell, N)) || (r = dalloc(&h->key, N)) ||
         (r = dalloc(&h->rank, N)) || (r = dalloc(&h->perm, N)) ||
         (r = dalloc(&h->hist, (size_t)mcap + 2)) || (r = dalloc(&h->start, (size_t)mcap + 2)) ||
         (r = dalloc(&h->bsum, tiles)) || (r = dalloc(&h->bbox, 8)) ||

@@ -123,7 +123,7 @@ struct Ptr {
                          // (w = -1 off-grid)
     int4* fcell;         // cell of size h at this step's start: x, y, z, 0 (w = -1 off-grid)
     float4* xb;          // positions at the last build
-    int4* cell_tmp;      // coarse cell of the pre-sort order
+
     int* key;            // bucket of each pre-sort particle
     int* rank;           // slot within its bucket (arbitrary before the stabilise pass)
     int* perm;           // new index -> old index

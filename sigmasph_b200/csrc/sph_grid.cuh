@@ -27,9 +27,9 @@ __global__ void k_grid_reset(Ptr P) {
 }
 
 // update_grid_id's first half (particle_system.py:1224-1234, :1304-1316): NaN
-// quarantine and the off-grid tally, the coarse cell of every particle and the box of
-// occupied coarse cells (used if this step builds), and how far the particles moved since
-// the last build.
+// quarantine and the off-grid tally, every particle's cell of size h (the bins of this
+// step), the box of occupied coarse cells (used if this step builds), and how far the
+// particles moved since the last build.
 __global__ void __launch_bounds__(kBlock) k_cells(Cst c, Ptr P) {
     int i = blockIdx.x * blockDim.x + threadIdx.x;
     int mn[3] = {0x7fffffff, 0x7fffffff, 0x7fffffff};
@@ -40,13 +40,12 @@ __global__ void __launch_bounds__(kBlock) k_cells(Cst c, Ptr P) {
     if (i < c.n) {
         float4 p = reinterpret_cast<const float4*>(P.cur.pos)[i];
         bool nan = isnan(p.x) || isnan(p.y) || isnan(p.z);
-        int4 cl;
+        int4 cl;   // coarse cell, for the box of a build
         cl.x = cell_of(p.x, c.hc);
         cl.y = cell_of(p.y, c.hc);
         cl.z = cell_of(p.z, c.hc);
-        cl.w = nan ? -1 : 0;
-        if (nan) { cl.x = cl.y = cl.z = 0; }
-        P.cell_tmp[i] = cl;
+        P.fcell[i] = nan ? make_int4(0, 0, 0, -1)
+                         : make_int4(cell_of(p.x, c.h), cell_of(p.y, c.h), cell_of(p.z, c.h), 0);
         if (nan) {
             offg = 1;
             offm = (double)P.cur.vel[4 * i + 3];
@@ -142,8 +141,10 @@ __global__ void __launch_bounds__(kBlock) k_keys(Cst c, Ptr P) {
     int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= c.n || !P.ac->rebuild) return;
     const GridLayout L = *P.layout;
-    int4 cl = P.cell_tmp[i];
-    int key = cl.w < 0 ? L.nbuckets : bucket_of(cl.x, cl.y, cl.z, L, c.mcap);
+    const float4 p = reinterpret_cast<const float4*>(P.cur.pos)[i];
+    const bool nan = isnan(p.x) || isnan(p.y) || isnan(p.z);
+    int key = nan ? L.nbuckets
+                  : bucket_of(cell_of(p.x, c.hc), cell_of(p.y, c.hc), cell_of(p.z, c.hc), L, c.mcap);
     P.key[i] = key;
     P.rank[i] = atomicAdd(&P.hist[key], 1);
 }
@@ -267,17 +268,9 @@ __global__ void __launch_bounds__(kBlock) k_stabilise(Cst c, Ptr P) {
     }
 }
 
-// Gathers every persistent field into the other buffer set: in the new order when this
-// step builds, else as they are (the two sets alternate every step either way).  Writes
-// the step-start cell of size h (the reference's bins) of every particle; a build also
-// records each particle's coarse cell and position.
-__global__ void __launch_bounds__(kBlock) k_gather(Cst c, Ptr P) {
-    int d = blockIdx.x * blockDim.x + threadIdx.x;
-    if (d >= c.n) return;
-    const bool build = P.ac->rebuild != 0;
-    const int s = build ? P.perm[d] : d;
-    const SphFieldSet& A = P.cur;
-    const SphFieldSet& B = P.nxt;
+// Copies every persistent field of particle s in set A to slot d of set B.
+__device__ __forceinline__ void copy_particle(const Cst& c, const SphFieldSet& A, int s, const SphFieldSet& B,
+                                              int d) {
     reinterpret_cast<float4*>(B.pos)[d] = __ldg(reinterpret_cast<const float4*>(A.pos) + s);
     reinterpret_cast<float4*>(B.vel)[d] = __ldg(reinterpret_cast<const float4*>(A.vel) + s);
     reinterpret_cast<float4*>(B.x0)[d] = __ldg(reinterpret_cast<const float4*>(A.x0) + s);
@@ -293,16 +286,33 @@ __global__ void __launch_bounds__(kBlock) k_gather(Cst c, Ptr P) {
         reinterpret_cast<float4*>(B.bcdisp)[d] = __ldg(reinterpret_cast<const float4*>(A.bcdisp) + s);
         reinterpret_cast<float4*>(B.acc)[d] = __ldg(reinterpret_cast<const float4*>(A.acc) + s);
     }
-    const float4 p = __ldg(reinterpret_cast<const float4*>(A.pos) + s);
+}
+
+// A build's reorder, first half: every persistent field into the other buffer set in
+// the new order, with each particle's coarse cell and bucket.  The particles stay in the
+// first set between builds, so steps that do not build move no field data.
+__global__ void __launch_bounds__(kBlock) k_gather(Cst c, Ptr P) {
+    const int d = blockIdx.x * blockDim.x + threadIdx.x;
+    if (d >= c.n || !P.ac->rebuild) return;
+    const int s = P.perm[d];
+    copy_particle(c, P.cur, s, P.nxt, d);
+    const float4 p = __ldg(reinterpret_cast<const float4*>(P.cur.pos) + s);
+    const bool nan = isnan(p.x) || isnan(p.y) || isnan(p.z);
+    P.cell[d] = nan ? make_int4(0, 0, 0, -1)
+                    : make_int4(cell_of(p.x, c.hc), cell_of(p.y, c.hc), cell_of(p.z, c.hc), P.key[s]);
+}
+
+// Second half: the reordered fields back into the first set, the cells of size h in the
+// new order, and the build positions.
+__global__ void __launch_bounds__(kBlock) k_gather_back(Cst c, Ptr P) {
+    const int d = blockIdx.x * blockDim.x + threadIdx.x;
+    if (d >= c.n || !P.ac->rebuild) return;
+    copy_particle(c, P.nxt, d, P.cur, d);
+    const float4 p = __ldg(reinterpret_cast<const float4*>(P.nxt.pos) + d);
     const bool nan = isnan(p.x) || isnan(p.y) || isnan(p.z);
     P.fcell[d] = nan ? make_int4(0, 0, 0, -1)
                      : make_int4(cell_of(p.x, c.h), cell_of(p.y, c.h), cell_of(p.z, c.h), 0);
-    if (build) {
-        int4 cl = P.cell_tmp[s];
-        cl.w = cl.w < 0 ? -1 : P.key[s];
-        P.cell[d] = cl;
-        P.xb[d] = p;
-    }
+    P.xb[d] = p;
 }
 
 // ------------------------------------------------------------------ neighbour enumeration

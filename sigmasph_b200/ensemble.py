@@ -277,7 +277,7 @@ class Ensemble:
         return choice
 
     def capture(self):
-        """One CUDA graph with two steps of every bucket (parity returns where it was)."""
+        """One CUDA graph with two steps of every bucket."""
         for b in self.buckets:                     # warm the per-handle state outside capture
             b.solver.step_many(2)
         torch.cuda.synchronize()
