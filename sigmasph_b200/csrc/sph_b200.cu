@@ -164,7 +164,7 @@ int rebuild(SphHandle* h, cudaStream_t st) {
     const Cst& c = h->c;
     prof_mark(h, "", st);
     LAUNCH("k_grid_reset", k_grid_reset<<<1, 32, 0, st>>>(P));
-    LAUNCH("k_cells", k_cells<<<nb, kBlock, 0, st>>>(c, P));
+    LAUNCH("k_cells", k_cells<<<std::min(nb, kCellsBlocks), kBlock, 0, st>>>(c, P));
     LAUNCH("k_layout", k_layout<<<1, 32, 0, st>>>(c, P));
     int zb = (int)std::min<int64_t>((c.mcap + 2 + kBlock - 1) / kBlock, 148 * 16);
     LAUNCH("k_zero_hist", k_zero_hist<<<zb, kBlock, 0, st>>>(c, P));
@@ -596,13 +596,14 @@ __global__ void k_pairs_export(Cst c, Ptr P, const unsigned int* dbits, const in
         if (off) { out_i[base + cnt] = i; out_j[base + cnt] = j; out_m[base + cnt] = mir; }
         ++cnt;
     };
+    auto emit3 = [&](int j, int mir, float4) { emit(j, mir); };
     if (kShift == 2) {
         for_each_neighbour(c, P, i, emit);
     } else if (kShift == 1) {
-        for_each_pst_neighbour(c, P, i, xi, emit);
+        for_each_pst_neighbour(c, P, i, xi, emit3);
     } else if (!(isnan(xi.x) || isnan(xi.y) || isnan(xi.z))) {
         stale_search(c, P, i, xi, cell_of(xi.x, c.h), cell_of(xi.y, c.h), cell_of(xi.z, c.h),
-                     __uint_as_float(*dbits), emit);
+                     __uint_as_float(*dbits), emit3);
     }
     if (!off) cnt_out[i] = cnt;
 }

@@ -31,8 +31,7 @@ __global__ void SPH_PAIR_BOUNDS_OCC4 k_lam(Cst c, Ptr P) {
     float4 pi = pos[i];
     F3 xi = f3(pi);
     float E[3][3] = {{0, 0, 0}, {0, 0, 0}, {0, 0, 0}};
-    for_each_neighbour(c, P, i, [&](int j, int mir) {
-        float4 pj = __ldg(pos + j);
+    auto pair = [&](int mir, float4 pj) {
         F3 xj = f3(pj);
         if (mir) xj = mirror3(mir, xj);
         F3 d = xj - xi;
@@ -46,7 +45,8 @@ __global__ void SPH_PAIR_BOUNDS_OCC4 k_lam(Cst c, Ptr P) {
             E[0][2] += Vj * (d.x * g.z); E[1][2] += Vj * (d.y * g.z);
             E[2][0] += Vj * (d.z * g.x); E[2][1] += Vj * (d.z * g.y); E[2][2] += Vj * (d.z * g.z);
         }
-    });
+    };
+    for_each_neighbour(c, P, i, [&](int j, int mir) { pair(mir, __ldg(pos + j)); });
     const float tol = c.p.l_eig_tol_lam;
     float L00, L11, L22, L01, L02, L12, lam;
     float4 evec = make_float4(0.f, 0.f, 0.f, 0.f);
@@ -365,7 +365,7 @@ __global__ void __launch_bounds__(kBlock) k_advect(Cst c, Ptr P) {
 // grips -- is within the bound, from the candidate lists: every entry tested for
 // distance at the live positions, the edge entries also for j's step-start cell (its
 // current cell unless its bit in xbits says it moved) against i's live cell.  Otherwise
-// (or when the candidate list overflowed) the stale-bin search.
+// (or when the candidate list overflowed) the stale-bin search.  f(j, mirror, pos_j).
 template <class F>
 __device__ __forceinline__ void for_each_pst_neighbour(const Cst& c, const Ptr& P, int i, F3 xi, F&& f) {
     if (isnan(xi.x) || isnan(xi.y) || isnan(xi.z)) return;
@@ -404,7 +404,7 @@ __device__ __forceinline__ void for_each_pst_neighbour(const Cst& c, const Ptr& 
             }
             if (!sweep_cell_ok(mir, jx, jy, jz, lx, ly, lz)) return;
         }
-        f(j, mir);
+        f(j, mir, pj);
     });
 }
 
@@ -426,8 +426,7 @@ __global__ void __launch_bounds__(kBlock, 5) k_pst(Cst c, Ptr P) {
     {
         const float Wd = c.W_dx0;
         const float inv_Wd = Wd > 0.0f ? 1.0f / Wd : 0.0f;
-        auto pair = [&](int j, int mir) {
-            float4 pj = __ldg(pos + j);
+        auto pair = [&](int j, int mir, float4 pj) {
             F3 xj = f3(pj);
             if (mir) xj = mirror3(mir, xj);
             F3 r = xi - xj;

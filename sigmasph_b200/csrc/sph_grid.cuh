@@ -29,55 +29,84 @@ __global__ void k_grid_reset(Ptr P) {
 // update_grid_id's first half (particle_system.py:1224-1234, :1304-1316): NaN
 // quarantine and the off-grid tally, every particle's cell of size h (the bins of this
 // step), the box of occupied coarse cells (used if this step builds), and how far the
-// particles moved since the last build.
+// particles moved since the last build.  Grid-stride over at most kCellsBlocks blocks,
+// reduced per block: one atomic per block and quantity (per-warp atomics on the box's six
+// words serialised at the L2).
+constexpr int kCellsBlocks = 148 * 8;
 __global__ void __launch_bounds__(kBlock) k_cells(Cst c, Ptr P) {
-    int i = blockIdx.x * blockDim.x + threadIdx.x;
     int mn[3] = {0x7fffffff, 0x7fffffff, 0x7fffffff};
     int mx[3] = {(int)0x80000000, (int)0x80000000, (int)0x80000000};
     int offg = 0;
     double offm = 0.0;
     float dst = 0.0f;
-    if (i < c.n) {
-        float4 p = reinterpret_cast<const float4*>(P.cur.pos)[i];
-        bool nan = isnan(p.x) || isnan(p.y) || isnan(p.z);
-        int4 cl;   // coarse cell, for the box of a build
-        cl.x = cell_of(p.x, c.hc);
-        cl.y = cell_of(p.y, c.hc);
-        cl.z = cell_of(p.z, c.hc);
+    const float4* __restrict__ pos = reinterpret_cast<const float4*>(P.cur.pos);
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < c.n; i += gridDim.x * blockDim.x) {
+        const float4 p = pos[i];
+        const bool nan = isnan(p.x) || isnan(p.y) || isnan(p.z);
         P.fcell[i] = nan ? make_int4(0, 0, 0, -1)
                          : make_int4(cell_of(p.x, c.h), cell_of(p.y, c.h), cell_of(p.z, c.h), 0);
         if (nan) {
-            offg = 1;
-            offm = (double)P.cur.vel[4 * i + 3];
+            offg += 1;
+            offm += (double)P.cur.vel[4 * i + 3];
         } else {
-            mn[0] = mx[0] = cl.x; mn[1] = mx[1] = cl.y; mn[2] = mx[2] = cl.z;
+            // coarse cell, for the box of a build
+            const int cx = cell_of(p.x, c.hc), cy = cell_of(p.y, c.hc), cz = cell_of(p.z, c.hc);
+            mn[0] = min(mn[0], cx); mx[0] = max(mx[0], cx);
+            mn[1] = min(mn[1], cy); mx[1] = max(mx[1], cy);
+            mn[2] = min(mn[2], cz); mx[2] = max(mx[2], cz);
             const float4 b = P.xb[i];
             // rounded up; a NaN build position (never built) reads as infinitely far
             const float d = norm3(F3{p.x - b.x, p.y - b.y, p.z - b.z}) * (1.0f + 1e-5f);
-            dst = isnan(d) ? INFINITY : d;
+            dst = fmaxf(dst, isnan(d) ? INFINITY : d);
         }
     }
-    block_max_atomic(dst, &P.ac->d_start_bits);
+    __shared__ int s_box[6][32];
+    __shared__ float s_d[32];
+    __shared__ int s_n[32];
+    __shared__ double s_m[32];
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = blockDim.x >> 5;
 #pragma unroll
-    for (int a = 0; a < 3; ++a) {
-        int v0 = mn[a], v1 = mx[a];
+    for (int a = 0; a < 3; ++a)
 #pragma unroll
         for (int o = 16; o > 0; o >>= 1) {
-            v0 = min(v0, __shfl_xor_sync(0xffffffffu, v0, o));
-            v1 = max(v1, __shfl_xor_sync(0xffffffffu, v1, o));
+            mn[a] = min(mn[a], __shfl_xor_sync(0xffffffffu, mn[a], o));
+            mx[a] = max(mx[a], __shfl_xor_sync(0xffffffffu, mx[a], o));
         }
-        if ((threadIdx.x & 31) == 0) {
-            if (v0 != 0x7fffffff) atomicMin(&P.bbox[a], v0);
-            if (v1 != (int)0x80000000) atomicMax(&P.bbox[3 + a], v1);
-        }
+    dst = warp_max(dst);
+    offm = warp_sum(offm);
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) offg += __shfl_xor_sync(0xffffffffu, offg, o);
+    if (lane == 0) {
+        for (int a = 0; a < 3; ++a) { s_box[a][wid] = mn[a]; s_box[3 + a][wid] = mx[a]; }
+        s_d[wid] = dst; s_n[wid] = offg; s_m[wid] = offm;
     }
-    unsigned any = __ballot_sync(0xffffffffu, offg != 0);
-    if (any) {
-        int cnt = __popc(any);
-        double m = warp_sum(offm);
-        if ((threadIdx.x & 31) == 0) {
-            atomicAdd(&P.sc->off_grid_num, cnt);
-            atomicAdd(&P.sc->off_grid_mass, m);
+    __syncthreads();
+    if (wid == 0) {
+        const bool in = lane < nw;
+#pragma unroll
+        for (int a = 0; a < 3; ++a) {
+            int v0 = in ? s_box[a][lane] : 0x7fffffff, v1 = in ? s_box[3 + a][lane] : (int)0x80000000;
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) {
+                v0 = min(v0, __shfl_xor_sync(0xffffffffu, v0, o));
+                v1 = max(v1, __shfl_xor_sync(0xffffffffu, v1, o));
+            }
+            if (lane == 0) {
+                if (v0 != 0x7fffffff) atomicMin(&P.bbox[a], v0);
+                if (v1 != (int)0x80000000) atomicMax(&P.bbox[3 + a], v1);
+            }
+        }
+        float d = warp_max(in ? s_d[lane] : 0.0f);
+        double m = warp_sum(in ? s_m[lane] : 0.0);
+        int g = in ? s_n[lane] : 0;
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) g += __shfl_xor_sync(0xffffffffu, g, o);
+        if (lane == 0) {
+            atomicMax(&P.ac->d_start_bits, __float_as_uint(fmaxf(d, 0.0f)));
+            if (g) {
+                atomicAdd(&P.sc->off_grid_num, g);
+                atomicAdd(&P.sc->off_grid_mass, m);
+            }
         }
     }
 }
@@ -483,6 +512,7 @@ __device__ __forceinline__ void split_entries(int m, At&& at, F&& f) {
 // 1348-1490) for query point xq in cell q of size h, without the candidate lists: the
 // coarse table of the last build searched wide enough for displacement D since it, each
 // candidate tested for distance at the current positions and for its step-start cell.
+// f(j, mirror, pos_j).
 template <class F>
 __device__ __forceinline__ void stale_search(const Cst& c, const Ptr& P, int i, F3 xq, int qx, int qy, int qz,
                                              float D, F&& f) {
@@ -497,9 +527,9 @@ __device__ __forceinline__ void stale_search(const Cst& c, const Ptr& P, int i, 
     const float rf = ceilf(D / c.hc);
     const int rlo = -(rf <= 8.0f ? max((int)rf, 1) : 8);
     sweep_coarse(c, P, L, i, xq, bi.x, bi.y, bi.z, w, rlo, w - 1, c.d2_lt, c.h,
-                 [&](int j, int mir, float4, float) {
+                 [&](int j, int mir, float4 pj, float) {
         const int4 fj = __ldg(P.fcell + j);
-        if (fj.w >= 0 && sweep_cell_ok(mir, fj.x, fj.y, fj.z, qx, qy, qz)) f(j, mir);
+        if (fj.w >= 0 && sweep_cell_ok(mir, fj.x, fj.y, fj.z, qx, qy, qz)) f(j, mir, pj);
     });
 }
 
@@ -512,11 +542,11 @@ __device__ __forceinline__ void stale_search(const Cst& c, const Ptr& P, int i, 
 __global__ void __launch_bounds__(kBlock) k_nbr_filter(Cst c, Ptr P) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= c.n) return;
+    const int vc = __ldg(P.vl_cnt + i);
     const int4 fi = P.fcell[i];
     int cnt = 0;
     const int n = c.n, K = c.K;
     int* __restrict__ nb = P.nbr;
-    const int vc = __ldg(P.vl_cnt + i);
     const float4* __restrict__ pos = reinterpret_cast<const float4*>(P.cur.pos);
     if (fi.w >= 0 && !vl_overflow(c, vc)) {
         const F3 xi = f3(pos[i]);
@@ -538,7 +568,7 @@ __global__ void __launch_bounds__(kBlock) k_nbr_filter(Cst c, Ptr P) {
     } else if (fi.w >= 0) {
         const F3 xi = f3(pos[i]);
         const float D = __uint_as_float(P.ac->d_start_bits);
-        stale_search(c, P, i, xi, fi.x, fi.y, fi.z, D, [&](int j, int mir) {
+        stale_search(c, P, i, xi, fi.x, fi.y, fi.z, D, [&](int j, int mir, float4) {
             if (cnt < K) nb[(size_t)cnt * n + i] = j | (mir << kMirShift);
             ++cnt;
         });
@@ -550,7 +580,7 @@ __global__ void __launch_bounds__(kBlock) k_nbr_filter(Cst c, Ptr P) {
                 P.ovf_off[i] = (int)base;
                 int* __restrict__ run = P.ovf + base;
                 int k = 0;
-                stale_search(c, P, i, xi, fi.x, fi.y, fi.z, D, [&](int j, int mir) {
+                stale_search(c, P, i, xi, fi.x, fi.y, fi.z, D, [&](int j, int mir, float4) {
                     if (k >= K) run[k - K] = j | (mir << kMirShift);
                     ++k;
                 });
