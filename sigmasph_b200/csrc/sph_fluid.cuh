@@ -240,8 +240,8 @@ __global__ void SPH_PAIR_BOUNDS_OCC4 k_force(Cst c, Ptr P) {
         float cl = c.p.c_signal * c.p.c_signal;
         F3 a = {0, 0, 0};
         float dvisc = 0.0f;
-        for_each_neighbour(c, P, i, [&](int j, int mir) {
-            float4 pj = __ldg(pos + j), vj4 = __ldg(vel + j);
+        for_each_neighbour_pos(c, P, i, pos, [&](int j, int mir, float4 pj) {
+            float4 vj4 = __ldg(vel + j);
             float p_j = __ldg(&dsp[j].w);
             F3 xj = f3(pj), vj = f3(vj4);
             if (mir) { xj = mirror3(mir, xj); vj = mirror3(mir, vj); }

@@ -593,6 +593,30 @@ __global__ void __launch_bounds__(kBlock) k_nbr_filter(Cst c, Ptr P) {
     P.nbr_cnt[i] = cnt;
 }
 
+// Calls f(j, mirror, pos_j) for this step's neighbours of i, requesting the next entry's
+// position while the current pair is evaluated (the passes stall on that gather).
+template <class F>
+__device__ __forceinline__ void for_each_neighbour_pos(const Cst& c, const Ptr& P, int i,
+                                                       const float4* __restrict__ pos, F&& f) {
+    const int cnt = __ldg(P.nbr_cnt + i);
+    const int m = cnt < c.K ? cnt : c.K;
+    const size_t n = (size_t)c.n;
+    const int* __restrict__ nb = P.nbr + i;
+    int e0 = m > 0 ? __ldg(nb) : 0;
+    int e1 = m > 1 ? __ldg(nb + n) : 0;
+    float4 p0 = m > 0 ? __ldg(pos + (e0 & kIdxMask)) : make_float4(0.f, 0.f, 0.f, 0.f);
+    for (int k = 0; k < m; ++k) {
+        const int e = e0;
+        const float4 pj = p0;
+        e0 = e1;
+        if (k + 2 < m) e1 = __ldg(nb + (size_t)(k + 2) * n);
+        if (k + 1 < m) p0 = __ldg(pos + (e0 & kIdxMask));
+        f(e & kIdxMask, (int)((unsigned)e >> kMirShift), pj);
+    }
+    if (cnt > c.K)
+        list_pairs(P.ovf + __ldg(P.ovf_off + i), 1, cnt - c.K, [&](int j, int mir) { f(j, mir, __ldg(pos + j)); });
+}
+
 // Calls f(j, mirror) for this step's neighbours of i: the list, then any overflow run.
 template <class F>
 __device__ __forceinline__ void for_each_neighbour(const Cst& c, const Ptr& P, int i, F&& f) {
