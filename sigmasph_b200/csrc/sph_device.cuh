@@ -18,6 +18,38 @@ constexpr int kBlock = 256;          // threads per block of the particle-parall
 // default budget) run three blocks per SM: 80 registers and a few spills measured 6%
 // faster per step than two blocks without spills.
 #define SPH_PAIR_BOUNDS_OCC3 __launch_bounds__(kBlock, 3)
+// Resident 256-thread blocks per SM of each pass over the lists (the register budget
+// follows: 64, 40 and 32 registers at 4, 6 and 8), as measured best on the 1M dam break
+// and the 2.38M bar: the passes are latency-bound, so resident warps pay until spills
+// grow (the shift pass: 5 -> 6 blocks 0.75 -> 0.70 ms, 7 and 8 slower; lambda 4 -> 6,
+// 0.30 -> 0.26 ms; the filter 8; the force and gradient passes spill heavily below 64
+// registers and stay at 4; the solid sweeps slow down at 4).  A build may override one
+// with -DSPH_OCC_<PASS>=n to time another.
+#ifndef SPH_OCC_LAM
+#define SPH_OCC_LAM 6
+#endif
+#ifndef SPH_OCC_LAMGRAD
+#define SPH_OCC_LAMGRAD 4
+#endif
+#ifndef SPH_OCC_FORCE
+#define SPH_OCC_FORCE 4
+#endif
+#ifndef SPH_OCC_PST
+#define SPH_OCC_PST 6
+#endif
+#ifndef SPH_OCC_FILTER
+#define SPH_OCC_FILTER 8
+#endif
+#ifndef SPH_OCC_SOLID_A
+#define SPH_OCC_SOLID_A 3
+#endif
+#ifndef SPH_OCC_SOLID_B
+#define SPH_OCC_SOLID_B 3
+#endif
+#ifndef SPH_OCC_SOLID_FORCE
+#define SPH_OCC_SOLID_FORCE 3
+#endif
+#define SPH_BOUNDS(occ) __launch_bounds__(kBlock, occ)
 constexpr int kMirShift = 30;        // neighbour entry = j | mirror code << 30
 constexpr int kIdxMask = (1 << 29) - 1;
 

@@ -24,7 +24,7 @@ __device__ __forceinline__ float4* as4(float* p) { return reinterpret_cast<float
 __device__ __forceinline__ const float4* as4c(const float* p) { return reinterpret_cast<const float4*>(p); }
 
 // ------------------------------------------------------------------ compute_lam pass 1
-__global__ void SPH_PAIR_BOUNDS_OCC4 k_lam(Cst c, Ptr P) {
+__global__ void SPH_BOUNDS(SPH_OCC_LAM) k_lam(Cst c, Ptr P) {
     int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= c.n) return;
     const float4* __restrict__ pos = as4c(P.cur.pos);
@@ -101,7 +101,7 @@ __global__ void SPH_PAIR_BOUNDS_OCC4 k_lam(Cst c, Ptr P) {
 }
 
 // ------------------------------------------------------------------ grad lambda + continuity
-__global__ void SPH_PAIR_BOUNDS_OCC4 k_lamgrad_cont(Cst c, Ptr P) {
+__global__ void SPH_BOUNDS(SPH_OCC_LAMGRAD) k_lamgrad_cont(Cst c, Ptr P) {
     int i = blockIdx.x * blockDim.x + threadIdx.x;
     double wdiff = 0.0;
     if (i < c.n) {
@@ -213,7 +213,7 @@ __global__ void __launch_bounds__(kBlock) k_eos(Cst c, Ptr P) {
 }
 
 // ------------------------------------------------------------------ pressure + viscosity + dt pairs
-__global__ void SPH_PAIR_BOUNDS_OCC4 k_force(Cst c, Ptr P) {
+__global__ void SPH_BOUNDS(SPH_OCC_FORCE) k_force(Cst c, Ptr P) {
     int i = blockIdx.x * blockDim.x + threadIdx.x;
     float amag = 0.0f, csq = 0.0f;
     if (i < c.n) {
@@ -408,7 +408,7 @@ __device__ __forceinline__ void for_each_pst_neighbour(const Cst& c, const Ptr& 
     });
 }
 
-__global__ void __launch_bounds__(kBlock, 5) k_pst(Cst c, Ptr P) {
+__global__ void SPH_BOUNDS(SPH_OCC_PST) k_pst(Cst c, Ptr P) {
     int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i == 0) {   // steps whose shift could not use the candidate lists
         const float dtot = __uint_as_float(P.ac->d_start_bits) + __uint_as_float(P.ac->max_disp_bits) +

@@ -539,7 +539,7 @@ __device__ __forceinline__ void stale_search(const Cst& c, const Ptr& P, int i, 
 // whose candidates overflowed gets all its pairs from the stale-bin search instead; past
 // K of those, the rest go in order to a run of the overflow pool (the search runs a
 // second time to write it).
-__global__ void __launch_bounds__(kBlock) k_nbr_filter(Cst c, Ptr P) {
+__global__ void SPH_BOUNDS(SPH_OCC_FILTER) k_nbr_filter(Cst c, Ptr P) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= c.n) return;
     const int vc = __ldg(P.vl_cnt + i);

@@ -365,7 +365,7 @@ __global__ void __launch_bounds__(kBlock) k_kc_inverse(Cst c, Ptr P) {
 }
 
 // ------------------------------------------------------------------ pass A
-__global__ void SPH_PAIR_BOUNDS_OCC3 k_solid_a(Cst c, Ptr P) {
+__global__ void SPH_BOUNDS(SPH_OCC_SOLID_A) k_solid_a(Cst c, Ptr P) {
     int i = blockIdx.x * blockDim.x + threadIdx.x;
     double wdiff = 0.0;
     if (i < c.n) {
@@ -589,7 +589,7 @@ __device__ __forceinline__ void block_count_add(unsigned v, unsigned long long* 
     if (threadIdx.x == 0 && s_cnt && dst) atomicAdd(dst, (unsigned long long)s_cnt);
 }
 
-__global__ void SPH_PAIR_BOUNDS_OCC3 k_solid_b(Cst c, Ptr P) {
+__global__ void SPH_BOUNDS(SPH_OCC_SOLID_B) k_solid_b(Cst c, Ptr P) {
     int i = blockIdx.x * blockDim.x + threadIdx.x;
     double pw = 0.0, wl = 0.0;
     bool capped_any = false;
@@ -877,7 +877,7 @@ __global__ void __launch_bounds__(kBlock) k_solid_commit(Cst c, Ptr P) {
 }
 
 // ------------------------------------------------------------------ stress force
-__global__ void SPH_PAIR_BOUNDS_OCC3 k_solid_force(Cst c, Ptr P) {
+__global__ void SPH_BOUNDS(SPH_OCC_SOLID_FORCE) k_solid_force(Cst c, Ptr P) {
     int i = blockIdx.x * blockDim.x + threadIdx.x;
     float amag = 0.0f, csq = 0.0f;
     double hgp = 0.0;
