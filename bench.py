@@ -161,10 +161,8 @@ class ClockSampler:
 
 
 def dist_setup():
-    ws = int(os.environ.get("WORLD_SIZE", "1"))
-    rank = int(os.environ.get("RANK", "0"))
-    local = int(os.environ.get("LOCAL_RANK", "0"))
-    return ws, rank, local
+    from sigmasph_b200.replicas import env_ranks
+    return env_ranks()
 
 
 def workload(args):
@@ -256,8 +254,10 @@ def run_strips(args):
     its own dt), two steps per CUDA-graph launch."""
     import torch
     from sigmasph_b200.ensemble import Ensemble, strip_specs
+    from sigmasph_b200.replicas import Replicas
     ws, rank, local = dist_setup()
     torch.cuda.set_device(local)
+    rep = Replicas("nccl")
     specs = strip_specs(256)
     ens = Ensemble(specs, buckets=args.buckets)
     tune = ens.autotune(candidates=(64, 128, 256), steps=4)
@@ -268,6 +268,8 @@ def run_strips(args):
     n = ens.particles
     K2 = max(args.steps // 2, 1)
     clocks = ClockSampler(local)
+    rep.barrier()
+    torch.cuda.synchronize()
     clocks.start()
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     e0.record()
@@ -275,17 +277,19 @@ def run_strips(args):
         ens.step2()
     e1.record()
     torch.cuda.synchronize()
+    rep.barrier()
     ck = clocks.stop()
-    ms = e0.elapsed_time(e1)
-    value = n * 2 * K2 / (ms / 1000.0)
+    ms = rep.max_over_ranks(e0.elapsed_time(e1))
+    value = rep.throughput(n * 2 * K2, ms / 1000.0)
     # end to end: after every launch read every strip's state (clock, dt, grip forces)
+    rep.barrier()
     t0 = time.perf_counter()
     nread = 0
     for _ in range(K2):
         ens.step2()
         for b in ens.buckets:
             nread += len(b.state())
-    el = time.perf_counter() - t0
+    el = rep.max_over_ranks(time.perf_counter() - t0)
     from sigmasph_b200 import abi
     import ctypes as C
     d2h = C.sizeof(abi.SphInstState) * len(specs) // 2
@@ -303,13 +307,16 @@ def run_strips(args):
             "config": {"workload": "256 plane-strain JC strips, packed size buckets, one graph launch per 2 steps",
                        "particles": n, "strips": len(specs), "buckets": tune,
                        "l2": "inputs larger than L2 (state + neighbour lists > 1 GB)"},
-            "e2e": {"value": n * 2 * K2 / el, "unit": UNIT, "h2d_bytes_per_step": 0,
+            "e2e": {"value": rep.throughput(n * 2 * K2, el), "unit": UNIT, "h2d_bytes_per_step": 0,
                     "d2h_bytes_per_step": d2h},
             "gpu_launches": launches * 2 * K2}
+    if ws > 1:
+        line["config"]["parallelism"] = "replicas (one ensemble per GPU)"
     if ck is not None:
         line["clocks"] = ck
-    if rank == 0:
+    if rep.reporter:
         print(json.dumps(line))
+    rep.close()
     return 0
 
 
@@ -338,13 +345,10 @@ def main():
         return run_strips(args)
 
     import torch
+    from sigmasph_b200.replicas import Replicas
     ws, rank, local = dist_setup()
     torch.cuda.set_device(local)
-    dist = None
-    if ws > 1:
-        import datetime
-        import torch.distributed as dist
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+    rep = Replicas("nccl")
     from sigmasph_b200 import abi
     from sigmasph_b200.config import SimConfig
     from sigmasph_b200.particle_system import ParticleSystem
@@ -368,15 +372,11 @@ def main():
     solver.step_many(args.warmup + (args.warmup & 1))
     torch.cuda.synchronize()
 
-    def barrier():
-        if dist is not None:
-            dist.barrier()
-
     # ---------------------------------------------------------------- timed region
     K = args.steps
     solver.list_stats(reset=True)
     clocks = ClockSampler(local)
-    barrier()
+    rep.barrier()
     torch.cuda.synchronize()
     clocks.start()
     e0 = torch.cuda.Event(enable_timing=True)
@@ -385,23 +385,19 @@ def main():
     solver.step_many(K)
     e1.record(stream)
     torch.cuda.synchronize()
-    barrier()
+    rep.barrier()
     ck = clocks.stop()
-    ms = e0.elapsed_time(e1)
-    if dist is not None:
-        t = torch.tensor([ms], device=f"cuda:{local}", dtype=torch.float64)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms = float(t.item())
+    ms = rep.max_over_ranks(e0.elapsed_time(e1))
     err = solver.error_word()
     lists = solver.list_stats()
-    value = ws * n * K / (ms / 1000.0)
+    value = rep.throughput(n * K, ms / 1000.0)
 
     # ---------------------------------------------------------------- e2e through the public API
     # Per step, as the reference's driver loop does (run_simulation.py:1186-1209): write
     # dt from page-locked host memory, solver.step(), read dt back (synchronises).
     Ke = args.e2e_steps or K
     dt = solver.dt[None]
-    barrier()
+    rep.barrier()
     torch.cuda.synchronize()
     t0 = time.perf_counter()
     for _ in range(Ke):
@@ -409,12 +405,8 @@ def main():
         solver.step()
         dt = solver.dt[None]
     torch.cuda.synchronize()
-    el = time.perf_counter() - t0
-    if dist is not None:
-        t = torch.tensor([el], device=f"cuda:{local}", dtype=torch.float64)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        el = float(t.item())
-    e2e = {"value": ws * n * Ke / el, "unit": UNIT, "h2d_bytes_per_step": 4,
+    el = rep.max_over_ranks(time.perf_counter() - t0)
+    e2e = {"value": rep.throughput(n * Ke, el), "unit": UNIT, "h2d_bytes_per_step": 4,
            "d2h_bytes_per_step": 4}
 
     # ---------------------------------------------------------------- per-kernel timing
@@ -468,9 +460,7 @@ def main():
             except Exception as e:  # the baseline is reported, not required
                 line["cpu_baseline"] = {"value": None, "error": str(e)}
         print(json.dumps(line))
-    if dist is not None:
-        dist.barrier()
-        dist.destroy_process_group()
+    rep.close()
     return 0
 
 

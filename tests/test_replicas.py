@@ -1,0 +1,94 @@
+"""The replica harness of a multi-GPU run (sigmasph_b200.replicas), on CPU: world size 2
+over gloo, each rank stepping its own copy of a small dam break with the CPU restatement
+in place of the GPU path (the harness is the same code bench.py runs over NCCL).
+
+Checks: the ranks' copies stay identical (replicas, not shards), every rank sees the same
+maximum time, the whole-job throughput counts both ranks' particles over that maximum,
+only rank 0 reports, and a rank that never joins makes the other's first collective fail
+within the group timeout instead of hanging."""
+import os
+import socket
+import tempfile
+
+import numpy as np
+import pytest
+import torch.multiprocessing as mp
+
+
+def _free_port():
+    with socket.socket() as s:
+        s.bind(("127.0.0.1", 0))
+        return s.getsockname()[1]
+
+
+def _env(rank, world, port):
+    os.environ.update({"RANK": str(rank), "LOCAL_RANK": str(rank), "WORLD_SIZE": str(world),
+                       "MASTER_ADDR": "127.0.0.1", "MASTER_PORT": str(port)})
+
+
+def _replica_rank(rank, world, port, out_dir):
+    _env(rank, world, port)
+    import time
+    from sigmasph_b200 import abi
+    from sigmasph_b200.config import SimConfig
+    from sigmasph_b200.particle_system import ParticleSystem
+    from sigmasph_b200.replicas import Replicas
+    from sigmasph_b200.scenes import dambreak3d, dx_for_particles
+    from sigmasph_b200.solver import build_params
+    from oracle.oracle import Oracle, state_from_sets
+
+    rep = Replicas("gloo", timeout_s=60)
+    ps = ParticleSystem(SimConfig(dambreak3d(dx=dx_for_particles(600))), device="cpu")
+    o = Oracle(build_params(ps), ps.particle_max_num, fp64=False)
+    o.set_state(state_from_sets(ps.state_numpy()), 1e-4)
+    o.stage(abi.STAGE_SORT)
+    rep.barrier()
+    t0 = time.perf_counter()
+    o.step(3)
+    own = time.perf_counter() - t0 + 0.05 * rank     # the ranks' times differ
+    rep.barrier()
+    t_max = rep.max_over_ranks(own)
+    s = o.get_state()
+    x = s["x"][np.argsort(s["pid"])]
+    sums = rep.gather(float(np.sum(x, dtype=np.float64)))
+    value = rep.throughput(ps.particle_max_num * 3, t_max)
+    np.save(os.path.join(out_dir, f"r{rank}.npy"),
+            np.array([own, t_max, value, ps.particle_max_num, float(rep.reporter)] + sums))
+    rep.close()
+
+
+def _lonely_rank(rank, world, port, out_dir):
+    _env(rank, world, port)
+    if rank == 1:
+        return                       # never joins
+    from sigmasph_b200.replicas import Replicas
+    ok = "joined"
+    try:
+        rep = Replicas("gloo", timeout_s=3)
+        rep.barrier()
+    except Exception as e:           # the rendezvous or the barrier times out
+        ok = type(e).__name__
+    with open(os.path.join(out_dir, "r0.txt"), "w") as f:
+        f.write(ok)
+
+
+def test_two_replicas_on_gloo():
+    with tempfile.TemporaryDirectory() as d:
+        mp.start_processes(_replica_rank, args=(2, _free_port(), d), nprocs=2, join=True,
+                           start_method="spawn")
+        r = [np.load(os.path.join(d, f"r{k}.npy")) for k in range(2)]
+    own = [x[0] for x in r]
+    assert r[0][1] == r[1][1] == pytest.approx(max(own))
+    n = r[0][3]
+    assert r[0][2] == r[1][2] == pytest.approx(2 * n * 3 / max(own))
+    assert (r[0][4], r[1][4]) == (1.0, 0.0)
+    sums0, sums1 = r[0][5:], r[1][5:]
+    assert list(sums0) == list(sums1) and sums0[0] == sums0[1]
+
+
+def test_missing_rank_fails_within_timeout():
+    with tempfile.TemporaryDirectory() as d:
+        mp.start_processes(_lonely_rank, args=(2, _free_port(), d), nprocs=2, join=True,
+                           start_method="spawn")
+        with open(os.path.join(d, "r0.txt")) as f:
+            assert f.read() != "joined"
