@@ -353,24 +353,36 @@ def main():
     from sigmasph_b200.config import SimConfig
     from sigmasph_b200.particle_system import ParticleSystem
     scene, desc, tag = workload(args)
-    ps = ParticleSystem(SimConfig(scene), device=f"cuda:{local}")
-    n = ps.particle_max_num
-    cpu_ps = None
-    if rank == 0 and ws == 1 and not args.no_cpu_baseline:
-        cpu_ps = ParticleSystem(SimConfig(scene), device="cpu")
-    solver = ps.build_solver()
     if args.jc_surrogate:
         if args.workload != "tensile_bar3d_jc":
             raise SystemExit("--jc-surrogate applies to --workload tensile_bar3d_jc")
         from sigmasph_b200.surrogate import JCSurrogate
-        solver.enable_jc_surrogate(JCSurrogate.load(args.jc_surrogate), tol=1e-3)
+        sur = JCSurrogate.load(args.jc_surrogate)
         desc = dict(desc, jc_surrogate=os.path.basename(args.jc_surrogate), jc_surrogate_tol=1e-3)
-    solver.initialize()
-    stream = torch.cuda.current_stream()
+    W = args.warmup + (args.warmup & 1)
 
-    # warm-up (builds the two-step CUDA graph)
-    solver.step_many(args.warmup + (args.warmup & 1))
-    torch.cuda.synchronize()
+    def warm_solver(single_step_graph):
+        """The workload's particle system and solver after W warm-up steps (the CUDA
+        graphs are captured there, outside any timed region)."""
+        ps_ = ParticleSystem(SimConfig(scene), device=f"cuda:{local}")
+        sv = ps_.build_solver()
+        if args.jc_surrogate:
+            sv.enable_jc_surrogate(sur, tol=1e-3)
+        sv.initialize()
+        if single_step_graph:
+            sv.step_many(W - 1)
+            sv.step()
+        else:
+            sv.step_many(W)
+        torch.cuda.synchronize()
+        return ps_, sv
+
+    ps, solver = warm_solver(False)
+    n = ps.particle_max_num
+    cpu_ps = None
+    if rank == 0 and ws == 1 and not args.no_cpu_baseline:
+        cpu_ps = ParticleSystem(SimConfig(scene), device="cpu")
+    stream = torch.cuda.current_stream()
 
     # ---------------------------------------------------------------- timed region
     K = args.steps
@@ -394,20 +406,26 @@ def main():
 
     # ---------------------------------------------------------------- e2e through the public API
     # Per step, as the reference's driver loop does (run_simulation.py:1186-1209): write
-    # dt from page-locked host memory, solver.step(), read dt back (synchronises).
+    # dt from page-locked host memory, solver.step(), read dt back (synchronises).  On a
+    # second copy of the workload, warmed up the same way, so that it covers the same
+    # steps of the simulation as the device-timed region.
     Ke = args.e2e_steps or K
-    dt = solver.dt[None]
+    ps_e, solver_e = warm_solver(True)
+    dt = solver_e.dt[None]
     rep.barrier()
     torch.cuda.synchronize()
     t0 = time.perf_counter()
     for _ in range(Ke):
-        solver.dt[None] = dt
-        solver.step()
-        dt = solver.dt[None]
+        solver_e.dt[None] = dt
+        solver_e.step()
+        dt = solver_e.dt[None]
     torch.cuda.synchronize()
     el = rep.max_over_ranks(time.perf_counter() - t0)
     e2e = {"value": rep.throughput(n * Ke, el), "unit": UNIT, "h2d_bytes_per_step": 4,
-           "d2h_bytes_per_step": 4}
+           "d2h_bytes_per_step": 4, "steps": Ke,
+           "window": "the same steps as the device-timed region, on a second copy of the workload"}
+    del solver_e, ps_e
+    torch.cuda.empty_cache()
 
     # ---------------------------------------------------------------- per-kernel timing
     solver.profile(True)

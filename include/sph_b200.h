@@ -274,7 +274,9 @@ int  sph_set_params(SphHandle* h, const SphParams* p);
  * cell table, reorder every persistent field, rebuild the neighbour lists. */
 int  sph_initialize(SphHandle* h, void* stream);
 /* SPHBase.step (sph_base.py:622-655) / HypoElasticSolver.step (SOLID.py:5227-5231),
- * nsteps times, asynchronously on `stream`; dt stays on the device. */
+ * nsteps times, asynchronously on `stream`; dt stays on the device.  Replays CUDA graphs
+ * of two steps and of one step, captured at the first call (eager launches while the
+ * per-kernel profile is on). */
 int  sph_step(SphHandle* h, int nsteps, void* stream);
 /* One named stage of the step, for stage-by-stage parity tests (SPH_STAGE_*). */
 int  sph_run_stage(SphHandle* h, int stage, void* stream);
@@ -309,7 +311,7 @@ int  sph_shift_pairs(SphHandle* h, float disp_bound, int32_t* pi, int32_t* pj, i
 int  sph_list_stats(SphHandle* h, uint64_t* out, int reset, void* stream);
 
 /* Per-kernel timing with CUDA events recorded on the launching stream around every
- * kernel of eagerly launched steps (sph_step with nsteps == 1, sph_run_stage).  Off by
+ * kernel of eagerly launched steps (sph_step while profiling, sph_run_stage).  Off by
  * default; graph replays are not instrumented. */
 int  sph_profile_enable(SphHandle* h, int on);
 /* Synchronises, then writes up to cap entries: '\n'-separated kernel names into names,

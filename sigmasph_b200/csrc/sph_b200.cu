@@ -52,6 +52,7 @@ struct SphHandle {
     SolidScratch solid;
     // CUDA graph of two consecutive steps
     cudaGraphExec_t graph2 = nullptr;
+    cudaGraphExec_t graph1 = nullptr;   // one step (sph_step with an odd count)
     cudaStream_t cap_stream = nullptr;
     // per-kernel event profile of eager launches
     bool prof_on = false;
@@ -140,6 +141,7 @@ Ptr make_ptr(SphHandle* h) {
 
 void drop_graph(SphHandle* h) {
     if (h->graph2) { cudaGraphExecDestroy(h->graph2); h->graph2 = nullptr; }
+    if (h->graph1) { cudaGraphExecDestroy(h->graph1); h->graph1 = nullptr; }
 }
 
 int scan_tiles(const SphHandle* h) { return (int)((h->c.mcap + 1 + kScanTile - 1) / kScanTile); }
@@ -148,8 +150,8 @@ int scan_tiles(const SphHandle* h) { return (int)((h->c.mcap + 1 + kScanTile - 1
 // k_layout reads it).
 int apply_force(SphHandle* h, cudaStream_t st) {
     if (!h->force_pending) return SPH_OK;
-    static const int one = 1;
-    CK(cudaMemcpyAsync(&h->ac->force_build, &one, sizeof(int), cudaMemcpyHostToDevice, st));
+    // any non-zero word asks for a build; a memset node is also capturable
+    CK(cudaMemsetAsync(&h->ac->force_build, 1, sizeof(int), st));
     h->force_pending = false;
     return SPH_OK;
 }
@@ -431,38 +433,57 @@ int sph_initialize(SphHandle* h, void* stream) {
     return SPH_OK;
 }
 
+// Captures `steps` consecutive steps into *out (the state stays in field set A, so one
+// graph serves any step).
+int capture_steps(SphHandle* h, int steps, cudaStream_t st, cudaGraphExec_t* out) {
+    if (!h->cap_stream) CK(cudaStreamCreateWithFlags(&h->cap_stream, cudaStreamNonBlocking));
+    cudaGraph_t g;
+    // finish everything queued on the caller's stream before capturing
+    CK(cudaStreamSynchronize(st));
+    CK(cudaStreamBeginCapture(h->cap_stream, cudaStreamCaptureModeThreadLocal));
+    h->capturing = true;
+    int r = SPH_OK;
+    for (int k = 0; k < steps && r == SPH_OK; ++k) r = one_step(h, h->cap_stream);
+    cudaError_t ec = cudaStreamEndCapture(h->cap_stream, &g);
+    h->capturing = false;
+    if (r != SPH_OK) { if (ec == cudaSuccess) cudaGraphDestroy(g); return r; }
+    CK(ec);
+    cudaError_t ei = cudaGraphInstantiate(out, g, 0);
+    cudaGraphDestroy(g);
+    CK(ei);
+    return SPH_OK;
+}
+
 int sph_step(SphHandle* h, int nsteps, void* stream) {
     if (!h || nsteps < 0) return SPH_ERR_ARG;
     if (!h->bound) return SPH_ERR_NOT_BOUND;
     if (h->n == 0 || nsteps == 0) return SPH_OK;
     cudaStream_t st = S(stream);
     if (int r = apply_force(h, st)) return r;
-    int pairs = nsteps / 2;
+    cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+    CK(cudaStreamIsCapturing(st, &cs));
+    if (cs != cudaStreamCaptureStatusNone) {
+        // the caller is recording a graph of its own: the steps' kernels go into it
+        for (int k = 0; k < nsteps; ++k)
+            if (int r = one_step(h, st)) return r;
+        return SPH_OK;
+    }
+    const int pairs = nsteps / 2;
     if (pairs > 0) {
         if (!h->graph2) {
-            if (!h->cap_stream) CK(cudaStreamCreateWithFlags(&h->cap_stream, cudaStreamNonBlocking));
-            cudaGraph_t g;
-            // finish everything queued on the caller's stream before capturing
-            CK(cudaStreamSynchronize(st));
-            CK(cudaStreamBeginCapture(h->cap_stream, cudaStreamCaptureModeThreadLocal));
-            int p0 = h->parity;
-            h->capturing = true;
-            int r1 = one_step(h, h->cap_stream);
-            int r2 = r1 ? r1 : one_step(h, h->cap_stream);
-            cudaError_t ec = cudaStreamEndCapture(h->cap_stream, &g);
-            h->capturing = false;
-            h->parity = p0;
-            if (r2 != SPH_OK) { if (ec == cudaSuccess) cudaGraphDestroy(g); return r2; }
-            CK(ec);
-            cudaError_t ei = cudaGraphInstantiate(&h->graph2, g, 0);
-            cudaGraphDestroy(g);
-            CK(ei);
+            if (int r = capture_steps(h, 2, st, &h->graph2)) return r;
         }
         for (int k = 0; k < pairs; ++k) CK(cudaGraphLaunch(h->graph2, st));
     }
     if (nsteps & 1) {
-        int r = one_step(h, st);
-        if (r) return r;
+        if (h->prof_on) {   // the per-kernel profile times eager launches
+            if (int r = one_step(h, st)) return r;
+        } else {
+            if (!h->graph1) {
+                if (int r = capture_steps(h, 1, st, &h->graph1)) return r;
+            }
+            CK(cudaGraphLaunch(h->graph1, st));
+        }
     }
     CK(cudaGetLastError());
     return SPH_OK;

@@ -237,23 +237,29 @@ def test_multistep_tracks_fp64_like_fp32_oracle(cuda):
 
 
 def test_graph_replay_equals_eager_steps(cuda):
-    """Two CUDA-graph steps are bit-identical to two eager steps (the step is
-    deterministic: stable sort, fixed pair order, no order-dependent atomics in fields)."""
+    """Replays of the two-step and the one-step CUDA graphs are bit-identical to eager
+    steps (the step is deterministic: stable sort, fixed pair order, no order-dependent
+    atomics in fields).  Eager: with the per-kernel profile on, steps launch eagerly."""
     outs = []
-    for graph in (False, True):
+    for mode in ("eager", "graph2", "graph1"):
         cfg = SimConfig(small_scene(5000))
         ps = ParticleSystem(cfg, device="cuda")
         perturb(ps)
         sv = ps.build_solver()
         sv.initialize()
-        if graph:
+        if mode == "graph2":
             sv.step_many(4)
         else:
-            for _ in range(4):
+            sv.profile(mode == "eager")
+            for _ in range(5):
                 sv.step()
+            sv.profile(False)
+        if mode == "graph2":
+            sv.step()
         outs.append(gpu_fields(ps))
     for k in ("x", "v", "V", "pressure", "pst_shift"):
         assert np.array_equal(outs[0][k], outs[1][k]), k
+        assert np.array_equal(outs[0][k], outs[2][k]), k
 
 
 def test_momentum_conserved_without_external_agents(cuda):
