@@ -906,6 +906,7 @@ int sph_ensemble_set(SphHandle* h, const SphMatRow* mat, const SphInstRow* inst,
     h->c.any_plastic = h->solid.any_plastic;
     h->c.all_gamma_one = h->solid.all_gamma_one;
     h->c.any_jc = h->solid.any_jc;
+    h->c.one_material = 0;
     h->force_pending = true;
     drop_graph(h);
     return SPH_OK;

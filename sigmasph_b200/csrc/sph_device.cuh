@@ -114,6 +114,7 @@ struct Cst {
     int any_plastic;     // some material row has a yield stress
     int all_gamma_one;   // every EOS is linear (exponent 1)
     int any_jc;          // some material row is Johnson-Cook (return statistics kept)
+    int one_material;    // one material row and no ensemble: every pair is same-material
     int block;           // threads per block of the solid particle kernels
     // candidate lists with a skin: every pair within h + skin at the last build, binned
     // in coarse cells of h + skin; complete while no particle moved more than dlim since

@@ -95,6 +95,9 @@ __global__ void SPH_BOUNDS(SPH_OCC_LAM) k_lam(Cst c, Ptr P) {
         evec = make_float4(Q[0][km], Q[1][km], Q[2][km], 0.0f);
     }
     P.lam[i] = lam;
+    // a fluid's shift.w is free: it carries lambda to the neighbours' gradient pass, which
+    // reads the shift record of every neighbour anyway (then k_eos puts p there)
+    if (!c.p.is_solid) P.cur.shift[4 * i + 3] = lam;
     P.lsym[2 * i] = make_float4(L00, L11, L22, L01);
     P.lsym[2 * i + 1] = make_float4(L02, L12, 0.0f, 0.0f);
     if (c.p.pst_normal_eigvec) P.lgrad[i] = evec;
@@ -137,8 +140,9 @@ __global__ void SPH_BOUNDS(SPH_OCC_LAMGRAD) k_lamgrad_cont(Cst c, Ptr P) {
             float rn;
             F3 g = wendland_dW2(r, rn2, rn, c);
             float Vj = w_of(pj, c);
+            const float4 sj = pst ? __ldg(shf + j) : make_float4(0.f, 0.f, 0.f, 0.f);
             if (need_lgrad) {
-                float ld = __ldg(lam + j) - lam_i;
+                float ld = (pst ? sj.w : __ldg(lam + j)) - lam_i;
                 F3 Lg = {L00 * g.x + L01 * g.y + L02 * g.z,
                          L01 * g.x + L11 * g.y + L12 * g.z,
                          L02 * g.x + L12 * g.y + L22 * g.z};
@@ -147,8 +151,7 @@ __global__ void SPH_BOUNDS(SPH_OCC_LAMGRAD) k_lamgrad_cont(Cst c, Ptr P) {
             float rho_j = vj4.w / pj.w;   // exact: rho_j - rho_i is a small difference
             F3 vh_j = vj;
             if (pst) {
-                float4 s = __ldg(shf + j);
-                F3 du_j = {s.x * inv_dt, s.y * inv_dt, s.z * inv_dt};
+                F3 du_j = {sj.x * inv_dt, sj.y * inv_dt, sj.z * inv_dt};
                 if (mir) du_j = mirror3(mir, du_j);
                 vh_j += du_j;
                 r0 += Vj * dot3(rho_j * du_j - rho_i * du_i, g) * inv_rho_i;
@@ -208,7 +211,9 @@ __global__ void __launch_bounds__(kBlock) k_eos(Cst c, Ptr P) {
     pi.w = V;
     pos[i] = pi;
     float m = P.cur.vel[4 * i + 3];
-    P.cur.disp[4 * i + 3] = tait_p(m / V, c);
+    const float p = tait_p(m / V, c);
+    P.cur.disp[4 * i + 3] = p;
+    P.cur.shift[4 * i + 3] = p;   // for the neighbours' force pass (see k_lam)
     P.acc[i] = make_float4(c.p.gravity[0], c.p.gravity[1], c.p.gravity[2], 0.0f);
 }
 
@@ -242,7 +247,8 @@ __global__ void SPH_BOUNDS(SPH_OCC_FORCE) k_force(Cst c, Ptr P) {
         float dvisc = 0.0f;
         for_each_neighbour_pos(c, P, i, pos, [&](int j, int mir, float4 pj) {
             float4 vj4 = __ldg(vel + j);
-            float p_j = __ldg(&dsp[j].w);
+            const float4 sj = ale ? __ldg(shf + j) : make_float4(0.f, 0.f, 0.f, 0.f);
+            float p_j = ale ? sj.w : __ldg(&dsp[j].w);   // k_eos copies p to shift.w
             F3 xj = f3(pj), vj = f3(vj4);
             if (mir) { xj = mirror3(mir, xj); vj = mirror3(mir, vj); }
             F3 r = xi - xj;
@@ -257,8 +263,7 @@ __global__ void SPH_BOUNDS(SPH_OCC_FORCE) k_force(Cst c, Ptr P) {
             dvisc += dot3(vi, fv);
             float rho_j = vj4.w / pj.w;   // exact: rho_j - rho_i is a small difference
             if (ale) {
-                float4 s = __ldg(shf + j);
-                F3 du_j = {s.x * inv_dt, s.y * inv_dt, s.z * inv_dt};
+                F3 du_j = {sj.x * inv_dt, sj.y * inv_dt, sj.z * inv_dt};
                 if (mir) du_j = mirror3(mir, du_j);
                 F3 t1 = (rho_j * dot3(du_j, g)) * vj - (rho_i * dot3(du_i, g)) * vi;
                 float b = dot3(rho_j * du_j - rho_i * du_i, g);
@@ -268,8 +273,13 @@ __global__ void SPH_BOUNDS(SPH_OCC_FORCE) k_force(Cst c, Ptr P) {
             if (c.p.dt_pair_mode != 0) {
                 float drho = fabsf(rho_i - rho_j);
                 if (drho > eps_rho) {
-                    float cij = fabsf(p_i - p_j) / drho;
-                    if (cij > cl) cl = cij;
+                    // the quotient only where it can beat the running maximum: the product
+                    // rounds within 1e-6 of cl drho, so the pre-test never drops a larger one
+                    const float dp = fabsf(p_i - p_j);
+                    if (dp > cl * drho * (1.0f - 1e-6f)) {
+                        float cij = dp / drho;
+                        if (cij > cl) cl = cij;
+                    }
                 }
             }
         });

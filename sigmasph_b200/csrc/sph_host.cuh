@@ -25,6 +25,7 @@ inline void fill_constants_from(const SphParams& p, int64_t n, Cst& c) {
     c.any_plastic = 0;
     c.all_gamma_one = 1;
     c.any_jc = 0;
+    c.one_material = p.n_materials <= 1;
     c.block = kBlock;
     // skin of the candidate lists: a tenth of the support.  The squared cut is rounded up
     // so that it holds every pair a float32 distance test could place within h + skin;

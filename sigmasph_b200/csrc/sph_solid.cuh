@@ -100,6 +100,7 @@ inline int solid_sync_rows(SolidScratch& s, const SphParams& p, Cst& c) {
         c.any_plastic = s.any_plastic;
         c.all_gamma_one = s.all_gamma_one;
         c.any_jc = s.any_jc;
+        c.one_material = 0;
         return SPH_OK;
     }
     SphMatRow rows[4] = {};
@@ -109,6 +110,7 @@ inline int solid_sync_rows(SolidScratch& s, const SphParams& p, Cst& c) {
     c.any_plastic = s.any_plastic;
     c.all_gamma_one = s.all_gamma_one;
     c.any_jc = s.any_jc;
+    c.one_material = p.n_materials <= 1;
     if (cudaMemcpy(s.mat, rows, sizeof(rows), cudaMemcpyHostToDevice) != cudaSuccess) return SPH_ERR_CUDA;
     return SPH_OK;
 }
@@ -149,6 +151,13 @@ __device__ __forceinline__ Sym load_s(const float* sdev, int i) {
     float4 a = __ldg(s), b = __ldg(s + 1);
     return {a.x, a.y, a.z, a.w, b.x, b.y};
 }
+// load_s and the plastic strain, which shares the record's second float4.
+__device__ __forceinline__ Sym load_s_ep(const float* sdev, int i, float& ep) {
+    const float4* s = reinterpret_cast<const float4*>(sdev) + 2 * i;
+    float4 a = __ldg(s), b = __ldg(s + 1);
+    ep = b.z;
+    return {a.x, a.y, a.z, a.w, b.x, b.y};
+}
 __device__ __forceinline__ Sym mirror_sym(int code, Sym s) {
     // M s M with M = diag(1, sy, sz): s_xy *= sy, s_xz *= sz, s_yz *= sy sz
     float sy = (code & 1) ? -1.0f : 1.0f, sz = (code & 2) ? -1.0f : 1.0f;
@@ -160,6 +169,10 @@ __device__ __forceinline__ float vm_sym(const Sym& s) {
 }
 __device__ __forceinline__ int eos_of(const Ptr& P, int i) {
     return (int)__ldg(P.cur.bcdisp + 4 * i + 3);
+}
+// Whether particle j has material row k (always, with one material and no ensemble).
+__device__ __forceinline__ bool same_material(const Cst& c, const Ptr& P, int j, int k) {
+    return c.one_material || eos_of(P, j) == k;
 }
 // Ensemble mode: a particle's material row is its instance, whose step state is
 // per instance; an ordinary scene keeps one state in the device scalars.
@@ -277,6 +290,7 @@ __device__ __forceinline__ void load_gradv(const Ptr& P, int j, float G[3][3]) {
     G[0][0] = a.x; G[0][1] = a.y; G[0][2] = a.z; G[1][0] = a.w;
     G[1][1] = b.x; G[1][2] = b.y; G[2][0] = b.z; G[2][1] = b.w; G[2][2] = d.x;
 }
+
 __device__ __forceinline__ void mirror_mat3(int code, float G[3][3]) {
     float s[3] = {1.0f, (code & 1) ? -1.0f : 1.0f, (code & 2) ? -1.0f : 1.0f};
 #pragma unroll
@@ -416,8 +430,7 @@ __global__ void SPH_BOUNDS(SPH_OCC_SOLID_A) k_solid_a(Cst c, Ptr P) {
                 r0 += Vj * dot3(rho_j * du_j - rho_i * du_i, g) * inv_rho_i;
             }
             r0 += Vj * dot3(vhat_i - vh_j, g);
-            int kj = eos_of(P, j);
-            if (kj == ki) {   // pair_delta (SOLID.py:4103-4114) on same-material pairs
+            if (same_material(c, P, j, ki)) {   // pair_delta (SOLID.py:4103-4114), same-material pairs
                 const float dj = di;          // same material row
                 float den = di + dj;
                 float dl = den > 1e-12f ? 2.0f * di * dj / den : 0.0f;
@@ -619,7 +632,8 @@ __global__ void SPH_BOUNDS(SPH_OCC_SOLID_B) k_solid_b(Cst c, Ptr P) {
                 float4 pj = __ldg(pos + j), vj4 = __ldg(vel + j), shj = __ldg(shf + j);
                 F3 xj = f3(pj);
                 F3 du_j = {shj.x * inv_dt, shj.y * inv_dt, shj.z * inv_dt};
-                Sym sj = load_s(sdev, j);
+                float epj;
+                Sym sj = load_s_ep(sdev, j, epj);
                 if (mir) { xj = mirror3(mir, xj); du_j = mirror3(mir, du_j); sj = mirror_sym(mir, sj); }
                 F3 r = xi - xj;
                 float rn2 = dot3(r, r), rn;
@@ -635,14 +649,11 @@ __global__ void SPH_BOUNDS(SPH_OCC_SOLID_B) k_solid_b(Cst c, Ptr P) {
                 A.xy += k * (a_j * sj.xy - a_i * s.xy - s.xy * dv);
                 A.xz += k * (a_j * sj.xz - a_i * s.xz - s.xz * dv);
                 A.yz += k * (a_j * sj.yz - a_i * s.yz - s.yz * dv);
-                if (plastic_any) {
-                    float epj = __ldg(sdev + 8 * j + 6);
-                    dep += k * (a_j * epj - a_i * ep - ep * dv);
-                }
+                if (plastic_any) dep += k * (a_j * epj - a_i * ep - ep * dv);
                 if (c.p.transport_e) {
                     float e_j = shj.w;
                     adv += wj * rho_j * (e_j - e_i) * dot3(du_j, g) * inv_rho_i;
-                    if (c.p.ale_diffusion > 0.0f && eos_of(P, j) == ki) {
+                    if (c.p.ale_diffusion > 0.0f && same_material(c, P, j, ki)) {
                         float psig = __fdividef(2.0f * (e_j - e_i) * (-dot3(r, g)), rn2 + c.eta2);
                         float rb = 0.5f * (rho_i + rho_j);
                         F3 su = du_i + du_j;
@@ -942,7 +953,7 @@ __global__ void SPH_BOUNDS(SPH_OCC_SOLID_FORCE) k_solid_force(Cst c, Ptr P) {
             a += am;
             if (c.p.viscosity > 0.0f) dei += -0.5f * dot3(am, vij);
             if (hg_inloop && rn > 1e-9f) {
-                float inv_rn = 1.0f / rn;
+                float inv_rn = rsqrtf(rn2);
                 F3 rh = {-r.x * inv_rn, -r.y * inv_rn, -r.z * inv_rn};
                 float Gj[3][3];
                 load_gradv(P, j, Gj);
@@ -968,11 +979,16 @@ __global__ void SPH_BOUNDS(SPH_OCC_SOLID_FORCE) k_solid_force(Cst c, Ptr P) {
                 F3 t = t1 - b * vi;
                 a += (w_j * inv_rho_i) * t;
             }
-            if (c.p.dt_pair_mode != 0 && (c.p.dt_pair_mode != 2 || eos_of(P, j) == ki)) {
+            if (c.p.dt_pair_mode != 0 && (c.p.dt_pair_mode != 2 || same_material(c, P, j, ki))) {
                 float drho = fabsf(rho_i - rho_j);
                 if (drho > eps_rho) {
-                    float cij = fabsf(p_i - p_j) / drho;
-                    if (cij > cl) cl = cij;
+                    // the quotient only where it can beat the running maximum: the product
+                    // rounds within 1e-6 of cl drho, so the pre-test never drops a larger one
+                    const float dp = fabsf(p_i - p_j);
+                    if (dp > cl * drho * (1.0f - 1e-6f)) {
+                        float cij = dp / drho;
+                        if (cij > cl) cl = cij;
+                    }
                 }
             }
         });

@@ -1,16 +1,16 @@
 """ParticleSystem: the reference's particle store (particle_system.py:23-1849) with its
 field API, over PyTorch tensors laid out for the sm_100a kernels.
 
-Every persistent per-particle field lives twice, in buffer sets A and B; each neighbour
-rebuild gathers the state from the current set into the other in the new (Morton cell)
-order, and the library reports which set is current.  The attributes below always read
+Every persistent per-particle field lives in buffer set A; set B is the scratch of the
+reorder (a neighbour-list build gathers A into B in the new Morton cell order and copies
+it back), and the library reports which set is current.  The attributes below always read
 and write the current set, so a caller sees exactly the reference's fields:
 
     ps.x, ps.V         set.pos   [n, 4]  (x, y, z, V)
     ps.v, ps.m         set.vel   [n, 4]  (vx, vy, vz, m)
     ps.x_0, ps.V_lo    set.x0    [n, 4]
     ps.u, ps.pressure  set.disp  [n, 4]
-    ps.pst_shift, ps.e_int   set.shift [n, 4]
+    ps.pst_shift, ps.e_int   set.shift [n, 4]  (fluid: w is the kernels' scratch)
     ps.sigma_dev, ps.eps_plastic, ps.temperature   set.sdev [n, 8] (solid)
     ps.bc_flag, ps.bc_id     set.bc     [n, 2] int32 (solid)
     ps.bc_disp, ps.eos_id    set.bcdisp [n, 4] (solid)
