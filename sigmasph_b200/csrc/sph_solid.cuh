@@ -283,6 +283,14 @@ __device__ __forceinline__ void grad_v_finish(const Cst& c, const Ptr& P, int i,
     reinterpret_cast<float4*>(g)[2] = make_float4(G[2][2], 0.0f, 0.0f, 0.0f);
 }
 struct NoExtra {};
+// The record's fourth word after the 3x3: the pressure k_solid_commit copied there.
+__device__ __forceinline__ float load_gradv_p(const Ptr& P, int j, float G[3][3]) {
+    const float4* g = reinterpret_cast<const float4*>(P.gradv + 12 * j);
+    float4 a = __ldg(g), b = __ldg(g + 1), d = __ldg(g + 2);
+    G[0][0] = a.x; G[0][1] = a.y; G[0][2] = a.z; G[1][0] = a.w;
+    G[1][1] = b.x; G[1][2] = b.y; G[2][0] = b.z; G[2][1] = b.w; G[2][2] = d.x;
+    return d.y;
+}
 
 __device__ __forceinline__ void load_gradv(const Ptr& P, int j, float G[3][3]) {
     const float4* g = reinterpret_cast<const float4*>(P.gradv + 12 * j);
@@ -882,7 +890,11 @@ __global__ void __launch_bounds__(kBlock) k_solid_commit(Cst c, Ptr P) {
     pi.w = V;
     pos[i] = pi;
     float m = P.cur.vel[4 * i + 3];
-    P.cur.disp[4 * i + 3] = solid_pressure(c, P, eos_of(P, i), m / V);
+    const float p = solid_pressure(c, P, eos_of(P, i), m / V);
+    P.cur.disp[4 * i + 3] = p;
+    // a spare word of the velocity-gradient record carries p to the neighbours' force
+    // pass, which reads that record of every neighbour for the in-loop damper anyway
+    P.gradv[12 * i + 9] = p;
     // gravity; de_int restarts for this step's force pass
     P.acc[i] = make_float4(c.p.gravity[0], c.p.gravity[1], c.p.gravity[2], 0.0f);
 }
@@ -928,47 +940,54 @@ __global__ void SPH_BOUNDS(SPH_OCC_SOLID_FORCE) k_solid_force(Cst c, Ptr P) {
         float dei = 0.0f, dhg = 0.0f;
         for_each_neighbour(c, P, i, [&](int j, int mir) {
             float4 pj = __ldg(pos + j), vj4 = __ldg(vel + j);
-            float p_j = __ldg(&dsp[j].w);
             F3 xj = f3(pj), vj = f3(vj4);
-            Sym sj = load_s(sdev, j);
-            if (mir) { xj = mirror3(mir, xj); vj = mirror3(mir, vj); sj = mirror_sym(mir, sj); }
+            if (mir) { xj = mirror3(mir, xj); vj = mirror3(mir, vj); }
             F3 r = xi - xj;
             float rn2 = dot3(r, r), rn;
             F3 g = wendland_dW2(r, rn2, rn, c);
             float w_j = w_of(pj, c);
+            const float rj = r_axi_of(pj.y, c);
+            const float ratio = axc ? 0.5f * (ri + rj) * inv_ri : 1.0f;
+            F3 vij = vi - vj;
+            // the in-loop damper first: j's velocity-gradient record also carries its
+            // pressure (k_solid_commit), and is dead once this term is summed
+            float p_j;
+            if (hg_inloop) {
+                float Gj[3][3];
+                p_j = load_gradv_p(P, j, Gj);
+                if (rn > 1e-9f) {
+                    float inv_rn = rsqrtf(rn2);
+                    F3 rh = {-r.x * inv_rn, -r.y * inv_rn, -r.z * inv_rn};
+                    if (mir) mirror_mat3(mir, Gj);
+                    F3 mr = -r;
+                    F3 dvh = {(vj.x - vi.x) - 0.5f * ((Gi[0][0] + Gj[0][0]) * mr.x + (Gi[0][1] + Gj[0][1]) * mr.y + (Gi[0][2] + Gj[0][2]) * mr.z),
+                              (vj.y - vi.y) - 0.5f * ((Gi[1][0] + Gj[1][0]) * mr.x + (Gi[1][1] + Gj[1][1]) * mr.y + (Gi[1][2] + Gj[1][2]) * mr.z),
+                              (vj.z - vi.z) - 0.5f * ((Gi[2][0] + Gj[2][0]) * mr.x + (Gi[2][1] + Gj[2][1]) * mr.y + (Gi[2][2] + Gj[2][2]) * mr.z)};
+                    float hg = dot3(dvh, rh);
+                    float damp = hg_pre * w_j * wendland_W(rn, c) * hg;
+                    F3 ah = damp * rh;
+                    ah.x *= ratio;
+                    a += ah;
+                    dhg += -0.5f * dot3(ah, vij);
+                }
+            } else {
+                p_j = __ldg(&dsp[j].w);
+            }
+            Sym sj = load_s(sdev, j);
+            if (mir) sj = mirror_sym(mir, sj);
             float pp = p_i + p_j;
             Sym ss = {s.xx + sj.xx - pp, s.yy + sj.yy - pp, s.zz + sj.zz - pp, s.xy + sj.xy, s.xz + sj.xz, s.yz + sj.yz};
             float ww = w_i * w_j;
             F3 f = {ww * (ss.xx * g.x + ss.xy * g.y + ss.xz * g.z),
                     ww * (ss.xy * g.x + ss.yy * g.y + ss.yz * g.z),
                     ww * (ss.xz * g.x + ss.yz * g.y + ss.zz * g.z)};
-            const float rj = r_axi_of(pj.y, c);
-            const float ratio = axc ? 0.5f * (ri + rj) * inv_ri : 1.0f;
             f.x *= ratio;
             a += inv_mw * f;
-            F3 vij = vi - vj;
             dei += -0.5f * dot3(f, vij) * inv_mw;
             float vxy = dot3(vij, r);
             F3 am = __fdividef(visc * w_j * vxy, rn * rn + c.eta2) * g;
             a += am;
             if (c.p.viscosity > 0.0f) dei += -0.5f * dot3(am, vij);
-            if (hg_inloop && rn > 1e-9f) {
-                float inv_rn = rsqrtf(rn2);
-                F3 rh = {-r.x * inv_rn, -r.y * inv_rn, -r.z * inv_rn};
-                float Gj[3][3];
-                load_gradv(P, j, Gj);
-                if (mir) mirror_mat3(mir, Gj);
-                F3 mr = -r;
-                F3 dvh = {(vj.x - vi.x) - 0.5f * ((Gi[0][0] + Gj[0][0]) * mr.x + (Gi[0][1] + Gj[0][1]) * mr.y + (Gi[0][2] + Gj[0][2]) * mr.z),
-                          (vj.y - vi.y) - 0.5f * ((Gi[1][0] + Gj[1][0]) * mr.x + (Gi[1][1] + Gj[1][1]) * mr.y + (Gi[1][2] + Gj[1][2]) * mr.z),
-                          (vj.z - vi.z) - 0.5f * ((Gi[2][0] + Gj[2][0]) * mr.x + (Gi[2][1] + Gj[2][1]) * mr.y + (Gi[2][2] + Gj[2][2]) * mr.z)};
-                float hg = dot3(dvh, rh);
-                float damp = hg_pre * w_j * wendland_W(rn, c) * hg;
-                F3 ah = damp * rh;
-                ah.x *= ratio;
-                a += ah;
-                dhg += -0.5f * dot3(ah, vij);
-            }
             float rho_j = vj4.w / pj.w;
             if (ale) {
                 float4 q = __ldg(shf + j);
