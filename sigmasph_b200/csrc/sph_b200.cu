@@ -40,6 +40,7 @@ struct SphHandle {
     int* nbr_cnt = nullptr;
     int* vl = nullptr;
     int* vl_cnt = nullptr;
+    int* nl_cnt = nullptr;
     int* ovf = nullptr;
     int* ovf_off = nullptr;
     unsigned* xbits = nullptr;
@@ -125,6 +126,7 @@ Ptr make_ptr(SphHandle* h) {
     P.nbr_cnt = h->nbr_cnt;
     P.vl = h->vl;
     P.vl_cnt = h->vl_cnt;
+    P.nl_cnt = h->nl_cnt;
     P.ovf = h->ovf;
     P.ovf_off = h->ovf_off;
     P.xbits = h->xbits;
@@ -229,7 +231,7 @@ void free_all(SphHandle* h) {
     h->prof_pool.clear();
     if (h->cap_stream) cudaStreamDestroy(h->cap_stream);
     void* ptrs[] = {h->cell, h->key, h->rank, h->perm, h->hist, h->start, h->bsum,
-                    h->bbox, h->layout, h->nbr, h->nbr_cnt, h->vl, h->vl_cnt, h->ovf, h->ovf_off, h->xbits, h->fcell, h->xb,
+                    h->bbox, h->layout, h->nbr, h->nbr_cnt, h->vl, h->vl_cnt, h->nl_cnt, h->ovf, h->ovf_off, h->xbits, h->fcell, h->xb,
                     h->sc, h->ac};
     for (void* q : ptrs) if (q) cudaFree(q);
     if (h->pinned) cudaFreeHost(h->pinned);
@@ -342,6 +344,7 @@ int sph_create(const SphParams* p, int64_t n_max, SphHandle** out) {
         (r = dalloc(&h->layout, 1)) || (r = dalloc(&h->nbr, N * (size_t)K)) ||
         (r = dalloc(&h->nbr_cnt, N)) || (r = dalloc(&h->sc, 1)) || (r = dalloc(&h->ac, 1)) ||
         (r = dalloc(&h->vl, N * (size_t)Kv)) || (r = dalloc(&h->vl_cnt, N)) ||
+        (r = dalloc(&h->nl_cnt, N)) ||
         (r = dalloc(&h->ovf, ovf_cap)) || (r = dalloc(&h->ovf_off, N)) ||
         (r = dalloc(&h->xbits, N / 32 + 1)) ||
         (r = dalloc(&h->fcell, N)) || (r = dalloc(&h->xb, N)) ||
@@ -369,6 +372,7 @@ int sph_create(const SphParams* p, int64_t n_max, SphHandle** out) {
         // no lists and no cells until the first build: empty counts, off-grid cells, an
         // empty layout
         cudaMemset(h->vl_cnt, 0, N * sizeof(int)) != cudaSuccess ||
+        cudaMemset(h->nl_cnt, 0, N * sizeof(int)) != cudaSuccess ||
         cudaMemset(h->cell, 0xff, N * sizeof(int4)) != cudaSuccess ||
         cudaMemset(h->fcell, 0xff, N * sizeof(int4)) != cudaSuccess ||
         cudaMemset(h->layout, 0, sizeof(GridLayout)) != cudaSuccess) {
@@ -696,19 +700,21 @@ extern "C" int sph_shift_pairs(SphHandle* h, float disp_bound, int32_t* pi, int3
     if (h->n == 0) return SPH_OK;
     // the step's displacement record (since the build, this step's advect, the grips),
     // replaced for this call when a bound is given
-    unsigned int* words[3] = {&h->ac->d_start_bits, &h->ac->max_disp_bits, &h->ac->max_grip_disp_bits};
-    unsigned int saved[3];
-    for (int k = 0; k < 3; ++k)
+    // (a given bound also drops the near lists, which belong to the step's start)
+    unsigned int* words[4] = {&h->ac->d_start_bits, &h->ac->max_disp_bits, &h->ac->max_grip_disp_bits,
+                              &h->ac->near_m_bits};
+    unsigned int saved[4];
+    for (int k = 0; k < 4; ++k)
         CK(cudaMemcpyAsync(&saved[k], words[k], sizeof(unsigned int), cudaMemcpyDeviceToHost, st));
     CK(cudaStreamSynchronize(st));
-    unsigned int set[3] = {0u, 0u, 0u};
+    unsigned int set[4] = {0u, 0u, 0u, 0u};
     if (disp_bound >= 0.0f) {
         std::memcpy(&set[0], &disp_bound, sizeof(float));
-        for (int k = 0; k < 3; ++k)
+        for (int k = 0; k < 4; ++k)
             CK(cudaMemcpyAsync(words[k], &set[k], sizeof(unsigned int), cudaMemcpyHostToDevice, st));
     }
     const int r = export_pairs<1>(h, pi, pj, mir, cap, count, st);
-    for (int k = 0; k < 3; ++k)
+    for (int k = 0; k < 4; ++k)
         CK(cudaMemcpyAsync(words[k], &saved[k], sizeof(unsigned int), cudaMemcpyHostToDevice, st));
     CK(cudaStreamSynchronize(st));
     return r;

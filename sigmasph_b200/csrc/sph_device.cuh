@@ -80,7 +80,7 @@ struct DevAccum {
     int force_build;             // set by the host: the next step builds
     int off_grid_build;          // off-grid count at the last build
     unsigned int ovf_used;       // overflow-pool entries taken this step
-    int pad3;
+    unsigned int near_m_bits;    // margin M of this step's near lists (0: none)
     double hg_power;         // sum_i mw_i de_hg_i of the in-loop damper (solid)
     unsigned long long n_steps, n_builds, n_shift_search;   // list statistics
 };
@@ -172,6 +172,8 @@ struct Ptr {
     int* ovf_off;        // [n] start of the particle's run
     int* vl;             // [Kv][n] candidates within h + skin at the last build, k-major
     int* vl_cnt;         // [n]
+    int* nl_cnt;         // [n] this step's near candidates (edge, h <= |r| < h + M), kept in
+                         // the neighbour list's last rows
     DevScalars* sc;
     DevAccum* ac;
     JcPtr jc;

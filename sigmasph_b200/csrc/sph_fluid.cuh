@@ -374,7 +374,9 @@ __global__ void __launch_bounds__(kBlock) k_advect(Cst c, Ptr P) {
 // displacement since the lists' build -- at the step's start plus this step's advect and
 // grips -- is within the bound, from the candidate lists: every entry tested for
 // distance at the live positions, the edge entries also for j's step-start cell (its
-// current cell unless its bit in xbits says it moved) against i's live cell.  Otherwise
+// current cell unless its bit in xbits says it moved) against i's live cell.  Of the
+// edge candidates, only those accepted at the step's start and the near ones need
+// reading when the step moved particles less than half the near margin.  Otherwise
 // (or when the candidate list overflowed) the stale-bin search.  f(j, mirror, pos_j).
 template <class F>
 __device__ __forceinline__ void for_each_pst_neighbour(const Cst& c, const Ptr& P, int i, F3 xi, F&& f) {
@@ -391,10 +393,18 @@ __device__ __forceinline__ void for_each_pst_neighbour(const Cst& c, const Ptr& 
     const bool py = xi.y < c.h, pz = xi.z < c.h;
     const int d = vl_deep(vc);
     const size_t n = (size_t)c.n;
-    const int* __restrict__ vl = P.vl + i;
-    const int* __restrict__ nb = P.nbr + i;
-    // the deep rows of the neighbour list, then the edge rows of the candidate list
-    split_entries(d + vl_edge(vc), [&](int k) { return k < d ? __ldg(nb + (size_t)k * n) : __ldg(vl + (size_t)(k - d) * n); },
+    // Near path, when this step moved no particle more than M / 2 since the filter: the
+    // step's neighbour list (deep rows, then the edge entries accepted at the start) and
+    // the near list.  Otherwise the deep rows and every edge candidate.
+    const float step_move = __uint_as_float(P.ac->max_disp_bits) + __uint_as_float(P.ac->max_grip_disp_bits);
+    const bool near = P.ac->near_m_bits != 0u && 2.0f * step_move <= __uint_as_float(P.ac->near_m_bits);
+    // near path: neighbour-list rows 0 .. cnt-1, then its near rows K - nn .. K - 1; full
+    // path: rows 0 .. d-1, then the candidate list's edge rows
+    const int a_end = near ? __ldg(P.nbr_cnt + i) : d;
+    const int b_cnt = near ? __ldg(P.nl_cnt + i) : vl_edge(vc);
+    const int* __restrict__ la = P.nbr + i;
+    const int* __restrict__ lb = near ? P.nbr + (size_t)(c.K - b_cnt) * n + i : P.vl + i;
+    split_entries(a_end + b_cnt, [&](int k) { return k < a_end ? __ldg(la + (size_t)k * n) : __ldg(lb + (size_t)(k - a_end) * n); },
                   [&](int k, int e) {
         const int j = e & kIdxMask, mir = (int)((unsigned)e >> kMirShift);
         if (mir && (((mir & 1) && !py) || ((mir & 2) && !pz))) return;

@@ -129,6 +129,15 @@ __global__ void k_layout(Cst c, Ptr P) {
     const int build = A.force_build || offg != A.off_grid_build || !(dstart + pred <= c.dlim);
     A.n_steps += 1ull;
     A.rebuild = build;
+    // the near lists' margin: three times the last step's move (at least h / 1000), and no
+    // more than the candidates cover beyond this step's start (2 (dlim - D_start)), so
+    // that the shift may use them whenever this step moves particles less than M / 2
+    {
+        const float ds = build ? 0.0f : dstart;
+        float m = fmaxf(3.0f * pred, 1e-3f * c.h);
+        m = fminf(m, 2.0f * (c.dlim - ds));
+        A.near_m_bits = (m > 0.0f) ? __float_as_uint(m) : 0u;
+    }
     if (!build) return;
     A.force_build = 0;
     A.off_grid_build = offg;
@@ -551,20 +560,36 @@ __global__ void SPH_BOUNDS(SPH_OCC_FILTER) k_nbr_filter(Cst c, Ptr P) {
     if (fi.w >= 0 && !vl_overflow(c, vc)) {
         const F3 xi = f3(pos[i]);
         const bool py = xi.y < c.h, pz = xi.z < c.h;
+        // the near list: edge candidates this step rejects that lie within h + M (or whose
+        // plane is within h + M), the only ones the shift can gain if particles move less
+        // than M / 2 during the step
+        const float m = __uint_as_float(P.ac->near_m_bits);
+        const float hm = c.h + m, d2_near = hm * hm * (1.0f + 1e-5f);
+        const bool ny = xi.y < hm, nz = xi.z < hm;
+        int nn = 0;
+        const int ne = vl_edge(vc);
         cnt = vl_deep(vc);
-        list_entries(P.vl + i, (size_t)n, vl_edge(vc), [&](int e) {
+        // accepted entries go after the deep rows; near ones fill the list from its last
+        // row down (deep + accepted + near <= the candidates <= Kv = K rows)
+        list_entries(P.vl + i, (size_t)n, ne, [&](int e) {
             const int j = e & kIdxMask, mir = (int)((unsigned)e >> kMirShift);
-            if (mir && (((mir & 1) && !py) || ((mir & 2) && !pz))) return;
+            if (mir && (((mir & 1) && !ny) || ((mir & 2) && !nz))) return;
             const float4 pj = __ldg(pos + j);
             F3 xj = f3(pj);
             if (mir) xj = mirror3(mir, xj);
-            if (!(dist2_rn(xi, xj) < c.d2_lt)) return;
-            if (!sweep_cell_ok(mir, cell_of_fast(pj.x, c.h, c.inv_h), cell_of_fast(pj.y, c.h, c.inv_h),
-                               cell_of_fast(pj.z, c.h, c.inv_h), fi.x, fi.y, fi.z))
-                return;
-            nb[(size_t)cnt * n + i] = e;   // deep + edge <= Kv = K
-            ++cnt;
+            const float d2 = dist2_rn(xi, xj);
+            if (!(d2 < d2_near)) return;
+            if (d2 < c.d2_lt && !(mir && (((mir & 1) && !py) || ((mir & 2) && !pz))) &&
+                sweep_cell_ok(mir, cell_of_fast(pj.x, c.h, c.inv_h), cell_of_fast(pj.y, c.h, c.inv_h),
+                              cell_of_fast(pj.z, c.h, c.inv_h), fi.x, fi.y, fi.z)) {
+                nb[(size_t)cnt * n + i] = e;
+                ++cnt;
+            } else {
+                nb[(size_t)(K - 1 - nn) * n + i] = e;
+                ++nn;
+            }
         });
+        P.nl_cnt[i] = nn;
     } else if (fi.w >= 0) {
         const F3 xi = f3(pos[i]);
         const float D = __uint_as_float(P.ac->d_start_bits);

@@ -140,6 +140,26 @@ def test_shift_pairs_from_lists(cuda, scene_fn, reach):
         assert crossed[2:].sum() > 0
 
 
+@pytest.mark.parametrize("kick", [0.0, 3.0], ids=["within_margin", "past_margin"])
+def test_shift_pairs_after_a_real_step(cuda, kick):
+    """The shift's pairs after the step's own advect: from the near list (the step moved
+    particles less than half the near margin, which follows the last step's move) or,
+    after a sudden velocity kick, from every candidate; either way the stale-bin pair set."""
+    ps, solver, _ = make_pair(small_scene(5000), fp64=False)
+    solver.initialize()
+    solver.step_many(3)
+    if kick:
+        v = ps.v.to_numpy()
+        v += np.random.default_rng(2).normal(0.0, kick, v.shape).astype(np.float32)
+        ps.v.from_numpy(v)
+    for s in range(abi.STAGE_ADVECT + 1):
+        solver.run_stage(s)
+    pid = ps.pid.to_numpy()
+    A = pair_set(*solver.shift_pairs(), pid)
+    B = pair_set(*solver.pairs(1), pid)
+    assert A == B
+
+
 def _oracle_pairs_at(ps, solver):
     """The oracle's neighbour pairs after its own sort of the GPU's current state."""
     orc = Oracle(build_params(ps), ps.particle_max_num, fp64=False)
