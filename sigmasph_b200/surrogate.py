@@ -241,6 +241,41 @@ def compare_bar(surrogate, dx=0.4, tol=1e-3, record_every=50, device="cuda"):
             "curve_surrogate": [[float(a), float(b)] for a, b in zip(ds[:m], fs[:m])]}
 
 
+def step_cost(surrogate, dx=0.113, tol=1e-3, seed=3, s_amp=0.35, ep_max=0.2, device="cuda"):
+    """Per-kernel cost of one eager step of the Johnson-Cook 3D round bar from a synthetic
+    plastic state (seeded random trace-free deviators of amplitude s_amp, plastic strains
+    uniform in [0, ep_max]), plain and with the surrogate: {mode: {step_ms, kernels, stats}}."""
+    from .scenes import tensile_bar3d
+    out = {}
+    for mode, sur in (("plain", None), ("surrogate", surrogate)):
+        ps = ParticleSystem(SimConfig(tensile_bar3d(dx=dx, plasticity="jc")), device=device)
+        rng = np.random.default_rng(seed)
+        n = ps.particle_max_num
+        sd = rng.normal(0.0, s_amp, (n, 3, 3))
+        sd = 0.5 * (sd + sd.transpose(0, 2, 1))
+        sd -= (np.trace(sd, axis1=1, axis2=2) / 3.0)[:, None, None] * np.eye(3)[None]
+        ps.sigma_dev.from_numpy(sd.astype(np.float32))
+        ps.eps_plastic.from_numpy(rng.uniform(0.0, ep_max, n).astype(np.float32))
+        sv = ps.build_solver()
+        if sur is not None:
+            sv.enable_jc_surrogate(sur, tol=tol)
+        sv.initialize()
+        sv.jc_stats(reset=True)
+        sv.profile(True)
+        sv.profile_read()
+        sv.step()
+        torch.cuda.synchronize()
+        prof = sv.profile_read()
+        sv.profile(False)
+        out[mode] = {"particles": n, "step_ms": sum(v[0] for v in prof.values()),
+                     "kernels": {k: v[0] for k, v in prof.items()
+                                 if k in ("k_solid_b", "k_mlp_tc", "k_jc_finish")},
+                     "stats": sv.jc_stats(), "error_word": sv.error_word()}
+        del sv, ps
+        torch.cuda.empty_cache()
+    return out
+
+
 def main(argv=None):
     import argparse
     import json
@@ -256,7 +291,13 @@ def main(argv=None):
     c.add_argument("--weights", required=True)
     c.add_argument("--dx", type=float, default=0.4)
     c.add_argument("--out", default=None)
+    k = sub.add_parser("cost", help="per-kernel cost of one step from a synthetic plastic state")
+    k.add_argument("--weights", required=True)
+    k.add_argument("--dx", type=float, default=0.113)
     a = ap.parse_args(argv)
+    if a.cmd == "cost":
+        print(json.dumps(step_cost(JCSurrogate.load(a.weights), dx=a.dx)))
+        return 0
     if a.cmd == "train":
         t0 = time.time()
         X, F, rates = config0_samples(total=a.samples)
