@@ -71,6 +71,11 @@ STEP_ALGO_BYTES = 600
 # lambda 56, grad v 64, Jaumann + ALE + return + energy 144, continuity 64, EOS + force +
 # in-loop hourglass + dt 132, advect + grips 88, PST 64, displace 60.
 STEP_ALGO_BYTES_SOLID = 1060
+# FP32 work per particle-step (the secondary bound): five pair passes over ~80 neighbours
+# at ~50 FLOP per pair (fluid, 2.6 dx); ten pair-pass equivalents over ~113 neighbours at
+# ~60 FLOP (3D solid at 3 dx, in-loop damper).
+STEP_FLOP_FLUID = 5 * 80 * 50
+STEP_FLOP_SOLID = 10 * 113 * 60
 
 
 def load_peaks():
@@ -448,6 +453,13 @@ def main():
                 "launch_ms": dom_ms, "traffic": traffic,
                 "traffic_source": ("ncu dram__bytes_read.sum + dram__bytes_write.sum per launch, "
                                    "profiles/%s.md" % tag) if traffic else None}
+    import ctypes as C
+    fma = C.c_double(0.0)
+    abi.check(abi.lib().sph_fma_peak(C.byref(fma), None), "sph_fma_peak")
+    step_flop = STEP_FLOP_FLUID if tag == "dambreak3d" else STEP_FLOP_SOLID
+    fp32_bound = {"flop_per_particle_step": step_flop, "achieved_tflops": step_flop * value / 1e12,
+                  "peak_tflops": fma.value, "frac": step_flop * value / 1e12 / fma.value if fma.value else None,
+                  "peak_source": "measured FP32 FMA microbenchmark (sph_fma_peak)"}
     step_bytes = STEP_ALGO_BYTES if tag == "dambreak3d" else STEP_ALGO_BYTES_SOLID
     step_gbs = step_bytes * value / 1e9
     step_roofline = {"bound": "hbm", "algorithmic_bytes_per_particle_step": step_bytes,
@@ -466,7 +478,7 @@ def main():
                 "e2e": e2e, "gpu_launches": int(round(launches_per_step * K)),
                 "neighbour_lists": {"timed_steps": lists["steps"], "builds": lists["builds"],
                                     "shift_searches": lists["shift_searches"]},
-                "roofline": roofline, "step_roofline": step_roofline,
+                "roofline": roofline, "step_roofline": step_roofline, "fp32_bound": fp32_bound,
                 "kernel_ms_per_step": {k: round(v, 5) for k, v in sorted(per_step_ms.items(),
                                                                        key=lambda t: -t[1])},
                 "error_word": err}

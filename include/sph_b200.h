@@ -320,6 +320,12 @@ int  sph_profile_enable(SphHandle* h, int on);
 int  sph_profile_read(SphHandle* h, char* names, int names_cap, double* ms, int* launches,
                       int cap, int* count);
 
+/* Measured FP32 fused multiply-add throughput of the current device (TFLOP/s, 2 FLOP per
+ * FMA) from a microbenchmark kernel: eight independent FMA chains per thread, eight
+ * 256-thread blocks per SM.  The denominator of the FP32-issue bound bench.py reports
+ * beside the HBM roofline.  Synchronises; allocates a 4 kB result buffer. */
+int  sph_fma_peak(double* tflops, void* stream);
+
 /* The FP64 reductions of sph_reduce without a handle and without allocating: no
  * counterpart in the reference.  For callers that cannot call cudaMalloc (a host running
  * inside another framework's fixed device-memory pool, code that may not allocate while

@@ -176,6 +176,7 @@ def lib():
         "sph_pairs": (C.c_int, [vp, C.c_int, vp, vp, vp, i64, C.POINTER(i64), vp]),
         "sph_shift_pairs": (C.c_int, [vp, C.c_float, vp, vp, vp, i64, C.POINTER(i64), vp]),
         "sph_list_stats": (C.c_int, [vp, vp, C.c_int, vp]),
+        "sph_fma_peak": (C.c_int, [vp, vp]),
         "sph_profile_enable": (C.c_int, [vp, C.c_int]),
         "sph_profile_read": (C.c_int, [vp, C.c_char_p, C.c_int, C.POINTER(C.c_double),
                                        C.POINTER(C.c_int), C.c_int, C.POINTER(C.c_int)]),

@@ -784,6 +784,53 @@ extern "C" int sph_profile_read(SphHandle* h, char* names, int names_cap, double
 // ------------------------------------------------------------------ Johnson-Cook surrogate
 extern "C" {
 
+namespace {
+// Eight independent FMA chains per thread, kFmaIters rounds; the sum is stored so that
+// nothing is optimised away.
+constexpr int kFmaIters = 4096;
+__global__ void __launch_bounds__(256) k_fma_peak(float* out, float a, float b) {
+    float x[8];
+#pragma unroll
+    for (int k = 0; k < 8; ++k) x[k] = (float)(threadIdx.x + k) * 1e-3f;
+    for (int it = 0; it < kFmaIters; ++it) {
+#pragma unroll
+        for (int k = 0; k < 8; ++k) x[k] = fmaf(x[k], a, b);
+    }
+    float s = 0.0f;
+#pragma unroll
+    for (int k = 0; k < 8; ++k) s += x[k];
+    if (s == 123.456f) out[blockIdx.x & 1023] = s;   // practically never; keeps the chains live
+}
+}  // namespace
+
+int sph_fma_peak(double* tflops, void* stream) {
+    if (!tflops) return SPH_ERR_ARG;
+    cudaStream_t st = S(stream);
+    int dev = 0, sms = 0;
+    CK(cudaGetDevice(&dev));
+    CK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+    float* out = nullptr;
+    CK(cudaMalloc((void**)&out, 1024 * sizeof(float)));
+    const int blocks = sms * 8;
+    cudaEvent_t e0, e1;
+    cudaEventCreate(&e0);
+    cudaEventCreate(&e1);
+    k_fma_peak<<<blocks, 256, 0, st>>>(out, 0.999f, 1e-4f);   // warm-up
+    cudaEventRecord(e0, st);
+    for (int r = 0; r < 10; ++r) k_fma_peak<<<blocks, 256, 0, st>>>(out, 0.999f, 1e-4f);
+    cudaEventRecord(e1, st);
+    cudaError_t e = cudaEventSynchronize(e1);
+    float ms = 0.0f;
+    if (e == cudaSuccess) e = cudaEventElapsedTime(&ms, e0, e1);
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    cudaFree(out);
+    CK(e);
+    const double flop = 10.0 * blocks * 256.0 * kFmaIters * 8.0 * 2.0;
+    *tflops = ms > 0.0f ? flop / (ms * 1e-3) / 1e12 : 0.0;
+    return SPH_OK;
+}
+
 int sph_mlp_param_count(void) { return kMlpParams; }
 int64_t sph_mlp_packed_bytes(void) { return (int64_t)kMlpPackedBytes; }
 
