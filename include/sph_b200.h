@@ -305,6 +305,17 @@ int  sph_pairs(SphHandle* h, int mode, int32_t* pi, int32_t* pj, int32_t* mir,
  * sph_pairs mode 1 whenever the bound holds.  Output as sph_pairs. */
 int  sph_shift_pairs(SphHandle* h, float disp_bound, int32_t* pi, int32_t* pj, int32_t* mir,
                      int64_t cap, int64_t* count, void* stream);
+/* One pass of the initial relaxation against the shift (relax_initial_configuration,
+ * DSPH.py:1113-1179): the neighbour lists at the current positions, lambda and its
+ * gradient, then each particle's drive g = pst_constrain(-h^2 S) from the run's own
+ * disorder sum; *residual = max |g| / dx0; the step beta g, capped at maxShift dx0, is
+ * left in the shift record.  residual_each: NULL, or a device array of n floats that
+ * receives each particle's |g| / dx0 in the current storage order (the reference's
+ * relax_res, DSPH.py:1100).  Synchronises. */
+int  sph_relax_pass(SphHandle* h, float beta, float* residual, float* residual_each,
+                    void* stream);
+/* Moves every particle by the step the last sph_relax_pass left in its shift record. */
+int  sph_relax_move(SphHandle* h, void* stream);
 /* Candidate-list statistics since creation or the last reset: out[0] steps, out[1] steps
  * that built the candidate lists, out[2] shift passes that searched the coarse table
  * instead of reading the lists.  reset != 0 zeroes them after reading. */

@@ -177,6 +177,8 @@ def lib():
         "sph_shift_pairs": (C.c_int, [vp, C.c_float, vp, vp, vp, i64, C.POINTER(i64), vp]),
         "sph_list_stats": (C.c_int, [vp, vp, C.c_int, vp]),
         "sph_fma_peak": (C.c_int, [vp, vp]),
+        "sph_relax_pass": (C.c_int, [vp, C.c_float, C.POINTER(C.c_float), vp, vp]),
+        "sph_relax_move": (C.c_int, [vp, vp]),
         "sph_profile_enable": (C.c_int, [vp, C.c_int]),
         "sph_profile_read": (C.c_int, [vp, C.c_char_p, C.c_int, C.POINTER(C.c_double),
                                        C.POINTER(C.c_int), C.c_int, C.POINTER(C.c_int)]),

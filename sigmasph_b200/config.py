@@ -128,6 +128,9 @@ REGISTRY = [
     ("L_EIG_TOL_LAM", ("Shifting",), "lEigTolLam", "float", 0.02),
     ("PST_GRIP_HOLD", ("Shifting",), "gripHold", "float", 0.0),
     ("PST_RELAX_STEPS", ("Shifting",), "initialRelaxation", "int", 0),
+    ("PST_RELAX_TOL", ("Shifting",), "initialRelaxationTolerance", "float", 0.03),
+    ("exportRelaxationNetcdf", ("Output",), "relaxationNetcdf", "bool", False),
+    ("exportRelaxationInterval", ("Output",), "relaxationInterval", "int", 1),
     ("HOURGLASS_ALPHA", ("Hourglass",), "alpha", "float", 0.0),
     ("HOURGLASS_FORM", ("Hourglass",), "form", "str", "rate"),
     ("HOURGLASS_STS_MODE", ("Hourglass", "superTimeStepping"), "mode", "str", "subcycle"),
@@ -154,8 +157,8 @@ UNSUPPORTED = {
 # Cards the format knows, and those whose content is accepted but not read here
 # (output switches of the reference's driver, which this package does not replace).
 KNOWN_CARDS = {"Domain", "Time", "Solver", "Materials", "Load", "Diffusion", "Shifting",
-               "Hourglass", "Output", "FluidBlocks", "SolidBlocks", "Constraints"}
-OUT_OF_SCOPE_CARDS = {"Burn", "Detonators", "VelocityLimit", "Erosion", "ParticlesFile"}
+               "Hourglass", "Output", "FluidBlocks", "SolidBlocks", "Constraints", "ParticlesFile"}
+OUT_OF_SCOPE_CARDS = {"Burn", "Detonators", "VelocityLimit", "Erosion"}
 
 
 def _coerce(kind, value, path):
@@ -236,15 +239,12 @@ class SimConfig:
             errors.append("Shifting.surfaceShift must be 'tangential' or 'none'")
         if float(resolved.get("PST_GRIP_HOLD") or 0.0) > 0.0:
             errors.append("Shifting.gripHold is not implemented by sigmasph_b200")
-        if int(resolved.get("PST_RELAX_STEPS") or 0) > 0:
-            errors.append("Shifting.initialRelaxation needs a ParticlesFile deck, which is not "
-                          "implemented by sigmasph_b200")
         if float(resolved.get("dampingCoefficient") or 0.0) != 0.0:
             errors.append("Solver.dampingCoefficient is not implemented by sigmasph_b200")
         if resolved.get("simulationMethod") == "deltaPlusSPH":
             if len(self.materials) > 1:
                 errors.append("a deltaPlusSPH deck has exactly one material")
-        self._check_blocks(raw, errors)
+        self._check_blocks(raw, errors, has_particles_file="ParticlesFile" in raw)
         if errors:
             raise SceneError("%s: %d problem%s in the scene file:\n  - %s" % (
                 os.path.basename(str(scene_file_path)), len(errors),
@@ -253,6 +253,15 @@ class SimConfig:
         for section in ("FluidBlocks", "SolidBlocks", "Constraints"):
             if section in raw:
                 self.config[section] = raw[section]
+        if "ParticlesFile" in raw:
+            # a relative path is taken from the working directory, as the reference does,
+            # else from the scene file's directory
+            pf = str(raw["ParticlesFile"])
+            if (not os.path.isabs(pf) and not os.path.exists(pf) and isinstance(scene_file_path, str)):
+                alt = os.path.join(os.path.dirname(os.path.abspath(scene_file_path)), pf)
+                if os.path.exists(alt):
+                    pf = alt
+            resolved["ParticlesFile"] = pf
 
     # ------------------------------------------------------------------ reading
     def _read_cards(self, raw, errors):
@@ -286,6 +295,12 @@ class SimConfig:
                 errors.append(f"{card}: expected an object")
                 continue
             walk(node, (card,))
+        # Output is the reference driver's card; only the relaxation dump's two switches
+        # (params.py:1245-1263) are read here, the rest is accepted as written
+        out = raw.get("Output") or {}
+        if isinstance(out, dict):
+            given["exportRelaxationNetcdf"] = bool(out.get("relaxationNetcdf", False))
+            given["exportRelaxationInterval"] = int(out.get("relaxationInterval", 1) or 1)
         # the presence of Hourglass.superTimeStepping is the switch (params.py:1330)
         hg = raw.get("Hourglass") or {}
         given["HOURGLASS_STS"] = bool(isinstance(hg, dict) and "superTimeStepping" in hg)
@@ -307,11 +322,13 @@ class SimConfig:
             mats[m.name] = m
         return mats
 
-    def _check_blocks(self, raw, errors):
+    def _check_blocks(self, raw, errors, has_particles_file=False):
         names = set(self.materials)
+        # a ParticlesFile deck's blocks only name the objects (no extents to lay)
+        required = ("objectId",) if has_particles_file else ("objectId", "start", "end")
         for section in ("FluidBlocks", "SolidBlocks"):
             for b in raw.get(section) or []:
-                for req in ("objectId", "start", "end"):
+                for req in required:
                     if req not in b:
                         errors.append(f"{section}: block without {req!r}")
                 mat = b.get("material")

@@ -720,6 +720,40 @@ extern "C" int sph_shift_pairs(SphHandle* h, float disp_bound, int32_t* pi, int3
     return r;
 }
 
+extern "C" int sph_relax_pass(SphHandle* h, float beta, float* residual, float* residual_each,
+                              void* stream) {
+    if (!h || !residual || !(beta >= 0.0f)) return SPH_ERR_ARG;
+    if (!h->bound) return SPH_ERR_NOT_BOUND;
+    cudaStream_t st = S(stream);
+    *residual = 0.0f;
+    if (h->n == 0) return SPH_OK;
+    if (int r = apply_force(h, st)) return r;
+    const int nb = blocks_for(h->n);
+    if (int r = rebuild(h, st)) return r;
+    Ptr P = make_ptr(h);
+    const Cst& c = h->c;
+    k_lam<<<nb, kBlock, 0, st>>>(c, P);
+    if (!h->p.pst_normal_eigvec) k_relax_lamgrad<<<nb, kBlock, 0, st>>>(c, P);
+    CK(cudaMemsetAsync(&h->ac->relax_max_bits, 0, sizeof(unsigned int), st));
+    k_relax<<<nb, kBlock, 0, st>>>(c, P, beta, residual_each);
+    unsigned int bits = 0u;
+    CK(cudaMemcpyAsync(&bits, &h->ac->relax_max_bits, sizeof(unsigned int), cudaMemcpyDeviceToHost, st));
+    CK(cudaStreamSynchronize(st));
+    std::memcpy(residual, &bits, sizeof(float));
+    CK(cudaGetLastError());
+    return SPH_OK;
+}
+
+extern "C" int sph_relax_move(SphHandle* h, void* stream) {
+    if (!h) return SPH_ERR_ARG;
+    if (!h->bound) return SPH_ERR_NOT_BOUND;
+    if (h->n == 0) return SPH_OK;
+    cudaStream_t st = S(stream);
+    k_relax_move<<<blocks_for(h->n), kBlock, 0, st>>>(h->c, make_ptr(h));
+    CK(cudaGetLastError());
+    return SPH_OK;
+}
+
 extern "C" int sph_list_stats(SphHandle* h, uint64_t* out, int reset, void* stream) {
     if (!h || !out) return SPH_ERR_ARG;
     cudaStream_t st = S(stream);

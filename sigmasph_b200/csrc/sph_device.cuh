@@ -81,6 +81,7 @@ struct DevAccum {
     int off_grid_build;          // off-grid count at the last build
     unsigned int ovf_used;       // overflow-pool entries taken this step
     unsigned int near_m_bits;    // margin M of this step's near lists (0: none)
+    unsigned int relax_max_bits; // the initial relaxation's residual (float bits)
     double hg_power;         // sum_i mw_i de_hg_i of the in-loop damper (solid)
     unsigned long long n_steps, n_builds, n_shift_search;   // list statistics
 };

@@ -428,6 +428,59 @@ __device__ __forceinline__ void for_each_pst_neighbour(const Cst& c, const Ptr& 
     });
 }
 
+// The disorder sum's pair term (pst_pair, DSPH.py:725-769): (1 + R (W / W(dx0))^n) grad W,
+// weighted by V_j (Colle) or m_j / mean rho (Sun).
+__device__ __forceinline__ F3 pst_pair_term(const Cst& c, const float4* __restrict__ vel, F3 xi,
+                                            float rho_i, float inv_Wd, int j, int mir, float4 pj) {
+    F3 xj = f3(pj);
+    if (mir) xj = mirror3(mir, xj);
+    F3 r = xi - xj;
+    float rn;
+    F3 g = wendland_dW2(r, dot3(r, r), rn, c);
+    float Wij = wendland_W(rn, c);
+    float f = 0.0f;
+    if (c.W_dx0 > 1e-10f) f = c.p.pst_R * ipow_or_pow(Wij * inv_Wd, c.p.pst_n);
+    if (c.p.pst_colle) {
+        float Vj = w_of(pj, c);
+        if (Vj > 1e-30f) return ((1.0f + f) * Vj) * g;
+    } else {
+        float mj_raw = __ldg(&vel[j].w);
+        float mj = mw_of(mj_raw, pj, c);
+        if (mj > 1e-10f) {
+            float rho_j = mj_raw / pj.w;
+            float ra = 0.5f * (rho_i + rho_j);
+            if (ra > 1e-10f) return ((1.0f + f) * (mj / ra)) * g;
+        }
+    }
+    return {0.0f, 0.0f, 0.0f};
+}
+
+// pst_constrain (DSPH.py:888-941): no shift, or only its tangential part (against the
+// lambda gradient or the smallest eigenvector), near the free surface; the plane-strain
+// z; no shift of a gripped solid particle.
+__device__ __forceinline__ F3 pst_constrain(const Cst& c, const Ptr& P, int i, F3 dr) {
+    float li = P.lam[i];
+    bool surf = li < c.p.pst_lambda_hi;
+    if (c.p.pst_surface_none) {
+        if (surf) dr = {0, 0, 0};
+    } else if (surf) {
+        if (li < c.p.pst_lambda_lo) dr = {0, 0, 0};
+        else {
+            F3 ns = f3(P.lgrad[i]);
+            if (c.p.two_d) ns.z = 0.0f;
+            float nn = norm3(ns);
+            if (nn > 1e-10f) {
+                F3 nh = {ns.x / nn, ns.y / nn, ns.z / nn};
+                float dd = dot3(dr, nh);
+                dr = dr - dd * nh;
+            }
+        }
+    }
+    if (c.p.two_d) dr.z = 0.0f;
+    if (c.p.is_solid && P.cur.bc[2 * i] != 0) dr = {0, 0, 0};
+    return dr;
+}
+
 __global__ void SPH_BOUNDS(SPH_OCC_PST) k_pst(Cst c, Ptr P) {
     int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i == 0) {   // steps whose shift could not use the candidate lists
@@ -444,31 +497,10 @@ __global__ void SPH_BOUNDS(SPH_OCC_PST) k_pst(Cst c, Ptr P) {
     const float m_i = __ldg(&vel[i].w);
     const float rho_i = m_i / pi.w;
     {
-        const float Wd = c.W_dx0;
-        const float inv_Wd = Wd > 0.0f ? 1.0f / Wd : 0.0f;
-        auto pair = [&](int j, int mir, float4 pj) {
-            F3 xj = f3(pj);
-            if (mir) xj = mirror3(mir, xj);
-            F3 r = xi - xj;
-            float rn;
-            F3 g = wendland_dW2(r, dot3(r, r), rn, c);
-            float Wij = wendland_W(rn, c);
-            float f = 0.0f;
-            if (Wd > 1e-10f) f = c.p.pst_R * ipow_or_pow(Wij * inv_Wd, c.p.pst_n);
-            if (c.p.pst_colle) {
-                float Vj = w_of(pj, c);
-                if (Vj > 1e-30f) sr += ((1.0f + f) * Vj) * g;
-            } else {
-                float mj_raw = __ldg(&vel[j].w);
-                float mj = mw_of(mj_raw, pj, c);
-                if (mj > 1e-10f) {
-                    float rho_j = mj_raw / pj.w;
-                    float ra = 0.5f * (rho_i + rho_j);
-                    if (ra > 1e-10f) sr += ((1.0f + f) * (mj / ra)) * g;
-                }
-            }
-        };
-        for_each_pst_neighbour(c, P, i, xi, pair);
+        const float inv_Wd = c.W_dx0 > 0.0f ? 1.0f / c.W_dx0 : 0.0f;
+        for_each_pst_neighbour(c, P, i, xi, [&](int j, int mir, float4 pj) {
+            sr += pst_pair_term(c, vel, xi, rho_i, inv_Wd, j, mir, pj);
+        });
     }
     float4 vi4 = vel[i];
     F3 vi = f3(vi4);
@@ -503,30 +535,83 @@ __global__ void SPH_BOUNDS(SPH_OCC_PST) k_pst(Cst c, Ptr P) {
         float dn = norm3(dr);
         if (dn > c.max_shift) dr = (c.max_shift / dn) * dr;
     }
-    // pst_constrain (DSPH.py:888-941)
-    float li = P.lam[i];
-    bool surf = li < c.p.pst_lambda_hi;
-    if (c.p.pst_surface_none) {
-        if (surf) dr = {0, 0, 0};
-    } else if (surf) {
-        if (li < c.p.pst_lambda_lo) dr = {0, 0, 0};
-        else {
-            F3 ns = f3(P.lgrad[i]);
-            if (c.p.two_d) ns.z = 0.0f;
-            float nn = norm3(ns);
-            if (nn > 1e-10f) {
-                F3 nh = {ns.x / nn, ns.y / nn, ns.z / nn};
-                float dd = dot3(dr, nh);
-                dr = dr - dd * nh;
-            }
-        }
-    }
-    if (c.p.two_d) dr.z = 0.0f;
-    if (c.p.is_solid && P.cur.bc[2 * i] != 0) dr = {0, 0, 0};
+    dr = pst_constrain(c, P, i, dr);
     float4* shf = as4(P.cur.shift);
     float4 s = shf[i];
     s.x = dr.x; s.y = dr.y; s.z = dr.z;
     shf[i] = s;
+}
+
+// ------------------------------------------------------------------ initial relaxation
+// relax_initial_configuration (DSPH.py:1113-1179): with the bins fresh, the drive
+// g_i = pst_constrain(-h^2 S_i) from the run's own disorder sum; the residual is
+// max |g_i| / dx0; the particle's step is beta g_i, capped at maxShift dx0, parked in the
+// shift record until k_relax_move applies it.  Volume and mass are held.
+
+// compute_lam's gradient pass alone (DSPH.py:591-609): grad lambda = sum V_j (lambda_j -
+// lambda_i) L_i grad W, for the constraint's surface normal.
+__global__ void __launch_bounds__(kBlock) k_relax_lamgrad(Cst c, Ptr P) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= c.n) return;
+    const float4* __restrict__ pos = as4c(P.cur.pos);
+    const F3 xi = f3(pos[i]);
+    const float4 l0 = P.lsym[2 * i], l1 = P.lsym[2 * i + 1];
+    const float L00 = l0.x, L11 = l0.y, L22 = l0.z, L01 = l0.w, L02 = l1.x, L12 = l1.y;
+    const float lam_i = P.lam[i];
+    F3 lg = {0, 0, 0};
+    for_each_neighbour(c, P, i, [&](int j, int mir) {
+        float4 pj = __ldg(pos + j);
+        F3 xj = f3(pj);
+        if (mir) xj = mirror3(mir, xj);
+        F3 r = xi - xj;
+        float rn;
+        F3 g = wendland_dW2(r, dot3(r, r), rn, c);
+        float ld = __ldg(P.lam + j) - lam_i;
+        F3 Lg = {L00 * g.x + L01 * g.y + L02 * g.z, L01 * g.x + L11 * g.y + L12 * g.z,
+                 L02 * g.x + L12 * g.y + L22 * g.z};
+        lg += (w_of(pj, c) * ld) * Lg;
+    });
+    if (c.p.two_d) lg.z = 0.0f;
+    P.lgrad[i] = make_float4(lg.x, lg.y, lg.z, 0.0f);
+}
+
+__global__ void __launch_bounds__(kBlock) k_relax(Cst c, Ptr P, float beta, float* res_each) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    float res = 0.0f;
+    if (i < c.n) {
+        const float4* __restrict__ pos = as4c(P.cur.pos);
+        const float4* __restrict__ vel = as4c(P.cur.vel);
+        const float4 pi = pos[i];
+        const F3 xi = f3(pi);
+        const float rho_i = __ldg(&vel[i].w) / pi.w;
+        const float inv_Wd = c.W_dx0 > 0.0f ? 1.0f / c.W_dx0 : 0.0f;
+        F3 S = {0, 0, 0};
+        for_each_neighbour(c, P, i, [&](int j, int mir) {
+            S += pst_pair_term(c, vel, xi, rho_i, inv_Wd, j, mir, __ldg(pos + j));
+        });
+        const F3 g = pst_constrain(c, P, i, (-(c.h * c.h)) * S);
+        const float gn = norm3(g);
+        res = gn / c.p.particle_diameter;
+        if (res_each) res_each[i] = res;
+        F3 dr = beta * g;
+        const float dn = norm3(dr);
+        if (dn > c.max_shift) dr = (c.max_shift / dn) * dr;
+        float4* shf = as4(P.cur.shift);
+        float4 s = shf[i];
+        s.x = dr.x; s.y = dr.y; s.z = dr.z;
+        shf[i] = s;
+    }
+    block_max_atomic(res, &P.ac->relax_max_bits);
+}
+
+__global__ void __launch_bounds__(kBlock) k_relax_move(Cst c, Ptr P) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= c.n) return;
+    float4* pos = as4(P.cur.pos);
+    const float4 s = as4c(P.cur.shift)[i];
+    float4 p = pos[i];
+    p.x += s.x; p.y += s.y; p.z += s.z;
+    pos[i] = p;
 }
 
 // ------------------------------------------------------------------ displace + SPHBase.step boundary

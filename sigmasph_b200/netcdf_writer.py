@@ -193,3 +193,31 @@ class NetCDFTrajectoryWriter:
         if self._f is not None:
             self._f.close()
             self._f = None
+
+
+def attach_relaxation_writer(ps, solver, path, interval=1):
+    """Output.relaxationNetcdf (run_simulation.py:686-713, params.py:1245-1263): a second
+    trajectory of the initial relaxation's passes.  Installs the solver's relax_frame_hook;
+    frame k holds the body after k passes with lam and `relax_residual` (each particle's
+    h^2 |S| / dx0) computed there, `time` is the pass number, every `interval`-th pass and
+    the last are written, and rows follow the laid positions (x_0 until the relaxation
+    ends) so a row is the same particle in every frame.  Call before solver.initialize();
+    close the returned writer afterwards."""
+    writer = NetCDFTrajectoryWriter(path, ps.domain_size, ps.is_solid, ps.two_d,
+                                    extra_fields=[("relax_residual", "relax_residual")])
+    interval = max(1, int(interval or 1))
+
+    def relax_frame(k, residual, final):
+        if k % interval and not final:
+            return
+        obj = ps.dump()
+        mask = (ps.object_id.to_numpy() >= 0).nonzero()
+        obj["relax_residual"] = solver.relax_res.to_numpy()[mask]
+        order = np.lexsort(ps.x_0.to_numpy()[mask].T[::-1])
+        n = len(order)
+        obj = {key: (a[order] if isinstance(a, np.ndarray) and a.shape[:1] == (n,) else a)
+               for key, a in obj.items()}
+        writer.write(obj, k)
+
+    solver.relax_frame_hook = relax_frame
+    return writer

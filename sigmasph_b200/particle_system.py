@@ -177,6 +177,10 @@ class ParticleSystem:
         xs, vs, rhos, mats, cols, objs, eos_ids = [], [], [], [], [], [], []
         mat_index = {name: m.index for name, m in c.get_materials().items()}
         self.object_collection = {}
+        pfile = c.get_cfg("ParticlesFile")
+        if pfile:
+            self._particles_from_file(pfile, blocks, mat_index, xs, vs, rhos, mats, cols, objs, eos_ids)
+            blocks = []
         for blk, mtag in blocks:
             for key in ("rotVelocity", "divVelocity"):
                 if blk.get(key) is not None:
@@ -320,6 +324,38 @@ class ParticleSystem:
         self._solver = None
 
     # ------------------------------------------------------------------ internals
+    def _particles_from_file(self, path, blocks, mat_index, xs, vs, rhos, mats, cols, objs, eos_ids):
+        """_load_particles_from_file (particle_system.py:728-854): the file's particles,
+        grouped by object id in ascending order; an object's material type, colour and
+        material row come from the block of that objectId, an object without one is laid
+        as solid with a grey of its id."""
+        from .particles_file import read_particles_file, ParticlesFileError
+        try:
+            data = read_particles_file(path, self.two_d)
+        except ParticlesFileError as e:
+            raise SceneError(str(e))
+        if data["size"] is not None and not np.allclose(data["size"], self.V0, rtol=1e-5, atol=0.0):
+            raise SceneError(f"ParticlesFile '{path}' gives particles their own sizes: the variable "
+                             f"smoothing length that needs is not implemented by sigmasph_b200")
+        by_id = {int(b["objectId"]): (b, m) for b, m in blocks}
+        oid = data["object_id"]
+        for obj in sorted(np.unique(oid).tolist()):
+            mask = oid == obj
+            n_b = int(mask.sum())
+            blk, mtag = by_id.get(obj, (None, self.material_solid))
+            color = blk["color"] if blk is not None else [100 + obj * 50] * 3
+            entry = {"objectId": obj, "particleNum": n_b}
+            if blk is not None and blk.get("material") is not None:
+                entry["material"] = blk["material"]
+            self.object_collection[obj] = entry
+            xs.append(data["position"][mask])
+            vs.append(data["velocity"][mask])
+            rhos.append(data["density"][mask])
+            mats.append(np.full(n_b, mtag, dtype=np.int32))
+            cols.append(np.tile(np.asarray(color, dtype=np.int32), (n_b, 1)))
+            objs.append(np.full(n_b, obj, dtype=np.int32))
+            eos_ids.append(np.full(n_b, mat_index.get(entry.get("material"), 0), dtype=np.int32))
+
     def _tensor(self, key):
         if key in self._derived:
             return self._derived[key]

@@ -86,6 +86,20 @@ def build_params(ps) -> abi.SphParams:
     return p
 
 
+class ResidualField:
+    """relax_res (DSPH.py:1097-1100): each particle's relaxation residual |g| / dx0 from
+    the latest pass, in the current storage order, one float per particle slot."""
+
+    def __init__(self, n, device):
+        self.t = torch.zeros(n, dtype=torch.float32, device=device)
+
+    def data_ptr(self):
+        return self.t.data_ptr()
+
+    def to_numpy(self):
+        return self.t.cpu().numpy()
+
+
 class _SolverBase:
     """SPHBase + the shared half of DSPHSolver (sph_base.py, DSPH.py)."""
 
@@ -116,6 +130,8 @@ class _SolverBase:
             self._set_dt(float(user_dt))
         self.dt_max = float(self._get_dt())
         self.lam = ps.lam
+        self.relax_frame_hook = None
+        self.relax_res = None
         from .particle_system import Field
         self.lam_grad = Field(ps, "lgrad", slice(0, 3))
         self.L_sym = Field(ps, "lsym", slice(0, 6))
@@ -168,8 +184,67 @@ class _SolverBase:
         abi.check(self.L.sph_initialize(self.h, _stream_ptr()), "sph_initialize")
 
     def initialize(self):
-        """SPHBase.initialize (sph_base.py:154): the first neighbour build."""
+        """SPHBase.initialize (sph_base.py:154): the first neighbour build; then, with the
+        shift on and Shifting.initialRelaxation > 0, the initial relaxation
+        (DSPH.py:1060-1063)."""
         self._initialize_grid()
+        self.relax_report = None
+        steps = int(self.ps.cfg.get_cfg("PST_RELAX_STEPS") or 0)
+        if steps > 0 and bool(self.ps.cfg.get_cfg("PST_ENABLED")):
+            tol = self.ps.cfg.get_cfg("PST_RELAX_TOL")
+            self.relax_report = self.relax_initial_configuration(steps, 0.03 if tol is None else float(tol))
+
+    def relax_initial_configuration(self, steps, tol, beta=0.05):
+        """relax_initial_configuration (DSPH.py:1113-1179): before t = 0, move the frozen
+        body by the run's own shift drive -- disorder sum, free-surface treatment, gripped
+        particles held -- until the residual max h^2 |S| / dx0 falls below `tol` or for
+        `steps` passes, each particle keeping its volume and mass; the relaxed positions
+        become x_0, the displacement and the stored shift are cleared.  Returns {passes,
+        residual_first, residual_last, converged, moved_max, moved_mean} (moves in units of
+        the spacing).
+
+        relax_frame_hook (DSPH.py:217-221), when set, is called as hook(k, residual, final)
+        with the body at the positions of pass k (k = 0 the laid positions) and lam and
+        relax_res (each particle's |g| / dx0, storage order) computed there: before every
+        move, and once more at the relaxed positions with final=True."""
+        ps = self.ps
+        pid0 = ps.pid.to_numpy()
+        x_start = ps.x.to_numpy()[np.argsort(pid0)].astype(np.float64)
+        res = C.c_float()
+        hook = self.relax_frame_hook
+        each = None
+        if hook is not None:
+            self.relax_res = ResidualField(ps.particle_max_num, ps.device)
+            each = self.relax_res.data_ptr()
+
+        def one_pass():
+            abi.check(self.L.sph_relax_pass(self.h, float(beta), C.byref(res), each,
+                                            _stream_ptr()), "sph_relax_pass")
+            return float(res.value)
+
+        first = last = 0.0
+        k = 0
+        for k in range(1, int(steps) + 1):
+            last = one_pass()
+            if hook is not None:
+                hook(k - 1, last, False)
+            abi.check(self.L.sph_relax_move(self.h, _stream_ptr()), "sph_relax_move")
+            if k == 1:
+                first = last
+            if last < tol:
+                break
+        if hook is not None:
+            hook(k, one_pass(), True)
+        ps.pst_shift.fill(0.0)
+        self._initialize_grid()
+        x = ps.x.to_numpy()
+        moved = np.linalg.norm(x[np.argsort(ps.pid.to_numpy())].astype(np.float64) - x_start,
+                               axis=1) / ps.particle_diameter
+        ps.x_0.copy_from(ps.x)
+        ps.u.fill(0.0)
+        return {"passes": k, "residual_first": first, "residual_last": last,
+                "converged": bool(last < tol), "moved_max": float(moved.max()),
+                "moved_mean": float(moved.mean())}
 
     def step(self):
         """SPHBase.step (sph_base.py:622-655): one asynchronous step."""

@@ -90,3 +90,19 @@ def test_unknown_and_unimplemented_keys_are_rejected():
 def test_comments_are_stripped():
     from sigmasph_b200.config import strip_json_comments
     assert json.loads(strip_json_comments('{"a": "x#y", # c\n "b": 2 // d\n}')) == {"a": "x#y", "b": 2}
+
+
+def test_relaxation_switches():
+    """Shifting.initialRelaxation / initialRelaxationTolerance and the relaxation dump's
+    Output switches resolve to the reference's names and defaults (params.py:1038-1052,
+    :1245-1263)."""
+    from sigmasph_b200.scenes import dambreak3d
+    sc = dambreak3d(dx=0.05)
+    cfg = SimConfig(sc)
+    assert (cfg.get_cfg("PST_RELAX_STEPS"), cfg.get_cfg("PST_RELAX_TOL")) == (0, 0.03)
+    assert (cfg.get_cfg("exportRelaxationNetcdf"), cfg.get_cfg("exportRelaxationInterval")) == (False, 1)
+    sc["Shifting"].update({"initialRelaxation": 40, "initialRelaxationTolerance": 0.01})
+    sc["Output"] = {"relaxationNetcdf": True, "relaxationInterval": 5, "netcdf": True}
+    cfg = SimConfig(sc)
+    assert (cfg.get_cfg("PST_RELAX_STEPS"), cfg.get_cfg("PST_RELAX_TOL")) == (40, 0.01)
+    assert (cfg.get_cfg("exportRelaxationNetcdf"), cfg.get_cfg("exportRelaxationInterval")) == (True, 5)

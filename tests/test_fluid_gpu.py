@@ -10,6 +10,8 @@ Tolerances (float32 arithmetic on both sides, different summation order):
   * after several steps the GPU's distance to the float64 oracle stays within 4x the
     float32 oracle's own distance to it (plus a small floor).
 """
+import ctypes as C
+
 import numpy as np
 import pytest
 import torch
@@ -158,6 +160,116 @@ def test_shift_pairs_after_a_real_step(cuda, kick):
     A = pair_set(*solver.shift_pairs(), pid)
     B = pair_set(*solver.pairs(1), pid)
     assert A == B
+
+
+def _jittered(sc, amp=0.15, seed=8):
+    """The scene's particle system with every particle moved off the lattice (so that the
+    shift has something to relax)."""
+    cfg = SimConfig(sc)
+    ps = ParticleSystem(cfg, device="cuda")
+    x = ps.x.to_numpy()
+    x += (np.random.default_rng(seed).uniform(-amp, amp, x.shape) * ps.particle_diameter).astype(np.float32)
+    ps.x.from_numpy(x.astype(np.float32))
+    ps.resync_displacement()
+    return ps
+
+
+def test_relaxation_pass_is_the_shift_drive(cuda):
+    """One pass of the initial relaxation (DSPH.py:1083-1111) against the oracle's own
+    shift: in Sun form at a fixed Mach number with no cap binding, the oracle's shift from
+    the same positions is -CFL Ma h^2 S after the free-surface constraint, and the pass
+    leaves beta times the constrained -h^2 S."""
+    sc = small_scene(5000)
+    sc["Shifting"].update({"mode": "sun", "maMode": "fixed", "maFixed": 0.1, "maxShift": 10.0})
+    ps = _jittered(sc)
+    solver = ps.build_solver()
+    orc = Oracle(build_params(ps), ps.particle_max_num, fp64=False)
+    orc.set_state(state_from_sets(ps.state_numpy()), solver.dt[None])
+    solver._initialize_grid()
+    res = C.c_float()
+    each = torch.full((ps.particle_max_num,), -1.0, dtype=torch.float32, device="cuda")
+    abi.check(solver.L.sph_relax_pass(solver.h, 0.05, C.byref(res), each.data_ptr(), None))
+    torch.cuda.synchronize()
+    g = gpu_fields(ps)["pst_shift"]
+    each = each.cpu().numpy()[np.argsort(ps.pid.to_numpy())]
+    for st_ in (abi.STAGE_SORT, abi.STAGE_LAM, abi.STAGE_PST):
+        orc.stage(st_)
+    want = oracle_fields(orc)["pst_shift"] * (0.05 / (float(ps.cfg.get_cfg("CFL")) * 0.1))
+    e = np.abs(g - want).max() / np.abs(want).max()
+    assert e <= 2e-5, e
+    h = float(ps.support_radius)
+    drive = np.linalg.norm(want, axis=1) / 0.05 / ps.particle_diameter
+    assert res.value == pytest.approx(drive.max(), rel=1e-4)
+    assert res.value == each.max()
+    assert np.abs(each - drive).max() <= 1e-4 * drive.max()
+
+
+@pytest.mark.parametrize("surface", ["none", "tangential"])
+def test_initial_relaxation_settles_the_body(cuda, surface):
+    """Shifting.initialRelaxation on a disordered block with free surfaces: the residual
+    (max h^2 |S| / dx0) falls several-fold over the passes (the drive of a pass is pinned to
+    the oracle above; near a free surface the kernel's truncation keeps a drive on the
+    layer just inside it, which sets the maximum).  The relaxed positions become x_0, the
+    displacement and the stored shift are cleared, and volume and mass are untouched."""
+    sc = small_scene(5000)
+    sc["Shifting"].update({"initialRelaxation": 300, "initialRelaxationTolerance": 0.03,
+                           "surfaceShift": surface})
+    ps = _jittered(sc, amp=0.1)
+    V0, m0 = ps.V.to_numpy().sum(dtype=np.float64), ps.m.to_numpy().sum(dtype=np.float64)
+    solver = ps.build_solver()
+    frames = []
+    solver.relax_frame_hook = lambda k, r, final: frames.append(
+        (k, r, final, solver.relax_res.to_numpy().max()))
+    solver.initialize()
+    rep = solver.relax_report
+    assert rep["passes"] >= 2 and rep["residual_last"] < 0.75 * rep["residual_first"], rep
+    assert rep["moved_max"] > 0.0
+    # the hook: passes 0 .. passes-1 before their moves, then the relaxed positions
+    assert [f[0] for f in frames] == list(range(rep["passes"] + 1))
+    assert [f[2] for f in frames] == [False] * rep["passes"] + [True]
+    assert frames[0][1] == rep["residual_first"] and frames[-2][1] == rep["residual_last"]
+    assert all(r == m for _, r, _, m in frames)
+    assert np.array_equal(ps.x_0.to_numpy(), ps.x.to_numpy())
+    assert not np.any(ps.u.to_numpy()) and not np.any(ps.pst_shift.to_numpy())
+    assert ps.V.to_numpy().sum(dtype=np.float64) == pytest.approx(V0, rel=1e-6)
+    assert ps.m.to_numpy().sum(dtype=np.float64) == m0
+    solver.step_many(4)
+    assert solver.error_word() & ~abi.EW_HASHED_GRID == 0
+
+
+def test_relaxation_trajectory(cuda, tmp_path):
+    """Output.relaxationNetcdf: frame k is the body after k passes (every second pass here,
+    and the last), rows in the laid order, relax_residual's maximum the pass's residual;
+    frame 0 is the body as laid and the last frame the body the run starts from."""
+    from scipy.io import netcdf_file
+    from sigmasph_b200.netcdf_writer import attach_relaxation_writer
+    sc = small_scene(3000)
+    sc["Shifting"].update({"initialRelaxation": 5, "initialRelaxationTolerance": 1e-6})
+    ps = _jittered(sc, amp=0.1)
+    laid = ps.x.to_numpy()
+    laid = laid[np.lexsort(ps.x_0.to_numpy().T[::-1])]
+    solver = ps.build_solver()
+    path = str(tmp_path / "relax.nc")
+    w = attach_relaxation_writer(ps, solver, path, interval=2)
+    seen = []
+    inner = solver.relax_frame_hook
+    solver.relax_frame_hook = lambda k, r, f: (seen.append(r), inner(k, r, f))
+    solver.initialize()
+    w.close()
+    rep = solver.relax_report
+    assert rep["passes"] == 5
+    x_end = ps.x.to_numpy()
+    with netcdf_file(path, "r", mmap=False) as f:
+        v = f.variables
+        assert list(v["time"][:]) == [0.0, 2.0, 4.0, 5.0]
+        assert np.array_equal(v["coordinates"][0], laid)
+        assert not np.array_equal(v["coordinates"][3], laid)
+        def rows(a):
+            a = np.asarray(a, dtype=np.float32)
+            return a[np.lexsort(a.T[::-1])]
+        assert np.array_equal(rows(v["coordinates"][3]), rows(x_end))
+        for fr, k in enumerate((0, 2, 4, 5)):
+            assert v["relax_residual"][fr].max() == np.float32(seen[k])
 
 
 def _oracle_pairs_at(ps, solver):
