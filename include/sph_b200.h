@@ -150,7 +150,13 @@ typedef struct SphParams {
     int32_t jc_surrogate;         /* 1: MLP return map with Newton fallback             */
     float   jc_surrogate_tol;     /* |f_yield| / sigma_y acceptance (1e-3)              */
     int32_t hg_sts_fixed;         /* > 0: that many damper sub-steps, else automatic    */
-    int32_t reserved[8];
+    /* --- the solid's in-loop viscosities (SOLID.py:640-716) --- */
+    float   q_l2;                 /* VNR bulk viscosity C_Q l^2 (0: off)                */
+    float   q_cl;                 /* C_Q l, for the viscosity's own CFL limit           */
+    float   av_alpha;             /* Monaghan pair viscosity alpha (0 with beta: off)   */
+    float   av_beta;
+    float   av_eps;               /* mu_ij regulariser epsilon (0.01)                   */
+    int32_t reserved[3];
 } SphParams;
 
 /* ------------------------------------------------------------------ buffers */
@@ -397,7 +403,9 @@ int  sph_jc_stats(SphHandle* h, uint64_t* out, int reset, void* stream);
  * mat[k] and inst[k] are instance k's material row and constants (host arrays, copied),
  * every particle's material id (bcdisp.w) must be its instance, constraint ids (bc.y)
  * 0 or 1 within the instance; dt0[k] (host) is the first step of instance k.  n_inst = 0
- * returns the handle to single-scene mode. */
+ * returns the handle to single-scene mode.  A handle with the bulk or the Monaghan
+ * viscosity on returns SPH_ERR_UNSUPPORTED (the instances' steps carry no viscosity
+ * limits). */
 int  sph_ensemble_set(SphHandle* h, const SphMatRow* mat, const SphInstRow* inst, int n_inst,
                       const float* dt0, void* stream);
 /* Copies the per-instance state into out[n_inst] (host; synchronises stream). */

@@ -46,6 +46,7 @@ struct Sim {
     // ---- hypoelastic solid (SOLID.py); sorted unless noted
     std::vector<M3<R>> sdev;                    // deviatoric stress (symmetric)
     std::vector<R> eps_p, e_int, temperature, de_int;
+    std::vector<R> q_visc, av_mu_max;           // derived (SOLID.py:1200-1204)
     std::vector<int32_t> bc_flag, bc_id, eos_id;
     std::vector<V3<R>> bc_disp;
     std::vector<M3<R>> grad_v, dsigma;          // derived
@@ -81,6 +82,7 @@ struct Sim {
         if (P.is_solid) {
             sdev.assign(n, M3<R>()); eps_p.assign(n, 0); e_int.assign(n, 0);
             temperature.assign(n, 0); de_int.assign(n, 0);
+            q_visc.assign(n, 0); av_mu_max.assign(n, 0);
             bc_flag.assign(n, 0); bc_id.assign(n, -1); eos_id.assign(n, 0); bc_disp.assign(n, {});
             grad_v.assign(n, M3<R>()); dsigma.assign(n, M3<R>());
             d_eps_p_rate.assign(n, 0); ale_adv.assign(n, 0); ale_diff.assign(n, 0);
@@ -883,6 +885,12 @@ struct Sim {
             wl += (double)(R(0.5) * m[i] * dtl * dtl * (dot(f, f) - gsq));
         }
         leftover_work += wl;
+        // SOLID.py:2182-2207: the explicit damper's and the viscosities' work of the
+        // previous step's force pass, banked with the dt it was done over
+        hg_work += (double)dtl * hg_step_power;
+        hg_step_power = 0;
+        if (P.track_visc_work) visc_work += (double)dtl * visc_step_power;
+        visc_step_power = 0;
     }
     void update_temperature() {
         for (int64_t i = 0; i < n; ++i) {
@@ -912,22 +920,32 @@ struct Sim {
 
     // SOLID.py:3204-3852
     void compute_stress_accelerations() {
+        const bool q_on = P.q_l2 > 0.0f;
+        const bool av_on = P.av_alpha > 0.0f || P.av_beta > 0.0f;
         for (int64_t i = 0; i < n; ++i) {
             acc[i] = {R(P.gravity[0]), R(P.gravity[1]), R(P.gravity[2])};
-            pressure[i] = solid_pressure(i, m[i] / V[i]);
+            const R rho = m[i] / V[i];
+            pressure[i] = solid_pressure(i, rho);
             de_int[i] = 0;
+            // SOLID.py:3393-3401: q from the trace of this step's grad v, compression only
+            q_visc[i] = 0;
+            if (q_on) {
+                R dvv = grad_v[i][0][0] + grad_v[i][1][1] + grad_v[i][2][2];
+                if (dvv < R(0)) q_visc[i] = R(P.q_l2) * rho * dvv * dvv;
+            }
         }
         const R dtl = dt;
         const R visc = R(10.0 * (double)P.viscosity);
         const bool hg_inloop = P.hourglass_alpha > 0.0f && !P.hourglass_sts;
         const bool ale = P.pst_enabled && P.pst_ale_momentum;
-        double hgw = 0;
-#pragma omp parallel for schedule(dynamic, 256) reduction(+ : hgw)
+        double hgw = 0, vw = 0;
+#pragma omp parallel for schedule(dynamic, 256) reduction(+ : hgw, vw)
         for (int64_t i = 0; i < n; ++i) {
             V3<R> dv;
-            R dei = 0, dhg = 0;
+            R dei = 0, dhg = 0, dvisc = 0, mu_max = 0;
             const R rho_i = m[i] / V[i];
             const R mwi = mw(i), wi = w(i);
+            const R ptot_i = pressure[i] + q_visc[i];
             for_all_neighbors(i, [&](int64_t j, int mir) {
                 V3<R> xj = xj_of(j, mir), vj = vj_of(j, mir);
                 M3<R> sj = sdev[j];
@@ -938,7 +956,7 @@ struct Sim {
                 for (int a = 0; a < 3; ++a) {
                     R t = 0;
                     for (int b = 0; b < 3; ++b) {
-                        R sig = (sdev[i][a][b] + sj[a][b]) - ((a == b) ? (pressure[i] + pressure[j]) : R(0));
+                        R sig = (sdev[i][a][b] + sj[a][b]) - ((a == b) ? (ptot_i + (pressure[j] + q_visc[j])) : R(0));
                         t += sig * g[b];
                     }
                     f[a] = wi * w(j) * t;
@@ -951,7 +969,32 @@ struct Sim {
                 R rn = norm(r);
                 V3<R> am = (visc * w(j) * vxy / (rn * rn + eta2)) * g;
                 dv += am;
-                if (P.viscosity > 0.0f) dei += -R(0.5) * dot(am, vij);
+                if (P.viscosity > 0.0f) {
+                    R wm = -R(0.5) * dot(am, vij);
+                    dei += wm;
+                    dvisc += -wm;
+                }
+                // SOLID.py:3727-3766: Monaghan's Pi_ij on approaching pairs
+                if (av_on && vxy < R(0)) {
+                    const R hav = h;
+                    R mu = hav * vxy / (rn * rn + R(P.av_eps) * hav * hav);
+                    R rho_j = m[j] / V[j];
+                    R rho_bar = R(0.5) * (rho_i + rho_j);
+                    R c_bar = R(0.5) * (R(P.mat_cp[eos_id[i]]) + R(P.mat_cp[eos_id[j]]));
+                    R pij = (-R(P.av_alpha) * c_bar * mu + R(P.av_beta) * mu * mu) / rho_bar;
+                    V3<R> ap = (-mw(j) * pij) * g;
+                    R mu_cfl = -mu;
+                    if (P.axisymmetric && P.axi_conservative_x) {
+                        R ratio = R(0.5) * (r_of(i) + r_of(j)) / r_of(i);
+                        ap[0] = ap[0] * ratio;
+                        mu_cfl = mu_cfl * ratio;
+                    }
+                    dv += ap;
+                    mu_max = std::max(mu_max, mu_cfl);
+                    R wp = -R(0.5) * dot(ap, vij);
+                    dei += wp;
+                    dvisc += -wp;
+                }
                 if (hg_inloop && rn > R(1e-9)) {
                     V3<R> rh = {-r[0] / rn, -r[1] / rn, -r[2] / rn};
                     M3<R> gvj = grad_v[j];
@@ -990,11 +1033,42 @@ struct Sim {
             }
             acc[i] += dv;
             de_int[i] = dei;
+            av_mu_max[i] = mu_max;
             hgw += (double)(mwi * dhg);
+            vw += (double)m[i] * (double)dvisc;
         }
         hg_step_power = hgw;
+        visc_step_power = vw;
     }
-    double hg_step_power = 0;
+    double hg_step_power = 0, visc_step_power = 0;
+
+    // SOLID.py:3939-4009: the two viscosities' own CFL limits, after the acoustic one
+    void clamp_dt_viscosities() {
+        const R cfl_h = R((double)P.CFL * (double)P.support_radius);
+        if (P.q_l2 > 0.0f) {
+            R cmax = 0;
+            for (int64_t i = 0; i < n; ++i) {
+                R dvv = grad_v[i][0][0] + grad_v[i][1][1] + grad_v[i][2][2];
+                if (dvv < R(0)) {
+                    R qc = R(P.q_cl) * (-dvv);
+                    R ci = R(P.mat_cp[eos_id[i]]);
+                    cmax = std::max(cmax, qc + std::sqrt(qc * qc + ci * ci));
+                }
+            }
+            if (cmax > R(0)) dt = std::min(dt, cfl_h / cmax);
+        }
+        if (P.av_alpha > 0.0f || P.av_beta > 0.0f) {
+            R cmax = 0;
+            for (int64_t i = 0; i < n; ++i) {
+                R mu = av_mu_max[i];
+                if (mu > R(0)) {
+                    R ci = R(P.mat_cp[eos_id[i]]);
+                    cmax = std::max(cmax, ci + R(1.2) * (R(P.av_alpha) * ci + R(P.av_beta) * mu));
+                }
+            }
+            if (cmax > R(0)) dt = std::min(dt, cfl_h / cmax);
+        }
+    }
 
     // SOLID.py:4241-4309 (the damper operator on the sub-stepped velocity y)
     void compute_hg_accel() {
@@ -1084,11 +1158,11 @@ struct Sim {
     }
     void solid_dt() {
         compute_adaptive_dt();
+        clamp_dt_viscosities();
         const bool hg = P.hourglass_alpha > 0.0f;
         sts_last = 0;
         if (!P.hourglass_sts) {
             if (hg) dt = std::min(dt, R(1.6 / (double)P.hg_rate));
-            hg_work += (double)dt * hg_step_power;
         } else if (hg) {
             int s = 1;
             if (P.hg_rate > 0.0f) {

@@ -71,7 +71,8 @@ PARAM_FIELDS = [
     ("hg_sts_refresh", _i32), ("ale_history", _i32), ("transport_e", _i32),
     ("ale_diffusion", _f32), ("num_constraints", _i32), ("ramp_time", _f32),
     ("jc_surrogate", _i32), ("jc_surrogate_tol", _f32), ("hg_sts_fixed", _i32),
-    ("reserved", _i32 * 8),
+    ("q_l2", _f32), ("q_cl", _f32), ("av_alpha", _f32), ("av_beta", _f32), ("av_eps", _f32),
+    ("reserved", _i32 * 3),
 ]
 
 

@@ -100,6 +100,11 @@ REGISTRY = [
     ("allowNegativePressure", ("Solver",), "allowNegativePressure", "bool", False),
     ("DISPLACEMENT_POSITIONS", ("Solver",), "displacementPositions", "bool", True),
     ("COMPENSATED_VOLUME", ("Solver",), "compensatedVolume", "bool", True),
+    ("BULK_VISCOSITY_Q", ("Solver", "bulkViscosity"), "quadratic", "float", 0.0),
+    ("BULK_VISCOSITY_LENGTH", ("Solver", "bulkViscosity"), "lengthScale", "str", "dx0"),
+    ("MONAGHAN_ALPHA", ("Solver", "artificialViscosity"), "alpha", "float", 0.0),
+    ("MONAGHAN_BETA", ("Solver", "artificialViscosity"), "beta", "float", 0.0),
+    ("MONAGHAN_EPS", ("Solver", "artificialViscosity"), "epsilon", "float", 0.01),
     ("dampingCoefficient", ("Solver",), "dampingCoefficient", "float", 0.0),
     ("OBJECTIVE_RATE", ("Solver",), "objectiveRate", "str", "jaumann"),
     ("KERNEL_CORRECTION", ("Solver",), "kernelCorrection", "bool", False),
@@ -152,6 +157,7 @@ UNSUPPORTED = {
     "OBJECTIVE_RATE": ("jaumann",),
     "HOURGLASS_FORM": ("rate",),
     "HOURGLASS_STS_MODE": ("subcycle",),
+    "BULK_VISCOSITY_LENGTH": ("dx0", "h"),
 }
 
 # Cards the format knows, and those whose content is accepted but not read here

@@ -83,6 +83,8 @@ struct DevAccum {
     unsigned int near_m_bits;    // margin M of this step's near lists (0: none)
     unsigned int relax_max_bits; // the initial relaxation's residual (float bits)
     double hg_power;         // sum_i mw_i de_hg_i of the in-loop damper (solid)
+    double visc_power;       // sum_i m_i de_visc_i, Morris + Monaghan (solid)
+    unsigned int visc_c_bits;    // max signal speed of the viscosities' CFL limits (solid)
     unsigned long long n_steps, n_builds, n_shift_search;   // list statistics
 };
 

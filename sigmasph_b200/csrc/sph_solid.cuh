@@ -8,11 +8,14 @@
 //   k_solid_b        ALE transport of s, eps_p, e (one sweep); epilogue: Jaumann update,
 //                    J2 / Johnson-Cook return, energy and temperature  (SOLID.py:1799-2293,
 //                    :2691-3004)
-//   k_solid_commit   the updated history, volume update, per-material EOS, gravity
-//   k_solid_force    stress divergence + Morris + in-loop hourglass + ALE momentum, the
-//                    work conjugate de_int, the dt pair estimate    (SOLID.py:3204-3852)
-//   k_solid_dt       CFL limits, the damper cap or sub-step count  (SOLID.py:4116-4161,
-//                    :4510-4539)
+//   k_solid_commit   the updated history, volume update, per-material EOS, the bulk
+//                    viscosity q, gravity; banks the previous step's damper, viscous
+//                    and diffusion work                            (SOLID.py:2182-2207)
+//   k_solid_force    stress divergence (p + q) + Morris + Monaghan + in-loop hourglass
+//                    + ALE momentum, the work conjugate de_int, the dt pair estimate
+//                                                                  (SOLID.py:3204-3852)
+//   k_solid_dt       CFL limits incl. the viscosities', the damper cap or sub-step
+//                    count                       (SOLID.py:3939-4009, :4116-4161, :4510-4539)
 //   k_half_kick, k_gradv, k_hg_stage x32, k_sts_finish   the sub-cycled damper between
 //                    the half kicks, with a device-side stage count (SOLID.py:4485-4615)
 //   k_solid_advect   plain advect when the damper is in-loop
@@ -283,13 +286,14 @@ __device__ __forceinline__ void grad_v_finish(const Cst& c, const Ptr& P, int i,
     reinterpret_cast<float4*>(g)[2] = make_float4(G[2][2], 0.0f, 0.0f, 0.0f);
 }
 struct NoExtra {};
-// The record's fourth word after the 3x3: the pressure k_solid_commit copied there.
-__device__ __forceinline__ float load_gradv_p(const Ptr& P, int j, float G[3][3]) {
+// The record's three words after the 3x3, written by k_solid_commit: the pressure, the
+// bulk viscosity q and the signal speed of q's own CFL limit.
+__device__ __forceinline__ float2 load_gradv_p(const Ptr& P, int j, float G[3][3]) {
     const float4* g = reinterpret_cast<const float4*>(P.gradv + 12 * j);
     float4 a = __ldg(g), b = __ldg(g + 1), d = __ldg(g + 2);
     G[0][0] = a.x; G[0][1] = a.y; G[0][2] = a.z; G[1][0] = a.w;
     G[1][1] = b.x; G[1][2] = b.y; G[2][0] = b.z; G[2][1] = b.w; G[2][2] = d.x;
-    return d.y;
+    return make_float2(d.y, d.z);
 }
 
 __device__ __forceinline__ void load_gradv(const Ptr& P, int j, float G[3][3]) {
@@ -859,8 +863,16 @@ __global__ void __launch_bounds__(kBlock) k_solid_commit(Cst c, Ptr P) {
     if (i == 0) {
         // ensembles keep their dt maxima per instance (reset in k_solid_load) and no
         // scene-wide diffusion work
-        if (c.n_inst == 0) P.sc->diff_work += (double)P.sc->dt * P.ac->w_diff_step;
+        // the previous step's works, with the dt they were done over (SOLID.py:2182-2207)
+        if (c.n_inst == 0) {
+            const double dt_prev = (double)P.sc->dt;
+            P.sc->diff_work += dt_prev * P.ac->w_diff_step;
+            P.sc->hg_work += dt_prev * P.ac->hg_power;
+            if (c.p.track_visc_work) P.sc->visc_work += dt_prev * P.ac->visc_power;
+        }
         P.ac->w_diff_step = 0.0;
+        P.ac->hg_power = 0.0;
+        P.ac->visc_power = 0.0;
         P.ac->max_c_sq_bits = __float_as_uint(c.p.c_signal * c.p.c_signal);
         P.ac->max_accel_bits = __float_as_uint(1e-10f);
     }
@@ -890,20 +902,38 @@ __global__ void __launch_bounds__(kBlock) k_solid_commit(Cst c, Ptr P) {
     pi.w = V;
     pos[i] = pi;
     float m = P.cur.vel[4 * i + 3];
-    const float p = solid_pressure(c, P, eos_of(P, i), m / V);
+    const int k = eos_of(P, i);
+    const float rho = m / V;
+    const float p = solid_pressure(c, P, k, rho);
     P.cur.disp[4 * i + 3] = p;
-    // a spare word of the velocity-gradient record carries p to the neighbours' force
-    // pass, which reads that record of every neighbour for the in-loop damper anyway
+    // the spare words of the velocity-gradient record carry p (and q) to the neighbours'
+    // force pass, which reads that record of every neighbour for the in-loop damper anyway
     P.gradv[12 * i + 9] = p;
+    if (c.p.q_l2 > 0.0f) {
+        // SOLID.py:3393-3401 and :3939-3975: q = C_Q l^2 rho (tr grad v)^2 under
+        // compression, and the signal speed Q + sqrt(Q^2 + c^2), Q = C_Q l |tr grad v|
+        const float4* g = reinterpret_cast<const float4*>(P.gradv + 12 * i);
+        const float dv = (g[0].x + g[1].x) + g[2].x;
+        float q = 0.0f, ce = 0.0f;
+        if (dv < 0.0f) {
+            q = c.p.q_l2 * rho * dv * dv;
+            const float qc = c.p.q_cl * (-dv), ci = P.mat[k].cp;
+            ce = qc + sqrtf(qc * qc + ci * ci);
+        }
+        reinterpret_cast<float2*>(P.gradv + 12 * i + 10)[0] = make_float2(q, ce);
+    }
     // gravity; de_int restarts for this step's force pass
     P.acc[i] = make_float4(c.p.gravity[0], c.p.gravity[1], c.p.gravity[2], 0.0f);
 }
 
 // ------------------------------------------------------------------ stress force
+// kVisc: a deck with the bulk viscosity q or Monaghan's Pi_ij (SOLID.py:3386-3401,
+// :3560-3570, :3727-3766); the plain instance keeps the registers of the common case.
+template <bool kVisc>
 __global__ void SPH_BOUNDS(SPH_OCC_SOLID_FORCE) k_solid_force(Cst c, Ptr P) {
     int i = blockIdx.x * blockDim.x + threadIdx.x;
-    float amag = 0.0f, csq = 0.0f;
-    double hgp = 0.0;
+    float amag = 0.0f, csq = 0.0f, cvisc = 0.0f;
+    double hgp = 0.0, vpw = 0.0;
     int kinst = 0;
     bool on = false;
     if (i < c.n) {
@@ -915,6 +945,14 @@ __global__ void SPH_BOUNDS(SPH_OCC_SOLID_FORCE) k_solid_force(Cst c, Ptr P) {
         float4 pi = pos[i], vi4 = vel[i];
         F3 xi = f3(pi), vi = f3(vi4);
         const float p_i = dsp[i].w;
+        const bool q_on = kVisc && c.p.q_l2 > 0.0f;
+        const bool av_on = kVisc && (c.p.av_alpha > 0.0f || c.p.av_beta > 0.0f);
+        float ptot_i = p_i, ce_q = 0.0f;
+        if (q_on) {
+            const float2 qc = reinterpret_cast<const float2*>(P.gradv + 12 * i + 10)[0];
+            ptot_i = p_i + qc.x;
+            ce_q = qc.y;
+        }
         const float rho_i = vi4.w / pi.w, inv_rho_i = 1.0f / rho_i;
         const float w_i = w_of(pi, c), mw_i = mw_of(vi4.w, pi, c), inv_mw = 1.0f / mw_i;
         const int ki = eos_of(P, i);
@@ -936,8 +974,9 @@ __global__ void SPH_BOUNDS(SPH_OCC_SOLID_FORCE) k_solid_force(Cst c, Ptr P) {
         const float eps_rho = 1e-3f * c.p.density0;
         const float csig = c.n_inst > 0 ? P.irow[ki].c_signal : c.p.c_signal;
         float cl = csig * csig;
+        const float c_i = kVisc ? P.mat[ki].cp : 0.0f;
         F3 a = {0, 0, 0};
-        float dei = 0.0f, dhg = 0.0f;
+        float dei = 0.0f, dhg = 0.0f, dvisc = 0.0f, mu_max = 0.0f;
         for_each_neighbour(c, P, i, [&](int j, int mir) {
             float4 pj = __ldg(pos + j), vj4 = __ldg(vel + j);
             F3 xj = f3(pj), vj = f3(vj4);
@@ -951,10 +990,12 @@ __global__ void SPH_BOUNDS(SPH_OCC_SOLID_FORCE) k_solid_force(Cst c, Ptr P) {
             F3 vij = vi - vj;
             // the in-loop damper first: j's velocity-gradient record also carries its
             // pressure (k_solid_commit), and is dead once this term is summed
-            float p_j;
+            float p_j, q_j = 0.0f;
             if (hg_inloop) {
                 float Gj[3][3];
-                p_j = load_gradv_p(P, j, Gj);
+                const float2 pq = load_gradv_p(P, j, Gj);
+                p_j = pq.x;
+                if (q_on) q_j = pq.y;
                 if (rn > 1e-9f) {
                     float inv_rn = rsqrtf(rn2);
                     F3 rh = {-r.x * inv_rn, -r.y * inv_rn, -r.z * inv_rn};
@@ -970,12 +1011,16 @@ __global__ void SPH_BOUNDS(SPH_OCC_SOLID_FORCE) k_solid_force(Cst c, Ptr P) {
                     a += ah;
                     dhg += -0.5f * dot3(ah, vij);
                 }
+            } else if (q_on) {
+                const float4 r8 = __ldg(reinterpret_cast<const float4*>(P.gradv + 12 * j) + 2);
+                p_j = r8.y;
+                q_j = r8.z;
             } else {
                 p_j = __ldg(&dsp[j].w);
             }
             Sym sj = load_s(sdev, j);
             if (mir) sj = mirror_sym(mir, sj);
-            float pp = p_i + p_j;
+            float pp = q_on ? ptot_i + (p_j + q_j) : p_i + p_j;
             Sym ss = {s.xx + sj.xx - pp, s.yy + sj.yy - pp, s.zz + sj.zz - pp, s.xy + sj.xy, s.xz + sj.xz, s.yz + sj.yz};
             float ww = w_i * w_j;
             F3 f = {ww * (ss.xx * g.x + ss.xy * g.y + ss.xz * g.z),
@@ -987,8 +1032,24 @@ __global__ void SPH_BOUNDS(SPH_OCC_SOLID_FORCE) k_solid_force(Cst c, Ptr P) {
             float vxy = dot3(vij, r);
             F3 am = __fdividef(visc * w_j * vxy, rn * rn + c.eta2) * g;
             a += am;
-            if (c.p.viscosity > 0.0f) dei += -0.5f * dot3(am, vij);
+            // the viscous work conjugates are summed once, as de_visc = -(their part of
+            // de_int), and folded into de_int after the loop: one add per pair fewer
+            if (c.p.viscosity > 0.0f) dvisc += 0.5f * dot3(am, vij);
             float rho_j = vj4.w / pj.w;
+            if (av_on && vxy < 0.0f) {
+                // Pi_ij = (-alpha cbar mu + beta mu^2) / rhobar on an approaching pair
+                const float mu = c.h * vxy / (rn * rn + c.p.av_eps * c.h * c.h);
+                const float rho_bar = 0.5f * (rho_i + rho_j);
+                const float c_j = c.one_material ? c_i : P.mat[eos_of(P, j)].cp;
+                const float c_bar = 0.5f * (c_i + c_j);
+                const float pij = (-c.p.av_alpha * c_bar * mu + c.p.av_beta * mu * mu) / rho_bar;
+                F3 ap = (-mw_of(vj4.w, pj, c) * pij) * g;
+                float mu_cfl = -mu;
+                if (axc) { ap.x *= ratio; mu_cfl *= ratio; }
+                a += ap;
+                mu_max = fmaxf(mu_max, mu_cfl);
+                dvisc += 0.5f * dot3(ap, vij);
+            }
             if (ale) {
                 float4 q = __ldg(shf + j);
                 F3 du_j = {q.x * inv_dt, q.y * inv_dt, q.z * inv_dt};
@@ -1012,6 +1073,7 @@ __global__ void SPH_BOUNDS(SPH_OCC_SOLID_FORCE) k_solid_force(Cst c, Ptr P) {
             }
         });
         if (c.p.axisymmetric) a.y += (s.yy - s.zz) / (rho_i * ri);
+        dei -= dvisc;
         float4 a0 = P.acc[i];
         F3 an = {a0.x + a.x, a0.y + a.y, a0.z + a.z};
         P.acc[i] = make_float4(an.x, an.y, an.z, dei);
@@ -1019,6 +1081,13 @@ __global__ void SPH_BOUNDS(SPH_OCC_SOLID_FORCE) k_solid_force(Cst c, Ptr P) {
         if (ongrid) amag = norm3(an);
         if (c.p.dt_pair_mode != 0) csq = cl;
         hgp = (double)(mw_i * dhg);
+        vpw = (double)vi4.w * (double)dvisc;
+        if (kVisc) {
+            // SOLID.py:3977-4009: Pi_ij's signal speed where a neighbour approaches
+            float ce_av = 0.0f;
+            if (mu_max > 0.0f) ce_av = c_i + 1.2f * (c.p.av_alpha * c_i + c.p.av_beta * mu_max);
+            cvisc = fmaxf(ce_q, ce_av);
+        }
     }
     if (c.n_inst > 0) {
         inst_max_atomic(amag, kinst, on, &SphInstState::max_accel_bits, P.inst);
@@ -1028,6 +1097,8 @@ __global__ void SPH_BOUNDS(SPH_OCC_SOLID_FORCE) k_solid_force(Cst c, Ptr P) {
     block_max_atomic(amag, &P.ac->max_accel_bits);
     block_max_atomic(csq, &P.ac->max_c_sq_bits);
     if (c.p.hourglass_alpha > 0.0f && !c.p.hourglass_sts) block_sum_atomic(hgp, &P.ac->hg_power);
+    if (kVisc) block_max_atomic(cvisc, &P.ac->visc_c_bits);
+    if (c.p.track_visc_work) block_sum_atomic(vpw, &P.ac->visc_power);
 }
 
 // ------------------------------------------------------------------ dt, damper cap / stage count
@@ -1065,12 +1136,17 @@ __global__ void k_solid_dt(Cst c, Ptr P) {
     P.sc->max_c_sq = mcs;
     P.sc->max_accel = ma;
     float dt = fminf(c.cfl_h / sqrtf(mcs), c.p.CFL * sqrtf(c.h / ma));
+    if (c.p.q_l2 > 0.0f || c.p.av_alpha > 0.0f || c.p.av_beta > 0.0f) {
+        // the two viscosities' own limits (SOLID.py:3939-4009) in one: min over both of
+        // CFL h / c is CFL h / (the larger c)
+        const float ce = __uint_as_float(P.ac->visc_c_bits);
+        P.ac->visc_c_bits = 0u;
+        if (ce > 0.0f) dt = fminf(dt, c.cfl_h / ce);
+    }
     const bool hg = c.p.hourglass_alpha > 0.0f;
     int s = 0;
     if (!c.p.hourglass_sts) {
         if (hg) dt = fminf(dt, (float)(1.6 / (double)c.p.hg_rate));
-        P.sc->hg_work += (double)dt * P.ac->hg_power;
-        P.ac->hg_power = 0.0;
     } else if (hg) {
         s = 1;
         if (c.p.hg_rate > 0.0f) {
@@ -1401,7 +1477,13 @@ inline int solid_substep_launch(const Cst& c, const Ptr& P, int n, cudaStream_t 
         }
     }
     if (in(SPH_STAGE_CONTINUITY)) { k_solid_commit<<<nb, bs, 0, st>>>(c, P); mark("k_solid_commit"); }
-    if (in(SPH_STAGE_FORCES)) { k_solid_force<<<nb, bs, 0, st>>>(c, P); mark("k_solid_force"); }
+    if (in(SPH_STAGE_FORCES)) {
+        if (c.p.q_l2 > 0.0f || c.p.av_alpha > 0.0f || c.p.av_beta > 0.0f)
+            k_solid_force<true><<<nb, bs, 0, st>>>(c, P);
+        else
+            k_solid_force<false><<<nb, bs, 0, st>>>(c, P);
+        mark("k_solid_force");
+    }
     if (in(SPH_STAGE_DT)) { k_solid_dt<<<inst_blocks(c), inst_threads(c), 0, st>>>(c, P); mark("k_solid_dt"); }
     if (in(SPH_STAGE_ADVECT)) {
         if (c.p.hourglass_sts && c.p.hourglass_alpha > 0.0f) {

@@ -96,4 +96,20 @@ def fill_solid_params(ps, p):
     p.ramp_time = float(g("rampTime") or 0.0)
     p.jc_surrogate = 0
     p.jc_surrogate_tol = 1e-3
-    p.track_visc_work = 0
+    # the in-loop viscosities (SOLID.py:667-716): q = C_Q l^2 rho (div v)^2 under
+    # compression, added to the pressure of the stress pair; Monaghan's Pi_ij on
+    # approaching pairs; C_Q l^2 and C_Q l folded in double as the reference folds them
+    q_bulk = float(g("BULK_VISCOSITY_Q") or 0.0)
+    q_len = str(g("BULK_VISCOSITY_LENGTH") or "dx0").lower()
+    q_length = float(dx0 if q_len == "dx0" else h)
+    p.q_l2 = q_bulk * q_length ** 2
+    p.q_cl = q_bulk * q_length
+    p.av_alpha = float(g("MONAGHAN_ALPHA") or 0.0)
+    p.av_beta = float(g("MONAGHAN_BETA") or 0.0)
+    eps = g("MONAGHAN_EPS")
+    p.av_eps = 0.01 if eps is None else float(eps)
+    av_on = p.av_alpha > 0.0 or p.av_beta > 0.0
+    # the solid's viscous work: Morris and Monaghan, not q (SOLID.py:1255-1264)
+    track = g("TRACK_VISCOUS_WORK")
+    p.track_visc_work = int((True if track is None else bool(track))
+                            and (float(g("viscosity")) > 0.0 or av_on))

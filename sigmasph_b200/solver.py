@@ -442,7 +442,8 @@ class HypoElasticSolver(_SolverBase):
         r = self._reduce()
         s = self._scalars()
         ke, ie, el = r[abi.RED_KE], r[abi.RED_IE], r[abi.RED_ELASTIC]
-        return {"ke": ke, "ie": ie, "se": el, "pe": r[abi.RED_PE], "hg": float(s.hg_work),
-                "wall": float(s.wall_work), "visc": 0.0, "leftover": float(s.leftover_work),
-                "leftover_raw": float(s.leftover_work), "pw": float(s.plastic_work),
-                "total": ke + ie}
+        pe, hg, lw = r[abi.RED_PE], float(s.hg_work), float(s.leftover_work)
+        return {"ke": ke, "ie": ie, "se": el, "pe": pe, "hg": hg,
+                "wall": float(s.wall_work), "visc": float(s.visc_work), "leftover": lw,
+                "leftover_raw": lw, "pw": float(s.plastic_work), "wd": float(s.diff_work),
+                "total": ke + ie + hg + pe - lw}

@@ -129,6 +129,27 @@ def strip_ps_deck(dx=0.1):
     return sc
 
 
+def bar3d_visc_deck():
+    """The bar with both in-loop viscosities: the VNR bulk viscosity (l = dx0) and
+    Monaghan's pair viscosity, beside the Morris term and the in-loop damper."""
+    sc = bar3d_deck()
+    sc["Solver"]["bulkViscosity"] = {"quadratic": 1.5}
+    sc["Solver"]["artificialViscosity"] = {"alpha": 1.0, "beta": 2.0}
+    return sc
+
+
+def axi_visc_deck():
+    """The axisymmetric dogbone (conservative axial form, sub-cycled damper) with q on the
+    kernel support (l = h) and Monaghan's viscosity."""
+    import json
+    from sigmasph_b200.config import strip_json_comments
+    with open(axi_deck()) as f:
+        sc = json.loads(strip_json_comments(f.read()))
+    sc["Solver"]["bulkViscosity"] = {"quadratic": 0.5, "lengthScale": "h"}
+    sc["Solver"]["artificialViscosity"] = {"alpha": 0.5, "beta": 1.0, "epsilon": 0.02}
+    return sc
+
+
 # The GPU writes the return-mapped stress, plastic strain and energy to scratch in the
 # LAM stage and commits them with the volume update, so they are compared after it.
 STAGE_FIELDS = {
@@ -145,8 +166,9 @@ TOL32 = {"de_int": 2e-4, "pressure": 1e-3, "grad_v": 1e-4}
 TOL64 = {"de_int": 1e-3, "pressure": 2e-3, "acc": 5e-4, "grad_v": 2e-4}
 
 
-@pytest.mark.parametrize("deck", [axi_deck, bar3d_deck, strip_ps_deck],
-                         ids=["axi_dogbone_jc_sts", "bar3d_j2_inloop", "plane_strain_jc"])
+@pytest.mark.parametrize("deck", [axi_deck, bar3d_deck, strip_ps_deck, bar3d_visc_deck, axi_visc_deck],
+                         ids=["axi_dogbone_jc_sts", "bar3d_j2_inloop", "plane_strain_jc",
+                              "bar3d_q_monaghan", "axi_q_monaghan"])
 def test_solid_stages_match_oracle(cuda, deck):
     ps, solver, o64, o32 = make_solid(deck())
     for s in range(8):
@@ -217,7 +239,8 @@ def test_solid_lists_between_builds_match_oracle(cuda, deck):
     assert A == B
 
 
-@pytest.mark.parametrize("deck", [axi_deck, bar3d_deck], ids=["axi_dogbone", "bar3d"])
+@pytest.mark.parametrize("deck", [axi_deck, bar3d_deck, bar3d_visc_deck],
+                         ids=["axi_dogbone", "bar3d", "bar3d_q_monaghan"])
 def test_solid_multistep_tracks_fp64(cuda, deck):
     ps, solver, o64, o32 = make_solid(deck())
     for o in (o64, o32):
@@ -240,6 +263,29 @@ def test_solid_multistep_tracks_fp64(cuda, deck):
     fo = s64["constraint_force"][:solver.num_constraints]
     assert np.abs(fg - fo).max() <= 1e-3 * np.abs(fo).max() + 1e-9
     assert solver.error_word() & ~(abi.EW_HASHED_GRID) == 0
+
+
+@pytest.mark.parametrize("deck", [bar3d_deck, bar3d_visc_deck], ids=["bar3d", "bar3d_q_monaghan"])
+def test_solid_work_channels(cuda, deck):
+    """The explicit damper's and the viscosities' work (SOLID.py:2182-2207): each step's
+    force-pass power banked at the next step's start with the dt it was done over, so
+    after N steps the totals hold N - 1 steps, as the float32 oracle's; the viscosity
+    limits of the time step are the oracle's (dt within 1e-6)."""
+    ps, solver, o64, o32 = make_solid(deck())
+    o32.stage(abi.STAGE_SORT)
+    solver.initialize()
+    nsteps = 6
+    solver.step_many(nsteps)
+    o32.step(nsteps)
+    sg, s32 = solver._scalars(), o32.scalars()
+    assert abs(sg.dt - s32["dt"]) <= 1e-5 * s32["dt"]
+    for k in ("visc_work", "hg_work"):
+        want, got = s32[k], getattr(sg, k)
+        assert want != 0.0, k
+        assert abs(got - want) <= 2e-3 * abs(want), (k, got, want)
+    b = solver.energy_budget()
+    assert b["visc"] == sg.visc_work and b["hg"] == sg.hg_work
+    assert b["total"] == pytest.approx(b["ke"] + b["ie"] + b["hg"] + b["pe"] - b["leftover"])
 
 
 def test_grip_force_and_time_bookkeeping(cuda):

@@ -131,3 +131,73 @@ def test_mlp_oracle_gradient_matches_finite_differences():
         e[q] = 1e-6
         fd = (mlp.loss_and_grad(w + e, X, T)[0] - mlp.loss_and_grad(w - e, X, T)[0]) / 2e-6
         assert fd == pytest.approx(g[q], rel=1e-5, abs=1e-9)
+
+
+def _viscous(sc, q=1.5, alpha=1.0, beta=2.0):
+    sc["Solver"]["bulkViscosity"] = {"quadratic": q}
+    sc["Solver"]["artificialViscosity"] = {"alpha": alpha, "beta": beta}
+    return sc
+
+
+def _forces(sc, v_of_x, fp64=True):
+    """The oracle's force stage on a free block with velocities v_of_x(x)."""
+    ps = ParticleSystem(SimConfig(sc), device="cpu")
+    x = ps.x.to_numpy().astype(np.float64)
+    ps.v.from_numpy(v_of_x(x).astype(np.float32))
+    p = build_params(ps)
+    o = Oracle(p, ps.particle_max_num, fp64=fp64)
+    o.set_state(state_from_sets(ps.state_numpy()), p.CFL * p.support_radius / p.c_signal)
+    for s in range(abi.STAGE_FORCES + 1):
+        o.stage(s)
+    return o, o.get_state()
+
+
+def test_viscosities_conserve_momentum():
+    """q enters the stress pair and Pi_ij is pair-symmetric against an antisymmetric
+    grad W (SOLID.py:3560-3570, :3727-3766): a free block keeps its momentum."""
+    ps = ParticleSystem(SimConfig(_viscous(free_block())), device="cpu")
+    rng = np.random.default_rng(5)
+    n = ps.particle_max_num
+    ps.v.from_numpy(rng.uniform(-2.0, 2.0, (n, 3)).astype(np.float32))
+    p = build_params(ps)
+    assert p.q_l2 > 0 and p.av_alpha == 1.0 and p.track_visc_work == 1
+    o = Oracle(p, n, fp64=True)
+    st = state_from_sets(ps.state_numpy())
+    o.set_state(st, p.CFL * p.support_radius / p.c_signal)
+    m = st["m"].astype(np.float64)
+    P0 = (m[:, None] * st["v"].astype(np.float64)).sum(0)
+    o.stage(abi.STAGE_SORT)
+    o.step(20)
+    r = o.get_state()
+    P1 = (r["m"][:, None] * r["v"]).sum(0)
+    gross = (r["m"][:, None] * np.abs(r["v"])).sum(0)
+    assert np.abs(P1 - P0).max() <= 1e-10 * gross.max()
+    assert o.scalars()["visc_work"] < 0.0     # dissipation is booked negative
+
+
+def test_viscous_work_conjugate_balances_the_power():
+    """de_int carries the work conjugate of every pair force (stress with q, Morris,
+    Pi_ij), so in 3D sum_i m_i (de_i + a_i . v_i) = 0 with no damper, gravity or ALE."""
+    sc = _viscous(free_block())
+    sc["Hourglass"] = {"alpha": 0.0}
+    rng = np.random.default_rng(6)
+    _, r = _forces(sc, lambda x: rng.uniform(-2.0, 2.0, x.shape))
+    m = r["m"]
+    pw = m * (r["acc"] * r["v"]).sum(1)
+    assert np.abs((m * r["de_int"] + pw).sum()) <= 1e-10 * np.abs(pw).sum()
+
+
+def test_viscosities_act_only_under_compression():
+    """Under a uniform expansion every pair separates and div v > 0: q and Pi_ij vanish
+    and the accelerations are the plain deck's.  Under the same compression both act."""
+    base = free_block()
+    base["Hourglass"] = {"alpha": 0.0}
+    c = np.array([3.0, 3.0, 3.0])
+    for sign, same in ((1.0, True), (-1.0, False)):
+        _, r0 = _forces(base, lambda x: sign * 0.5 * (x - c))
+        _, r1 = _forces(_viscous(json.loads(json.dumps(base))), lambda x: sign * 0.5 * (x - c))
+        d = np.abs(r1["acc"] - r0["acc"]).max()
+        if same:
+            assert d == 0.0
+        else:
+            assert d > 1e-3 * np.abs(r0["acc"]).max()
