@@ -84,6 +84,31 @@ def strip_specs(count=256, seed=20260101, n_min=2000, n_max=60000, target=6_000_
     return out
 
 
+def shard(specs, world, rank):
+    """The strips `rank` steps when `world` GPUs share one ensemble: largest first, each to
+    the rank holding the fewest particles so far (ties to the lower rank), so the ranks'
+    particle counts differ by at most one strip.  Deterministic; returned in spec order."""
+    load = [0] * int(world)
+    owner = [0] * len(specs)
+    for k in sorted(range(len(specs)), key=lambda k: (-specs[k].particles, k)):
+        r = min(range(int(world)), key=lambda q: (load[q], q))
+        owner[k] = r
+        load[r] += specs[k].particles
+    return [k for k in range(len(specs)) if owner[k] == rank]
+
+
+STATE_COLUMNS = ("sim_time", "dt", "load_s", "sts_stages", "force_x0", "force_y0", "force_z0",
+                 "force_x1", "force_y1", "force_z1", "disp_x0", "disp_y0", "disp_z0",
+                 "disp_x1", "disp_y1", "disp_z1")
+
+
+def state_row(st):
+    """One strip's state (Ensemble.state) as a float64 row in STATE_COLUMNS order."""
+    return np.concatenate([[st["sim_time"], st["dt"], st["load_s"], st["sts_stages"]],
+                           np.asarray(st["force"], np.float64).ravel(),
+                           np.asarray(st["disp"], np.float64).ravel()]).astype(np.float64)
+
+
 def strip_deck(s: StripSpec):
     """One strip as an ordinary plane-strain scene in physical units (mm, GPa, ms): steel
     (rho 7.9e-6, E 200, nu 0.3, linear EOS), Johnson-Cook (C 0, no thermal softening),
@@ -302,3 +327,9 @@ class Ensemble:
     def state(self, k):
         b, j = self._where[k]
         return self.buckets[b].state()[j]
+
+    def state_rows(self):
+        """Every strip's state as float64 rows (STATE_COLUMNS), in spec order; one read
+        per bucket."""
+        per = [b.state() for b in self.buckets]
+        return np.stack([state_row(per[b][j]) for b, j in (self._where[k] for k in range(len(self.specs)))])

@@ -1,9 +1,11 @@
-"""Replica runs of one workload on N GPUs of a node, one process per GPU.
+"""Multi-GPU runs of one workload on N GPUs of a node, one process per GPU.
 
-The per-step particle path does not shard at one-GPU scale (the reference runs one scene
-per process, run_simulation.py:649-708, and one B200 holds the largest scene with room to
-spare), so each rank steps its own copy of the workload and the data path has no
-collective.  The only collectives are the timing's, taken by every rank in the same order:
+A single scene does not shard at one-GPU scale (the reference runs one scene per process,
+run_simulation.py:649-708, and one B200 holds the largest scene with room to spare), so
+each rank steps its own copy of it (replicas).  An ensemble of independent strips is
+sharded instead: each rank steps its share (sigmasph_b200.ensemble.shard) and the strips'
+final states are gathered once, in float64 (gather_rows).  Neither data path has a
+per-step collective.  The timing's collectives are taken by every rank in the same order:
 a barrier on each side of the timed region and the maximum of the ranks' times.  The
 whole-job throughput is the units all ranks processed over that maximum.
 
@@ -66,6 +68,35 @@ class Replicas:
         out = [torch.zeros_like(t) for _ in range(self.world)]
         self.dist.all_gather(out, t)
         return [float(o.item()) for o in out]
+
+    def sum_over_ranks(self, x):
+        """The sum of x over the ranks, in float64 (every rank gets it)."""
+        if self.dist is None:
+            return float(x)
+        import torch
+        t = torch.tensor([float(x)], dtype=torch.float64, device=self._device())
+        self.dist.all_reduce(t, op=self.dist.ReduceOp.SUM)
+        return float(t.item())
+
+    def gather_rows(self, rows, index, total):
+        """Rows (k, m) float64 of the units this rank owns, at global positions `index`:
+        the (total, m) table of all ranks, on every rank.  One float64 sum-reduction of a
+        table that is zero outside each rank's own rows, so every entry is exact; a last
+        column counts the owners, and a unit owned by no rank or by two is an error."""
+        import numpy as np
+        rows = np.asarray(rows, dtype=np.float64).reshape(len(index), -1)
+        m = rows.shape[1]
+        table = np.zeros((int(total), m + 1), dtype=np.float64)
+        table[np.asarray(index, dtype=np.int64), :m] = rows
+        table[np.asarray(index, dtype=np.int64), m] = 1.0
+        if self.dist is not None:
+            import torch
+            t = torch.from_numpy(table).to(self._device())
+            self.dist.all_reduce(t, op=self.dist.ReduceOp.SUM)
+            table = t.cpu().numpy()
+        if not np.all(table[:, m] == 1.0):
+            raise RuntimeError("gather_rows: every unit must be owned by exactly one rank")
+        return table[:, :m]
 
     def throughput(self, units_per_rank, seconds):
         """Whole-job units per second: every rank processed units_per_rank in at most

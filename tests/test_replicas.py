@@ -92,3 +92,67 @@ def test_missing_rank_fails_within_timeout():
                            start_method="spawn")
         with open(os.path.join(d, "r0.txt")) as f:
             assert f.read() != "joined"
+
+
+def test_shard_balances_the_strips():
+    """Largest first to the least-loaded rank: disjoint, complete, and the ranks' particle
+    counts differ by at most one strip (the 256-strip ensemble's specs, no GPU)."""
+    from sigmasph_b200.ensemble import shard, strip_specs
+    specs = strip_specs(256)
+    biggest = max(s.particles for s in specs)
+    for world in (1, 2, 3, 4, 8):
+        parts = [shard(specs, world, r) for r in range(world)]
+        flat = sorted(k for p in parts for k in p)
+        assert flat == list(range(len(specs)))
+        loads = [sum(specs[k].particles for k in p) for p in parts]
+        assert max(loads) - min(loads) <= biggest, (world, loads)
+        assert all(p == sorted(p) for p in parts)
+
+
+def _shard_rank(rank, world, port, out_dir):
+    _env(rank, world, port)
+    from sigmasph_b200.ensemble import shard, strip_specs, state_row, STATE_COLUMNS
+    from sigmasph_b200.replicas import Replicas
+    rep = Replicas("gloo", timeout_s=60)
+    specs = strip_specs(256)
+    own = shard(specs, world, rank)
+    # stand-in states: what a strip reports, made from its index so the table is checkable
+    rows = [state_row({"sim_time": 0.5 + k, "dt": 1e-5 * (k + 1), "load_s": -0.0 if k == 3 else k / 256,
+                       "sts_stages": k % 7, "force": np.full((2, 3), -1.25 * k),
+                       "disp": np.arange(6.0).reshape(2, 3) * k}) for k in own]
+    table = rep.gather_rows(np.array(rows), own, len(specs))
+    total = rep.sum_over_ranks(sum(specs[k].particles for k in own))
+    np.save(os.path.join(out_dir, f"t{rank}.npy"), np.concatenate([[total], table.ravel()]))
+    # rank 1 also claims rank 0's first strip: that one unit is owned twice
+    other = shard(specs, world, 0)[0]
+    idx = own if rank == 0 else own + [other]
+    extra = rows if rank == 0 else rows + [rows[0]]
+    try:
+        rep.gather_rows(np.array(extra), idx, len(specs))
+        twice = "accepted"
+    except RuntimeError:
+        twice = "refused"
+    with open(os.path.join(out_dir, f"t{rank}.txt"), "w") as f:
+        f.write(twice + " " + str(len(STATE_COLUMNS)))
+    rep.close()
+
+
+def test_sharded_ensemble_gather_on_gloo():
+    """Two ranks each own half the strips; the float64 gather rebuilds the full table
+    exactly on both ranks, the particle total counts every strip once, and a strip that
+    two ranks claim is an error rather than a sum."""
+    from sigmasph_b200.ensemble import strip_specs, state_row
+    with tempfile.TemporaryDirectory() as d:
+        mp.start_processes(_shard_rank, args=(2, _free_port(), d), nprocs=2, join=True,
+                           start_method="spawn")
+        out = [np.load(os.path.join(d, f"t{r}.npy")) for r in range(2)]
+        notes = [open(os.path.join(d, f"t{r}.txt")).read().split() for r in range(2)]
+    specs = strip_specs(256)
+    want = np.array([state_row({"sim_time": 0.5 + k, "dt": 1e-5 * (k + 1),
+                                "load_s": -0.0 if k == 3 else k / 256, "sts_stages": k % 7,
+                                "force": np.full((2, 3), -1.25 * k),
+                                "disp": np.arange(6.0).reshape(2, 3) * k}) for k in range(256)])
+    for o in out:
+        assert o[0] == sum(s.particles for s in specs)
+        assert np.array_equal(o[1:].reshape(want.shape), want)
+    assert notes[0][0] == notes[1][0] == "refused" and int(notes[0][1]) == want.shape[1]
