@@ -82,6 +82,8 @@ struct DevAccum {
     unsigned int ovf_used;       // overflow-pool entries taken this step
     unsigned int near_m_bits;    // margin M of this step's near lists (0: none)
     unsigned int relax_max_bits; // the initial relaxation's residual (float bits)
+    unsigned int m_min_bits, m_max_bits;   // this step's particle masses, as bit patterns
+                                           // (equal: every particle has that mass)
     double hg_power;         // sum_i mw_i de_hg_i of the in-loop damper (solid)
     double visc_power;       // sum_i m_i de_visc_i, Morris + Monaghan (solid)
     unsigned int visc_c_bits;    // max signal speed of the viscosities' CFL limits (solid)
@@ -366,6 +368,24 @@ __device__ __forceinline__ void block_sum_atomic(double v, double* dst) {
         double s = lane < nw ? red[lane] : 0.0;
         s = warp_sum(s);
         if (lane == 0 && s != 0.0) atomicAdd(dst, s);
+    }
+    __syncthreads();
+}
+// Block minimum and maximum of 32-bit patterns, atomically folded into *dmin and *dmax.
+__device__ __forceinline__ void block_minmax_bits(unsigned int lo, unsigned int hi,
+                                                  unsigned int* dmin, unsigned int* dmax) {
+    __shared__ unsigned int red[2][32];
+    lo = __reduce_min_sync(0xffffffffu, lo);
+    hi = __reduce_max_sync(0xffffffffu, hi);
+    int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    if (lane == 0) { red[0][wid] = lo; red[1][wid] = hi; }
+    __syncthreads();
+    if (wid == 0) {
+        int nw = (blockDim.x + 31) >> 5;
+        unsigned int a = lane < nw ? red[0][lane] : 0xffffffffu, b = lane < nw ? red[1][lane] : 0u;
+        a = __reduce_min_sync(0xffffffffu, a);
+        b = __reduce_max_sync(0xffffffffu, b);
+        if (lane == 0) { atomicMin(dmin, a); atomicMax(dmax, b); }
     }
     __syncthreads();
 }

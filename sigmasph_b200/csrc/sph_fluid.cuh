@@ -314,10 +314,12 @@ __global__ void __launch_bounds__(kBlock) k_advect(Cst c, Ptr P) {
     const float dt = P.sc->dt;
     double wl = 0.0, wv = 0.0;
     float vmag = 0.0f, disp = 0.0f;
+    unsigned int mlo = 0xffffffffu, mhi = 0u;
     if (i < c.n) {
         float4 a4 = P.acc[i];
         float4* vel = as4(P.cur.vel);
         float4 v4 = vel[i];
+        mlo = mhi = __float_as_uint(v4.w);
         const float gx = c.p.gravity[0], gy = c.p.gravity[1], gz = c.p.gravity[2];
         float gsq = gx * gx + gy * gy + gz * gz;
         F3 f = {a4.x - gx, a4.y - gy, a4.z - gz};
@@ -366,6 +368,8 @@ __global__ void __launch_bounds__(kBlock) k_advect(Cst c, Ptr P) {
     }
     if (c.p.pst_enabled && c.p.pst_ma_mode == 1) block_max_atomic(vmag, &P.ac->max_v_bits);
     block_max_atomic(disp, &P.ac->max_disp_bits);
+    // the Sun shift weighs each neighbour by its mass: one mass for all spares that gather
+    if (c.p.pst_enabled && !c.p.pst_colle) block_minmax_bits(mlo, mhi, &P.ac->m_min_bits, &P.ac->m_max_bits);
 }
 
 // ------------------------------------------------------------------ apply_pst (DSPH.py:725-1046)
@@ -430,8 +434,10 @@ __device__ __forceinline__ void for_each_pst_neighbour(const Cst& c, const Ptr& 
 
 // The disorder sum's pair term (pst_pair, DSPH.py:725-769): (1 + R (W / W(dx0))^n) grad W,
 // weighted by V_j (Colle) or m_j / mean rho (Sun).
+// m_uni: every particle's mass is m_u (the neighbour's is not gathered).
 __device__ __forceinline__ F3 pst_pair_term(const Cst& c, const float4* __restrict__ vel, F3 xi,
-                                            float rho_i, float inv_Wd, int j, int mir, float4 pj) {
+                                            float rho_i, float inv_Wd, int j, int mir, float4 pj,
+                                            bool m_uni = false, float m_u = 0.0f) {
     F3 xj = f3(pj);
     if (mir) xj = mirror3(mir, xj);
     F3 r = xi - xj;
@@ -444,7 +450,7 @@ __device__ __forceinline__ F3 pst_pair_term(const Cst& c, const float4* __restri
         float Vj = w_of(pj, c);
         if (Vj > 1e-30f) return ((1.0f + f) * Vj) * g;
     } else {
-        float mj_raw = __ldg(&vel[j].w);
+        float mj_raw = m_uni ? m_u : __ldg(&vel[j].w);
         float mj = mw_of(mj_raw, pj, c);
         if (mj > 1e-10f) {
             float rho_j = mj_raw / pj.w;
@@ -498,8 +504,12 @@ __global__ void SPH_BOUNDS(SPH_OCC_PST) k_pst(Cst c, Ptr P) {
     const float rho_i = m_i / pi.w;
     {
         const float inv_Wd = c.W_dx0 > 0.0f ? 1.0f / c.W_dx0 : 0.0f;
+        // filled by this step's fluid advect; a solid step leaves them unequal
+        const unsigned int mlo = P.ac->m_min_bits;
+        const bool m_uni = !c.p.pst_colle && mlo == P.ac->m_max_bits;
+        const float m_u = __uint_as_float(mlo);
         for_each_pst_neighbour(c, P, i, xi, [&](int j, int mir, float4 pj) {
-            sr += pst_pair_term(c, vel, xi, rho_i, inv_Wd, j, mir, pj);
+            sr += pst_pair_term(c, vel, xi, rho_i, inv_Wd, j, mir, pj, m_uni, m_u);
         });
     }
     float4 vi4 = vel[i];

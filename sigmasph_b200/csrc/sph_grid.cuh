@@ -124,6 +124,8 @@ __global__ void k_layout(Cst c, Ptr P) {
     const float pred = __uint_as_float(A.max_disp_bits) + __uint_as_float(A.max_grip_disp_bits);
     A.max_disp_bits = 0u;       // this step's move accumulates from here
     A.max_grip_disp_bits = 0u;
+    A.m_min_bits = 0xffffffffu; // filled by this step's advect (fluid)
+    A.m_max_bits = 0u;
     A.ovf_used = 0u;
     const int offg = P.sc->off_grid_num;
     const int build = A.force_build || offg != A.off_grid_build || !(dstart + pred <= c.dlim);

@@ -30,12 +30,17 @@ def perturb(ps, seed=20260101, dv=0.05, drho=0.003, dshift=2e-3):
     ps.pst_shift.from_numpy(sh)
 
 
-def make_pair(scene, fp64=True, device="cuda", perturbed=True, oracles=None):
-    """(ps, solver, oracle) at the same initial state, both before the first sort."""
+def make_pair(scene, fp64=True, device="cuda", perturbed=True, oracles=None, mass_jitter=0.0):
+    """(ps, solver, oracle) at the same initial state, both before the first sort;
+    mass_jitter > 0 gives every particle its own mass (m (1 + U(-j, j)))."""
     cfg = SimConfig(scene)
     ps = ParticleSystem(cfg, device=device)
     if perturbed:
         perturb(ps)
+    if mass_jitter > 0.0:
+        m = ps.m.to_numpy().astype(np.float64)
+        m *= 1.0 + np.random.default_rng(17).uniform(-mass_jitter, mass_jitter, m.shape)
+        ps.m.from_numpy(m.astype(np.float32))
     solver = ps.build_solver()
     st0 = state_from_sets(ps.state_numpy())
     p = build_params(ps)

@@ -321,8 +321,20 @@ def test_large_move_forces_a_build(cuda):
 @pytest.mark.parametrize("scene_fn", [lambda: small_scene(), axi_fluid_scene, quarter_scene],
                          ids=["3d", "axisymmetric", "quarter_yz"])
 def test_stages_match_oracle(cuda, scene_fn):
-    sc = scene_fn()
-    ps, solver, o64 = make_pair(sc, fp64=True)
+    _stages_match_oracle(scene_fn())
+
+
+def test_stages_match_oracle_with_own_masses(cuda):
+    """Every particle with its own mass: the shift gathers each neighbour's mass (with one
+    mass for all it reads none)."""
+    _stages_match_oracle(small_scene(), mass_jitter=0.02)
+
+
+def _stages_match_oracle(sc, mass_jitter=0.0):
+    ps, solver, o64 = make_pair(sc, fp64=True, mass_jitter=mass_jitter)
+    if mass_jitter:
+        m = ps.m.to_numpy()
+        assert m.min() < m.max()
     st0 = state_from_sets(ps.state_numpy())
     o32 = Oracle(build_params(ps), ps.particle_max_num, fp64=False)
     o32.set_state(st0, solver.dt[None])
