@@ -12,13 +12,23 @@ than the 126 MB L2, so no flush is needed between steps.  The line reports how m
 the timed steps built the lists.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference]
-                    [--workload dambreak3d|tensile_bar3d|tensile_bar3d_jc] [--dx DX]
+                    [--workload dambreak3d|tensile_bar3d|tensile_bar3d_jc|strips256] [--dx DX]
 
 `--workload tensile_bar3d` times the hypoelastic solid step instead: the 3D round-bar
 tensile test (sigmasph_b200.scenes.tensile_bar3d), about 2.3M particles at dx = 0.113 mm.
+`--workload strips256` times 256 independent plane-strain strips (about 6M particles) as
+packed ensembles.
 
-Under torchrun (N > 1) every rank runs an independent replica of the workload (the
-path does not shard at one-GPU scale: replicas only); the time is the max over ranks.
+Besides `value` and `e2e`, the line carries `roofline` (the dominant kernel's algorithmic
+bytes over its event-timed launch, against the measured HBM copy peak, with its ncu DRAM
+traffic), `step_roofline` (the whole step's algorithmic bytes), `fp32_bound` (the step's
+estimated FP32 work against the FP32 FMA peak that `sph_fma_peak` measures on the same
+GPU at the start of the run), `kernel_ms_per_step` (CUDA-event profile of eager steps
+after the timed ones), `neighbour_lists` (list builds among the timed steps) and `clocks`.
+
+Under torchrun (N > 1) every rank runs an independent replica of a single scene (it does
+not shard at one-GPU scale: replicas only); the strip ensemble is sharded instead, each
+rank stepping its share of the strips.  The time is the max over ranks.
 `--impl reference` times the reference's algorithm on the host cores: the CPU
 restatement of the reference's kernels (the reference itself is Taichi, not installed
 and not installable here), float32, all host threads, on rank 0 only.

@@ -138,7 +138,7 @@ typedef struct SphParams {
     float   hourglass_alpha;
     int32_t hourglass_sts;        /* 0 in-loop damper + dt clamp, 1 sub-cycled          */
     int32_t hourglass_sts_cap;    /* max sub-cycle stages                               */
-    float   hourglass_sts_safety; /* 1.6 */
+    float   hourglass_sts_safety; /* RKL: the fraction of s^2+s dt may use (0.8)     */
     float   hg_S;                 /* lattice kernel sum of the damper (SOLID.py:1632)   */
     float   hg_W_dx0;             /* W(dx0)                                            */
     int32_t hg_sts_refresh;       /* recompute grad v after the half kick               */
@@ -156,7 +156,9 @@ typedef struct SphParams {
     float   av_alpha;             /* Monaghan pair viscosity alpha (0 with beta: off)   */
     float   av_beta;
     float   av_eps;               /* mu_ij regulariser epsilon (0.01)                   */
-    int32_t reserved[3];
+    int32_t hg_sts_rkl;           /* sub-cycled damper as s-stage RKL1 (else forward
+                                     Euler sub-steps), SOLID.py:4510-4576              */
+    int32_t reserved[2];
 } SphParams;
 
 /* ------------------------------------------------------------------ buffers */

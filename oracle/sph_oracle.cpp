@@ -1164,12 +1164,21 @@ struct Sim {
         if (!P.hourglass_sts) {
             if (hg) dt = std::min(dt, R(1.6 / (double)P.hg_rate));
         } else if (hg) {
+            // sts_stage_count (SOLID.py:4510-4539)
             int s = 1;
             if (P.hg_rate > 0.0f) {
-                double want = (double)P.hg_rate * (double)dt;
-                s = P.hg_sts_fixed > 0 ? P.hg_sts_fixed : std::max(1, (int)std::ceil(want / 1.6));
-                s = std::min(s, 32);
-                double cap = s * 1.6 / (double)P.hg_rate;
+                double want = (double)P.hg_rate * (double)dt, cap;
+                if (!P.hg_sts_rkl) {
+                    s = P.hg_sts_fixed > 0 ? P.hg_sts_fixed : std::max(1, (int)std::ceil(want / 1.6));
+                    s = std::min(s, 32);
+                    cap = s * 1.6 / (double)P.hg_rate;
+                } else {
+                    const double safety = (double)P.hourglass_sts_safety;
+                    if (P.hg_sts_fixed > 0) s = P.hg_sts_fixed;
+                    else
+                        while ((double)(s * s + s) * safety < want && s < 32) ++s;
+                    cap = safety * (double)(s * s + s) / (double)P.hg_rate;
+                }
                 if ((double)dt > cap) dt = R(cap);
             }
             sts_last = s;
@@ -1186,10 +1195,28 @@ struct Sim {
             if (P.hg_sts_refresh) compute_velocity_gradient();
             hg_ke_pre = kinetic();
             for (int64_t i = 0; i < n; ++i) hg_yb[i] = v[i];
-            R sub = R((double)dt / s);
-            for (int st = 0; st < s; ++st) {
-                compute_hg_accel();
-                for (int64_t i = 0; i < n; ++i) hg_yb[i] = hg_yb[i] + sub * hg_a[i];
+            if (!P.hg_sts_rkl) {
+                R sub = R((double)dt / s);
+                for (int st = 0; st < s; ++st) {
+                    compute_hg_accel();
+                    for (int64_t i = 0; i < n; ++i) hg_yb[i] = hg_yb[i] + sub * hg_a[i];
+                }
+            } else {
+                // hourglass_sts, 'rkl' (SOLID.py:4541-4576): Y_j = mu Y_(j-1) + nu Y_(j-2)
+                // + mu w1 dt M Y_(j-1), Y_0 = Y_1 = v, coefficients in double, then float
+                std::vector<V3<R>> ya(hg_yb);
+                const double w1 = 2.0 / (double)(s * s + s);
+                for (int j = 1; j <= s; ++j) {
+                    double mu = 1.0, nu = 0.0;
+                    if (j > 1) { mu = (2.0 * j - 1.0) / j; nu = (1.0 - j) / j; }
+                    const R muf = R(mu), nuf = R(nu), mut = R(mu * w1 * (double)dt);
+                    compute_hg_accel();
+                    for (int64_t i = 0; i < n; ++i) {
+                        V3<R> y = (muf * hg_yb[i] + nuf * ya[i]) + mut * hg_a[i];
+                        ya[i] = hg_yb[i];
+                        hg_yb[i] = y;
+                    }
+                }
             }
             for (int64_t i = 0; i < n; ++i) v[i] = hg_yb[i];
             hg_work += hg_ke_pre - kinetic();

@@ -156,7 +156,7 @@ UNSUPPORTED = {
     "DT_PAIR_SOUND_SPEED": ("all", "samematerial", "off"),
     "OBJECTIVE_RATE": ("jaumann",),
     "HOURGLASS_FORM": ("rate",),
-    "HOURGLASS_STS_MODE": ("subcycle",),
+    "HOURGLASS_STS_MODE": ("subcycle", "rkl"),
     "BULK_VISCOSITY_LENGTH": ("dx0", "h"),
 }
 
@@ -247,6 +247,11 @@ class SimConfig:
             errors.append("Shifting.gripHold is not implemented by sigmasph_b200")
         if float(resolved.get("dampingCoefficient") or 0.0) != 0.0:
             errors.append("Solver.dampingCoefficient is not implemented by sigmasph_b200")
+        if int(resolved.get("HOURGLASS_STS_STAGES") or 0) > 32:
+            # the device runs at most 32 damper stages per step (the reference's automatic
+            # count stops there too; only a fixed RKL count can ask for more)
+            errors.append("Hourglass.superTimeStepping.stages above 32 is not implemented by "
+                          "sigmasph_b200")
         if resolved.get("simulationMethod") == "deltaPlusSPH":
             if len(self.materials) > 1:
                 errors.append("a deltaPlusSPH deck has exactly one material")

@@ -1102,6 +1102,28 @@ __global__ void SPH_BOUNDS(SPH_OCC_SOLID_FORCE) k_solid_force(Cst c, Ptr P) {
 }
 
 // ------------------------------------------------------------------ dt, damper cap / stage count
+// sts_stage_count (SOLID.py:4510-4539): the smallest stage count whose interval covers
+// rate dt -- n forward-Euler sub-steps reach 1.6 n, s RKL1 stages safety (s^2 + s) --
+// or the deck's fixed count; *cap is the dt that count carries.
+__device__ __forceinline__ int sts_stage_count(const Cst& c, const Ptr& P, double rate, float dt,
+                                               double& cap) {
+    const double want = rate * (double)dt;
+    int s;
+    if (!c.p.hg_sts_rkl) {
+        s = c.p.hg_sts_fixed > 0 ? c.p.hg_sts_fixed : max(1, (int)ceil(want / 1.6));
+        if (s > kStsMaxStages) { s = kStsMaxStages; atomicOr(&P.sc->err, SPH_EW_STS_CAP); }
+        cap = s * 1.6 / rate;
+    } else {
+        const double safety = (double)c.p.hourglass_sts_safety;
+        s = 1;
+        if (c.p.hg_sts_fixed > 0) s = min(c.p.hg_sts_fixed, kStsMaxStages);
+        else
+            while ((double)(s * s + s) * safety < want && s < kStsMaxStages) ++s;
+        cap = safety * (double)(s * s + s) / rate;
+    }
+    return s;
+}
+
 __global__ void k_solid_dt(Cst c, Ptr P) {
     if (c.n_inst > 0) {
         // per instance: its own CFL dt, damper cap or stage count; grips cleared
@@ -1115,9 +1137,8 @@ __global__ void k_solid_dt(Cst c, Ptr P) {
                 if (!c.p.hourglass_sts) {
                     dt = fminf(dt, (float)(1.6 / rate));
                 } else {
-                    s = c.p.hg_sts_fixed > 0 ? c.p.hg_sts_fixed : max(1, (int)ceil(rate * (double)dt / 1.6));
-                    if (s > kStsMaxStages) { s = kStsMaxStages; atomicOr(&P.sc->err, SPH_EW_STS_CAP); }
-                    const double cap = s * 1.6 / rate;
+                    double cap;
+                    s = sts_stage_count(c, P, rate, dt, cap);
                     if ((double)dt > cap) dt = (float)cap;
                 }
             } else if (c.p.hourglass_alpha > 0.0f && c.p.hourglass_sts) {
@@ -1150,10 +1171,8 @@ __global__ void k_solid_dt(Cst c, Ptr P) {
     } else if (hg) {
         s = 1;
         if (c.p.hg_rate > 0.0f) {
-            double want = (double)c.p.hg_rate * (double)dt;
-            s = c.p.hg_sts_fixed > 0 ? c.p.hg_sts_fixed : max(1, (int)ceil(want / 1.6));
-            if (s > kStsMaxStages) { s = kStsMaxStages; atomicOr(&P.sc->err, SPH_EW_STS_CAP); }
-            double cap = s * 1.6 / (double)c.p.hg_rate;
+            double cap;
+            s = sts_stage_count(c, P, (double)c.p.hg_rate, dt, cap);
             if ((double)dt > cap) dt = (float)cap;
         }
     }
@@ -1190,6 +1209,7 @@ __global__ void __launch_bounds__(kBlock) k_half_kick(Cst c, Ptr P) {
         b5.x = v.z;
         P.aux[6 * i + 5] = b5;
         y_store(P, i, 0, f3(v));
+        if (c.p.hg_sts_rkl) y_store(P, i, 1, f3(v));   // RKL: Y_0 = Y_1 = v
         ke = (double)(0.5f * v.w * (v.x * v.x + v.y * v.y + v.z * v.z));
     }
     block_sum_atomic(ke, &P.sc->hg_work);   // + KE before the damper
@@ -1239,8 +1259,22 @@ __global__ void __launch_bounds__(kBlock) k_hg_stage(Cst c, Ptr P, int stage) {
         if (axc) ah.x *= 0.5f * (ri + r_axi_of(pj.y, c)) * inv_ri;
         acc += ah;
     });
-    const float sub = (float)((double)dt_at(c, P, ki) / (double)s);
-    y_store(P, i, wb, yi + sub * acc);
+    if (!c.p.hg_sts_rkl) {
+        const float sub = (float)((double)dt_at(c, P, ki) / (double)s);
+        y_store(P, i, wb, yi + sub * acc);
+    } else {
+        // RKL1 stage j (SOLID.py:4563-4575): Y_j = mu Y_(j-1) + nu Y_(j-2) + mu w1 dt M Y_(j-1),
+        // the coefficients in double and then float, as the host passes them there;
+        // Y_(j-2) is this particle's own entry of the buffer Y_j replaces
+        const int j = stage + 1;
+        double mu = 1.0, nu = 0.0;
+        if (j > 1) { mu = (2.0 * j - 1.0) / j; nu = (1.0 - j) / j; }
+        const double w1 = 2.0 / (double)(s * s + s);
+        const float muf = (float)mu, nuf = (float)nu;
+        const float mut = (float)(mu * w1 * (double)dt_at(c, P, ki));
+        const F3 yo = y_load(P, i, wb);
+        y_store(P, i, wb, (muf * yi + nuf * yo) + mut * acc);
+    }
 }
 
 __global__ void __launch_bounds__(kBlock) k_sts_finish(Cst c, Ptr P) {

@@ -76,7 +76,9 @@ def fill_solid_params(ps, p):
     p.hourglass_alpha = float(g("HOURGLASS_ALPHA") or 0.0)
     p.hourglass_sts = int(bool(g("HOURGLASS_STS")))
     p.hourglass_sts_cap = 32
-    p.hourglass_sts_safety = 1.6
+    sf = g("HOURGLASS_STS_SAFETY")
+    p.hourglass_sts_safety = 0.8 if sf is None else float(sf)
+    p.hg_sts_rkl = int(str(g("HOURGLASS_STS_MODE") or "subcycle").lower() == "rkl")
     p.hg_sts_fixed = int(g("HOURGLASS_STS_STAGES") or 0)
     rg = g("HOURGLASS_STS_REFRESH")
     p.hg_sts_refresh = int(True if rg is None else bool(rg))

@@ -106,3 +106,23 @@ def test_relaxation_switches():
     cfg = SimConfig(sc)
     assert (cfg.get_cfg("PST_RELAX_STEPS"), cfg.get_cfg("PST_RELAX_TOL")) == (40, 0.01)
     assert (cfg.get_cfg("exportRelaxationNetcdf"), cfg.get_cfg("exportRelaxationInterval")) == (True, 5)
+
+
+def test_sts_modes():
+    """Hourglass.superTimeStepping: 'subcycle' and 'rkl' (params.py:1170-1191); a fixed
+    count above the device's 32 stages is refused."""
+    from sigmasph_b200.solver import build_params
+    from sigmasph_b200.config import strip_json_comments
+    with open(DECKS["tensile_axi_dogbone_dx0.1"]) as f:
+        base = json.loads(strip_json_comments(f.read()))
+    for mode, rkl in (("subcycle", 0), ("rkl", 1)):
+        sc = json.loads(json.dumps(base))
+        sc["Hourglass"]["superTimeStepping"] = {"mode": mode, "safety": 0.7}
+        ps = ParticleSystem(SimConfig(sc), device="cpu")
+        p = build_params(ps)
+        assert p.hourglass_sts == 1 and p.hg_sts_rkl == rkl
+        assert p.hourglass_sts_safety == pytest.approx(0.7)
+    sc = json.loads(json.dumps(base))
+    sc["Hourglass"]["superTimeStepping"] = {"mode": "rkl", "stages": 40}
+    with pytest.raises(SceneError, match="above 32"):
+        SimConfig(sc)

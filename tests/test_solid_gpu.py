@@ -150,6 +150,17 @@ def axi_visc_deck():
     return sc
 
 
+def axi_rkl_deck():
+    """The axisymmetric dogbone with its sub-cycled damper as s-stage RKL1
+    (Hourglass.superTimeStepping.mode "rkl", SOLID.py:4510-4576)."""
+    import json
+    from sigmasph_b200.config import strip_json_comments
+    with open(axi_deck()) as f:
+        sc = json.loads(strip_json_comments(f.read()))
+    sc["Hourglass"]["superTimeStepping"]["mode"] = "rkl"
+    return sc
+
+
 # The GPU writes the return-mapped stress, plastic strain and energy to scratch in the
 # LAM stage and commits them with the volume update, so they are compared after it.
 STAGE_FIELDS = {
@@ -166,9 +177,10 @@ TOL32 = {"de_int": 2e-4, "pressure": 1e-3, "grad_v": 1e-4}
 TOL64 = {"de_int": 1e-3, "pressure": 2e-3, "acc": 5e-4, "grad_v": 2e-4}
 
 
-@pytest.mark.parametrize("deck", [axi_deck, bar3d_deck, strip_ps_deck, bar3d_visc_deck, axi_visc_deck],
+@pytest.mark.parametrize("deck", [axi_deck, bar3d_deck, strip_ps_deck, bar3d_visc_deck, axi_visc_deck,
+                                  axi_rkl_deck],
                          ids=["axi_dogbone_jc_sts", "bar3d_j2_inloop", "plane_strain_jc",
-                              "bar3d_q_monaghan", "axi_q_monaghan"])
+                              "bar3d_q_monaghan", "axi_q_monaghan", "axi_rkl"])
 def test_solid_stages_match_oracle(cuda, deck):
     ps, solver, o64, o32 = make_solid(deck())
     for s in range(8):
@@ -239,8 +251,8 @@ def test_solid_lists_between_builds_match_oracle(cuda, deck):
     assert A == B
 
 
-@pytest.mark.parametrize("deck", [axi_deck, bar3d_deck, bar3d_visc_deck],
-                         ids=["axi_dogbone", "bar3d", "bar3d_q_monaghan"])
+@pytest.mark.parametrize("deck", [axi_deck, bar3d_deck, bar3d_visc_deck, axi_rkl_deck],
+                         ids=["axi_dogbone", "bar3d", "bar3d_q_monaghan", "axi_rkl"])
 def test_solid_multistep_tracks_fp64(cuda, deck):
     ps, solver, o64, o32 = make_solid(deck())
     for o in (o64, o32):

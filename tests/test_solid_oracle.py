@@ -201,3 +201,26 @@ def test_viscosities_act_only_under_compression():
             assert d == 0.0
         else:
             assert d > 1e-3 * np.abs(r0["acc"]).max()
+
+
+@pytest.mark.parametrize("mode", ["subcycle", "rkl"])
+def test_sts_carries_a_rigid_translation(mode):
+    """The sub-cycled damper annihilates only what the linear velocity field does not
+    explain; under RKL1 each stage's mu + nu = 1 carries the null space through
+    (SOLID.py:4493-4502).  A free block translating rigidly keeps its velocity through
+    several steps of s > 1 stages."""
+    sc = free_block()
+    sc["Hourglass"] = {"alpha": 4.0, "superTimeStepping": {"mode": mode}}
+    ps = ParticleSystem(SimConfig(sc), device="cpu")
+    n = ps.particle_max_num
+    v0 = np.array([1.0, 0.5, -0.3], np.float32)
+    ps.v.from_numpy(np.tile(v0, (n, 1)))
+    p = build_params(ps)
+    assert p.hg_sts_rkl == (mode == "rkl")
+    o = Oracle(p, n, fp64=False)
+    o.set_state(state_from_sets(ps.state_numpy()), p.CFL * p.support_radius / p.c_signal)
+    o.stage(abi.STAGE_SORT)
+    o.step(5)
+    assert o.scalars()["sts_stages"] > 1
+    r = o.get_state()
+    assert np.abs(r["v"] - v0).max() <= 1e-5 * np.abs(v0).max()
