@@ -158,7 +158,9 @@ typedef struct SphParams {
     float   av_eps;               /* mu_ij regulariser epsilon (0.01)                   */
     int32_t hg_sts_rkl;           /* sub-cycled damper as s-stage RKL1 (else forward
                                      Euler sub-steps), SOLID.py:4510-4576              */
-    int32_t reserved[2];
+    int32_t objective_none;       /* Solver.objectiveRate "none": no spin terms in the
+                                     stress rate (SOLID.py:368, :2721-2722)            */
+    int32_t reserved[1];
 } SphParams;
 
 /* ------------------------------------------------------------------ buffers */

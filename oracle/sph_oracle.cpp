@@ -786,7 +786,8 @@ struct Sim {
                 R dev = ed[a][b] - ((a == b) ? tr / R(3) : R(0));
                 R ws = 0, sw = 0;
                 for (int k = 0; k < 3; ++k) { ws += sp[a][k] * s[k][b]; sw += s[a][k] * sp[k][b]; }
-                sd[a][b] = G2 * dev + (ws - sw);
+                // SOLID.py:2721-2722: the spin terms only under the Jaumann rate
+                sd[a][b] = P.objective_none ? G2 * dev : G2 * dev + (ws - sw);
             }
             R dep = 0;
             if (ale) {

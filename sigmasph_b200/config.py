@@ -154,7 +154,7 @@ UNSUPPORTED = {
     "PST_CLAMP": ("displacement", "velocity", "both"),
     "PST_NORMAL": ("gradlam", "eigvec"),
     "DT_PAIR_SOUND_SPEED": ("all", "samematerial", "off"),
-    "OBJECTIVE_RATE": ("jaumann",),
+    "OBJECTIVE_RATE": ("jaumann", "none"),
     "HOURGLASS_FORM": ("rate",),
     "HOURGLASS_STS_MODE": ("subcycle", "rkl"),
     "BULK_VISCOSITY_LENGTH": ("dx0", "h"),

@@ -687,6 +687,7 @@ __global__ void SPH_BOUNDS(SPH_OCC_SOLID_B) k_solid_b(Cst c, Ptr P) {
         float S[3][3] = {{s.xx, s.xy, s.xz}, {s.xy, s.yy, s.yz}, {s.xz, s.yz, s.zz}};
         const SphMatRow& Mi = P.mat[ki];
         const float G2 = 2.0f * Mi.G;
+        const bool spin = !c.p.objective_none;
         float Sn[3][3];
 #pragma unroll
         for (int a = 0; a < 3; ++a)
@@ -695,7 +696,7 @@ __global__ void SPH_BOUNDS(SPH_OCC_SOLID_B) k_solid_b(Cst c, Ptr P) {
                 float dev = ed[a][b] - ((a == b) ? tr / 3.0f : 0.0f);
                 float ws = sp[a][0] * S[0][b] + sp[a][1] * S[1][b] + sp[a][2] * S[2][b];
                 float sw = S[a][0] * sp[0][b] + S[a][1] * sp[1][b] + S[a][2] * sp[2][b];
-                Sn[a][b] = G2 * dev + (ws - sw);
+                Sn[a][b] = spin ? G2 * dev + (ws - sw) : G2 * dev;
             }
         Sn[0][0] += A.xx; Sn[1][1] += A.yy; Sn[2][2] += A.zz;
         Sn[0][1] += A.xy; Sn[1][0] += A.xy; Sn[0][2] += A.xz; Sn[2][0] += A.xz; Sn[1][2] += A.yz; Sn[2][1] += A.yz;

@@ -78,6 +78,7 @@ def fill_solid_params(ps, p):
     p.hourglass_sts_cap = 32
     sf = g("HOURGLASS_STS_SAFETY")
     p.hourglass_sts_safety = 0.8 if sf is None else float(sf)
+    p.objective_none = int(str(g("OBJECTIVE_RATE") or "jaumann").lower() == "none")
     p.hg_sts_rkl = int(str(g("HOURGLASS_STS_MODE") or "subcycle").lower() == "rkl")
     p.hg_sts_fixed = int(g("HOURGLASS_STS_STAGES") or 0)
     rg = g("HOURGLASS_STS_REFRESH")

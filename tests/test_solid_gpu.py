@@ -150,6 +150,13 @@ def axi_visc_deck():
     return sc
 
 
+def bar3d_no_spin_deck():
+    """The bar with Solver.objectiveRate "none": the stress rate without its spin terms."""
+    sc = bar3d_deck()
+    sc["Solver"]["objectiveRate"] = "none"
+    return sc
+
+
 def axi_rkl_deck():
     """The axisymmetric dogbone with its sub-cycled damper as s-stage RKL1
     (Hourglass.superTimeStepping.mode "rkl", SOLID.py:4510-4576)."""
@@ -178,9 +185,9 @@ TOL64 = {"de_int": 1e-3, "pressure": 2e-3, "acc": 5e-4, "grad_v": 2e-4}
 
 
 @pytest.mark.parametrize("deck", [axi_deck, bar3d_deck, strip_ps_deck, bar3d_visc_deck, axi_visc_deck,
-                                  axi_rkl_deck],
+                                  axi_rkl_deck, bar3d_no_spin_deck],
                          ids=["axi_dogbone_jc_sts", "bar3d_j2_inloop", "plane_strain_jc",
-                              "bar3d_q_monaghan", "axi_q_monaghan", "axi_rkl"])
+                              "bar3d_q_monaghan", "axi_q_monaghan", "axi_rkl", "bar3d_no_spin"])
 def test_solid_stages_match_oracle(cuda, deck):
     ps, solver, o64, o32 = make_solid(deck())
     for s in range(8):

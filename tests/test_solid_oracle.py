@@ -224,3 +224,32 @@ def test_sts_carries_a_rigid_translation(mode):
     assert o.scalars()["sts_stages"] > 1
     r = o.get_state()
     assert np.abs(r["v"] - v0).max() <= 1e-5 * np.abs(v0).max()
+
+
+def test_objective_rate_none_drops_the_spin():
+    """Under a rigid rotation the strain rate vanishes in the interior, so there the
+    Jaumann rate turns the stress with the body while objectiveRate "none" leaves it
+    (SOLID.py:2721-2722)."""
+    out = {}
+    for rate in ("jaumann", "none"):
+        sc = free_block()
+        sc["Solver"]["objectiveRate"] = rate
+        sc["Hourglass"] = {"alpha": 0.0}
+        ps = ParticleSystem(SimConfig(sc), device="cpu")
+        x = ps.x.to_numpy().astype(np.float64)
+        c = x.mean(0)
+        w = np.array([0.0, 0.0, 2.0])
+        ps.v.from_numpy(np.cross(w, x - c).astype(np.float32))
+        s = np.zeros((ps.particle_max_num, 3, 3), np.float32)
+        s[:, 0, 0], s[:, 1, 1] = 0.01, -0.01          # deviatoric, below yield
+        ps.sigma_dev.from_numpy(s)
+        p = build_params(ps)
+        assert p.objective_none == (rate == "none")
+        o = Oracle(p, ps.particle_max_num, fp64=True)
+        o.set_state(state_from_sets(ps.state_numpy()), 1e-4)
+        for st in (abi.STAGE_SORT, abi.STAGE_LAM, abi.STAGE_CONTINUITY):
+            o.stage(st)
+        r = o.get_state()
+        inner = np.all(np.abs(r["x"] - c) < 1.5, axis=1)
+        out[rate] = np.abs(r["sdev"][inner][:, 3]).max()   # s_xy: the rotated shear
+    assert out["jaumann"] > 1e-6 and out["none"] <= 1e-3 * out["jaumann"], out
