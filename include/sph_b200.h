@@ -160,7 +160,8 @@ typedef struct SphParams {
                                      Euler sub-steps), SOLID.py:4510-4576              */
     int32_t objective_none;       /* Solver.objectiveRate "none": no spin terms in the
                                      stress rate (SOLID.py:368, :2721-2722)            */
-    int32_t reserved[1];
+    int32_t axi_image_signed;     /* conservative axial stress pair: a mirror image's
+                                     radius is its signed coordinate (SOLID.py:3598-3609)*/
 } SphParams;
 
 /* ------------------------------------------------------------------ buffers */

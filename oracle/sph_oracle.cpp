@@ -962,7 +962,11 @@ struct Sim {
                     }
                     f[a] = wi * w(j) * t;
                 }
-                if (P.axisymmetric && P.axi_conservative_x) f[0] = f[0] * (R(0.5) * (r_of(i) + r_of(j)) / r_of(i));
+                if (P.axisymmetric && P.axi_conservative_x) {
+                    // SOLID.py:3598-3609: a mirror image at its signed radius under "signed"
+                    const R rs = (mir && P.axi_image_signed) ? r_of(i) - r_of(j) : r_of(i) + r_of(j);
+                    f[0] = f[0] * (R(0.5) * rs / r_of(i));
+                }
                 dv += {f[0] / mwi, f[1] / mwi, f[2] / mwi};
                 V3<R> vij = v[i] - vj;
                 dei += -R(0.5) * dot(f, vij) / mwi;

@@ -72,7 +72,7 @@ PARAM_FIELDS = [
     ("ale_diffusion", _f32), ("num_constraints", _i32), ("ramp_time", _f32),
     ("jc_surrogate", _i32), ("jc_surrogate_tol", _f32), ("hg_sts_fixed", _i32),
     ("q_l2", _f32), ("q_cl", _f32), ("av_alpha", _f32), ("av_beta", _f32), ("av_eps", _f32),
-    ("hg_sts_rkl", _i32), ("objective_none", _i32), ("reserved", _i32 * 1),
+    ("hg_sts_rkl", _i32), ("objective_none", _i32), ("axi_image_signed", _i32),
 ]
 
 

@@ -87,6 +87,9 @@ REGISTRY = [
     ("axisymmetric", ("Domain",), "axisymmetric", "bool", False),
     ("symmetryPlanes", ("Domain",), "symmetryPlanes", "str", ""),
     ("AXI_R_MIN", ("Domain",), "axisRadiusMin", "float", 0.5),
+    ("AXI_CONSERVATIVE_X", ("Domain",), "conservativeAxialMomentum", "bool", True),
+    ("AXI_CONSERVATIVE_R", ("Domain",), "conservativeRadialForce", "bool", False),
+    ("AXI_IMAGE_RADIUS", ("Domain",), "axialImageRadius", "str", "ring"),
     ("DOMAIN_BOUNDARY", ("Domain",), "boundary", "str", "open"),
     ("DOMAIN_RESTITUTION", ("Domain",), "restitution", "float", 0.5),
     ("CFL", ("Time",), "CFL", "float", None),
@@ -97,6 +100,7 @@ REGISTRY = [
     ("DT_PAIR_SOUND_SPEED", ("Time",), "pairSoundSpeed", "str", "samematerial"),
     ("simulationMethod", ("Solver",), "type", "str", None),
     ("viscosity", ("Solver",), "viscosity", "float", None),
+    ("stiffness", ("Solver",), "stiffness", "float", 50000.0),   # rotating-patch IC only
     ("allowNegativePressure", ("Solver",), "allowNegativePressure", "bool", False),
     ("DISPLACEMENT_POSITIONS", ("Solver",), "displacementPositions", "bool", True),
     ("COMPENSATED_VOLUME", ("Solver",), "compensatedVolume", "bool", True),
@@ -158,6 +162,8 @@ UNSUPPORTED = {
     "HOURGLASS_FORM": ("rate",),
     "HOURGLASS_STS_MODE": ("subcycle", "rkl"),
     "BULK_VISCOSITY_LENGTH": ("dx0", "h"),
+    "AXI_IMAGE_RADIUS": ("ring", "signed"),
+    "AXI_CONSERVATIVE_R": (False,),
 }
 
 # Cards the format knows, and those whose content is accepted but not read here

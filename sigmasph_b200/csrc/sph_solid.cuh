@@ -1027,7 +1027,8 @@ __global__ void SPH_BOUNDS(SPH_OCC_SOLID_FORCE) k_solid_force(Cst c, Ptr P) {
             F3 f = {ww * (ss.xx * g.x + ss.xy * g.y + ss.xz * g.z),
                     ww * (ss.xy * g.x + ss.yy * g.y + ss.yz * g.z),
                     ww * (ss.xz * g.x + ss.yz * g.y + ss.zz * g.z)};
-            f.x *= ratio;
+            // axialImageRadius "signed": an image's radius is the coordinate it sits at
+            f.x *= (mir && c.p.axi_image_signed) ? 0.5f * (ri - rj) * inv_ri : ratio;
             a += inv_mw * f;
             dei += -0.5f * dot3(f, vij) * inv_mw;
             float vxy = dot3(vij, r);

@@ -126,3 +126,24 @@ def test_sts_modes():
     sc["Hourglass"]["superTimeStepping"] = {"mode": "rkl", "stages": 40}
     with pytest.raises(SceneError, match="above 32"):
         SimConfig(sc)
+
+
+def test_axisymmetric_forms():
+    """Domain.conservativeAxialMomentum / axialImageRadius select the axial pair forms
+    (params.py:302-355); conservativeRadialForce true is refused, not ignored."""
+    from sigmasph_b200.solver import build_params
+    from sigmasph_b200.config import strip_json_comments
+    with open(DECKS["tensile_axi_dogbone_dx0.1"]) as f:
+        base = json.loads(strip_json_comments(f.read()))
+    ps = ParticleSystem(SimConfig(base), device="cpu")
+    p0 = build_params(ps)
+    assert (p0.axi_conservative_x, p0.axi_image_signed) == (1, 0)
+    sc = json.loads(json.dumps(base))
+    sc["Domain"].update({"conservativeAxialMomentum": False, "axialImageRadius": "signed"})
+    p1 = build_params(ParticleSystem(SimConfig(sc), device="cpu"))
+    assert (p1.axi_conservative_x, p1.axi_image_signed) == (0, 0)
+    assert p1.hg_rate < p0.hg_rate                 # no axis ratio in the damper's rate
+    sc = json.loads(json.dumps(base))
+    sc["Domain"]["conservativeRadialForce"] = True
+    with pytest.raises(SceneError, match="AXI_CONSERVATIVE_R"):
+        SimConfig(sc)

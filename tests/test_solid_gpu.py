@@ -157,6 +157,29 @@ def bar3d_no_spin_deck():
     return sc
 
 
+def _axi_json():
+    import json
+    from sigmasph_b200.config import strip_json_comments
+    with open(axi_deck()) as f:
+        return json.loads(strip_json_comments(f.read()))
+
+
+def axi_signed_deck():
+    """Domain.axialImageRadius "signed": the axial stress pair reads a mirror image's
+    radius as the coordinate it sits at (SOLID.py:3598-3609)."""
+    sc = _axi_json()
+    sc["Domain"]["axialImageRadius"] = "signed"
+    return sc
+
+
+def axi_plain_axial_deck():
+    """Domain.conservativeAxialMomentum false: no pair-radius rescaling of the axial
+    forces, and the damper's rate without the axis ratio."""
+    sc = _axi_json()
+    sc["Domain"]["conservativeAxialMomentum"] = False
+    return sc
+
+
 def axi_rkl_deck():
     """The axisymmetric dogbone with its sub-cycled damper as s-stage RKL1
     (Hourglass.superTimeStepping.mode "rkl", SOLID.py:4510-4576)."""
@@ -185,9 +208,10 @@ TOL64 = {"de_int": 1e-3, "pressure": 2e-3, "acc": 5e-4, "grad_v": 2e-4}
 
 
 @pytest.mark.parametrize("deck", [axi_deck, bar3d_deck, strip_ps_deck, bar3d_visc_deck, axi_visc_deck,
-                                  axi_rkl_deck, bar3d_no_spin_deck],
+                                  axi_rkl_deck, bar3d_no_spin_deck, axi_signed_deck, axi_plain_axial_deck],
                          ids=["axi_dogbone_jc_sts", "bar3d_j2_inloop", "plane_strain_jc",
-                              "bar3d_q_monaghan", "axi_q_monaghan", "axi_rkl", "bar3d_no_spin"])
+                              "bar3d_q_monaghan", "axi_q_monaghan", "axi_rkl", "bar3d_no_spin",
+                              "axi_signed_image", "axi_plain_axial"])
 def test_solid_stages_match_oracle(cuda, deck):
     ps, solver, o64, o32 = make_solid(deck())
     for s in range(8):
