@@ -162,6 +162,9 @@ typedef struct SphParams {
                                      stress rate (SOLID.py:368, :2721-2722)            */
     int32_t axi_image_signed;     /* conservative axial stress pair: a mirror image's
                                      radius is its signed coordinate (SOLID.py:3598-3609)*/
+    int32_t axi_conservative_r;   /* axisymmetric conservative radial form: the pair
+                                     radius in every radial pair force, the source
+                                     (p + q - s_tt) / (rho r)  (SOLID.py:3444-3466)    */
 } SphParams;
 
 /* ------------------------------------------------------------------ buffers */

@@ -962,11 +962,19 @@ struct Sim {
                     }
                     f[a] = wi * w(j) * t;
                 }
-                if (P.axisymmetric && P.axi_conservative_x) {
+                const bool axc = P.axisymmetric && P.axi_conservative_x;
+                const bool axr = P.axisymmetric && P.axi_conservative_r;
+                if (axc) {
                     // SOLID.py:3598-3609: a mirror image at its signed radius under "signed"
                     const R rs = (mir && P.axi_image_signed) ? r_of(i) - r_of(j) : r_of(i) + r_of(j);
                     f[0] = f[0] * (R(0.5) * rs / r_of(i));
                 }
+                if (axr) {
+                    // SOLID.py:3609-3614: the radial form, an image always at its signed radius
+                    const R rs = mir ? r_of(i) - r_of(j) : r_of(i) + r_of(j);
+                    f[1] = f[1] * (R(0.5) * rs / r_of(i));
+                }
+                const R pratio = (axc || axr) ? R(0.5) * (r_of(i) + r_of(j)) / r_of(i) : R(1);
                 dv += {f[0] / mwi, f[1] / mwi, f[2] / mwi};
                 V3<R> vij = v[i] - vj;
                 dei += -R(0.5) * dot(f, vij) / mwi;
@@ -989,11 +997,9 @@ struct Sim {
                     R pij = (-R(P.av_alpha) * c_bar * mu + R(P.av_beta) * mu * mu) / rho_bar;
                     V3<R> ap = (-mw(j) * pij) * g;
                     R mu_cfl = -mu;
-                    if (P.axisymmetric && P.axi_conservative_x) {
-                        R ratio = R(0.5) * (r_of(i) + r_of(j)) / r_of(i);
-                        ap[0] = ap[0] * ratio;
-                        mu_cfl = mu_cfl * ratio;
-                    }
+                    if (axc) ap[0] = ap[0] * pratio;
+                    if (axr) ap[1] = ap[1] * pratio;
+                    if (axc || axr) mu_cfl = mu_cfl * pratio;
                     dv += ap;
                     mu_max = std::max(mu_max, mu_cfl);
                     R wp = -R(0.5) * dot(ap, vij);
@@ -1016,7 +1022,8 @@ struct Sim {
                     R damp = R(P.hourglass_alpha) * (R(P.mat_rho0[k]) / rho_i) * (R(P.mat_cp[k]) / h)
                              * (w(j) / R(P.V0)) * (Wij / R(P.hg_W_dx0)) * hg;
                     V3<R> ah = damp * rh;
-                    if (P.axisymmetric && P.axi_conservative_x) ah[0] = ah[0] * (R(0.5) * (r_of(i) + r_of(j)) / r_of(i));
+                    if (axc) ah[0] = ah[0] * pratio;
+                    if (axr) ah[1] = ah[1] * pratio;
                     dv += ah;
                     dhg += -R(0.5) * dot(ah, vij);
                 }
@@ -1033,8 +1040,14 @@ struct Sim {
                 }
             });
             if (P.axisymmetric) {
+                // SOLID.py:3444-3466: the sources the pair sums do not generate
                 R inv = R(1) / (rho_i * r_axi(i));
-                dv[1] += (sdev[i][1][1] - sdev[i][2][2]) * inv;
+                V3<R> ag = {P.axi_conservative_x ? R(0) : sdev[i][0][1] * inv,
+                            P.axi_conservative_r ? (ptot_i - sdev[i][2][2]) * inv
+                                                 : (sdev[i][1][1] - sdev[i][2][2]) * inv,
+                            R(0)};
+                dv += ag;
+                if (P.axi_conservative_r) dei += -dot(v[i], ag);
             }
             acc[i] += dv;
             de_int[i] = dei;
@@ -1102,7 +1115,11 @@ struct Sim {
                 R damp = R(P.hourglass_alpha) * (R(P.mat_rho0[k]) / rho_i) * (R(P.mat_cp[k]) / h)
                          * (w(j) / R(P.V0)) * (Wij / R(P.hg_W_dx0)) * hg;
                 V3<R> ah = damp * rh;
-                if (P.axisymmetric && P.axi_conservative_x) ah[0] = ah[0] * (R(0.5) * (r_of(i) + r_of(j)) / r_of(i));
+                if (P.axisymmetric && (P.axi_conservative_x || P.axi_conservative_r)) {
+                    const R ratio = R(0.5) * (r_of(i) + r_of(j)) / r_of(i);
+                    if (P.axi_conservative_x) ah[0] = ah[0] * ratio;
+                    if (P.axi_conservative_r) ah[1] = ah[1] * ratio;
+                }
                 a += ah;
             });
             hg_a[i] = a;

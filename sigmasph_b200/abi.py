@@ -73,6 +73,7 @@ PARAM_FIELDS = [
     ("jc_surrogate", _i32), ("jc_surrogate_tol", _f32), ("hg_sts_fixed", _i32),
     ("q_l2", _f32), ("q_cl", _f32), ("av_alpha", _f32), ("av_beta", _f32), ("av_eps", _f32),
     ("hg_sts_rkl", _i32), ("objective_none", _i32), ("axi_image_signed", _i32),
+    ("axi_conservative_r", _i32),
 ]
 
 

@@ -163,7 +163,6 @@ UNSUPPORTED = {
     "HOURGLASS_STS_MODE": ("subcycle", "rkl"),
     "BULK_VISCOSITY_LENGTH": ("dx0", "h"),
     "AXI_IMAGE_RADIUS": ("ring", "signed"),
-    "AXI_CONSERVATIVE_R": (False,),
 }
 
 # Cards the format knows, and those whose content is accepted but not read here

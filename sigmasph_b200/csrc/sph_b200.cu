@@ -288,7 +288,7 @@ int sph_params_layout(char* buf, int cap) {
     F(kernel_correction) F(l_eig_tol) F(hourglass_alpha) F(hourglass_sts) F(hourglass_sts_cap)
     F(hourglass_sts_safety) F(hg_S) F(hg_W_dx0) F(hg_sts_refresh) F(ale_history) F(transport_e)
     F(ale_diffusion) F(num_constraints) F(ramp_time) F(jc_surrogate) F(jc_surrogate_tol)
-    F(q_l2) F(q_cl) F(av_alpha) F(av_beta) F(av_eps) F(hg_sts_rkl) F(objective_none) F(axi_image_signed)
+    F(q_l2) F(q_cl) F(av_alpha) F(av_beta) F(av_eps) F(hg_sts_rkl) F(objective_none) F(axi_image_signed) F(axi_conservative_r)
 #undef F
     if (buf && cap > 0) {
         size_t k = std::min<size_t>(s.size(), (size_t)cap - 1);

@@ -962,6 +962,7 @@ __global__ void SPH_BOUNDS(SPH_OCC_SOLID_FORCE) k_solid_force(Cst c, Ptr P) {
         const bool ale = c.p.pst_enabled && c.p.pst_ale_momentum;
         const bool hg_inloop = c.p.hourglass_alpha > 0.0f && !c.p.hourglass_sts;
         const bool axc = c.p.axisymmetric && c.p.axi_conservative_x;
+        const bool axr = c.p.axisymmetric && c.p.axi_conservative_r;
         const float ri = r_axi_of(pi.y, c), inv_ri = 1.0f / ri;
         float Gi[3][3];
         if (hg_inloop) load_gradv(P, i, Gi);
@@ -987,7 +988,9 @@ __global__ void SPH_BOUNDS(SPH_OCC_SOLID_FORCE) k_solid_force(Cst c, Ptr P) {
             F3 g = wendland_dW2(r, rn2, rn, c);
             float w_j = w_of(pj, c);
             const float rj = r_axi_of(pj.y, c);
-            const float ratio = axc ? 0.5f * (ri + rj) * inv_ri : 1.0f;
+            // the pair radius over r_i, on the axial (axc) and radial (axr) pair forces
+            const float ratio = (axc || axr) ? 0.5f * (ri + rj) * inv_ri : 1.0f;
+            const float rx = axc ? ratio : 1.0f, ry = axr ? ratio : 1.0f;
             F3 vij = vi - vj;
             // the in-loop damper first: j's velocity-gradient record also carries its
             // pressure (k_solid_commit), and is dead once this term is summed
@@ -1008,7 +1011,8 @@ __global__ void SPH_BOUNDS(SPH_OCC_SOLID_FORCE) k_solid_force(Cst c, Ptr P) {
                     float hg = dot3(dvh, rh);
                     float damp = hg_pre * w_j * wendland_W(rn, c) * hg;
                     F3 ah = damp * rh;
-                    ah.x *= ratio;
+                    ah.x *= rx;
+                    ah.y *= ry;
                     a += ah;
                     dhg += -0.5f * dot3(ah, vij);
                 }
@@ -1027,8 +1031,11 @@ __global__ void SPH_BOUNDS(SPH_OCC_SOLID_FORCE) k_solid_force(Cst c, Ptr P) {
             F3 f = {ww * (ss.xx * g.x + ss.xy * g.y + ss.xz * g.z),
                     ww * (ss.xy * g.x + ss.yy * g.y + ss.yz * g.z),
                     ww * (ss.xz * g.x + ss.yz * g.y + ss.zz * g.z)};
-            // axialImageRadius "signed": an image's radius is the coordinate it sits at
-            f.x *= (mir && c.p.axi_image_signed) ? 0.5f * (ri - rj) * inv_ri : ratio;
+            // axialImageRadius "signed" (and the radial form always): a mirror image's
+            // radius is the coordinate it sits at
+            const float signed_ratio = 0.5f * (ri - rj) * inv_ri;
+            f.x *= (axc && mir && c.p.axi_image_signed) ? signed_ratio : rx;
+            if (axr) f.y *= mir ? signed_ratio : ratio;
             a += inv_mw * f;
             dei += -0.5f * dot3(f, vij) * inv_mw;
             float vxy = dot3(vij, r);
@@ -1047,7 +1054,9 @@ __global__ void SPH_BOUNDS(SPH_OCC_SOLID_FORCE) k_solid_force(Cst c, Ptr P) {
                 const float pij = (-c.p.av_alpha * c_bar * mu + c.p.av_beta * mu * mu) / rho_bar;
                 F3 ap = (-mw_of(vj4.w, pj, c) * pij) * g;
                 float mu_cfl = -mu;
-                if (axc) { ap.x *= ratio; mu_cfl *= ratio; }
+                ap.x *= rx;
+                ap.y *= ry;
+                mu_cfl *= ratio;
                 a += ap;
                 mu_max = fmaxf(mu_max, mu_cfl);
                 dvisc += 0.5f * dot3(ap, vij);
@@ -1074,7 +1083,14 @@ __global__ void SPH_BOUNDS(SPH_OCC_SOLID_FORCE) k_solid_force(Cst c, Ptr P) {
                 }
             }
         });
-        if (c.p.axisymmetric) a.y += (s.yy - s.zz) / (rho_i * ri);
+        if (c.p.axisymmetric) {
+            // the geometric sources the pair sums do not generate (SOLID.py:3444-3466)
+            const float inv_rho_r = 1.0f / (rho_i * ri);
+            F3 ag = {axc ? 0.0f : s.xy * inv_rho_r,
+                     axr ? (ptot_i - s.zz) * inv_rho_r : (s.yy - s.zz) * inv_rho_r, 0.0f};
+            a += ag;
+            if (axr) dei += -dot3(vi, ag);   // the hoop stress power
+        }
         dei -= dvisc;
         float4 a0 = P.acc[i];
         F3 an = {a0.x + a.x, a0.y + a.y, a0.z + a.z};
@@ -1234,6 +1250,7 @@ __global__ void __launch_bounds__(kBlock) k_hg_stage(Cst c, Ptr P, int stage) {
     float Gi[3][3];
     load_gradv(P, i, Gi);
     const bool axc = c.p.axisymmetric && c.p.axi_conservative_x;
+    const bool axr = c.p.axisymmetric && c.p.axi_conservative_r;
     const float ri = r_axi_of(pi.y, c), inv_ri = 1.0f / ri;
     const float hg_pre = c.p.hourglass_alpha * (P.mat[ki].rho0 / rho_i) * (P.mat[ki].cp * c.inv_h)
                          / (c.p.V0 * (float)c.p.hg_W_dx0);
@@ -1258,7 +1275,11 @@ __global__ void __launch_bounds__(kBlock) k_hg_stage(Cst c, Ptr P, int stage) {
         float hg = dot3(dvh, rh);
         float damp = hg_pre * w_of(pj, c) * wendland_W(rn, c) * hg;
         F3 ah = damp * rh;
-        if (axc) ah.x *= 0.5f * (ri + r_axi_of(pj.y, c)) * inv_ri;
+        if (axc || axr) {
+            const float ratio = 0.5f * (ri + r_axi_of(pj.y, c)) * inv_ri;
+            if (axc) ah.x *= ratio;
+            if (axr) ah.y *= ratio;
+        }
         acc += ah;
     });
     if (!c.p.hg_sts_rkl) {

@@ -73,6 +73,7 @@ def fill_solid_params(ps, p):
     # Domain.conservativeAxialMomentum (default on) and axialImageRadius (SOLID.py:262-315)
     cx = g("AXI_CONSERVATIVE_X")
     p.axi_conservative_x = int(bool(ps.axisymmetric) and (True if cx is None else bool(cx)))
+    p.axi_conservative_r = int(bool(ps.axisymmetric) and bool(g("AXI_CONSERVATIVE_R")))
     p.axi_image_signed = int(bool(p.axi_conservative_x)
                              and str(g("AXI_IMAGE_RADIUS") or "ring").lower() == "signed")
     dx0 = ps.particle_diameter
@@ -89,7 +90,8 @@ def fill_solid_params(ps, p):
     p.hg_sts_refresh = int(True if rg is None else bool(rg))
     p.hg_S = reference_kernel_sum(dx0, h, ps.two_d)
     p.hg_W_dx0 = wendland_scalar(dx0, h, ps.two_d)
-    ratio_max = 1.0 + h / (2.0 * ps.axi_r_min) if p.axi_conservative_x else 1.0
+    ratio_max = (1.0 + h / (2.0 * ps.axi_r_min)
+                 if (p.axi_conservative_x or p.axi_conservative_r) else 1.0)
     p.hg_rate = (p.hourglass_alpha * c_p / ps.h_min * reference_kernel_sum(dx0, h, ps.two_d)
                  * ratio_max) if p.hourglass_alpha > 0.0 else 0.0
     hist = g("PST_ALE_HISTORY")

@@ -129,8 +129,8 @@ def test_sts_modes():
 
 
 def test_axisymmetric_forms():
-    """Domain.conservativeAxialMomentum / axialImageRadius select the axial pair forms
-    (params.py:302-355); conservativeRadialForce true is refused, not ignored."""
+    """Domain.conservativeAxialMomentum / conservativeRadialForce / axialImageRadius
+    select the axisymmetric pair forms (params.py:302-355)."""
     from sigmasph_b200.solver import build_params
     from sigmasph_b200.config import strip_json_comments
     with open(DECKS["tensile_axi_dogbone_dx0.1"]) as f:
@@ -143,7 +143,9 @@ def test_axisymmetric_forms():
     p1 = build_params(ParticleSystem(SimConfig(sc), device="cpu"))
     assert (p1.axi_conservative_x, p1.axi_image_signed) == (0, 0)
     assert p1.hg_rate < p0.hg_rate                 # no axis ratio in the damper's rate
+    assert p0.axi_conservative_r == 0
     sc = json.loads(json.dumps(base))
-    sc["Domain"]["conservativeRadialForce"] = True
-    with pytest.raises(SceneError, match="AXI_CONSERVATIVE_R"):
-        SimConfig(sc)
+    sc["Domain"].update({"conservativeAxialMomentum": False, "conservativeRadialForce": True})
+    p2 = build_params(ParticleSystem(SimConfig(sc), device="cpu"))
+    assert (p2.axi_conservative_x, p2.axi_conservative_r) == (0, 1)
+    assert p2.hg_rate == p0.hg_rate                # the axis ratio is back with either form

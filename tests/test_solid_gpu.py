@@ -180,6 +180,15 @@ def axi_plain_axial_deck():
     return sc
 
 
+def axi_radial_deck():
+    """Domain.conservativeRadialForce with Monaghan's viscosity and q: the pair radius in
+    every radial pair force (stress with an image's signed radius, Pi_ij, the damper) and
+    the source (p + q - s_tt) / (rho r) with its hoop power (SOLID.py:3444-3466)."""
+    sc = axi_visc_deck()
+    sc["Domain"]["conservativeRadialForce"] = True
+    return sc
+
+
 def axi_rkl_deck():
     """The axisymmetric dogbone with its sub-cycled damper as s-stage RKL1
     (Hourglass.superTimeStepping.mode "rkl", SOLID.py:4510-4576)."""
@@ -208,10 +217,11 @@ TOL64 = {"de_int": 1e-3, "pressure": 2e-3, "acc": 5e-4, "grad_v": 2e-4}
 
 
 @pytest.mark.parametrize("deck", [axi_deck, bar3d_deck, strip_ps_deck, bar3d_visc_deck, axi_visc_deck,
-                                  axi_rkl_deck, bar3d_no_spin_deck, axi_signed_deck, axi_plain_axial_deck],
+                                  axi_rkl_deck, bar3d_no_spin_deck, axi_signed_deck, axi_plain_axial_deck,
+                                  axi_radial_deck],
                          ids=["axi_dogbone_jc_sts", "bar3d_j2_inloop", "plane_strain_jc",
                               "bar3d_q_monaghan", "axi_q_monaghan", "axi_rkl", "bar3d_no_spin",
-                              "axi_signed_image", "axi_plain_axial"])
+                              "axi_signed_image", "axi_plain_axial", "axi_radial"])
 def test_solid_stages_match_oracle(cuda, deck):
     ps, solver, o64, o32 = make_solid(deck())
     for s in range(8):

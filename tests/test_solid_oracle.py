@@ -253,3 +253,47 @@ def test_objective_rate_none_drops_the_spin():
         inner = np.all(np.abs(r["x"] - c) < 1.5, axis=1)
         out[rate] = np.abs(r["sdev"][inner][:, 3]).max()   # s_xy: the rotated shear
     assert out["jaumann"] > 1e-6 and out["none"] <= 1e-3 * out["jaumann"], out
+
+
+def _axi_power_imbalance(radial):
+    """sum_i m_i (de_i + a_i . v_i) / sum_i |m_i a_i . v_i| of the axisymmetric dogbone's
+    force stage (no damper, viscosity, shift or grips), with the conservative axial form
+    and the conservative radial form on or off."""
+    from sigmasph_b200.config import strip_json_comments
+    with open(scene_path("tensile_axi_dogbone_dx0.1.json")) as f:
+        sc = json.loads(strip_json_comments(f.read()))
+    sc["Domain"].update({"conservativeAxialMomentum": True, "conservativeRadialForce": radial})
+    sc["Hourglass"] = {"alpha": 0.0}
+    sc["Solver"]["viscosity"] = 0.0
+    sc["Shifting"] = {"enabled": False}
+    sc.pop("Constraints", None)
+    ps = ParticleSystem(SimConfig(sc), device="cpu")
+    rng = np.random.default_rng(3)
+    n = ps.particle_max_num
+    v = rng.uniform(-1.0, 1.0, (n, 3)).astype(np.float32)
+    v[:, 2] = 0.0
+    ps.v.from_numpy(v)
+    s = rng.normal(0.0, 0.05, (n, 3, 3))
+    s = 0.5 * (s + s.transpose(0, 2, 1))
+    s -= (np.trace(s, axis1=1, axis2=2) / 3.0)[:, None, None] * np.eye(3)
+    s[:, 0, 2] = s[:, 2, 0] = s[:, 1, 2] = s[:, 2, 1] = 0.0
+    ps.sigma_dev.from_numpy(s.astype(np.float32))
+    p = build_params(ps)
+    assert p.axi_conservative_r == int(radial)
+    o = Oracle(p, n, fp64=True)
+    o.set_state(state_from_sets(ps.state_numpy()), 1e-5)
+    for st in range(abi.STAGE_FORCES + 1):
+        o.stage(st)
+    r = o.get_state()
+    pw = r["m"] * (r["acc"] * r["v"]).sum(1)
+    return abs((r["m"] * r["de_int"] + pw).sum()) / np.abs(pw).sum()
+
+
+def test_conservative_radial_form_closes_the_ring_power():
+    """Domain.conservativeRadialForce carries the pair radius in the radial pair forces and
+    banks the hoop power -v . a_geom in de_int (SOLID.py:3444-3466, :3609-3614), so the
+    pair work telescopes in the ring measure m: the power imbalance of the force stage
+    falls by two orders of magnitude (what is left is the axis images, which are not
+    reciprocal pairs)."""
+    plain, radial = _axi_power_imbalance(False), _axi_power_imbalance(True)
+    assert plain > 1e-3 and radial < 0.02 * plain, (plain, radial)
