@@ -131,8 +131,9 @@ __global__ void SPH_BOUNDS(SPH_OCC_LAMGRAD) k_lamgrad_cont(Cst c, Ptr P) {
         const F3 vhat_i = vi + du_i;
         F3 lg = {0, 0, 0};
         float r0 = 0.0f, r1 = 0.0f;
-        for_each_neighbour(c, P, i, [&](int j, int mir) {
-            float4 pj = __ldg(pos + j), vj4 = __ldg(vel + j);
+        // the next neighbour's position is requested while this pair is evaluated
+        for_each_neighbour_pos(c, P, i, pos, [&](int j, int mir, float4 pj) {
+            float4 vj4 = __ldg(vel + j);
             F3 xj = f3(pj), vj = f3(vj4);
             if (mir) { xj = mirror3(mir, xj); vj = mirror3(mir, vj); }
             F3 r = xi - xj;
