@@ -929,8 +929,9 @@ __global__ void __launch_bounds__(kBlock) k_solid_commit(Cst c, Ptr P) {
 
 // ------------------------------------------------------------------ stress force
 // kVisc: a deck with the bulk viscosity q or Monaghan's Pi_ij (SOLID.py:3386-3401,
-// :3560-3570, :3727-3766); the plain instance keeps the registers of the common case.
-template <bool kVisc>
+// :3560-3570, :3727-3766); kAxi: an axisymmetric deck (its pair-radius forms and
+// geometric sources).  The plain instances keep the registers of the common case.
+template <bool kVisc, bool kAxi>
 __global__ void SPH_BOUNDS(SPH_OCC_SOLID_FORCE) k_solid_force(Cst c, Ptr P) {
     int i = blockIdx.x * blockDim.x + threadIdx.x;
     float amag = 0.0f, csq = 0.0f, cvisc = 0.0f;
@@ -961,8 +962,8 @@ __global__ void SPH_BOUNDS(SPH_OCC_SOLID_FORCE) k_solid_force(Cst c, Ptr P) {
         const Sym s = load_s(sdev, i);
         const bool ale = c.p.pst_enabled && c.p.pst_ale_momentum;
         const bool hg_inloop = c.p.hourglass_alpha > 0.0f && !c.p.hourglass_sts;
-        const bool axc = c.p.axisymmetric && c.p.axi_conservative_x;
-        const bool axr = c.p.axisymmetric && c.p.axi_conservative_r;
+        const bool axc = kAxi && c.p.axi_conservative_x;
+        const bool axr = kAxi && c.p.axi_conservative_r;
         const float ri = r_axi_of(pi.y, c), inv_ri = 1.0f / ri;
         float Gi[3][3];
         if (hg_inloop) load_gradv(P, i, Gi);
@@ -990,7 +991,6 @@ __global__ void SPH_BOUNDS(SPH_OCC_SOLID_FORCE) k_solid_force(Cst c, Ptr P) {
             const float rj = r_axi_of(pj.y, c);
             // the pair radius over r_i, on the axial (axc) and radial (axr) pair forces
             const float ratio = (axc || axr) ? 0.5f * (ri + rj) * inv_ri : 1.0f;
-            const float rx = axc ? ratio : 1.0f, ry = axr ? ratio : 1.0f;
             F3 vij = vi - vj;
             // the in-loop damper first: j's velocity-gradient record also carries its
             // pressure (k_solid_commit), and is dead once this term is summed
@@ -1011,8 +1011,8 @@ __global__ void SPH_BOUNDS(SPH_OCC_SOLID_FORCE) k_solid_force(Cst c, Ptr P) {
                     float hg = dot3(dvh, rh);
                     float damp = hg_pre * w_j * wendland_W(rn, c) * hg;
                     F3 ah = damp * rh;
-                    ah.x *= rx;
-                    ah.y *= ry;
+                    if (axc) ah.x *= ratio;
+                    if (axr) ah.y *= ratio;
                     a += ah;
                     dhg += -0.5f * dot3(ah, vij);
                 }
@@ -1033,9 +1033,11 @@ __global__ void SPH_BOUNDS(SPH_OCC_SOLID_FORCE) k_solid_force(Cst c, Ptr P) {
                     ww * (ss.xz * g.x + ss.yz * g.y + ss.zz * g.z)};
             // axialImageRadius "signed" (and the radial form always): a mirror image's
             // radius is the coordinate it sits at
-            const float signed_ratio = 0.5f * (ri - rj) * inv_ri;
-            f.x *= (axc && mir && c.p.axi_image_signed) ? signed_ratio : rx;
-            if (axr) f.y *= mir ? signed_ratio : ratio;
+            if (axc || axr) {
+                const float signed_ratio = 0.5f * (ri - rj) * inv_ri;
+                if (axc) f.x *= (mir && c.p.axi_image_signed) ? signed_ratio : ratio;
+                if (axr) f.y *= mir ? signed_ratio : ratio;
+            }
             a += inv_mw * f;
             dei += -0.5f * dot3(f, vij) * inv_mw;
             float vxy = dot3(vij, r);
@@ -1054,9 +1056,11 @@ __global__ void SPH_BOUNDS(SPH_OCC_SOLID_FORCE) k_solid_force(Cst c, Ptr P) {
                 const float pij = (-c.p.av_alpha * c_bar * mu + c.p.av_beta * mu * mu) / rho_bar;
                 F3 ap = (-mw_of(vj4.w, pj, c) * pij) * g;
                 float mu_cfl = -mu;
-                ap.x *= rx;
-                ap.y *= ry;
-                mu_cfl *= ratio;
+                if (axc || axr) {
+                    if (axc) ap.x *= ratio;
+                    if (axr) ap.y *= ratio;
+                    mu_cfl *= ratio;
+                }
                 a += ap;
                 mu_max = fmaxf(mu_max, mu_cfl);
                 dvisc += 0.5f * dot3(ap, vij);
@@ -1083,7 +1087,7 @@ __global__ void SPH_BOUNDS(SPH_OCC_SOLID_FORCE) k_solid_force(Cst c, Ptr P) {
                 }
             }
         });
-        if (c.p.axisymmetric) {
+        if (kAxi) {
             // the geometric sources the pair sums do not generate (SOLID.py:3444-3466)
             const float inv_rho_r = 1.0f / (rho_i * ri);
             F3 ag = {axc ? 0.0f : s.xy * inv_rho_r,
@@ -1535,10 +1539,14 @@ inline int solid_substep_launch(const Cst& c, const Ptr& P, int n, cudaStream_t 
     }
     if (in(SPH_STAGE_CONTINUITY)) { k_solid_commit<<<nb, bs, 0, st>>>(c, P); mark("k_solid_commit"); }
     if (in(SPH_STAGE_FORCES)) {
-        if (c.p.q_l2 > 0.0f || c.p.av_alpha > 0.0f || c.p.av_beta > 0.0f)
-            k_solid_force<true><<<nb, bs, 0, st>>>(c, P);
-        else
-            k_solid_force<false><<<nb, bs, 0, st>>>(c, P);
+        const bool visc = c.p.q_l2 > 0.0f || c.p.av_alpha > 0.0f || c.p.av_beta > 0.0f;
+        if (c.p.axisymmetric) {
+            if (visc) k_solid_force<true, true><<<nb, bs, 0, st>>>(c, P);
+            else k_solid_force<false, true><<<nb, bs, 0, st>>>(c, P);
+        } else {
+            if (visc) k_solid_force<true, false><<<nb, bs, 0, st>>>(c, P);
+            else k_solid_force<false, false><<<nb, bs, 0, st>>>(c, P);
+        }
         mark("k_solid_force");
     }
     if (in(SPH_STAGE_DT)) { k_solid_dt<<<inst_blocks(c), inst_threads(c), 0, st>>>(c, P); mark("k_solid_dt"); }
