@@ -68,7 +68,7 @@ ALGO_BYTES = {
     "k_pst": 16 + 16 + 4 + 16 + 16,   # pos vel lam lgrad read; shift write
     "k_finish": 16 * 6 + 16 * 4,
     "k_gather": 2 * (16 * 5 + 4) + 16,
-    # solid passes: the survey's compulsory own-particle figures of the passes they fuse
+    # solid passes: the compulsory own-particle bytes of the reference passes they fuse
     "k_solid_a": 56 + 64,              # grad lambda + grad v
     "k_solid_b": 144,                  # Jaumann + ALE(s, eps_p, e) + return map + e update
     "k_solid_force": 132,              # EOS + stress force + in-loop hourglass + dt pairs

@@ -32,7 +32,7 @@
 extern "C" {
 #endif
 
-#define SPH_ABI_VERSION 3
+#define SPH_ABI_VERSION 4
 
 /* ---------------------------------------------------------------- status codes */
 #define SPH_OK                 0
@@ -165,6 +165,16 @@ typedef struct SphParams {
     int32_t axi_conservative_r;   /* axisymmetric conservative radial form: the pair
                                      radius in every radial pair force, the source
                                      (p + q - s_tt) / (rho r)  (SOLID.py:3444-3466)    */
+    /* --- several solid materials (SOLID.py:222-245) --- */
+    int32_t delta_pairs_all;      /* Diffusion.pairs "all": the delta-SPH diffusion also on
+                                     pairs of two materials, with the harmonic mean of the
+                                     two deltas (DSPH.py:1271-1282, SOLID.py:4102-4114)  */
+    int32_t c0_mixed;             /* the materials' EOS sound speeds differ: pair terms take
+                                     the mean of the two (pair_c0), the shift particle i's
+                                     own (local_c0)         (DSPH.py:483-530, SOLID.py:244) */
+    int32_t hg_mixed_impedance;   /* the materials' rho0 c_p differ: the damper's pair force
+                                     carries 2 Z_j / (Z_i + Z_j)  (SOLID.py:228-229,
+                                     :4184-4239)                                        */
 } SphParams;
 
 /* ------------------------------------------------------------------ buffers */
@@ -300,6 +310,13 @@ int  sph_set_dt(SphHandle* h, float dt, void* stream);
 int  sph_get_dt(SphHandle* h, float* dt, void* stream);
 /* Copies the device scalars (synchronises `stream`). */
 int  sph_get_scalars(SphHandle* h, SphScalars* out, void* stream);
+/* HypoElasticSolver.get_constraint_data (SOLID.py:5198-5225): the FP64 force and the
+ * displacement of grips 0 .. k-1 of the last step into force[k][3] and disp[k][3] (host
+ * arrays; either may be NULL).  The force is summed over the grip's particles in FP64
+ * (x 2 pi in axisymmetry), as apply_constraints does (SOLID.py:5026-5055).  k must not
+ * exceed the scene's constraint count; a fluid handle or an ensemble returns
+ * SPH_ERR_ARG (an ensemble's grips are per instance: sph_ensemble_state).  Synchronises. */
+int  sph_constraints(SphHandle* h, double* force, double* disp, int k, void* stream);
 int  sph_clear_error(SphHandle* h, void* stream);
 /* FP64 reductions: compute_kinetic_energy / _off_grid / potential / elastic /
  * internal / total_mass (sph_base.py:425-557, DSPH.py:1670-1712) and compute_momentum /
@@ -351,20 +368,24 @@ int  sph_profile_read(SphHandle* h, char* names, int names_cap, double* ms, int*
  * beside the HBM roofline.  Synchronises; allocates a 4 kB result buffer. */
 int  sph_fma_peak(double* tflops, void* stream);
 
-/* The FP64 reductions of sph_reduce without a handle and without allocating: no
- * counterpart in the reference.  For callers that cannot call cudaMalloc (a host running
- * inside another framework's fixed device-memory pool, code that may not allocate while
- * a CUDA graph is being captured, FFI callers that hold only raw device pointers).  The
- * caller passes the current buffer set's pos, vel and shift arrays ([n][4] float32,
- * 16-byte aligned; shift may be NULL for a fluid) and `out`, a device array of
+/* The FP64 reductions of sph_reduce for a FLUID, without a handle and without
+ * allocating: no counterpart in the reference.  For callers that cannot call cudaMalloc
+ * (a host running inside another framework's fixed device-memory pool, code that may not
+ * allocate while a CUDA graph is being captured, FFI callers that hold only raw device
+ * pointers).  The caller passes the current buffer set's pos, vel and shift arrays
+ * ([n][4] float32, 16-byte aligned; shift may be NULL) and `out`, a device array of
  * SPH_RED_COUNT doubles it owns; the result is written there asynchronously on `stream`.
+ * A solid's parameters (is_solid) return SPH_ERR_UNSUPPORTED and write nothing: its
+ * elastic energy needs every particle's stress and material row, which this call is not
+ * given (use sph_reduce on the solid's handle).  n = 0 writes zeros.
  * The scratch is a fixed array compiled into the library (1.44 MB on each GPU that loads
  * it, held until the process exits), which caps n at SPH_NOALLOC_MAX_PARTICLES: larger n
  * returns SPH_ERR_SCRATCH_CAP and launches nothing.  The first call on a device looks up
  * that array's device address (cudaGetSymbolAddress) with the device current; make it
- * before any stream capture.  All calls share the array, so calls whose GPU work overlaps
- * (other streams, other host threads) race: serialise them.  The sum is deterministic
- * (per-block partials added in a fixed order). */
+ * before any stream capture.  The address is kept for the life of the process: a
+ * cudaDeviceReset between calls is not supported.  All calls share the array, so calls
+ * whose GPU work overlaps (other streams, other host threads) race: serialise them.  The
+ * sum is deterministic (per-block partials added in a fixed order). */
 #define SPH_NOALLOC_MAX_PARTICLES 4194304
 int  sph_reduce_noalloc(const SphParams* p, const float* pos, const float* vel,
                         const float* shift, int64_t n, double* out, void* stream);

@@ -317,15 +317,19 @@ struct Sim {
                 }
                 V3<R> vd = vi - vj;
                 r0 += w(j) * dot(vd, g);
-                // the solid's pair_delta (SOLID.py:4103-4114) on same-material pairs only
+                // the solid's pair_delta (SOLID.py:4103-4114) on same-material pairs, or on
+                // every pair under Diffusion.pairs "all" (DSPH.py:1271-1282), sized on
+                // pair_c0 (DSPH.py:483-511)
                 R cpair = coef;
                 bool diffuse = P.delta_sph > 0.0f;
                 if (P.is_solid) {
                     R di = R(P.mat_delta[eos_id[i]]), dj = R(P.mat_delta[eos_id[j]]);
                     R den = di + dj;
                     R dl = den > R(1e-12) ? R(2) * di * dj / den : R(0);
-                    diffuse = eos_id[i] == eos_id[j] && dl > R(0);
-                    cpair = dl * h * R(P.c0);
+                    diffuse = (P.delta_pairs_all || eos_id[i] == eos_id[j]) && dl > R(0);
+                    const R c0p = P.c0_mixed ? R(0.5) * (R(P.mat_c0[eos_id[i]]) + R(P.mat_c0[eos_id[j]]))
+                                             : R(P.c0);
+                    cpair = dl * h * c0p;
                 }
                 if (diffuse) {
                     R rn2 = dot(r, r);
@@ -525,15 +529,18 @@ struct Sim {
         for (int64_t i = 0; i < n; ++i) {
             V3<R> s;
             for_all_neighbors(i, [&](int64_t j, int mir) { s += pst_pair(i, j, mir); });
+            // local_c0 (DSPH.py:520-530): the particle's own material's speed when the
+            // materials' EOS speeds differ
+            const R c0l = (P.is_solid && P.c0_mixed) ? R(P.mat_c0[eos_id[i]]) : R(P.c0);
             R Ma;
             if (P.pst_ma_mode == 2) Ma = R(P.pst_ma_fixed);
             else {
                 R vref = P.pst_ma_mode == 1 ? max_v : norm(v[i]);
-                Ma = vref / R(P.c0);
+                Ma = vref / c0l;
             }
             V3<R> dr;
             if (P.pst_colle) {
-                R c = R(-2.0 * (double)P.support_radius) * R(P.c0) * Ma;
+                R c = R(-2.0 * (double)P.support_radius) * c0l * Ma;
                 V3<R> dvv = c * s;
                 if (P.pst_clamp_vel) {
                     R cap = R(P.pst_m_delta) * norm(v[i]);
@@ -624,6 +631,13 @@ struct Sim {
         return o;
     }
     R matc_G(int64_t p) const { return R(P.mat_G[eos_id[p]]); }
+    // _hg_impedance_ratio (SOLID.py:4184-4239): 2 Z_j / (Z_i + Z_j), Z = rho0 c_p
+    R hg_impedance_ratio(int64_t i, int64_t j) const {
+        const R zi = R(P.mat_rho0[eos_id[i]]) * R(P.mat_cp[eos_id[i]]);
+        const R zj = R(P.mat_rho0[eos_id[j]]) * R(P.mat_cp[eos_id[j]]);
+        const R den = zi + zj;
+        return den > R(0) ? R(2) * zj / den : R(1);
+    }
     R r_of(int64_t p) const { return std::max(x[p][1], R(P.axi_r_min)); }
 
     // SOLID.py:5001-5017
@@ -1021,6 +1035,7 @@ struct Sim {
                     int k = eos_id[i];
                     R damp = R(P.hourglass_alpha) * (R(P.mat_rho0[k]) / rho_i) * (R(P.mat_cp[k]) / h)
                              * (w(j) / R(P.V0)) * (Wij / R(P.hg_W_dx0)) * hg;
+                    if (P.hg_mixed_impedance) damp = damp * hg_impedance_ratio(i, j);
                     V3<R> ah = damp * rh;
                     if (axc) ah[0] = ah[0] * pratio;
                     if (axr) ah[1] = ah[1] * pratio;
@@ -1114,6 +1129,7 @@ struct Sim {
                 int k = eos_id[i];
                 R damp = R(P.hourglass_alpha) * (R(P.mat_rho0[k]) / rho_i) * (R(P.mat_cp[k]) / h)
                          * (w(j) / R(P.V0)) * (Wij / R(P.hg_W_dx0)) * hg;
+                if (P.hg_mixed_impedance) damp = damp * hg_impedance_ratio(i, j);
                 V3<R> ah = damp * rh;
                 if (P.axisymmetric && (P.axi_conservative_x || P.axi_conservative_r)) {
                     const R ratio = R(0.5) * (r_of(i) + r_of(j)) / r_of(i);

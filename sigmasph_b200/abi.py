@@ -12,7 +12,7 @@ import os
 _HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(_HERE, "_build", "libsph_b200.so")
 
-ABI_VERSION = 3
+ABI_VERSION = 4
 
 SPH_OK = 0
 STATUS_NAMES = {
@@ -74,6 +74,7 @@ PARAM_FIELDS = [
     ("q_l2", _f32), ("q_cl", _f32), ("av_alpha", _f32), ("av_beta", _f32), ("av_eps", _f32),
     ("hg_sts_rkl", _i32), ("objective_none", _i32), ("axi_image_signed", _i32),
     ("axi_conservative_r", _i32),
+    ("delta_pairs_all", _i32), ("c0_mixed", _i32), ("hg_mixed_impedance", _i32),
 ]
 
 
@@ -173,6 +174,7 @@ def lib():
         "sph_set_dt": (C.c_int, [vp, C.c_float, vp]),
         "sph_get_dt": (C.c_int, [vp, C.POINTER(C.c_float), vp]),
         "sph_get_scalars": (C.c_int, [vp, C.POINTER(SphScalars), vp]),
+        "sph_constraints": (C.c_int, [vp, vp, vp, C.c_int, vp]),
         "sph_clear_error": (C.c_int, [vp, vp]),
         "sph_reduce": (C.c_int, [vp, C.POINTER(C.c_double), vp]),
         "sph_pairs": (C.c_int, [vp, C.c_int, vp, vp, vp, i64, C.POINTER(i64), vp]),

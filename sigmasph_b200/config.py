@@ -158,6 +158,7 @@ UNSUPPORTED = {
     "PST_CLAMP": ("displacement", "velocity", "both"),
     "PST_NORMAL": ("gradlam", "eigvec"),
     "DT_PAIR_SOUND_SPEED": ("all", "samematerial", "off"),
+    "DELTA_PAIRS": ("samematerial", "all"),
     "OBJECTIVE_RATE": ("jaumann", "none"),
     "HOURGLASS_FORM": ("rate",),
     "HOURGLASS_STS_MODE": ("subcycle", "rkl"),

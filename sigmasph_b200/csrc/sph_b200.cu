@@ -289,6 +289,7 @@ int sph_params_layout(char* buf, int cap) {
     F(hourglass_sts_safety) F(hg_S) F(hg_W_dx0) F(hg_sts_refresh) F(ale_history) F(transport_e)
     F(ale_diffusion) F(num_constraints) F(ramp_time) F(jc_surrogate) F(jc_surrogate_tol)
     F(q_l2) F(q_cl) F(av_alpha) F(av_beta) F(av_eps) F(hg_sts_rkl) F(objective_none) F(axi_image_signed) F(axi_conservative_r)
+    F(delta_pairs_all) F(c0_mixed) F(hg_mixed_impedance)
 #undef F
     if (buf && cap > 0) {
         size_t k = std::min<size_t>(s.size(), (size_t)cap - 1);
@@ -562,6 +563,19 @@ int sph_get_scalars(SphHandle* h, SphScalars* out, void* stream) {
     CK(cudaMemcpyAsync(h->pinned, h->sc, sizeof(SphScalars), cudaMemcpyDeviceToHost, S(stream)));
     CK(cudaStreamSynchronize(S(stream)));
     memcpy(out, h->pinned, sizeof(SphScalars));
+    return SPH_OK;
+}
+
+int sph_constraints(SphHandle* h, double* force, double* disp, int k, void* stream) {
+    if (!h || !h->p.is_solid || h->solid.n_inst > 0 || k < 0 || k > h->p.num_constraints) return SPH_ERR_ARG;
+    cudaStream_t st = S(stream);
+    CK(cudaMemcpyAsync(h->pinned, h->sc, sizeof(SphScalars), cudaMemcpyDeviceToHost, st));
+    CK(cudaStreamSynchronize(st));
+    for (int g = 0; g < k; ++g)
+        for (int d = 0; d < 3; ++d) {
+            if (force) force[3 * g + d] = h->pinned->constraint_force[g][d];
+            if (disp) disp[3 * g + d] = h->pinned->constraint_disp[g][d];
+        }
     return SPH_OK;
 }
 

@@ -521,6 +521,9 @@ __global__ void SPH_BOUNDS(SPH_OCC_PST) k_pst(Cst c, Ptr P) {
         const int k = (int)__ldg(P.cur.bcdisp + 4 * i + 3);
         c0 = P.irow[k].c0;
         dt = P.inst[k].dt;
+    } else if (c.p.c0_mixed) {
+        // local_c0 (DSPH.py:520-530): the particle's own material's EOS sound speed
+        c0 = P.mat[(int)__ldg(P.cur.bcdisp + 4 * i + 3)].c0;
     }
     float Ma;
     if (c.p.pst_ma_mode == 2) Ma = c.p.pst_ma_fixed;

@@ -14,7 +14,10 @@
 // holds until the process exits.  Every call shares that one array and overwrites the
 // rows it uses (nothing in it has to start at zero: each block writes its whole row
 // before the second pass reads it).  Two calls whose work overlaps on the GPU (on
-// different streams, or from several host threads) race on it; serialise them.
+// different streams, or from several host threads) race on it; serialise them.  The
+// array's address is looked up once per device and kept, so a cudaDeviceReset between
+// calls is not supported.  A solid is refused (SPH_ERR_UNSUPPORTED): its elastic energy
+// needs the stress and material rows, which this entry point is not given.
 #include <cuda_runtime.h>
 
 #include <mutex>
@@ -27,6 +30,8 @@ using namespace sph;
 
 constexpr int kNoAllocMaxBlocks = 16384;
 constexpr int64_t kNoAllocMaxParticles = (int64_t)kNoAllocMaxBlocks * kBlock;
+static_assert(kNoAllocMaxParticles == SPH_NOALLOC_MAX_PARTICLES,
+              "the public cap in sph_b200.h must equal the scratch array's real capacity");
 constexpr int kMaxDevices = 64;
 
 static __device__ __align__(256) double g_partials[kNoAllocMaxBlocks * SPH_RED_COUNT];
@@ -99,9 +104,11 @@ extern "C" int sph_reduce_noalloc(const SphParams* p, const float* pos, const fl
                                   const float* shift, int64_t n, double* out, void* stream) {
     if (!p || !out || n < 0) return SPH_ERR_ARG;
     if (p->struct_size != (int32_t)sizeof(SphParams)) return SPH_ERR_ARG;
+    // a solid's elastic energy needs each particle's stress and material row, which this
+    // entry point is not given: refused rather than returned as a silent zero
+    if (p->is_solid) return SPH_ERR_UNSUPPORTED;
     if (n > kNoAllocMaxParticles) return SPH_ERR_SCRATCH_CAP;
     if (n > 0 && (!pos || !vel)) return SPH_ERR_ARG;
-    if (p->is_solid && n > 0 && !shift) return SPH_ERR_ARG;
     auto misaligned = [](const void* q) { return (reinterpret_cast<uintptr_t>(q) & 15u) != 0; };
     if ((pos && misaligned(pos)) || (vel && misaligned(vel)) || (shift && misaligned(shift)) ||
         (reinterpret_cast<uintptr_t>(out) & 7u) != 0)

@@ -228,6 +228,17 @@ __device__ __forceinline__ float solid_pressure(const Cst& c, const Ptr& P, int 
     return p;
 }
 
+// _hg_impedance_ratio (SOLID.py:4184-4239): the damper's pair force carries particle i's
+// acoustic impedance Z = rho0 c_p; 2 Z_j / (Z_i + Z_j) turns it into the pair's harmonic
+// mean, so the force is antisymmetric across a material interface (exactly 1 when the two
+// impedances are equal).
+__device__ __forceinline__ float hg_impedance_ratio(const Ptr& P, int ki, int j) {
+    const int kj = eos_of(P, j);
+    const float zi = P.mat[ki].rho0 * P.mat[ki].cp, zj = P.mat[kj].rho0 * P.mat[kj].cp;
+    const float den = zi + zj;
+    return den > 0.0f ? 2.0f * zj / den : 1.0f;
+}
+
 // ------------------------------------------------------------------ load factor
 __global__ void k_solid_load(Cst c, Ptr P) {
     if (c.n_inst > 0) {
@@ -442,13 +453,17 @@ __global__ void SPH_BOUNDS(SPH_OCC_SOLID_A) k_solid_a(Cst c, Ptr P) {
                 r0 += Vj * dot3(rho_j * du_j - rho_i * du_i, g) * inv_rho_i;
             }
             r0 += Vj * dot3(vhat_i - vh_j, g);
-            if (same_material(c, P, j, ki)) {   // pair_delta (SOLID.py:4103-4114), same-material pairs
-                const float dj = di;          // same material row
+            // pair_delta and pair_c0 (SOLID.py:4102-4114, DSPH.py:483-511) on same-material
+            // pairs, or on every pair under Diffusion.pairs "all" (DSPH.py:1271-1282)
+            const int kj = c.one_material ? ki : eos_of(P, j);
+            if (kj == ki || c.p.delta_pairs_all) {
+                const float dj = kj == ki ? di : P.mat[kj].delta;
                 float den = di + dj;
                 float dl = den > 1e-12f ? 2.0f * di * dj / den : 0.0f;
                 if (dl > 0.0f) {
+                    const float c0p = c.p.c0_mixed ? 0.5f * (P.mat[ki].c0 + P.mat[kj].c0) : c0i;
                     float psig = __fdividef(2.0f * (rho_j - rho_i) * (-dot3(r, g)), rn2 + c.eta2);
-                    float rate = dl * c.h * c0i * Vj * psig * inv_rho_i;
+                    float rate = dl * c.h * c0p * Vj * psig * inv_rho_i;
                     r0 += rate;
                     r1 += rate;
                 }
@@ -1010,6 +1025,7 @@ __global__ void SPH_BOUNDS(SPH_OCC_SOLID_FORCE) k_solid_force(Cst c, Ptr P) {
                               (vj.z - vi.z) - 0.5f * ((Gi[2][0] + Gj[2][0]) * mr.x + (Gi[2][1] + Gj[2][1]) * mr.y + (Gi[2][2] + Gj[2][2]) * mr.z)};
                     float hg = dot3(dvh, rh);
                     float damp = hg_pre * w_j * wendland_W(rn, c) * hg;
+                    if (c.p.hg_mixed_impedance) damp *= hg_impedance_ratio(P, ki, j);
                     F3 ah = damp * rh;
                     if (axc) ah.x *= ratio;
                     if (axr) ah.y *= ratio;
@@ -1278,6 +1294,7 @@ __global__ void __launch_bounds__(kBlock) k_hg_stage(Cst c, Ptr P, int stage) {
                   (yj.z - yi.z) - 0.5f * ((Gi[2][0] + Gj[2][0]) * mr.x + (Gi[2][1] + Gj[2][1]) * mr.y + (Gi[2][2] + Gj[2][2]) * mr.z)};
         float hg = dot3(dvh, rh);
         float damp = hg_pre * w_of(pj, c) * wendland_W(rn, c) * hg;
+        if (c.p.hg_mixed_impedance) damp *= hg_impedance_ratio(P, ki, j);
         F3 ah = damp * rh;
         if (axc || axr) {
             const float ratio = 0.5f * (ri + r_axi_of(pj.y, c)) * inv_ri;

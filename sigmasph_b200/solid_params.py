@@ -7,7 +7,7 @@ import math
 
 import numpy as np
 
-from .materials import PLASTIC_JOHNSON_COOK, PLASTIC_LINEAR, EOS_LINEAR
+from .materials import PLASTIC_JOHNSON_COOK
 
 
 def wendland_scalar(r, h, two_d):
@@ -61,10 +61,14 @@ def fill_solid_params(ps, p):
             p.jc_C[k], p.jc_eps0_dot[k] = m.jc["C"], m.jc["eps0_dot"]
             p.jc_T0[k], p.jc_Tm[k] = m.jc["T0"], m.jc["Tm"]
             p.jc_m[k], p.jc_chi[k] = m.jc["m"], m.jc["chi"]
-    if any(m.eos_kind != EOS_LINEAR and m.exponent != 1.0 for m in mats):
-        pass  # a Tait solid keeps its exponent per material (mat_gamma)
     c_p = max(m.c_p for m in mats)
     p.c_signal = c_p
+    # SOLID.py:222-245: do the materials differ in acoustic impedance rho0 c_p (the
+    # damper's pair force) or in EOS sound speed (the delta-SPH and Colle coefficients)?
+    # Compared as the reference compares them, on the resolved double-precision values.
+    p.hg_mixed_impedance = int(len({m.rho0 * m.c_p for m in mats}) > 1)
+    p.c0_mixed = int(len({m.c_eos for m in mats}) > 1)
+    p.delta_pairs_all = int(str(g("DELTA_PAIRS") or "samematerial").lower() != "samematerial")
     mode = str(g("DT_PAIR_SOUND_SPEED") or "samematerial").lower()
     p.dt_pair_mode = {"off": 0, "all": 1, "samematerial": 2}[mode]
     p.kernel_correction = int(bool(g("KERNEL_CORRECTION")))

@@ -398,16 +398,20 @@ class HypoElasticSolver(_SolverBase):
         return float(self._scalars().plastic_work)
 
     def get_constraint_data(self):
-        """SOLID.py:5198-5225."""
-        if self.num_constraints == 0:
+        """SOLID.py:5198-5225: each grip's FP64 force and displacement of the last step
+        (sph_constraints)."""
+        k = self.num_constraints
+        if k == 0:
             return []
-        s = self._scalars()
+        force = np.zeros((k, 3), dtype=np.float64)
+        disp = np.zeros((k, 3), dtype=np.float64)
+        abi.check(self.L.sph_constraints(self.h, force.ctypes.data, disp.ctypes.data, k, _stream_ptr()),
+                  "sph_constraints")
         out = []
-        for k in range(self.num_constraints):
-            name = self.constraints_list[k].get("name", f"constraint_{k}")
-            out.append({"index": k, "name": name,
-                        "displacement": np.array([s.constraint_disp[k][d] for d in range(3)]),
-                        "force": np.array([s.constraint_force[k][d] for d in range(3)])})
+        for g in range(k):
+            name = self.constraints_list[g].get("name", f"constraint_{g}")
+            out.append({"index": g, "name": name, "displacement": disp[g].copy(),
+                        "force": force[g].copy()})
         return out
 
     # ------------------------------------------------------------------ JC surrogate

@@ -5,7 +5,8 @@ geometry and the material models' float64 `_py` mirrors from it, with a stand-in
 `taichi` module that turns the decorators into no-ops; no Taichi kernel runs).  The
 fixture it writes is committed and is all the tests read.
 
-    python tests/golden/make_golden.py [/path/to/reference]
+    python tests/golden/make_golden.py /path/to/reference
+    SIGMASPH_REFERENCE=/path/to/reference python tests/golden/make_golden.py
 """
 import hashlib
 import json
@@ -15,7 +16,9 @@ import tempfile
 
 import numpy as np
 
-REF = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
+REF = sys.argv[1] if len(sys.argv) > 1 else os.environ.get("SIGMASPH_REFERENCE")
+if not REF:
+    sys.exit("usage: make_golden.py /path/to/sigmaSPH (or set SIGMASPH_REFERENCE)")
 HERE = os.path.dirname(os.path.abspath(__file__))
 REPO = os.path.dirname(os.path.dirname(HERE))
 

@@ -200,6 +200,48 @@ def axi_rkl_deck():
     return sc
 
 
+def bar3d_kc_deck():
+    """The bar with Solver.kernelCorrection: grad v through the regularised inverse of E
+    (SOLID.py:1757-1771, spd_inverse.py:45-101), which departs from the identity at the
+    bar's free surface, where the float64 inverse is taken."""
+    sc = bar3d_deck()
+    sc["Solver"]["kernelCorrection"] = True
+    return sc
+
+
+def axi_kc_deck():
+    """The axisymmetric dogbone with Solver.kernelCorrection (the 2x2 inverse)."""
+    sc = _axi_json()
+    sc["Solver"]["kernelCorrection"] = True
+    return sc
+
+
+def two_material_bar_deck(pairs="samematerial"):
+    """A square bar of two materials, steel below y = 0 and aluminium above, J2 both, with
+    the in-loop damper, Colle shifting at a fixed Mach number and delta-SPH: the EOS sound
+    speeds and the acoustic impedances differ, so pair_c0, local_c0 and the damper's
+    impedance ratio are all live (SOLID.py:222-245, :4184-4239, DSPH.py:483-530)."""
+    sc = bar3d_deck()
+    sc["Materials"].append({"name": "aluminium", "density0": 2.7e-6, "eos": {"type": "linear"},
+                            "strength": {"type": "hypoElastic", "youngsModulus": 70.0,
+                                         "poissonRatio": 0.33,
+                                         "plasticity": {"model": "linear", "yieldStress": 0.1,
+                                                        "hardeningModulus": 0.5}}})
+    sc["Diffusion"]["pairs"] = pairs
+    blk = dict(sc["SolidBlocks"][0])
+    blk.pop("shape")
+    sc["SolidBlocks"] = [dict(blk, start=[-2.0, -12.0, -2.0], end=[2.0, -0.2, 2.0]),
+                         dict(blk, objectId=1, material="aluminium", density=2.7e-6,
+                              start=[-2.0, 0.0, -2.0], end=[2.0, 12.0, 2.0])]
+    return sc
+
+
+def two_material_bar_all_deck():
+    """The two-material bar with Diffusion.pairs "all": the diffusion crosses the
+    interface with the harmonic mean of the two deltas."""
+    return two_material_bar_deck("all")
+
+
 # The GPU writes the return-mapped stress, plastic strain and energy to scratch in the
 # LAM stage and commits them with the volume update, so they are compared after it.
 STAGE_FIELDS = {
@@ -218,16 +260,25 @@ TOL64 = {"de_int": 1e-3, "pressure": 2e-3, "acc": 5e-4, "grad_v": 2e-4}
 
 @pytest.mark.parametrize("deck", [axi_deck, bar3d_deck, strip_ps_deck, bar3d_visc_deck, axi_visc_deck,
                                   axi_rkl_deck, bar3d_no_spin_deck, axi_signed_deck, axi_plain_axial_deck,
-                                  axi_radial_deck],
+                                  axi_radial_deck, bar3d_kc_deck, axi_kc_deck, two_material_bar_deck,
+                                  two_material_bar_all_deck],
                          ids=["axi_dogbone_jc_sts", "bar3d_j2_inloop", "plane_strain_jc",
                               "bar3d_q_monaghan", "axi_q_monaghan", "axi_rkl", "bar3d_no_spin",
-                              "axi_signed_image", "axi_plain_axial", "axi_radial"])
+                              "axi_signed_image", "axi_plain_axial", "axi_radial",
+                              "bar3d_kernel_correction", "axi_kernel_correction",
+                              "two_materials", "two_materials_pairs_all"])
 def test_solid_stages_match_oracle(cuda, deck):
     ps, solver, o64, o32 = make_solid(deck())
+    p = solver.params
+    if deck in (two_material_bar_deck, two_material_bar_all_deck):
+        assert p.n_materials == 2 and p.c0_mixed and p.hg_mixed_impedance
     for s in range(8):
         solver.run_stage(s)
         o64.stage(s)
         o32.stage(s)
+        if s == abi.STAGE_LAM and p.kernel_correction and not p.two_d:
+            # the free surface is in the deck: there the inverse is taken in float64
+            assert (ps.lam.to_numpy() < 0.75).any()
         if s == abi.STAGE_SORT:
             gi, gj, gm = solver.pairs(0)
             oi, oj, om = o32.pairs()
@@ -359,6 +410,31 @@ def test_grip_force_and_time_bookkeeping(cuda):
     F0, F1 = d[0]["force"][0], d[1]["force"][0]
     assert F0 > 0 and F1 < 0 and abs(F0 + F1) <= 0.05 * abs(F0)
     assert d[1]["displacement"][0] == pytest.approx(10.0 * sv.load_s[None], rel=1e-5)
+
+
+def test_constraint_data_through_the_abi(cuda):
+    """sph_constraints (get_constraint_data, SOLID.py:5198-5225): each grip's FP64 force and
+    displacement after a step equal the float32 oracle's apply_constraints sums; more grips
+    than the scene has, and a fluid handle, are refused."""
+    ps, solver, _, o32 = make_solid(bar3d_deck())
+    for s in range(8):
+        solver.run_stage(s)
+        o32.stage(s)
+    d = solver.get_constraint_data()
+    s32 = o32.scalars()
+    assert [e["name"] for e in d] == ["low", "high"]
+    F = np.array([e["force"] for e in d])
+    U = np.array([e["displacement"] for e in d])
+    Fo, Uo = s32["constraint_force"][:2], s32["constraint_disp"][:2]
+    assert np.abs(F).max() > 0.0
+    assert np.abs(F - Fo).max() <= 1e-4 * np.abs(Fo).max()
+    assert np.allclose(U, Uo, rtol=1e-6, atol=0.0)
+    buf = np.zeros(3 * 8)
+    assert solver.L.sph_constraints(solver.h, buf.ctypes.data, None, 3, None) == -1
+    from sigmasph_b200.scenes import dambreak3d, dx_for_particles
+    fps = ParticleSystem(SimConfig(dambreak3d(dx=dx_for_particles(2000))), device="cuda")
+    fsv = fps.build_solver()
+    assert fsv.L.sph_constraints(fsv.h, buf.ctypes.data, None, 0, None) == -1
 
 
 def test_solid_reductions_match_numpy(cuda):

@@ -116,6 +116,76 @@ def test_free_block_conserves_momentum():
     assert r["eps_p"].max() > 0.0       # the random field yields somewhere
 
 
+ALUMINIUM = {"name": "aluminium", "density0": 2.7e-6, "eos": {"type": "linear"},
+             "strength": {"type": "hypoElastic", "youngsModulus": 70.0, "poissonRatio": 0.33,
+                          "plasticity": {"model": "linear", "yieldStress": 0.02,
+                                         "hardeningModulus": 0.5}}}
+
+
+def two_material_block(dx=0.5, pairs="samematerial"):
+    """The free block as two materials, steel below y = 3 and aluminium above: their EOS
+    sound speeds and their acoustic impedances rho0 c_p differ."""
+    sc = free_block(dx)
+    sc["Materials"].append(ALUMINIUM)
+    sc["Diffusion"]["pairs"] = pairs
+    sc["SolidBlocks"] = [
+        {"objectId": 0, "start": [0.0, 0.0, 0.0], "end": [6.0, 2.9, 6.0], "material": "steel",
+         "density": 7.9e-6},
+        {"objectId": 1, "start": [0.0, 3.0, 0.0], "end": [6.0, 6.0, 6.0], "material": "aluminium",
+         "density": 2.7e-6}]
+    return sc
+
+
+def test_two_materials_set_the_mixed_flags():
+    """SOLID.py:222-245: c0_mixed when the EOS speeds differ, hg_mixed_impedance when
+    rho0 c_p differ; Diffusion.pairs "all" lets the diffusion cross the interface."""
+    p1 = build_params(ParticleSystem(SimConfig(free_block()), device="cpu"))
+    assert (p1.c0_mixed, p1.hg_mixed_impedance, p1.delta_pairs_all) == (0, 0, 0)
+    ps = ParticleSystem(SimConfig(two_material_block(pairs="all")), device="cpu")
+    p2 = build_params(ps)
+    assert (p2.n_materials, p2.c0_mixed, p2.hg_mixed_impedance, p2.delta_pairs_all) == (2, 1, 1, 1)
+    assert sorted(set(np.rint(ps.state_numpy()["bcdisp"][:, 3]).astype(int))) == [0, 1]
+    from sigmasph_b200.config import SceneError
+    sc = two_material_block()
+    sc["Diffusion"]["pairs"] = "some"
+    with pytest.raises(SceneError):
+        SimConfig(sc)
+
+
+@pytest.mark.parametrize("ratio", [True, False], ids=["impedance_ratio", "own_impedance"])
+def test_two_material_damper_conserves_momentum(ratio):
+    """_hg_impedance_ratio (SOLID.py:4184-4239): the in-loop damper's pair force carries
+    rho0 c_p; with the pair's harmonic mean (2 Z_j / (Z_i + Z_j) on particle i's own) it is
+    antisymmetric across the steel/aluminium interface and the free two-material block
+    conserves momentum to round-off; with each particle's own impedance it does not.  The
+    Morris viscosity is off: its pair term m_i w_j (...) is antisymmetric only between
+    particles of one density, so across the interface it moves momentum by construction
+    in the reference too."""
+    sc = two_material_block()
+    sc["Solver"]["viscosity"] = 0.0
+    ps = ParticleSystem(SimConfig(sc), device="cpu")
+    rng = np.random.default_rng(4)
+    n = ps.particle_max_num
+    ps.v.from_numpy(rng.uniform(-2.0, 2.0, (n, 3)).astype(np.float32))
+    p = build_params(ps)
+    p.hg_mixed_impedance = int(ratio)
+    o = Oracle(p, n, fp64=True)
+    st = state_from_sets(ps.state_numpy())
+    o.set_state(st, p.CFL * p.support_radius / p.c_signal)
+    m = st["m"].astype(np.float64)
+    P0 = (m[:, None] * st["v"].astype(np.float64)).sum(0)
+    o.stage(abi.STAGE_SORT)
+    o.step(10)
+    r = o.get_state()
+    P1 = (r["m"][:, None] * r["v"]).sum(0)
+    gross = (r["m"][:, None] * np.abs(r["v"])).sum(0)
+    drift = np.abs(P1 - P0).max() / gross.max()
+    if ratio:
+        assert drift <= 1e-10, drift
+    else:
+        assert drift > 1e-6, drift
+
+
 def test_mlp_oracle_gradient_matches_finite_differences():
     """The float64 surrogate-MLP oracle (the checker of the GPU training kernels):
     analytic gradient against central differences."""
