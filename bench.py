@@ -23,8 +23,12 @@ Besides `value` and `e2e`, the line carries `roofline` (the dominant kernel's al
 bytes over its event-timed launch, against the measured HBM copy peak, with its ncu DRAM
 traffic), `step_roofline` (the whole step's algorithmic bytes), `fp32_bound` (the step's
 estimated FP32 work against the FP32 FMA peak that `sph_fma_peak` measures on the same
-GPU at the start of the run), `kernel_ms_per_step` (CUDA-event profile of eager steps
-after the timed ones), `neighbour_lists` (list builds among the timed steps) and `clocks`.
+GPU), `kernel_ms_per_step` (CUDA events around every kernel of eager steps on a copy of
+the workload warmed up the same way: the same steps of the simulation as the timed
+window), `neighbour_lists` (list builds among the timed steps), `steady_state` (a longer
+window after the timed one, where the flow is faster and the lists are built more often:
+the build cost amortised), `drift` (the energy balance over the timed window from the
+library's FP64 reductions) and `clocks`.
 
 Under torchrun (N > 1) every rank runs an independent replica of a single scene (it does
 not shard at one-GPU scale: replicas only); the strip ensemble is sharded instead, each
@@ -98,25 +102,21 @@ def load_peaks():
     return 6650.0, "fallback"
 
 
-def read_traffic(kernel, tag, n):
-    """DRAM bytes per launch of `kernel` from the committed ncu summary of the workload
-    (profiles/<tag>.md, the "DRAM B/particle" column of the --set full table), scaled to
-    n particles: the traffic of these kernels grows in proportion to the particles."""
-    p = os.path.join(ROOT, "profiles", f"{tag}.md")
-    if not os.path.exists(p):
-        return None
-    col = None
-    with open(p) as f:
-        for line in f:
-            cells = [c.strip() for c in line.strip().strip("|").split("|")]
-            if "DRAM B/particle" in cells:
-                col = cells.index("DRAM B/particle")
-            elif col is not None and cells and cells[0] == kernel and len(cells) > col:
-                try:
-                    return float(cells[col]) * n
-                except ValueError:
-                    return None
-    return None
+# DRAM bytes per particle of one launch of the dominant kernels (ncu dram__bytes_read.sum
+# + dram__bytes_write.sum over the particles of the captured case, in the workload's own
+# configuration at 256k particles: a --set full capture at full size is too large to run
+# safely).  The traffic of these kernels grows in proportion to the particles, so the line
+# scales them by the particle count.  Measured with the commands recorded beside the
+# figures under profiles/.
+NCU_DRAM_BYTES_PER_PARTICLE = {
+    "dambreak3d": {},
+    "tensile_bar3d": {},
+}
+
+
+def scaled_traffic(kernel, tag, n):
+    per = NCU_DRAM_BYTES_PER_PARTICLE.get(tag, {}).get(kernel)
+    return None if per is None else per * n
 
 
 class ClockSampler:
@@ -361,7 +361,10 @@ def main():
                          "sigmasph_b200/data/jc_surrogate_config0.npy")
     ap.add_argument("--e2e-steps", type=int, default=None)
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--profile-steps", type=int, default=4)
+    ap.add_argument("--profile-steps", type=int, default=0,
+                    help="eager profiled steps (0: as many as the timed window)")
+    ap.add_argument("--steady-steps", type=int, default=200,
+                    help="a longer window after the timed one, for the amortised build cost")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
@@ -413,6 +416,7 @@ def main():
     # ---------------------------------------------------------------- timed region
     K = args.steps
     solver.list_stats(reset=True)
+    bud0 = solver.energy_budget()
     clocks = ClockSampler(local)
     rep.barrier()
     torch.cuda.synchronize()
@@ -429,6 +433,42 @@ def main():
     err = solver.error_word()
     lists = solver.list_stats()
     value = rep.throughput(n * K, ms / 1000.0)
+    bud1 = solver.energy_budget()
+
+    # ---------------------------------------------------------------- steady state
+    # The window above starts right after the warm-up, while the flow is slow and the
+    # candidate lists are rarely built; a longer window after it shows the build cost
+    # amortised at the rate the flow sets later on.
+    Ks = args.steady_steps
+    steady = None
+    if Ks > 0:
+        solver.list_stats(reset=True)
+        rep.barrier()
+        torch.cuda.synchronize()
+        e0.record(stream)
+        solver.step_many(Ks)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        ms_s = rep.max_over_ranks(e0.elapsed_time(e1))
+        ls = solver.list_stats()
+        steady = {"steps": Ks, "after_steps": W + K, "builds": ls["builds"],
+                  "ms_per_step": ms_s / Ks, "value": rep.throughput(n * Ks, ms_s / 1000.0),
+                  "unit": UNIT}
+
+    # energy balance over the timed window (the library's FP64 reductions): the fluid's
+    # E_bal = ke + se + pe - visc + wall - leftover changes only by the budget's residual
+    # (delta-SPH diffusion, shift, wall clamp; DSPH.py:1800-1852), the solid's total
+    # (ke + ie + hg + pe - leftover) by the viscous and wall work
+    def e_bal(b):
+        if tag == "dambreak3d":
+            return b["ke"] + b["se"] + b["pe"] - b["visc"] + b["wall"] - b["leftover"]
+        return b["total"]
+    scale = max(abs(bud0["pe"]), abs(bud0["ke"]) + abs(bud0.get("ie", 0.0)), 1e-300)
+    drift = {"window_steps": K, "E_bal_start": e_bal(bud0), "E_bal_end": e_bal(bud1),
+             "E_bal_change_rel": (e_bal(bud1) - e_bal(bud0)) / scale,
+             "diffusion_work_in_window_rel": (bud1["wd"] - bud0["wd"]) / scale,
+             "scale": "max(|pe|, ke + ie) at the window's start",
+             "fp64_oracle_comparison": "tests/test_drift_gpu.py (1000 steps at 128k particles)"}
 
     # ---------------------------------------------------------------- e2e through the public API
     # Per step, as the reference's driver loop does (run_simulation.py:1186-1209): write
@@ -454,26 +494,33 @@ def main():
     torch.cuda.empty_cache()
 
     # ---------------------------------------------------------------- per-kernel timing
-    solver.profile(True)
-    for _ in range(args.profile_steps):
-        solver.step()
-    prof = solver.profile_read()
-    solver.profile(False)
-    launches_per_step = sum(c for _, c in prof.values()) / max(args.profile_steps, 1)
-    per_step_ms = {k: v[0] / args.profile_steps for k, v in prof.items()}
+    # CUDA events around every kernel of eagerly launched steps, on a third copy warmed up
+    # the same way: the same steps of the simulation as the timed window.
+    ps_p, solver_p = warm_solver(False)
+    solver_p.profile(True)
+    solver_p.profile_read()
+    Kp = min(K, args.profile_steps) if args.profile_steps > 0 else K
+    for _ in range(Kp):
+        solver_p.step()
+    prof = solver_p.profile_read()
+    solver_p.profile(False)
+    del solver_p, ps_p
+    torch.cuda.empty_cache()
+    launches_per_step = sum(c for _, c in prof.values()) / max(Kp, 1)
+    per_step_ms = {k: v[0] / Kp for k, v in prof.items()}
     dom = max(prof, key=lambda k: per_step_ms[k])
     if dom not in ALGO_BYTES:
         dom = max((k for k in prof if k in ALGO_BYTES), key=lambda k: per_step_ms[k])
     dom_ms = prof[dom][0] / prof[dom][1]
     peak, peak_kind = load_peaks()
     achieved = ALGO_BYTES[dom] * n / (dom_ms / 1000.0) / 1e9
-    traffic = read_traffic(dom, tag, n)
+    traffic = scaled_traffic(dom, tag, n)
     roofline = {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peak,
                 "unit": "GB/s", "frac": achieved / peak, "peak_source": peak_kind,
                 "algorithmic_bytes_per_particle": ALGO_BYTES[dom],
                 "launch_ms": dom_ms, "traffic": traffic,
-                "traffic_source": ("ncu dram__bytes_read.sum + dram__bytes_write.sum per launch, "
-                                   "profiles/%s.md" % tag) if traffic else None}
+                "traffic_source": ("ncu dram__bytes_read.sum + dram__bytes_write.sum of a launch at "
+                                   "256k particles, scaled by the particle count") if traffic else None}
     import ctypes as C
     fma = C.c_double(0.0)
     abi.check(abi.lib().sph_fma_peak(C.byref(fma), None), "sph_fma_peak")
@@ -499,6 +546,8 @@ def main():
                 "e2e": e2e, "gpu_launches": int(round(launches_per_step * K)),
                 "neighbour_lists": {"timed_steps": lists["steps"], "builds": lists["builds"],
                                     "shift_searches": lists["shift_searches"]},
+                "steady_state": steady, "drift": drift,
+                "kernel_profile_window": f"{Kp} eager steps, the same steps of the simulation as the timed window",
                 "roofline": roofline, "step_roofline": step_roofline, "fp32_bound": fp32_bound,
                 "kernel_ms_per_step": {k: round(v, 5) for k, v in sorted(per_step_ms.items(),
                                                                        key=lambda t: -t[1])},

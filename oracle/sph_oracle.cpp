@@ -143,34 +143,80 @@ struct Sim {
 
     void initialize_particle_system() {
         // update_grid_id (:1300-1318)
-        std::fill(gpn.begin(), gpn.end(), 0);
-        off_grid_num = 0;
-        off_grid_mass = 0;
+        int32_t ogn = 0;
+        double ogm = 0;
+#pragma omp parallel for schedule(static) reduction(+ : ogn, ogm)
         for (int64_t i = 0; i < n; ++i) {
             int32_t g = (int32_t)T;
             auto c = pos_to_index(x[i]);
             cell_id[i] = c;
             if (on_grid(x[i])) g = hash_cell(c);
-            else { off_grid_num += 1; off_grid_mass += (double)m[i]; }
+            else { ogn += 1; ogm += (double)m[i]; }
             grid_ids[i] = g;
-            gpn[g] += 1;
         }
-        gpn_temp = gpn;
-        // PrefixSumExecutor (inclusive)
-        for (int64_t b = 1; b <= T; ++b) gpn[b] += gpn[b - 1];
-        // counting_sort (:1320-1340), executed serially so the order is reproducible
-        for (int64_t i = 0; i < n; ++i) {
-            int64_t I = n - 1 - i;
-            int32_t g = grid_ids[I];
-            int32_t base = (g - 1 >= 0) ? gpn[g - 1] : 0;
-            gpn_temp[g] -= 1;
-            grid_ids_new[I] = gpn_temp[g] + base;
+        off_grid_num = ogn;
+        off_grid_mass = ogm;
+        // counting_sort (:1320-1340) + PrefixSumExecutor.  Read serially, the reference's
+        // sort leaves a bucket's particles in their previous order: it is a stable sort by
+        // bucket, done here as a parallel LSD radix sort (stable by construction), and
+        // gpn[b] is the inclusive count of particles in buckets <= b.
+        std::vector<int32_t> order = stable_bucket_order();
+#pragma omp parallel for schedule(static)
+        for (int64_t p = 0; p < n; ++p) grid_ids_new[order[p]] = (int32_t)p;
+#pragma omp parallel for schedule(static)
+        for (int64_t p = 0; p < n; ++p) {
+            const int64_t k = grid_ids[order[p]];
+            const int64_t knext = (p + 1 < n) ? (int64_t)grid_ids[order[p + 1]] : T + 1;
+            for (int64_t b = k; b < knext; ++b) gpn[b] = (int32_t)(p + 1);
         }
+        const int64_t kfirst = n > 0 ? (int64_t)grid_ids[order[0]] : T + 1;
+#pragma omp parallel for schedule(static)
+        for (int64_t b = 0; b < kfirst; ++b) gpn[b] = 0;
         for_each_sorted([&](auto& fld) {
             auto tmp = fld;
+#pragma omp parallel for schedule(static)
             for (int64_t i = 0; i < n; ++i) tmp[grid_ids_new[i]] = fld[i];
             fld.swap(tmp);
         });
+    }
+
+    // Particle indices stably sorted by grid_ids (keys 0 .. T): LSD radix sort, 8 bits per
+    // pass, each pass counting per thread over contiguous chunks.
+    std::vector<int32_t> stable_bucket_order() const {
+        std::vector<int32_t> a(n), b(n);
+        for (int64_t i = 0; i < n; ++i) a[i] = (int32_t)i;
+        const int nt = std::max(1, omp_get_max_threads());
+        const int64_t chunk = (n + nt - 1) / nt;
+        int passes = 0;
+        while ((T >> (8 * passes)) > 0) ++passes;
+        std::vector<int64_t> hist((size_t)nt * 256);
+        for (int pass = 0; pass < passes; ++pass) {
+            const int sh = 8 * pass;
+            std::fill(hist.begin(), hist.end(), 0);
+#pragma omp parallel num_threads(nt)
+            {
+                const int t = omp_get_thread_num();
+                const int64_t lo = std::min<int64_t>(n, t * chunk), hi = std::min<int64_t>(n, lo + chunk);
+                int64_t* h = &hist[(size_t)t * 256];
+                for (int64_t q = lo; q < hi; ++q) h[(grid_ids[a[q]] >> sh) & 255] += 1;
+            }
+            int64_t run = 0;
+            for (int d = 0; d < 256; ++d)
+                for (int t = 0; t < nt; ++t) {
+                    const int64_t c = hist[(size_t)t * 256 + d];
+                    hist[(size_t)t * 256 + d] = run;
+                    run += c;
+                }
+#pragma omp parallel num_threads(nt)
+            {
+                const int t = omp_get_thread_num();
+                const int64_t lo = std::min<int64_t>(n, t * chunk), hi = std::min<int64_t>(n, lo + chunk);
+                int64_t* h = &hist[(size_t)t * 256];
+                for (int64_t q = lo; q < hi; ++q) b[h[(grid_ids[a[q]] >> sh) & 255]++] = a[q];
+            }
+            a.swap(b);
+        }
+        return a;
     }
 
     // for_all_neighbors (particle_system.py:1348-1490).  `live` chooses the centre
@@ -348,6 +394,7 @@ struct Sim {
             div_rate1[i] = r1;
             w_diff_step += -(double)V[i] * (double)pressure[i] * (double)r1;
         }
+#pragma omp parallel for schedule(static)
         for (int64_t i = 0; i < n; ++i) {
             R dVdt = -V[i] * divergence[i];
             if (P.compensated_volume) {
@@ -371,8 +418,9 @@ struct Sim {
     // ------------------------------------------------------------ forces (DSPH.py:1497-1650)
     void compute_forces() {
         // compute_non_pressure_forces
-        for (int64_t i = 0; i < n; ++i) acc[i] = {R(P.gravity[0]), R(P.gravity[1]), R(P.gravity[2])};
+#pragma omp parallel for schedule(static)
         for (int64_t i = 0; i < n; ++i) {
+            acc[i] = {R(P.gravity[0]), R(P.gravity[1]), R(P.gravity[2])};
             pressure[i] = pressure_from_density(m[i] / V[i]);
             de_visc[i] = 0;
         }
@@ -451,17 +499,16 @@ struct Sim {
         V3<R> g = {R(P.gravity[0]), R(P.gravity[1]), R(P.gravity[2])};
         R gsq = dot(g, g);
         double wv = 0, wl = 0;
+#pragma omp parallel for schedule(static) reduction(+ : wv, wl)
         for (int64_t i = 0; i < n; ++i) {
             V3<R> f = acc[i] - g;
             wl += (double)(R(0.5) * m[i] * dtl * dtl * (dot(f, f) - gsq));
             if (P.track_visc_work) wv += (double)m[i] * (double)de_visc[i];
-        }
-        visc_work += (double)dtl * wv;
-        leftover_work += wl;
-        for (int64_t i = 0; i < n; ++i) {
             v[i] += dtl * acc[i];
             displace(i, dtl * v[i]);
         }
+        visc_work += (double)dtl * wv;
+        leftover_work += wl;
     }
     void displace(int64_t p, const V3<R>& d) {
         if (P.displacement_positions) { u[p] += d; x[p] = x0[p] + u[p]; }
@@ -522,6 +569,7 @@ struct Sim {
     void apply_pst() {
         if (P.pst_ma_mode == 1) {
             R mv = 0;
+#pragma omp parallel for schedule(static) reduction(max : mv)
             for (int64_t i = 0; i < n; ++i) if (on_grid(x[i])) mv = std::max(mv, norm(v[i]));
             max_v = mv;
         }
@@ -559,19 +607,24 @@ struct Sim {
             }
             pst_shift[i] = pst_constrain(i, dr);
         }
+#pragma omp parallel for schedule(static)
         for (int64_t i = 0; i < n; ++i) displace(i, pst_shift[i]);
     }
 
     // ------------------------------------------------------------ boundary (sph_base.py:160-655)
-    void simulate_collisions(int64_t i, const V3<R>& nv) {
+    // the wall work of one collision (added by the caller)
+    double simulate_collisions(int64_t i, const V3<R>& nv) {
         R vn = dot(v[i], nv);
         if (vn > R(0)) {
             R c = R(P.wall_restitution);
-            wall_work += (double)(R(0.5) * m[i] * vn * vn * R(1.0 - (double)P.wall_restitution * P.wall_restitution));
             v[i] -= (R(1.0 + (double)c) * vn) * nv;
+            return (double)(R(0.5) * m[i] * vn * vn * R(1.0 - (double)P.wall_restitution * P.wall_restitution));
         }
+        return 0.0;
     }
     void enforce_walls(int faces) {  // faces: bit0 x, bit1 y-low, bit2 y-high, bit3 z
+        double ww = 0;
+#pragma omp parallel for schedule(static) reduction(+ : ww)
         for (int64_t i = 0; i < n; ++i) {
             V3<R> pos = x[i];
             V3<R> cn;
@@ -584,8 +637,9 @@ struct Sim {
                 if (do_lo && pos[k] <= lo) { cn[k] += R(-1); place_component(i, k, lo); }
             }
             R cl = norm(cn);
-            if (cl > R(1e-6)) simulate_collisions(i, {cn[0] / cl, cn[1] / cl, cn[2] / cl});
+            if (cl > R(1e-6)) ww += simulate_collisions(i, {cn[0] / cl, cn[1] / cl, cn[2] / cl});
         }
+        wall_work += ww;
     }
     void boundary() {
         if (P.axisymmetric) {

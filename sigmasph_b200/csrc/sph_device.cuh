@@ -294,11 +294,50 @@ __device__ __forceinline__ F3 wendland_dW2(F3 r, float d2, float& rn, const Cst&
     return {0.0f, 0.0f, 0.0f};
 }
 
+// The factor f of grad_i W = f r (r = x_i - x_j) from the squared separation: the
+// arithmetic of wendland_dW2 without the vector.
+__device__ __forceinline__ float wendland_dW_factor(float d2, const Cst& c) {
+    const float rn = d2 > 0.0f ? d2 * rsqrtf(d2) : 0.0f;
+    const float q = rn * c.inv_h;
+    if (q < 1.0f && rn > 1.0e-5f) {
+        const float t = 1.0f - q;
+        return -(c.kgrad * c.inv_h * (t * t * t));
+    }
+    return 0.0f;
+}
+
+// W and grad_i W from the squared separation in one evaluation: the same arithmetic as
+// wendland_dW2 followed by wendland_W(rn).
+__device__ __forceinline__ F3 wendland_W_dW2(F3 r, float d2, float& W, const Cst& c) {
+    const float rn = d2 > 0.0f ? d2 * rsqrtf(d2) : 0.0f;
+    const float q = rn * c.inv_h;
+    W = 0.0f;
+    if (q < 1.0f) {
+        const float t = 1.0f - q;
+        const float t2 = t * t;
+        W = c.alpha * (t2 * t2) * (4.0f * q + 1.0f);
+        if (rn > 1.0e-5f) {
+            const float f = -(c.kgrad * c.inv_h * (t2 * t));
+            return f * r;
+        }
+    }
+    return {0.0f, 0.0f, 0.0f};
+}
+
 // x^n for the Monaghan tensile-correction exponent (an integer in every deck; any other
-// value goes through powf).
+// value goes through powf).  Repeated products in the order ((x x) x) ..., unrolled.
 __device__ __forceinline__ float ipow_or_pow(float x, int n) {
-    if (n >= 0 && n <= 8) {
-        float r = 1.0f;
+    float r;
+    switch (n) {
+        case 0: return 1.0f;
+        case 1: return x;
+        case 2: return x * x;
+        case 3: r = x * x; return r * x;
+        case 4: r = x * x; r = r * x; return r * x;
+        default: break;
+    }
+    if (n > 4 && n <= 8) {
+        r = 1.0f;
         for (int k = 0; k < n; ++k) r *= x;
         return r;
     }

@@ -30,23 +30,20 @@ __global__ void SPH_BOUNDS(SPH_OCC_LAM) k_lam(Cst c, Ptr P) {
     const float4* __restrict__ pos = as4c(P.cur.pos);
     float4 pi = pos[i];
     F3 xi = f3(pi);
-    float E[3][3] = {{0, 0, 0}, {0, 0, 0}, {0, 0, 0}};
+    // E = sum V_j (x_j - x_i) (x) grad W (DSPH.py:611-681).  grad W = f r with r = x_i - x_j,
+    // so each pair adds -V_j f r (x) r: a symmetric matrix, accumulated as its six entries
+    float e00 = 0.f, e11 = 0.f, e22 = 0.f, e01 = 0.f, e02 = 0.f, e12 = 0.f;
     auto pair = [&](int mir, float4 pj) {
         F3 xj = f3(pj);
         if (mir) xj = mirror3(mir, xj);
-        F3 d = xj - xi;
-        F3 r = xi - xj;
-        float rn;
-        F3 g = wendland_dW2(r, dot3(r, r), rn, c);
-        float Vj = w_of(pj, c);
-        E[0][0] += Vj * (d.x * g.x); E[0][1] += Vj * (d.x * g.y);
-        E[1][0] += Vj * (d.y * g.x); E[1][1] += Vj * (d.y * g.y);
-        if (!c.p.two_d) {
-            E[0][2] += Vj * (d.x * g.z); E[1][2] += Vj * (d.y * g.z);
-            E[2][0] += Vj * (d.z * g.x); E[2][1] += Vj * (d.z * g.y); E[2][2] += Vj * (d.z * g.z);
-        }
+        const F3 r = xi - xj;
+        const float f = wendland_dW_factor(dot3(r, r), c);
+        const F3 sr = (-(w_of(pj, c) * f)) * r;
+        e00 += sr.x * r.x; e01 += sr.x * r.y; e11 += sr.y * r.y;
+        if (!c.p.two_d) { e02 += sr.x * r.z; e12 += sr.y * r.z; e22 += sr.z * r.z; }
     };
     for_each_neighbour(c, P, i, [&](int j, int mir) { pair(mir, __ldg(pos + j)); });
+    const float E[3][3] = {{e00, e01, e02}, {e01, e11, e12}, {e02, e12, e22}};
     const float tol = c.p.l_eig_tol_lam;
     float L00, L11, L22, L01, L02, L12, lam;
     float4 evec = make_float4(0.f, 0.f, 0.f, 0.f);
@@ -123,12 +120,6 @@ __global__ void SPH_BOUNDS(SPH_OCC_LAMGRAD) k_lamgrad_cont(Cst c, Ptr P) {
         const float inv_dt = 1.0f / dt;
         const bool pst = c.p.pst_enabled;
         const bool need_lgrad = !c.p.pst_normal_eigvec;
-        F3 du_i = {0, 0, 0};
-        if (pst) {
-            float4 s = shf[i];
-            du_i = {s.x * inv_dt, s.y * inv_dt, s.z * inv_dt};
-        }
-        const F3 vhat_i = vi + du_i;
         F3 lg = {0, 0, 0};
         float r0 = 0.0f, r1 = 0.0f;
         // the next neighbour's position is requested while this pair is evaluated
@@ -150,14 +141,16 @@ __global__ void SPH_BOUNDS(SPH_OCC_LAMGRAD) k_lamgrad_cont(Cst c, Ptr P) {
                 lg += (Vj * ld) * Lg;
             }
             float rho_j = vj4.w / pj.w;   // exact: rho_j - rho_i is a small difference
-            F3 vh_j = vj;
+            // the velocity divergence with the shift's mass flux (DSPH.py:1240-1262):
+            // V_j [(rho_j du_j - rho_i du_i) . gW / rho_i + (v_i + du_i - v_j - du_j) . gW],
+            // whose du_i terms cancel: V_j [(v_i - v_j) . gW + (rho_j - rho_i) / rho_i du_j . gW]
+            float rr = dot3(vi - vj, g);
             if (pst) {
                 F3 du_j = {sj.x * inv_dt, sj.y * inv_dt, sj.z * inv_dt};
                 if (mir) du_j = mirror3(mir, du_j);
-                vh_j += du_j;
-                r0 += Vj * dot3(rho_j * du_j - rho_i * du_i, g) * inv_rho_i;
+                rr += (rho_j - rho_i) * inv_rho_i * dot3(du_j, g);
             }
-            r0 += Vj * dot3(vhat_i - vh_j, g);
+            r0 += Vj * rr;
             if (c.p.delta_sph > 0.0f) {
                 // psi . grad W = 2 (rho_j - rho_i) (-r . grad W) / (|r|^2 + eta^2)
                 float psig = __fdividef(2.0f * (rho_j - rho_i) * (-dot3(r, g)), rn2 + c.eta2);
@@ -235,11 +228,6 @@ __global__ void SPH_BOUNDS(SPH_OCC_FORCE) k_force(Cst c, Ptr P) {
         const float mw_i = mw_of(vi4.w, pi, c);
         const float dt = P.sc->dt;
         const bool ale = c.p.pst_enabled && c.p.pst_ale_momentum;
-        F3 du_i = {0, 0, 0};
-        if (ale) {
-            float4 s = shf[i];
-            du_i = {s.x / dt, s.y / dt, s.z / dt};
-        }
         const float eps_rho = 1e-3f * c.p.density0;
         const float inv_mw_i = 1.0f / mw_i, inv_rho_i = 1.0f / rho_i, inv_dt = 1.0f / dt;
         const float wi_mw = w_i * inv_mw_i;
@@ -258,18 +246,19 @@ __global__ void SPH_BOUNDS(SPH_OCC_FORCE) k_force(Cst c, Ptr P) {
             float w_j = w_of(pj, c);
             // -w_i w_j (p_i + p_j) grad W / mw_i
             a += (-wi_mw * w_j * (p_i + p_j)) * g;
-            float vxy = dot3(vi - vj, r);
+            const F3 vij = vi - vj;
+            float vxy = dot3(vij, r);
             F3 fv = __fdividef(c.visc_coef * w_j * vxy, rn * rn + c.eta2) * g;
             a += fv;
             dvisc += dot3(vi, fv);
             float rho_j = vj4.w / pj.w;   // exact: rho_j - rho_i is a small difference
             if (ale) {
+                // the ALE momentum term w_j [div(rho v du) - v_i div(rho du)] / rho_i
+                // (DSPH.py:1630-1640), whose rho_i du_i parts cancel:
+                // w_j rho_j (du_j . gW) (v_j - v_i) / rho_i
                 F3 du_j = {sj.x * inv_dt, sj.y * inv_dt, sj.z * inv_dt};
                 if (mir) du_j = mirror3(mir, du_j);
-                F3 t1 = (rho_j * dot3(du_j, g)) * vj - (rho_i * dot3(du_i, g)) * vi;
-                float b = dot3(rho_j * du_j - rho_i * du_i, g);
-                F3 t = t1 - b * vi;
-                a += (w_j * inv_rho_i) * t;
+                a += (-(w_j * inv_rho_i) * (rho_j * dot3(du_j, g))) * vij;
             }
             if (c.p.dt_pair_mode != 0) {
                 float drho = fabsf(rho_i - rho_j);
@@ -442,9 +431,8 @@ __device__ __forceinline__ F3 pst_pair_term(const Cst& c, const float4* __restri
     F3 xj = f3(pj);
     if (mir) xj = mirror3(mir, xj);
     F3 r = xi - xj;
-    float rn;
-    F3 g = wendland_dW2(r, dot3(r, r), rn, c);
-    float Wij = wendland_W(rn, c);
+    float Wij;
+    F3 g = wendland_W_dW2(r, dot3(r, r), Wij, c);
     float f = 0.0f;
     if (c.W_dx0 > 1e-10f) f = c.p.pst_R * ipow_or_pow(Wij * inv_Wd, c.p.pst_n);
     if (c.p.pst_colle) {
@@ -454,9 +442,10 @@ __device__ __forceinline__ F3 pst_pair_term(const Cst& c, const float4* __restri
         float mj_raw = m_uni ? m_u : __ldg(&vel[j].w);
         float mj = mw_of(mj_raw, pj, c);
         if (mj > 1e-10f) {
-            float rho_j = mj_raw / pj.w;
+            // m_j / mean rho: a sum of densities, rounded quotients suffice (no cancellation)
+            float rho_j = __fdividef(mj_raw, pj.w);
             float ra = 0.5f * (rho_i + rho_j);
-            if (ra > 1e-10f) return ((1.0f + f) * (mj / ra)) * g;
+            if (ra > 1e-10f) return ((1.0f + f) * __fdividef(mj, ra)) * g;
         }
     }
     return {0.0f, 0.0f, 0.0f};

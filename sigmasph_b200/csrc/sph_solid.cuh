@@ -385,19 +385,18 @@ __global__ void __launch_bounds__(kBlock) k_kc_inverse(Cst c, Ptr P) {
     if (i >= c.n) return;
     const float4* __restrict__ pos = as4c(P.cur.pos);
     F3 xi = f3(pos[i]);
-    float E[3][3] = {{0, 0, 0}, {0, 0, 0}, {0, 0, 0}};
+    // E = sum V_j (x_j - x_i) (x) grad W, symmetric (grad W = f r): six entries
+    float e00 = 0.f, e11 = 0.f, e22 = 0.f, e01 = 0.f, e02 = 0.f, e12 = 0.f;
     for_each_neighbour(c, P, i, [&](int j, int mir) {
         float4 pj = __ldg(pos + j);
         F3 xj = f3(pj);
         if (mir) xj = mirror3(mir, xj);
-        F3 d = xj - xi, r = xi - xj;
-        float rn;
-        F3 g = wendland_dW2(r, dot3(r, r), rn, c);
-        float Vj = w_of(pj, c);
-        E[0][0] += Vj * (d.x * g.x); E[0][1] += Vj * (d.x * g.y); E[0][2] += Vj * (d.x * g.z);
-        E[1][0] += Vj * (d.y * g.x); E[1][1] += Vj * (d.y * g.y); E[1][2] += Vj * (d.y * g.z);
-        E[2][0] += Vj * (d.z * g.x); E[2][1] += Vj * (d.z * g.y); E[2][2] += Vj * (d.z * g.z);
+        const F3 r = xi - xj;
+        const F3 sr = (-(w_of(pj, c) * wendland_dW_factor(dot3(r, r), c))) * r;
+        e00 += sr.x * r.x; e01 += sr.x * r.y; e02 += sr.x * r.z;
+        e11 += sr.y * r.y; e12 += sr.y * r.z; e22 += sr.z * r.z;
     });
+    const float E[3][3] = {{e00, e01, e02}, {e01, e11, e12}, {e02, e12, e22}};
     store_kc_inverse(c, P, i, E, P.lam[i]);
 }
 
@@ -421,9 +420,6 @@ __global__ void SPH_BOUNDS(SPH_OCC_SOLID_A) k_solid_a(Cst c, Ptr P) {
         const float dt = dt_at(c, P, ki), inv_dt = 1.0f / dt;
         const float di = P.mat[ki].delta;
         const float c0i = c.n_inst > 0 ? P.irow[ki].c0 : c.p.c0;
-        F3 du_i = {0, 0, 0};
-        if (pst) { float4 s = shf[i]; du_i = {s.x * inv_dt, s.y * inv_dt, s.z * inv_dt}; }
-        const F3 vhat_i = vi + du_i;
         F3 lg = {0, 0, 0};
         float r0 = 0.0f, r1 = 0.0f;
         float G[3][3] = {{0, 0, 0}, {0, 0, 0}, {0, 0, 0}};
@@ -440,19 +436,21 @@ __global__ void SPH_BOUNDS(SPH_OCC_SOLID_A) k_solid_a(Cst c, Ptr P) {
                      L02 * g.x + L12 * g.y + L22 * g.z};
             lg += (Vj * ld) * Lg;
             F3 dv = vj - vi;
-            G[0][0] += Vj * (dv.x * g.x); G[0][1] += Vj * (dv.x * g.y); G[0][2] += Vj * (dv.x * g.z);
-            G[1][0] += Vj * (dv.y * g.x); G[1][1] += Vj * (dv.y * g.y); G[1][2] += Vj * (dv.y * g.z);
-            G[2][0] += Vj * (dv.z * g.x); G[2][1] += Vj * (dv.z * g.y); G[2][2] += Vj * (dv.z * g.z);
+            const F3 vd = Vj * dv;
+            G[0][0] += vd.x * g.x; G[0][1] += vd.x * g.y; G[0][2] += vd.x * g.z;
+            G[1][0] += vd.y * g.x; G[1][1] += vd.y * g.y; G[1][2] += vd.y * g.z;
+            G[2][0] += vd.z * g.x; G[2][1] += vd.z * g.y; G[2][2] += vd.z * g.z;
             float rho_j = vj4.w / pj.w;
-            F3 vh_j = vj;
+            // velocity divergence with the shift's mass flux, its du_i terms cancelled
+            // (DSPH.py:1240-1262): V_j [(v_i - v_j) . gW + (rho_j - rho_i) / rho_i du_j . gW]
+            float rr = -dot3(dv, g);
             if (pst) {
                 float4 s = __ldg(shf + j);
                 F3 du_j = {s.x * inv_dt, s.y * inv_dt, s.z * inv_dt};
                 if (mir) du_j = mirror3(mir, du_j);
-                vh_j += du_j;
-                r0 += Vj * dot3(rho_j * du_j - rho_i * du_i, g) * inv_rho_i;
+                rr += (rho_j - rho_i) * inv_rho_i * dot3(du_j, g);
             }
-            r0 += Vj * dot3(vhat_i - vh_j, g);
+            r0 += Vj * rr;
             // pair_delta and pair_c0 (SOLID.py:4102-4114, DSPH.py:483-511) on same-material
             // pairs, or on every pair under Diffusion.pairs "all" (DSPH.py:1271-1282)
             const int kj = c.one_material ? ki : eos_of(P, j);
@@ -496,11 +494,10 @@ __global__ void SPH_PAIR_BOUNDS_OCC4 k_gradv(Cst c, Ptr P) {
         F3 r = xi - xj;
         float rn;
         F3 g = wendland_dW2(r, dot3(r, r), rn, c);
-        float Vj = w_of(pj, c);
-        F3 dv = vj - vi;
-        G[0][0] += Vj * (dv.x * g.x); G[0][1] += Vj * (dv.x * g.y); G[0][2] += Vj * (dv.x * g.z);
-        G[1][0] += Vj * (dv.y * g.x); G[1][1] += Vj * (dv.y * g.y); G[1][2] += Vj * (dv.y * g.z);
-        G[2][0] += Vj * (dv.z * g.x); G[2][1] += Vj * (dv.z * g.y); G[2][2] += Vj * (dv.z * g.z);
+        const F3 vd = w_of(pj, c) * (vj - vi);
+        G[0][0] += vd.x * g.x; G[0][1] += vd.x * g.y; G[0][2] += vd.x * g.z;
+        G[1][0] += vd.y * g.x; G[1][1] += vd.y * g.y; G[1][2] += vd.y * g.z;
+        G[2][0] += vd.z * g.x; G[2][1] += vd.z * g.y; G[2][2] += vd.z * g.z;
     });
     grad_v_finish<NoExtra>(c, P, i, G, pi, vi.y);
 }
@@ -667,16 +664,17 @@ __global__ void SPH_BOUNDS(SPH_OCC_SOLID_B) k_solid_b(Cst c, Ptr P) {
                 F3 g = wendland_dW2(r, rn2, rn, c);
                 float rho_j = vj4.w / pj.w;
                 float wj = w_of(pj, c);
-                float a_j = rho_j * dot3(du_j, g), a_i = rho_i * dot3(du_i, g);
-                float dv = dot3(rho_j * du_j - rho_i * du_i, g);
-                float k = wj * inv_rho_i;
-                A.xx += k * (a_j * sj.xx - a_i * s.xx - s.xx * dv);
-                A.yy += k * (a_j * sj.yy - a_i * s.yy - s.yy * dv);
-                A.zz += k * (a_j * sj.zz - a_i * s.zz - s.zz * dv);
-                A.xy += k * (a_j * sj.xy - a_i * s.xy - s.xy * dv);
-                A.xz += k * (a_j * sj.xz - a_i * s.xz - s.xz * dv);
-                A.yz += k * (a_j * sj.yz - a_i * s.yz - s.yz * dv);
-                if (plastic_any) dep += k * (a_j * epj - a_i * ep - ep * dv);
+                // w_j [(rho_j du_j . gW) phi_j - (rho_i du_i . gW) phi_i - phi_i div(rho du)]
+                // / rho_i (SOLID.py:1799-1862), whose rho_i du_i parts cancel:
+                // w_j rho_j (du_j . gW) (phi_j - phi_i) / rho_i
+                const float ka = wj * inv_rho_i * (rho_j * dot3(du_j, g));
+                A.xx += ka * (sj.xx - s.xx);
+                A.yy += ka * (sj.yy - s.yy);
+                A.zz += ka * (sj.zz - s.zz);
+                A.xy += ka * (sj.xy - s.xy);
+                A.xz += ka * (sj.xz - s.xz);
+                A.yz += ka * (sj.yz - s.yz);
+                if (plastic_any) dep += ka * (epj - ep);
                 if (c.p.transport_e) {
                     float e_j = shj.w;
                     adv += wj * rho_j * (e_j - e_i) * dot3(du_j, g) * inv_rho_i;
@@ -987,8 +985,6 @@ __global__ void SPH_BOUNDS(SPH_OCC_SOLID_FORCE) k_solid_force(Cst c, Ptr P) {
         const float visc = visc_at(c, P, ki);
         kinst = ki;
         on = true;
-        F3 du_i = {0, 0, 0};
-        if (ale) { float4 q = shf[i]; du_i = {q.x * inv_dt, q.y * inv_dt, q.z * inv_dt}; }
         const float eps_rho = 1e-3f * c.p.density0;
         const float csig = c.n_inst > 0 ? P.irow[ki].c_signal : c.p.c_signal;
         float cl = csig * csig;
@@ -1082,13 +1078,12 @@ __global__ void SPH_BOUNDS(SPH_OCC_SOLID_FORCE) k_solid_force(Cst c, Ptr P) {
                 dvisc += 0.5f * dot3(ap, vij);
             }
             if (ale) {
+                // the ALE momentum term with its rho_i du_i parts cancelled (as the fluid's):
+                // w_j rho_j (du_j . gW) (v_j - v_i) / rho_i
                 float4 q = __ldg(shf + j);
                 F3 du_j = {q.x * inv_dt, q.y * inv_dt, q.z * inv_dt};
                 if (mir) du_j = mirror3(mir, du_j);
-                F3 t1 = (rho_j * dot3(du_j, g)) * vj - (rho_i * dot3(du_i, g)) * vi;
-                float b = dot3(rho_j * du_j - rho_i * du_i, g);
-                F3 t = t1 - b * vi;
-                a += (w_j * inv_rho_i) * t;
+                a += (-(w_j * inv_rho_i) * (rho_j * dot3(du_j, g))) * vij;
             }
             if (c.p.dt_pair_mode != 0 && (c.p.dt_pair_mode != 2 || same_material(c, P, j, ki))) {
                 float drho = fabsf(rho_i - rho_j);

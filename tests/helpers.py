@@ -128,3 +128,35 @@ def field_errors(g, r, keys):
         scale = np.abs(b).max()
         out[k] = float(np.abs(a - b).max() / scale) if scale > 0 else float(np.abs(a - b).max())
     return out
+
+
+# Per-particle relative error: |g_i - r_i| / max(|r_i|, PP_FLOOR * max |r|).  Values above
+# 1% of the field's largest are compared relative to themselves, so a particle whose
+# value is small but wrong shows, which the field-wide max |g - r| / max |r| hides.
+PP_FLOOR = 1e-2
+
+
+def pp_errors(g, r, keys, floor=PP_FLOOR):
+    """max over particles (and components) of the per-particle relative error, per field."""
+    out = {}
+    for k in keys:
+        a, b = np.asarray(g[k], dtype=np.float64), np.asarray(r[k], dtype=np.float64)
+        scale = np.abs(b).max()
+        den = np.maximum(np.abs(b), floor * scale)
+        d = np.abs(a - b)
+        out[k] = float((d / np.where(den > 0, den, 1.0)).max()) if scale > 0 else float(d.max())
+    return out
+
+
+def check_pp(g, r32, r64, keys, factor=4.0, slack=1e-5):
+    """Every particle of the GPU field is as close to the float64 oracle, relative to its
+    own value (floor PP_FLOOR of the largest), as the float32 oracle's worst particle is:
+    max_i e_i(GPU, FP64) <= factor * max_i e_i(FP32, FP64) + slack.  Both sides carry
+    float32 rounding in a different order, so a factor of a few covers the summation-order
+    noise; a wrong particle anywhere above 1% of the field's largest fails it."""
+    eg = pp_errors(g, r64, keys)
+    eo = pp_errors(r32, r64, keys)
+    for k in keys:
+        assert eg[k] <= factor * eo[k] + slack, (k, eg[k], eo[k])
+    return eg, eo
+

@@ -1,0 +1,128 @@
+"""Energy, momentum and per-field drift of the GPU path against the all-FP64 oracle build
+over a long run: the 3D dam break at 128k particles (dx = 9.449 mm, the float64 oracle's
+size of that scene), 1000 steps, with the float32 oracle beside it as the yardstick of
+what float32 arithmetic alone drifts.
+
+The balance is the reference's own (DSPH.py:1800-1852): total = ke + se + pe, and
+    total(t) - total(0) = visc - wall + leftover + residual,
+so E_bal = ke + se + pe - visc + wall - leftover changes only by the residual (delta-SPH
+diffusion, shift, wall clamp).  That residual is the same physics on all three runs;
+what differs between them is arithmetic.  Checked every 100 steps:
+  * E_bal of the GPU minus E_bal of the FP64 oracle, against the FP32 oracle's distance,
+    both relative to |pe(0)| (the column's potential energy, the budget's largest term);
+  * linear momentum (gravity and the walls change it; the three runs must agree);
+  * x (over dx0), v, V and p, field-wide and per particle (floor 1% of the largest).
+The GPU must stay within 4x the FP32 oracle's distance to FP64 (plus a floor).  With
+SPH_DRIFT_REPORT set, the table is written there as JSON.
+"""
+import json
+import os
+
+import numpy as np
+import pytest
+
+from sigmasph_b200.config import SimConfig
+from sigmasph_b200.particle_system import ParticleSystem
+from sigmasph_b200.scenes import dambreak3d
+from sigmasph_b200.solver import build_params
+from oracle.oracle import Oracle, state_from_sets
+from tests.helpers import gpu_fields, oracle_fields, field_errors, pp_errors
+
+pytestmark = pytest.mark.gpu
+
+DX_128K = 0.009449
+STEPS = 1000
+EVERY = 100
+
+
+def tait_energy(p, m, V):
+    """DSPHSolver.compute_elastic_energy in float64 (DSPH.py:1670-1712)."""
+    rho0, S, gam = float(p.density0), float(p.stiffness), float(p.exponent)
+    rho = m / V
+    x = rho / rho0
+    e = (S / rho0) * ((x ** (gam - 1.0) - 1.0) / (gam - 1.0) + 1.0 / x - 1.0)
+    if not p.allow_negative_pressure:
+        e = np.where(rho < rho0, 0.0, e)
+    return float((m * e).sum())
+
+
+def budget(p, f, sc):
+    """ke, se, pe, momentum and E_bal from a reference-layout state and the work scalars."""
+    m = np.asarray(f["m"], dtype=np.float64)
+    v = np.asarray(f["v"], dtype=np.float64)
+    x = np.asarray(f["x"], dtype=np.float64)
+    g = np.array([p.gravity[0], p.gravity[1], p.gravity[2]], dtype=np.float64)
+    ke = float((0.5 * m * (v * v).sum(1)).sum())
+    pe = float(-(m * (x @ g)).sum())
+    se = tait_energy(p, m, np.asarray(f["V"], dtype=np.float64))
+    P = (m[:, None] * v).sum(0)
+    e_bal = ke + se + pe - sc["visc_work"] + sc["wall_work"] - sc["leftover_work"]
+    return {"ke": ke, "se": se, "pe": pe, "P": P, "gross": float((m * np.linalg.norm(v, axis=1)).sum()),
+            "E_bal": e_bal, "visc": sc["visc_work"], "wall": sc["wall_work"],
+            "leftover": sc["leftover_work"], "wd": sc["diff_work"]}
+
+
+def gpu_scalars(solver):
+    s = solver._scalars()
+    return {k: float(getattr(s, k)) for k in ("visc_work", "wall_work", "leftover_work", "diff_work")}
+
+
+def test_dambreak_128k_drift_against_fp64(cuda):
+    Oracle.threads(os.cpu_count())
+    ps = ParticleSystem(SimConfig(dambreak3d(dx=DX_128K)), device="cuda")
+    n = ps.particle_max_num
+    assert 120000 < n < 140000
+    solver = ps.build_solver()
+    p = build_params(ps)
+    st0 = state_from_sets(ps.state_numpy())
+    dt0 = solver.dt[None]
+    o64 = Oracle(p, n, fp64=True)
+    o32 = Oracle(p, n, fp64=False)
+    for o in (o64, o32):
+        o.set_state(st0, dt0)
+        o.stage(0)
+    solver.initialize()
+    b0 = budget(p, gpu_fields(ps), gpu_scalars(solver))
+    e_ref = abs(b0["pe"])
+    rows = []
+    keys = ["x", "v", "V", "pressure"]
+    for k in range(EVERY, STEPS + 1, EVERY):
+        solver.step_many(EVERY)
+        o64.step(EVERY)
+        o32.step(EVERY)
+        g, r64, r32 = gpu_fields(ps), oracle_fields(o64), oracle_fields(o32)
+        bg = budget(p, g, gpu_scalars(solver))
+        b64 = budget(p, r64, o64.scalars())
+        b32 = budget(p, r32, o32.scalars())
+        # the library's own FP64 reductions (float32 terms per particle, as the reference
+        # forms them, summed in float64) agree with float64 sums of its state
+        red = solver.energy_budget()
+        assert red["ke"] == pytest.approx(bg["ke"], rel=1e-6)
+        assert red["pe"] == pytest.approx(bg["pe"], rel=1e-6)
+        assert red["se"] == pytest.approx(bg["se"], rel=1e-6, abs=1e-12 * e_ref)
+        eg, e32 = field_errors(g, r64, keys), field_errors(r32, r64, keys)
+        pg, p32 = pp_errors(g, r64, keys), pp_errors(r32, r64, keys)
+        # positions in units of the spacing
+        eg["x"] = float(np.abs(g["x"] - r64["x"]).max() / ps.particle_diameter)
+        e32["x"] = float(np.abs(r32["x"] - r64["x"]).max() / ps.particle_diameter)
+        rows.append({
+            "step": k,
+            "E_bal_drift_fp64": (b64["E_bal"] - b0["E_bal"]) / e_ref,
+            "E_bal_gpu_minus_fp64": (bg["E_bal"] - b64["E_bal"]) / e_ref,
+            "E_bal_fp32_minus_fp64": (b32["E_bal"] - b64["E_bal"]) / e_ref,
+            "P_gpu_minus_fp64": float(np.abs(bg["P"] - b64["P"]).max() / b64["gross"]),
+            "P_fp32_minus_fp64": float(np.abs(b32["P"] - b64["P"]).max() / b64["gross"]),
+            "field_gpu": eg, "field_fp32": e32, "pp_gpu": pg, "pp_fp32": p32,
+            "ke_fp64": b64["ke"], "pe_fp64": b64["pe"], "se_fp64": b64["se"],
+        })
+    out = os.environ.get("SPH_DRIFT_REPORT")
+    if out:
+        with open(out, "w") as f:
+            json.dump({"scene": "3D dam break", "dx_m": DX_128K, "particles": n, "steps": STEPS,
+                       "E_ref": e_ref, "rows": rows}, f, indent=1)
+    last = rows[-1]
+    assert abs(last["E_bal_gpu_minus_fp64"]) <= 4.0 * abs(last["E_bal_fp32_minus_fp64"]) + 1e-6, last
+    assert last["P_gpu_minus_fp64"] <= 4.0 * last["P_fp32_minus_fp64"] + 1e-6, last
+    for key in keys:
+        assert last["field_gpu"][key] <= 4.0 * last["field_fp32"][key] + 1e-5, (key, last)
+    assert solver.error_word() & ~0x2 == 0

@@ -23,7 +23,7 @@ from sigmasph_b200.scenes import dambreak3d, dx_for_particles
 from sigmasph_b200.solver import build_params
 from oracle.oracle import Oracle, state_from_sets
 from tests.helpers import (make_pair, pair_set, gpu_fields, oracle_fields, field_errors,
-                           perturb, check_shift_pairs)
+                           perturb, check_shift_pairs, check_pp)
 
 pytestmark = pytest.mark.gpu
 
@@ -345,12 +345,14 @@ def _stages_match_oracle(sc, mass_jitter=0.0):
         if s not in STAGE_FIELDS:
             continue
         g = gpu_fields(ps)
-        e32 = field_errors(g, oracle_fields(o32), STAGE_FIELDS[s])
-        e64 = field_errors(g, oracle_fields(o64), STAGE_FIELDS[s])
+        r32, r64 = oracle_fields(o32), oracle_fields(o64)
+        e32 = field_errors(g, r32, STAGE_FIELDS[s])
+        e64 = field_errors(g, r64, STAGE_FIELDS[s])
         for k, e in e32.items():
             assert e <= LOOSE32.get(k, 2e-5), (s, k, e)
         for k, e in e64.items():
             assert e <= LOOSE64.get(k, 1e-4), (s, k, e)
+        check_pp(g, r32, r64, STAGE_FIELDS[s])
         if s == abi.STAGE_ADVECT:
             dg, d32 = solver.dt[None], o32.scalars()["dt"]
             assert abs(dg - d32) <= 1e-6 * d32
@@ -377,6 +379,7 @@ def test_multistep_tracks_fp64_like_fp32_oracle(cuda):
     eo = field_errors(r32, r64, keys)
     for k in keys:
         assert eg[k] <= 4.0 * eo[k] + 1e-6, (k, eg[k], eo[k])
+    check_pp(g, r32, r64, keys, slack=1e-5)
     assert solver.error_word() & ~abi.EW_HASHED_GRID == 0
 
 

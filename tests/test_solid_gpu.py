@@ -12,7 +12,7 @@ from sigmasph_b200.particle_system import ParticleSystem
 from sigmasph_b200.scenes import scene_path
 from sigmasph_b200.solver import build_params
 from oracle.oracle import Oracle, state_from_sets
-from tests.helpers import pair_set, perturb, check_shift_pairs
+from tests.helpers import pair_set, perturb, check_shift_pairs, check_pp
 
 pytestmark = pytest.mark.gpu
 
@@ -288,12 +288,14 @@ def test_solid_stages_match_oracle(cuda, deck):
         if s not in STAGE_FIELDS:
             continue
         g = solid_gpu_fields(ps)
-        e32 = errs(g, solid_oracle_fields(o32), STAGE_FIELDS[s])
-        e64 = errs(g, solid_oracle_fields(o64), STAGE_FIELDS[s])
+        r32, r64 = solid_oracle_fields(o32), solid_oracle_fields(o64)
+        e32 = errs(g, r32, STAGE_FIELDS[s])
+        e64 = errs(g, r64, STAGE_FIELDS[s])
         for k, e in e32.items():
             assert e <= TOL32.get(k, 5e-5), (s, k, e, e32)
         for k, e in e64.items():
             assert e <= TOL64.get(k, 2e-4), (s, k, e, e64)
+        check_pp(g, r32, r64, STAGE_FIELDS[s])
     sg = solver._scalars()
     s32 = o32.scalars()
     assert sg.sts_stages == int(s32["sts_stages"])
@@ -361,6 +363,7 @@ def test_solid_multistep_tracks_fp64(cuda, deck):
     eo = errs(r32, r64, keys)
     for k in keys:
         assert eg[k] <= 4.0 * eo[k] + 2e-6, (k, eg[k], eo[k])
+    check_pp(g, r32, r64, keys, slack=1e-5)
     sg = solver._scalars()
     s64 = o64.scalars()
     fg = np.array([[sg.constraint_force[k][d] for d in range(3)] for k in range(solver.num_constraints)])
