@@ -43,7 +43,6 @@ struct SphHandle {
     int* nl_cnt = nullptr;
     int* ovf = nullptr;
     int* ovf_off = nullptr;
-    unsigned* xbits = nullptr;
     int4* fcell = nullptr;
     float4* xb = nullptr;
     bool force_pending = true;      // the next step builds the candidate lists
@@ -129,13 +128,13 @@ Ptr make_ptr(SphHandle* h) {
     P.nl_cnt = h->nl_cnt;
     P.ovf = h->ovf;
     P.ovf_off = h->ovf_off;
-    P.xbits = h->xbits;
     P.fcell = h->fcell;
     P.xb = h->xb;
     P.sc = h->sc;
     P.ac = h->ac;
     P.jc = solid_jc_ptr(h->solid);
     P.mat = h->solid.mat;
+    P.gsym = h->solid.gsym;
     P.irow = h->solid.irow;
     P.inst = h->solid.inst;
     return P;
@@ -198,7 +197,6 @@ int fluid_substep_and_boundary(SphHandle* h, cudaStream_t st) {
     LAUNCH("k_dt", k_dt<<<1, 32, 0, st>>>(c, P));
     LAUNCH("k_advect", k_advect<<<nb, kBlock, 0, st>>>(c, P));
     if (h->p.pst_enabled) {
-        LAUNCH("k_crossed", k_crossed<<<nb, kBlock, 0, st>>>(c, P));
         LAUNCH("k_pst", k_pst<<<nb, kBlock, 0, st>>>(c, P));
         LAUNCH("k_finish", k_finish<<<nb, kBlock, 0, st>>>(c, P, 3));
     } else {
@@ -231,7 +229,7 @@ void free_all(SphHandle* h) {
     h->prof_pool.clear();
     if (h->cap_stream) cudaStreamDestroy(h->cap_stream);
     void* ptrs[] = {h->cell, h->key, h->rank, h->perm, h->hist, h->start, h->bsum,
-                    h->bbox, h->layout, h->nbr, h->nbr_cnt, h->vl, h->vl_cnt, h->nl_cnt, h->ovf, h->ovf_off, h->xbits, h->fcell, h->xb,
+                    h->bbox, h->layout, h->nbr, h->nbr_cnt, h->vl, h->vl_cnt, h->nl_cnt, h->ovf, h->ovf_off, h->fcell, h->xb,
                     h->sc, h->ac};
     for (void* q : ptrs) if (q) cudaFree(q);
     if (h->pinned) cudaFreeHost(h->pinned);
@@ -347,7 +345,6 @@ int sph_create(const SphParams* p, int64_t n_max, SphHandle** out) {
         (r = dalloc(&h->vl, N * (size_t)Kv)) || (r = dalloc(&h->vl_cnt, N)) ||
         (r = dalloc(&h->nl_cnt, N)) ||
         (r = dalloc(&h->ovf, ovf_cap)) || (r = dalloc(&h->ovf_off, N)) ||
-        (r = dalloc(&h->xbits, N / 32 + 1)) ||
         (r = dalloc(&h->fcell, N)) || (r = dalloc(&h->xb, N)) ||
         cudaMallocHost((void**)&h->pinned, sizeof(SphScalars)) != cudaSuccess) {
         if (!r) r = SPH_ERR_NOMEM;
@@ -529,7 +526,6 @@ int sph_run_stage(SphHandle* h, int stage, void* stream) {
         case SPH_STAGE_ADVECT: k_advect<<<nb, kBlock, 0, st>>>(c, P); break;
         case SPH_STAGE_PST:
             if (h->p.pst_enabled) {
-                k_crossed<<<nb, kBlock, 0, st>>>(c, P);
                 k_pst<<<nb, kBlock, 0, st>>>(c, P);
                 k_finish<<<nb, kBlock, 0, st>>>(c, P, 1);
             }
@@ -636,10 +632,11 @@ __global__ void k_pairs_export(Cst c, Ptr P, const unsigned int* dbits, const in
         ++cnt;
     };
     auto emit3 = [&](int j, int mir, float4) { emit(j, mir); };
+    auto emit5 = [&](int j, int mir, float4, F3, float) { emit(j, mir); };
     if (kShift == 2) {
         for_each_neighbour(c, P, i, emit);
     } else if (kShift == 1) {
-        for_each_pst_neighbour(c, P, i, xi, emit3);
+        for_each_pst_neighbour(c, P, i, xi, emit5);
     } else if (!(isnan(xi.x) || isnan(xi.y) || isnan(xi.z))) {
         stale_search(c, P, i, xi, cell_of(xi.x, c.h), cell_of(xi.y, c.h), cell_of(xi.z, c.h),
                      __uint_as_float(*dbits), emit3);
@@ -661,7 +658,6 @@ int export_pairs(SphHandle* h, int32_t* pi, int32_t* pj, int32_t* mir, int64_t c
     std::vector<int> cnt(n);
     cudaMemsetAsync(dbits, 0, sizeof(unsigned int), st);
     k_disp_since_build<<<blocks_for(n), kBlock, 0, st>>>(h->c, P, dbits);
-    if (kShift == 1) k_crossed<<<blocks_for(n), kBlock, 0, st>>>(h->c, P);
     k_pairs_export<kShift><<<blocks_for(n), kBlock, 0, st>>>(h->c, P, dbits, nullptr, dcnt, nullptr, nullptr,
                                                              nullptr);
     cudaMemcpyAsync(cnt.data(), dcnt, n * sizeof(int), cudaMemcpyDeviceToHost, st);

@@ -26,7 +26,7 @@ constexpr int kBlock = 256;          // threads per block of the particle-parall
 // registers and stay at 4; the solid sweeps slow down at 4).  A build may override one
 // with -DSPH_OCC_<PASS>=n to time another.
 #ifndef SPH_OCC_LAM
-#define SPH_OCC_LAM 6
+#define SPH_OCC_LAM 7
 #endif
 #ifndef SPH_OCC_LAMGRAD
 #define SPH_OCC_LAMGRAD 4
@@ -156,6 +156,8 @@ struct Ptr {
     float4* div;
     float* gradv;
     float4* aux;
+    float4* gsym;        // [n][2] solid: the symmetric part of grad v (S00 S11 S22 S01 | S02 S12)
+                         // with the pressure p and the bulk viscosity q in the last two words
     // scratch
     int4* cell;          // coarse cell at the last build, current order: x, y, z, bucket
                          // (w = -1 off-grid)
@@ -172,7 +174,6 @@ struct Ptr {
     GridLayout* layout;
     int* nbr;            // [K][n] this step's neighbours, k-major
     int* nbr_cnt;        // [n] true count; entries past K sit in the overflow pool
-    unsigned* xbits;     // [n / 32] bit per particle: its cell changed since the step's start
     int* ovf;            // [ovf_cap] overflow pool, one run per overflowing particle
     int* ovf_off;        // [n] start of the particle's run
     int* vl;             // [Kv][n] candidates within h + skin at the last build, k-major

@@ -242,16 +242,20 @@ __global__ void SPH_BOUNDS(SPH_OCC_FORCE) k_force(Cst c, Ptr P) {
             if (mir) { xj = mirror3(mir, xj); vj = mirror3(mir, vj); }
             F3 r = xi - xj;
             float rn;
-            F3 g = wendland_dW2(r, dot3(r, r), rn, c);
+            const float rn2 = dot3(r, r);
+            F3 g = wendland_dW2(r, rn2, rn, c);
             float w_j = w_of(pj, c);
             // -w_i w_j (p_i + p_j) grad W / mw_i
             a += (-wi_mw * w_j * (p_i + p_j)) * g;
             const F3 vij = vi - vj;
             float vxy = dot3(vij, r);
-            F3 fv = __fdividef(c.visc_coef * w_j * vxy, rn * rn + c.eta2) * g;
+            F3 fv = __fdividef(c.visc_coef * w_j * vxy, rn2 + c.eta2) * g;
             a += fv;
             dvisc += dot3(vi, fv);
-            float rho_j = vj4.w / pj.w;   // exact: rho_j - rho_i is a small difference
+            // rho_j to within 2 ulp: enough for the ALE term; the dt pair test, which takes
+            // the difference rho_i - rho_j, forms the exact quotient whenever the rounded one
+            // is within 1% of its threshold (2 ulp of rho_j is 2.4e-7 rho_j << 1e-2 eps_rho)
+            const float rho_j = __fdividef(vj4.w, pj.w);
             if (ale) {
                 // the ALE momentum term w_j [div(rho v du) - v_i div(rho du)] / rho_i
                 // (DSPH.py:1630-1640), whose rho_i du_i parts cancel:
@@ -260,8 +264,8 @@ __global__ void SPH_BOUNDS(SPH_OCC_FORCE) k_force(Cst c, Ptr P) {
                 if (mir) du_j = mirror3(mir, du_j);
                 a += (-(w_j * inv_rho_i) * (rho_j * dot3(du_j, g))) * vij;
             }
-            if (c.p.dt_pair_mode != 0) {
-                float drho = fabsf(rho_i - rho_j);
+            if (c.p.dt_pair_mode != 0 && fabsf(rho_i - rho_j) > eps_rho * (1.0f - 1e-2f)) {
+                float drho = fabsf(rho_i - vj4.w / pj.w);   // exact, as the reference's test
                 if (drho > eps_rho) {
                     // the quotient only where it can beat the running maximum: the product
                     // rounds within 1e-6 of cl drho, so the pre-test never drops a larger one
@@ -367,8 +371,8 @@ __global__ void __launch_bounds__(kBlock) k_advect(Cst c, Ptr P) {
 // the bins of this step's start (particle_system.py:1377-1411).  While the particles'
 // displacement since the lists' build -- at the step's start plus this step's advect and
 // grips -- is within the bound, from the candidate lists: every entry tested for
-// distance at the live positions, the edge entries also for j's step-start cell (its
-// current cell unless its bit in xbits says it moved) against i's live cell.  Of the
+// distance at the live positions, the edge entries also for j's step-start cell (fcell,
+// written by k_cells) against i's live cell.  Of the
 // edge candidates, only those accepted at the step's start and the near ones need
 // reading when the step moved particles less than half the near margin.  Otherwise
 // (or when the candidate list overflowed) the stale-bin search.  f(j, mirror, pos_j).
@@ -380,7 +384,11 @@ __device__ __forceinline__ void for_each_pst_neighbour(const Cst& c, const Ptr& 
     const int lx = cell_of(xi.x, c.h), ly = cell_of(xi.y, c.h), lz = cell_of(xi.z, c.h);
     const int vc = __ldg(P.vl_cnt + i);
     if (!(dtot <= c.dlim) || vl_overflow(c, vc)) {
-        stale_search(c, P, i, xi, lx, ly, lz, dtot, f);
+        stale_search(c, P, i, xi, lx, ly, lz, dtot, [&](int j, int mir, float4 pj) {
+            F3 xj = f3(pj);
+            if (mir) xj = mirror3(mir, xj);
+            f(j, mir, pj, xj, dist2_rn(xi, xj));
+        });
         return;
     }
     const float4* __restrict__ pos = as4c(P.cur.pos);
@@ -405,21 +413,41 @@ __device__ __forceinline__ void for_each_pst_neighbour(const Cst& c, const Ptr& 
         const float4 pj = __ldg(pos + j);
         F3 xj = f3(pj);
         if (mir) xj = mirror3(mir, xj);
-        if (!(dist2_rn(xi, xj) < c.d2_lt)) return;
+        const float d2 = dist2_rn(xi, xj);
+        if (!(d2 < c.d2_lt)) return;
         if (k >= d) {
-            int jx, jy, jz;
-            if ((__ldg(P.xbits + (j >> 5)) >> (j & 31)) & 1u) {
-                const int4 fj = __ldg(P.fcell + j);
-                jx = fj.x; jy = fj.y; jz = fj.z;
-            } else {
-                jx = cell_of_fast(pj.x, c.h, c.inv_h);
-                jy = cell_of_fast(pj.y, c.h, c.inv_h);
-                jz = cell_of_fast(pj.z, c.h, c.inv_h);
-            }
-            if (!sweep_cell_ok(mir, jx, jy, jz, lx, ly, lz)) return;
+            // j's cell of size h at this step's start (k_cells)
+            const int4 fj = __ldg(P.fcell + j);
+            if (!sweep_cell_ok(mir, fj.x, fj.y, fj.z, lx, ly, lz)) return;
         }
-        f(j, mir, pj);
+        f(j, mir, pj, xj, d2);
     });
+}
+
+// The disorder sum's pair term from the shift pass's own test: the mirrored position xj and
+// the squared separation d2 the neighbour test formed.  Arithmetic of pst_pair_term below.
+__device__ __forceinline__ F3 pst_term_d2(const Cst& c, const float4* __restrict__ vel, F3 xi, float rho_i,
+                                          float inv_Wd, int j, float4 pj, F3 xj, float d2, bool m_uni,
+                                          float m_u) {
+    const F3 r = xi - xj;
+    float Wij;
+    const F3 g = wendland_W_dW2(r, d2, Wij, c);
+    float f = 0.0f;
+    if (c.W_dx0 > 1e-10f) f = c.p.pst_R * ipow_or_pow(Wij * inv_Wd, c.p.pst_n);
+    if (c.p.pst_colle) {
+        const float Vj = w_of(pj, c);
+        if (Vj > 1e-30f) return ((1.0f + f) * Vj) * g;
+    } else {
+        const float mj_raw = m_uni ? m_u : __ldg(&vel[j].w);
+        const float mj = mw_of(mj_raw, pj, c);
+        if (mj > 1e-10f) {
+            // m_j / mean rho: a sum of densities, rounded quotients suffice (no cancellation)
+            const float rho_j = __fdividef(mj_raw, pj.w);
+            const float ra = 0.5f * (rho_i + rho_j);
+            if (ra > 1e-10f) return ((1.0f + f) * __fdividef(mj, ra)) * g;
+        }
+    }
+    return {0.0f, 0.0f, 0.0f};
 }
 
 // The disorder sum's pair term (pst_pair, DSPH.py:725-769): (1 + R (W / W(dx0))^n) grad W,
@@ -498,8 +526,8 @@ __global__ void SPH_BOUNDS(SPH_OCC_PST) k_pst(Cst c, Ptr P) {
         const unsigned int mlo = P.ac->m_min_bits;
         const bool m_uni = !c.p.pst_colle && mlo == P.ac->m_max_bits;
         const float m_u = __uint_as_float(mlo);
-        for_each_pst_neighbour(c, P, i, xi, [&](int j, int mir, float4 pj) {
-            sr += pst_pair_term(c, vel, xi, rho_i, inv_Wd, j, mir, pj, m_uni, m_u);
+        for_each_pst_neighbour(c, P, i, xi, [&](int j, int, float4 pj, F3 xj, float d2) {
+            sr += pst_term_d2(c, vel, xi, rho_i, inv_Wd, j, pj, xj, d2, m_uni, m_u);
         });
     }
     float4 vi4 = vel[i];

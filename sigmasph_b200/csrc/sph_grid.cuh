@@ -652,20 +652,5 @@ __device__ __forceinline__ void for_each_neighbour(const Cst& c, const Ptr& P, i
     if (cnt > c.K) list_pairs(P.ovf + __ldg(P.ovf_off + i), 1, cnt - c.K, f);
 }
 
-// One bit per particle: its cell of size h changed since this step's start (the shift
-// pass needs a moved particle's step-start cell; the others' is their current cell).
-// NaN positions count as moved.
-__global__ void __launch_bounds__(kBlock) k_crossed(Cst c, Ptr P) {
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    bool x = false;
-    if (i < c.n) {
-        const float4 p = reinterpret_cast<const float4*>(P.cur.pos)[i];
-        const int4 f = P.fcell[i];
-        x = isnan(p.x) || isnan(p.y) || isnan(p.z) || cell_of_fast(p.x, c.h, c.inv_h) != f.x ||
-            cell_of_fast(p.y, c.h, c.inv_h) != f.y || cell_of_fast(p.z, c.h, c.inv_h) != f.z;
-    }
-    const unsigned b = __ballot_sync(0xffffffffu, x);
-    if ((threadIdx.x & 31) == 0 && i < c.n) P.xbits[i >> 5] = b;
-}
 
 }  // namespace sph

@@ -55,15 +55,17 @@ struct SolidScratch {
     SphMatRow* mat = nullptr;
     SphInstRow* irow = nullptr;
     SphInstState* inst = nullptr;
+    float4* gsym = nullptr;          // [n][2] symmetric grad v, p, q (the damper's pair record)
     int n_inst = 0;
     bool any_plastic = false, all_gamma_one = true, any_jc = false;
 };
 constexpr int kMaxInstances = 1024;
 
 inline void solid_fill_constants(Cst&) {}
-inline int solid_alloc(SolidScratch& s, const SphParams& p, int64_t) {
+inline int solid_alloc(SolidScratch& s, const SphParams& p, int64_t n) {
     if (!p.is_solid) return SPH_OK;
     if (cudaMalloc(&s.stats, 4 * sizeof(unsigned long long)) != cudaSuccess ||
+        cudaMalloc(&s.gsym, (size_t)(n > 0 ? n : 1) * 2 * sizeof(float4)) != cudaSuccess ||
         cudaMalloc(&s.mat, kMaxInstances * sizeof(SphMatRow)) != cudaSuccess ||
         cudaMalloc(&s.irow, kMaxInstances * sizeof(SphInstRow)) != cudaSuccess ||
         cudaMalloc(&s.inst, kMaxInstances * sizeof(SphInstState)) != cudaSuccess)
@@ -135,7 +137,7 @@ inline int solid_jc_alloc(SolidScratch& s, int64_t n) {
 }
 inline void solid_free(SolidScratch& s) {
     void* ps[] = {s.q_count, s.q_idx, s.q_feat, s.q_pred, s.W, s.packed, s.stats, s.mlp_err,
-                  s.mat, s.irow, s.inst};
+                  s.mat, s.irow, s.inst, s.gsym};
     for (void* q : ps) if (q) cudaFree(q);
     s = SolidScratch();
 }
@@ -295,18 +297,36 @@ __device__ __forceinline__ void grad_v_finish(const Cst& c, const Ptr& P, int i,
     reinterpret_cast<float4*>(g)[0] = make_float4(G[0][0], G[0][1], G[0][2], G[1][0]);
     reinterpret_cast<float4*>(g)[1] = make_float4(G[1][1], G[1][2], G[2][0], G[2][1]);
     reinterpret_cast<float4*>(g)[2] = make_float4(G[2][2], 0.0f, 0.0f, 0.0f);
+    // the damper's pair term reads only r^T (G_i + G_j) r, i.e. the symmetric parts (the
+    // record's last two words, p and q, are k_solid_commit's)
+    P.gsym[2 * i] = make_float4(G[0][0], G[1][1], G[2][2], 0.5f * (G[0][1] + G[1][0]));
+    reinterpret_cast<float2*>(P.gsym + 2 * i + 1)[0] =
+        make_float2(0.5f * (G[0][2] + G[2][0]), 0.5f * (G[1][2] + G[2][1]));
+}
+struct SymG { float xx, yy, zz, xy, xz, yz; };
+// r^T S r for a symmetric S.
+__device__ __forceinline__ float quad_sym(const SymG& S, F3 r) {
+    return r.x * (S.xx * r.x + 2.0f * (S.xy * r.y + S.xz * r.z)) + r.y * (S.yy * r.y + 2.0f * S.yz * r.z) +
+           S.zz * (r.z * r.z);
+}
+// Particle j's symmetric grad v (and p, q in the last two words) as a mirror image: M S M
+// with M = diag(1, sy, sz) flips S_xy by sy, S_xz by sz, S_yz by sy sz.
+__device__ __forceinline__ SymG load_gsym(const Ptr& P, int j, int mir, float& pj, float& qj) {
+    const float4 a = __ldg(P.gsym + 2 * j), b = __ldg(P.gsym + 2 * j + 1);
+    pj = b.z;
+    qj = b.w;
+    SymG S = {a.x, a.y, a.z, a.w, b.x, b.y};
+    if (mir) {
+        const float sy = (mir & 1) ? -1.0f : 1.0f, sz = (mir & 2) ? -1.0f : 1.0f;
+        S.xy *= sy; S.xz *= sz; S.yz *= sy * sz;
+    }
+    return S;
+}
+__device__ __forceinline__ SymG own_gsym(const Ptr& P, int i) {
+    const float4 a = P.gsym[2 * i], b = P.gsym[2 * i + 1];
+    return {a.x, a.y, a.z, a.w, b.x, b.y};
 }
 struct NoExtra {};
-// The record's three words after the 3x3, written by k_solid_commit: the pressure, the
-// bulk viscosity q and the signal speed of q's own CFL limit.
-__device__ __forceinline__ float2 load_gradv_p(const Ptr& P, int j, float G[3][3]) {
-    const float4* g = reinterpret_cast<const float4*>(P.gradv + 12 * j);
-    float4 a = __ldg(g), b = __ldg(g + 1), d = __ldg(g + 2);
-    G[0][0] = a.x; G[0][1] = a.y; G[0][2] = a.z; G[1][0] = a.w;
-    G[1][1] = b.x; G[1][2] = b.y; G[2][0] = b.z; G[2][1] = b.w; G[2][2] = d.x;
-    return make_float2(d.y, d.z);
-}
-
 __device__ __forceinline__ void load_gradv(const Ptr& P, int j, float G[3][3]) {
     const float4* g = reinterpret_cast<const float4*>(P.gradv + 12 * j);
     float4 a = __ldg(g), b = __ldg(g + 1), d = __ldg(g + 2);
@@ -314,13 +334,6 @@ __device__ __forceinline__ void load_gradv(const Ptr& P, int j, float G[3][3]) {
     G[1][1] = b.x; G[1][2] = b.y; G[2][0] = b.z; G[2][1] = b.w; G[2][2] = d.x;
 }
 
-__device__ __forceinline__ void mirror_mat3(int code, float G[3][3]) {
-    float s[3] = {1.0f, (code & 1) ? -1.0f : 1.0f, (code & 2) ? -1.0f : 1.0f};
-#pragma unroll
-    for (int a = 0; a < 3; ++a)
-#pragma unroll
-        for (int b = 0; b < 3; ++b) G[a][b] *= s[a] * s[b];
-}
 
 // ------------------------------------------------------------------ kernel-correction inverse
 // The regularised inverse of E at the consumer's tolerance (spd_inverse.py:86-101), formed
@@ -920,9 +933,11 @@ __global__ void __launch_bounds__(kBlock) k_solid_commit(Cst c, Ptr P) {
     const float rho = m / V;
     const float p = solid_pressure(c, P, k, rho);
     P.cur.disp[4 * i + 3] = p;
-    // the spare words of the velocity-gradient record carry p (and q) to the neighbours'
-    // force pass, which reads that record of every neighbour for the in-loop damper anyway
+    // the spare words of the symmetric velocity-gradient record carry p (and q) to the
+    // neighbours' force pass, which reads that record of every neighbour for the in-loop
+    // damper anyway
     P.gradv[12 * i + 9] = p;
+    float q_i = 0.0f;
     if (c.p.q_l2 > 0.0f) {
         // SOLID.py:3393-3401 and :3939-3975: q = C_Q l^2 rho (tr grad v)^2 under
         // compression, and the signal speed Q + sqrt(Q^2 + c^2), Q = C_Q l |tr grad v|
@@ -935,7 +950,9 @@ __global__ void __launch_bounds__(kBlock) k_solid_commit(Cst c, Ptr P) {
             ce = qc + sqrtf(qc * qc + ci * ci);
         }
         reinterpret_cast<float2*>(P.gradv + 12 * i + 10)[0] = make_float2(q, ce);
+        q_i = q;
     }
+    reinterpret_cast<float2*>(P.gsym + 2 * i + 1)[1] = make_float2(p, q_i);
     // gravity; de_int restarts for this step's force pass
     P.acc[i] = make_float4(c.p.gravity[0], c.p.gravity[1], c.p.gravity[2], 0.0f);
 }
@@ -978,8 +995,8 @@ __global__ void SPH_BOUNDS(SPH_OCC_SOLID_FORCE) k_solid_force(Cst c, Ptr P) {
         const bool axc = kAxi && c.p.axi_conservative_x;
         const bool axr = kAxi && c.p.axi_conservative_r;
         const float ri = r_axi_of(pi.y, c), inv_ri = 1.0f / ri;
-        float Gi[3][3];
-        if (hg_inloop) load_gradv(P, i, Gi);
+        SymG Si = {0, 0, 0, 0, 0, 0};
+        if (hg_inloop) Si = own_gsym(P, i);
         const float hg_pre = c.p.hourglass_alpha * (P.mat[ki].rho0 * inv_rho_i) * (P.mat[ki].cp * c.inv_h)
                              / (c.p.V0 * (float)c.p.hg_W_dx0);
         const float visc = visc_at(c, P, ki);
@@ -1007,19 +1024,18 @@ __global__ void SPH_BOUNDS(SPH_OCC_SOLID_FORCE) k_solid_force(Cst c, Ptr P) {
             // pressure (k_solid_commit), and is dead once this term is summed
             float p_j, q_j = 0.0f;
             if (hg_inloop) {
-                float Gj[3][3];
-                const float2 pq = load_gradv_p(P, j, Gj);
-                p_j = pq.x;
-                if (q_on) q_j = pq.y;
+                float qq;
+                const SymG Sj = load_gsym(P, j, mir, p_j, qq);
+                if (q_on) q_j = qq;
                 if (rn > 1e-9f) {
                     float inv_rn = rsqrtf(rn2);
                     F3 rh = {-r.x * inv_rn, -r.y * inv_rn, -r.z * inv_rn};
-                    if (mir) mirror_mat3(mir, Gj);
-                    F3 mr = -r;
-                    F3 dvh = {(vj.x - vi.x) - 0.5f * ((Gi[0][0] + Gj[0][0]) * mr.x + (Gi[0][1] + Gj[0][1]) * mr.y + (Gi[0][2] + Gj[0][2]) * mr.z),
-                              (vj.y - vi.y) - 0.5f * ((Gi[1][0] + Gj[1][0]) * mr.x + (Gi[1][1] + Gj[1][1]) * mr.y + (Gi[1][2] + Gj[1][2]) * mr.z),
-                              (vj.z - vi.z) - 0.5f * ((Gi[2][0] + Gj[2][0]) * mr.x + (Gi[2][1] + Gj[2][1]) * mr.y + (Gi[2][2] + Gj[2][2]) * mr.z)};
-                    float hg = dot3(dvh, rh);
+                    // hg = [(v_j - v_i) - <G> (x_j - x_i)] . rhat with x_j - x_i = |r| rhat:
+                    // (v_j - v_i) . rhat - |r| rhat^T <S> rhat, <S> the mean symmetric part
+                    // (the antisymmetric part of <G> drops out of the quadratic form)
+                    const SymG Ss = {Si.xx + Sj.xx, Si.yy + Sj.yy, Si.zz + Sj.zz, Si.xy + Sj.xy,
+                                     Si.xz + Sj.xz, Si.yz + Sj.yz};
+                    float hg = dot3(vj - vi, rh) - 0.5f * rn * quad_sym(Ss, rh);
                     float damp = hg_pre * w_j * wendland_W(rn, c) * hg;
                     if (c.p.hg_mixed_impedance) damp *= hg_impedance_ratio(P, ki, j);
                     F3 ah = damp * rh;
@@ -1029,9 +1045,9 @@ __global__ void SPH_BOUNDS(SPH_OCC_SOLID_FORCE) k_solid_force(Cst c, Ptr P) {
                     dhg += -0.5f * dot3(ah, vij);
                 }
             } else if (q_on) {
-                const float4 r8 = __ldg(reinterpret_cast<const float4*>(P.gradv + 12 * j) + 2);
-                p_j = r8.y;
-                q_j = r8.z;
+                const float4 r8 = __ldg(P.gsym + 2 * j + 1);
+                p_j = r8.z;
+                q_j = r8.w;
             } else {
                 p_j = __ldg(&dsp[j].w);
             }
@@ -1262,8 +1278,7 @@ __global__ void __launch_bounds__(kBlock) k_hg_stage(Cst c, Ptr P, int stage) {
     F3 xi = f3(pi);
     F3 yi = y_load(P, i, rb);
     const float rho_i = __ldg(&vel[i].w) / pi.w;
-    float Gi[3][3];
-    load_gradv(P, i, Gi);
+    const SymG Si = own_gsym(P, i);
     const bool axc = c.p.axisymmetric && c.p.axi_conservative_x;
     const bool axr = c.p.axisymmetric && c.p.axi_conservative_r;
     const float ri = r_axi_of(pi.y, c), inv_ri = 1.0f / ri;
@@ -1274,20 +1289,18 @@ __global__ void __launch_bounds__(kBlock) k_hg_stage(Cst c, Ptr P, int stage) {
         float4 pj = __ldg(pos + j);
         F3 xj = f3(pj);
         F3 yj = y_load(P, j, rb);
-        float Gj[3][3];
-        load_gradv(P, j, Gj);
-        if (mir) { xj = mirror3(mir, xj); yj = mirror3(mir, yj); mirror_mat3(mir, Gj); }
+        float pj_unused, qj_unused;
+        const SymG Sj = load_gsym(P, j, mir, pj_unused, qj_unused);
+        if (mir) { xj = mirror3(mir, xj); yj = mirror3(mir, yj); }
         F3 r = xi - xj;
         float rn2 = dot3(r, r);
         float rn = rn2 > 0.0f ? rn2 * rsqrtf(rn2) : 0.0f;
         if (!(rn > 1e-9f)) return;
         float inv_rn = 1.0f / rn;
         F3 rh = {-r.x * inv_rn, -r.y * inv_rn, -r.z * inv_rn};
-        F3 mr = -r;
-        F3 dvh = {(yj.x - yi.x) - 0.5f * ((Gi[0][0] + Gj[0][0]) * mr.x + (Gi[0][1] + Gj[0][1]) * mr.y + (Gi[0][2] + Gj[0][2]) * mr.z),
-                  (yj.y - yi.y) - 0.5f * ((Gi[1][0] + Gj[1][0]) * mr.x + (Gi[1][1] + Gj[1][1]) * mr.y + (Gi[1][2] + Gj[1][2]) * mr.z),
-                  (yj.z - yi.z) - 0.5f * ((Gi[2][0] + Gj[2][0]) * mr.x + (Gi[2][1] + Gj[2][1]) * mr.y + (Gi[2][2] + Gj[2][2]) * mr.z)};
-        float hg = dot3(dvh, rh);
+        // as the in-loop damper: (y_j - y_i) . rhat - |r| rhat^T <S> rhat
+        const SymG Ss = {Si.xx + Sj.xx, Si.yy + Sj.yy, Si.zz + Sj.zz, Si.xy + Sj.xy, Si.xz + Sj.xz, Si.yz + Sj.yz};
+        float hg = dot3(yj - yi, rh) - 0.5f * rn * quad_sym(Ss, rh);
         float damp = hg_pre * w_of(pj, c) * wendland_W(rn, c) * hg;
         if (c.p.hg_mixed_impedance) damp *= hg_impedance_ratio(P, ki, j);
         F3 ah = damp * rh;
@@ -1574,7 +1587,6 @@ inline int solid_substep_launch(const Cst& c, const Ptr& P, int n, cudaStream_t 
         k_constraints<<<nb, bs, 0, st>>>(c, P); mark("k_constraints");
     }
     if (in(SPH_STAGE_PST) && c.p.pst_enabled) {
-        k_crossed<<<nb, bs, 0, st>>>(c, P); mark("k_crossed");
         k_pst<<<nb, bs, 0, st>>>(c, P); mark("k_pst");
         k_finish<<<nb, bs, 0, st>>>(c, P, last_stage >= SPH_STAGE_BOUNDARY ? 3 : 1); mark("k_finish");
     } else if (in(SPH_STAGE_BOUNDARY)) {
