@@ -218,7 +218,9 @@ def cpu_baseline(ps, steps_target_s=15.0, max_steps=6, threads=None):
             "kind": "port",
             "sample": f"{k} step(s) of the full {ps.particle_max_num}-particle workload after 1 "
                       f"warm-up step, CPU restatement of the reference kernels (float32, "
-                      f"OpenMP, {nt} threads); the reference's own Taichi run is not installable"}
+                      f"OpenMP, {nt} threads, every per-particle loop parallel: grid ids, sort and "
+                      f"permutation, pair sweeps, advect, walls and reductions); the reference's "
+                      f"own Taichi run is not installable"}
 
 
 def run_reference(args):
@@ -257,7 +259,8 @@ def run_reference(args):
                              "sample": f"the full {n}-particle workload, 1 warm-up + {k} timed "
                                        f"step(s) (of the {args.steps} asked, bounded to ~90 s); "
                                        "CPU restatement of the reference kernels, float32, "
-                                       "OpenMP (the reference's Taichi is not installable here)"},
+                                       "OpenMP with every per-particle loop parallel, sort "
+                                       "included (the reference's Taichi is not installable here)"},
             "e2e": {"value": val, "unit": UNIT, "h2d_bytes_per_step": 0,
                     "d2h_bytes_per_step": 0}}
     print(json.dumps(line))

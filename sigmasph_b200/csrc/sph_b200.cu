@@ -182,7 +182,7 @@ int rebuild(SphHandle* h, cudaStream_t st) {
     LAUNCH("k_gather", k_gather<<<nb, kBlock, 0, st>>>(c, P));
     LAUNCH("k_gather_back", k_gather_back<<<nb, kBlock, 0, st>>>(c, P));
     LAUNCH("k_vlist_build", k_vlist_build<<<nb, kBlock, 0, st>>>(c, P));
-    LAUNCH("k_nbr_filter", k_nbr_filter<<<nb, kBlock, 0, st>>>(c, P));
+    LAUNCH("k_nbr_filter", SHAPED(plain_shape(c), k_nbr_filter, <<<nb, kBlock, 0, st>>>(c, P)));
     return SPH_OK;
 }
 
@@ -190,14 +190,15 @@ int fluid_substep_and_boundary(SphHandle* h, cudaStream_t st) {
     const int nb = blocks_for(h->n);
     const Cst& c = h->c;
     Ptr P = make_ptr(h);
-    LAUNCH("k_lam", k_lam<<<nb, kBlock, 0, st>>>(c, P));
-    LAUNCH("k_lamgrad_cont", k_lamgrad_cont<<<nb, kBlock, 0, st>>>(c, P));
+    const bool plain = plain_shape(c);
+    LAUNCH("k_lam", SHAPED(plain, k_lam, <<<nb, kBlock, 0, st>>>(c, P)));
+    LAUNCH("k_lamgrad_cont", SHAPED(plain, k_lamgrad_cont, <<<nb, kBlock, 0, st>>>(c, P)));
     LAUNCH("k_eos", k_eos<<<nb, kBlock, 0, st>>>(c, P));
-    LAUNCH("k_force", k_force<<<nb, kBlock, 0, st>>>(c, P));
+    LAUNCH("k_force", SHAPED(plain, k_force, <<<nb, kBlock, 0, st>>>(c, P)));
     LAUNCH("k_dt", k_dt<<<1, 32, 0, st>>>(c, P));
     LAUNCH("k_advect", k_advect<<<nb, kBlock, 0, st>>>(c, P));
     if (h->p.pst_enabled) {
-        LAUNCH("k_pst", k_pst<<<nb, kBlock, 0, st>>>(c, P));
+        LAUNCH("k_pst", SHAPED(plain, k_pst, <<<nb, kBlock, 0, st>>>(c, P)));
         LAUNCH("k_finish", k_finish<<<nb, kBlock, 0, st>>>(c, P, 3));
     } else {
         LAUNCH("k_finish", k_finish<<<nb, kBlock, 0, st>>>(c, P, 2));
@@ -517,16 +518,16 @@ int sph_run_stage(SphHandle* h, int stage, void* stream) {
     switch (stage) {
         case SPH_STAGE_SORT: { int r = rebuild(h, st); if (r) return r; break; }
         case SPH_STAGE_LAM:
-            k_lam<<<nb, kBlock, 0, st>>>(c, P);
-            k_lamgrad_cont<<<nb, kBlock, 0, st>>>(c, P);
+            SHAPED(plain_shape(c), k_lam, <<<nb, kBlock, 0, st>>>(c, P));
+            SHAPED(plain_shape(c), k_lamgrad_cont, <<<nb, kBlock, 0, st>>>(c, P));
             break;
         case SPH_STAGE_CONTINUITY: k_eos<<<nb, kBlock, 0, st>>>(c, P); break;
-        case SPH_STAGE_FORCES: k_force<<<nb, kBlock, 0, st>>>(c, P); break;
+        case SPH_STAGE_FORCES: SHAPED(plain_shape(c), k_force, <<<nb, kBlock, 0, st>>>(c, P)); break;
         case SPH_STAGE_DT: k_dt<<<1, 32, 0, st>>>(c, P); break;
         case SPH_STAGE_ADVECT: k_advect<<<nb, kBlock, 0, st>>>(c, P); break;
         case SPH_STAGE_PST:
             if (h->p.pst_enabled) {
-                k_pst<<<nb, kBlock, 0, st>>>(c, P);
+                SHAPED(plain_shape(c), k_pst, <<<nb, kBlock, 0, st>>>(c, P));
                 k_finish<<<nb, kBlock, 0, st>>>(c, P, 1);
             }
             break;
@@ -636,7 +637,7 @@ __global__ void k_pairs_export(Cst c, Ptr P, const unsigned int* dbits, const in
     if (kShift == 2) {
         for_each_neighbour(c, P, i, emit);
     } else if (kShift == 1) {
-        for_each_pst_neighbour(c, P, i, xi, emit5);
+        for_each_pst_neighbour<false>(c, P, i, xi, emit5);
     } else if (!(isnan(xi.x) || isnan(xi.y) || isnan(xi.z))) {
         stale_search(c, P, i, xi, cell_of(xi.x, c.h), cell_of(xi.y, c.h), cell_of(xi.z, c.h),
                      __uint_as_float(*dbits), emit3);
@@ -742,7 +743,7 @@ extern "C" int sph_relax_pass(SphHandle* h, float beta, float* residual, float* 
     if (int r = rebuild(h, st)) return r;
     Ptr P = make_ptr(h);
     const Cst& c = h->c;
-    k_lam<<<nb, kBlock, 0, st>>>(c, P);
+    k_lam<false><<<nb, kBlock, 0, st>>>(c, P);
     if (!h->p.pst_normal_eigvec) k_relax_lamgrad<<<nb, kBlock, 0, st>>>(c, P);
     CK(cudaMemsetAsync(&h->ac->relax_max_bits, 0, sizeof(unsigned int), st));
     k_relax<<<nb, kBlock, 0, st>>>(c, P, beta, residual_each);

@@ -32,7 +32,7 @@ constexpr int kBlock = 256;          // threads per block of the particle-parall
 #define SPH_OCC_LAMGRAD 4
 #endif
 #ifndef SPH_OCC_FORCE
-#define SPH_OCC_FORCE 4
+#define SPH_OCC_FORCE 5
 #endif
 #ifndef SPH_OCC_PST
 #define SPH_OCC_PST 6
@@ -352,6 +352,31 @@ __device__ __forceinline__ float w_of(float4 pos, const Cst& c) {
 __device__ __forceinline__ float mw_of(float m, float4 pos, const Cst& c) {
     return c.p.axisymmetric ? m / fmaxf(pos.y, c.p.axi_r_min) : m;
 }
+
+// The deck's shape as the pair passes see it.  Shape<true> is a 3D deck with no mirror
+// plane and no axisymmetry (the dam break, the round bar): neighbour entries carry no
+// mirror code and the weights are the stored volumes, known when the pass is compiled.
+// Shape<false> reads those switches from the parameters.
+__host__ __device__ __forceinline__ bool plain_shape(const Cst& c) {
+    return !c.mirror_y && !c.mirror_z && !c.p.axisymmetric && !c.p.two_d;
+}
+template <bool kPlain>
+struct Shape {
+    __device__ static __forceinline__ bool two_d(const Cst& c) { return !kPlain && c.p.two_d; }
+    __device__ static __forceinline__ bool axi(const Cst& c) { return !kPlain && c.p.axisymmetric; }
+    __device__ static __forceinline__ float w(float4 pos, const Cst& c) { return kPlain ? pos.w : w_of(pos, c); }
+    __device__ static __forceinline__ float mw(float m, float4 pos, const Cst& c) {
+        return kPlain ? m : mw_of(m, pos, c);
+    }
+    __device__ static __forceinline__ int idx(int e) { return kPlain ? e : (e & kIdxMask); }
+    __device__ static __forceinline__ int mir(int e) { return kPlain ? 0 : (int)((unsigned)e >> kMirShift); }
+};
+// Launches the instance of a shape-templated pass for the deck.
+#define SHAPED(plain, kernel, ...)            \
+    do {                                      \
+        if (plain) kernel<true> __VA_ARGS__;  \
+        else kernel<false> __VA_ARGS__;       \
+    } while (0)
 
 // One particle's terms of every FP64 reduction.
 __device__ __forceinline__ void reduce_terms(const Cst& c, float4 p, float4 v, float e_int,

@@ -16,6 +16,8 @@
 // post-EOS pressure the force pass reads and shares its sweep; the step-work reduction is
 // folded into advect; the displacement of the shift is folded into the boundary pass.
 #pragma once
+#include <type_traits>
+
 #include "sph_grid.cuh"
 
 namespace sph {
@@ -24,7 +26,9 @@ __device__ __forceinline__ float4* as4(float* p) { return reinterpret_cast<float
 __device__ __forceinline__ const float4* as4c(const float* p) { return reinterpret_cast<const float4*>(p); }
 
 // ------------------------------------------------------------------ compute_lam pass 1
+template <bool kPlain>
 __global__ void SPH_BOUNDS(SPH_OCC_LAM) k_lam(Cst c, Ptr P) {
+    using S = Shape<kPlain>;
     int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= c.n) return;
     const float4* __restrict__ pos = as4c(P.cur.pos);
@@ -38,16 +42,16 @@ __global__ void SPH_BOUNDS(SPH_OCC_LAM) k_lam(Cst c, Ptr P) {
         if (mir) xj = mirror3(mir, xj);
         const F3 r = xi - xj;
         const float f = wendland_dW_factor(dot3(r, r), c);
-        const F3 sr = (-(w_of(pj, c) * f)) * r;
+        const F3 sr = (-(S::w(pj, c) * f)) * r;
         e00 += sr.x * r.x; e01 += sr.x * r.y; e11 += sr.y * r.y;
-        if (!c.p.two_d) { e02 += sr.x * r.z; e12 += sr.y * r.z; e22 += sr.z * r.z; }
+        if (!S::two_d(c)) { e02 += sr.x * r.z; e12 += sr.y * r.z; e22 += sr.z * r.z; }
     };
-    for_each_neighbour(c, P, i, [&](int j, int mir) { pair(mir, __ldg(pos + j)); });
+    for_each_neighbour<kPlain>(c, P, i, [&](int j, int mir) { pair(mir, __ldg(pos + j)); });
     const float E[3][3] = {{e00, e01, e02}, {e01, e11, e12}, {e02, e12, e22}};
     const float tol = c.p.l_eig_tol_lam;
     float L00, L11, L22, L01, L02, L12, lam;
     float4 evec = make_float4(0.f, 0.f, 0.f, 0.f);
-    if (c.p.two_d) {
+    if (S::two_d(c)) {
         // eig_sym_2x2 (DSPH.py:35-47) on (E00, E01, E11) and spd_inverse_2x2 (spd_inverse.py:53-83)
         float a = E[0][0], b0 = E[0][1], dd = E[1][1];
         float det = sqrtf((a - dd) * (a - dd) + 4.0f * b0 * b0);
@@ -101,7 +105,9 @@ __global__ void SPH_BOUNDS(SPH_OCC_LAM) k_lam(Cst c, Ptr P) {
 }
 
 // ------------------------------------------------------------------ grad lambda + continuity
+template <bool kPlain>
 __global__ void SPH_BOUNDS(SPH_OCC_LAMGRAD) k_lamgrad_cont(Cst c, Ptr P) {
+    using S = Shape<kPlain>;
     int i = blockIdx.x * blockDim.x + threadIdx.x;
     double wdiff = 0.0;
     if (i < c.n) {
@@ -123,7 +129,7 @@ __global__ void SPH_BOUNDS(SPH_OCC_LAMGRAD) k_lamgrad_cont(Cst c, Ptr P) {
         F3 lg = {0, 0, 0};
         float r0 = 0.0f, r1 = 0.0f;
         // the next neighbour's position is requested while this pair is evaluated
-        for_each_neighbour_pos(c, P, i, pos, [&](int j, int mir, float4 pj) {
+        for_each_neighbour_pos<kPlain>(c, P, i, pos, [&](int j, int mir, float4 pj) {
             float4 vj4 = __ldg(vel + j);
             F3 xj = f3(pj), vj = f3(vj4);
             if (mir) { xj = mirror3(mir, xj); vj = mirror3(mir, vj); }
@@ -131,7 +137,7 @@ __global__ void SPH_BOUNDS(SPH_OCC_LAMGRAD) k_lamgrad_cont(Cst c, Ptr P) {
             float rn2 = dot3(r, r);
             float rn;
             F3 g = wendland_dW2(r, rn2, rn, c);
-            float Vj = w_of(pj, c);
+            float Vj = S::w(pj, c);
             const float4 sj = pst ? __ldg(shf + j) : make_float4(0.f, 0.f, 0.f, 0.f);
             if (need_lgrad) {
                 float ld = (pst ? sj.w : __ldg(lam + j)) - lam_i;
@@ -160,11 +166,11 @@ __global__ void SPH_BOUNDS(SPH_OCC_LAMGRAD) k_lamgrad_cont(Cst c, Ptr P) {
             }
         });
         if (need_lgrad) {
-            if (c.p.two_d) lg.z = 0.0f;
+            if (S::two_d(c)) lg.z = 0.0f;
             P.lgrad[i] = make_float4(lg.x, lg.y, lg.z, 0.0f);
         }
         float dv = r0;
-        if (c.p.axisymmetric) dv -= vi.y / fmaxf(pi.y, c.p.axi_r_min);
+        if (S::axi(c)) dv -= vi.y / fmaxf(pi.y, c.p.axi_r_min);
         P.div[i] = make_float4(dv, r1, 0.0f, 0.0f);
         wdiff = -(double)pi.w * (double)__ldg(P.cur.disp + 4 * i + 3) * (double)r1;
     }
@@ -212,7 +218,9 @@ __global__ void __launch_bounds__(kBlock) k_eos(Cst c, Ptr P) {
 }
 
 // ------------------------------------------------------------------ pressure + viscosity + dt pairs
+template <bool kPlain>
 __global__ void SPH_BOUNDS(SPH_OCC_FORCE) k_force(Cst c, Ptr P) {
+    using S = Shape<kPlain>;
     int i = blockIdx.x * blockDim.x + threadIdx.x;
     float amag = 0.0f, csq = 0.0f;
     if (i < c.n) {
@@ -224,8 +232,8 @@ __global__ void SPH_BOUNDS(SPH_OCC_FORCE) k_force(Cst c, Ptr P) {
         F3 xi = f3(pi), vi = f3(vi4);
         const float p_i = dsp[i].w;
         const float rho_i = vi4.w / pi.w;
-        const float w_i = w_of(pi, c);
-        const float mw_i = mw_of(vi4.w, pi, c);
+        const float w_i = S::w(pi, c);
+        const float mw_i = S::mw(vi4.w, pi, c);
         const float dt = P.sc->dt;
         const bool ale = c.p.pst_enabled && c.p.pst_ale_momentum;
         const float eps_rho = 1e-3f * c.p.density0;
@@ -234,7 +242,7 @@ __global__ void SPH_BOUNDS(SPH_OCC_FORCE) k_force(Cst c, Ptr P) {
         float cl = c.p.c_signal * c.p.c_signal;
         F3 a = {0, 0, 0};
         float dvisc = 0.0f;
-        for_each_neighbour_pos(c, P, i, pos, [&](int j, int mir, float4 pj) {
+        for_each_neighbour_pos<kPlain>(c, P, i, pos, [&](int j, int mir, float4 pj) {
             float4 vj4 = __ldg(vel + j);
             const float4 sj = ale ? __ldg(shf + j) : make_float4(0.f, 0.f, 0.f, 0.f);
             float p_j = ale ? sj.w : __ldg(&dsp[j].w);   // k_eos copies p to shift.w
@@ -244,7 +252,7 @@ __global__ void SPH_BOUNDS(SPH_OCC_FORCE) k_force(Cst c, Ptr P) {
             float rn;
             const float rn2 = dot3(r, r);
             F3 g = wendland_dW2(r, rn2, rn, c);
-            float w_j = w_of(pj, c);
+            float w_j = S::w(pj, c);
             // -w_i w_j (p_i + p_j) grad W / mw_i
             a += (-wi_mw * w_j * (p_i + p_j)) * g;
             const F3 vij = vi - vj;
@@ -376,8 +384,9 @@ __global__ void __launch_bounds__(kBlock) k_advect(Cst c, Ptr P) {
 // edge candidates, only those accepted at the step's start and the near ones need
 // reading when the step moved particles less than half the near margin.  Otherwise
 // (or when the candidate list overflowed) the stale-bin search.  f(j, mirror, pos_j).
-template <class F>
+template <bool kPlain, class F>
 __device__ __forceinline__ void for_each_pst_neighbour(const Cst& c, const Ptr& P, int i, F3 xi, F&& f) {
+    using S = Shape<kPlain>;
     if (isnan(xi.x) || isnan(xi.y) || isnan(xi.z)) return;
     const float dtot = __uint_as_float(P.ac->d_start_bits) + __uint_as_float(P.ac->max_disp_bits) +
                        __uint_as_float(P.ac->max_grip_disp_bits);
@@ -408,7 +417,7 @@ __device__ __forceinline__ void for_each_pst_neighbour(const Cst& c, const Ptr& 
     const int* __restrict__ lb = near ? P.nbr + (size_t)(c.K - b_cnt) * n + i : P.vl + i;
     split_entries(a_end + b_cnt, [&](int k) { return k < a_end ? __ldg(la + (size_t)k * n) : __ldg(lb + (size_t)(k - a_end) * n); },
                   [&](int k, int e) {
-        const int j = e & kIdxMask, mir = (int)((unsigned)e >> kMirShift);
+        const int j = S::idx(e), mir = S::mir(e);
         if (mir && (((mir & 1) && !py) || ((mir & 2) && !pz))) return;
         const float4 pj = __ldg(pos + j);
         F3 xj = f3(pj);
@@ -426,6 +435,10 @@ __device__ __forceinline__ void for_each_pst_neighbour(const Cst& c, const Ptr& 
 
 // The disorder sum's pair term from the shift pass's own test: the mirrored position xj and
 // the squared separation d2 the neighbour test formed.  Arithmetic of pst_pair_term below.
+// kForm 1 (Sun) and 2 (Colle) fix the deck's exponent n = 4 with W(dx0) > 0 when the pass
+// is compiled; kForm 0 reads the form, n and W(dx0) from the parameters.
+constexpr int kPstAny = 0, kPstSun4 = 1, kPstColle4 = 2;
+template <bool kPlain, int kForm>
 __device__ __forceinline__ F3 pst_term_d2(const Cst& c, const float4* __restrict__ vel, F3 xi, float rho_i,
                                           float inv_Wd, int j, float4 pj, F3 xj, float d2, bool m_uni,
                                           float m_u) {
@@ -433,13 +446,18 @@ __device__ __forceinline__ F3 pst_term_d2(const Cst& c, const float4* __restrict
     float Wij;
     const F3 g = wendland_W_dW2(r, d2, Wij, c);
     float f = 0.0f;
-    if (c.W_dx0 > 1e-10f) f = c.p.pst_R * ipow_or_pow(Wij * inv_Wd, c.p.pst_n);
-    if (c.p.pst_colle) {
-        const float Vj = w_of(pj, c);
+    if (kForm != kPstAny) {
+        const float x = Wij * inv_Wd;
+        f = c.p.pst_R * (((x * x) * x) * x);   // ipow_or_pow(x, 4)
+    } else if (c.W_dx0 > 1e-10f) {
+        f = c.p.pst_R * ipow_or_pow(Wij * inv_Wd, c.p.pst_n);
+    }
+    if (kForm == kPstColle4 || (kForm == kPstAny && c.p.pst_colle)) {
+        const float Vj = Shape<kPlain>::w(pj, c);
         if (Vj > 1e-30f) return ((1.0f + f) * Vj) * g;
     } else {
         const float mj_raw = m_uni ? m_u : __ldg(&vel[j].w);
-        const float mj = mw_of(mj_raw, pj, c);
+        const float mj = Shape<kPlain>::mw(mj_raw, pj, c);
         if (mj > 1e-10f) {
             // m_j / mean rho: a sum of densities, rounded quotients suffice (no cancellation)
             const float rho_j = __fdividef(mj_raw, pj.w);
@@ -505,6 +523,7 @@ __device__ __forceinline__ F3 pst_constrain(const Cst& c, const Ptr& P, int i, F
     return dr;
 }
 
+template <bool kPlain>
 __global__ void SPH_BOUNDS(SPH_OCC_PST) k_pst(Cst c, Ptr P) {
     int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i == 0) {   // steps whose shift could not use the candidate lists
@@ -526,9 +545,18 @@ __global__ void SPH_BOUNDS(SPH_OCC_PST) k_pst(Cst c, Ptr P) {
         const unsigned int mlo = P.ac->m_min_bits;
         const bool m_uni = !c.p.pst_colle && mlo == P.ac->m_max_bits;
         const float m_u = __uint_as_float(mlo);
-        for_each_pst_neighbour(c, P, i, xi, [&](int j, int, float4 pj, F3 xj, float d2) {
-            sr += pst_term_d2(c, vel, xi, rho_i, inv_Wd, j, pj, xj, d2, m_uni, m_u);
-        });
+        // one walk per form of the pair term, so that the loop carries no test of the form
+        auto walk = [&](auto form) {
+            constexpr int kForm = decltype(form)::value;
+            for_each_pst_neighbour<kPlain>(c, P, i, xi, [&](int j, int, float4 pj, F3 xj, float d2) {
+                sr += pst_term_d2<kPlain, kForm>(c, vel, xi, rho_i, inv_Wd, j, pj, xj, d2, m_uni, m_u);
+            });
+        };
+        if (c.W_dx0 > 1e-10f && c.p.pst_n == 4)
+            c.p.pst_colle ? walk(std::integral_constant<int, kPstColle4>())
+                          : walk(std::integral_constant<int, kPstSun4>());
+        else
+            walk(std::integral_constant<int, kPstAny>());
     }
     float4 vi4 = vel[i];
     F3 vi = f3(vi4);

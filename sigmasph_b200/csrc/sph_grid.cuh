@@ -499,9 +499,9 @@ __device__ __forceinline__ void list_entries(const int* __restrict__ nb, size_t 
         f(e);
     }
 }
-template <class F>
+template <bool kPlain = false, class F>
 __device__ __forceinline__ void list_pairs(const int* __restrict__ nb, size_t n, int m, F&& f) {
-    list_entries(nb, n, m, [&](int e) { f(e & kIdxMask, (int)((unsigned)e >> kMirShift)); });
+    list_entries(nb, n, m, [&](int e) { f(Shape<kPlain>::idx(e), Shape<kPlain>::mir(e)); });
 }
 
 // Entries 0 .. m-1 of a list made of pieces, with the same two-entry prefetch: at(k)
@@ -550,7 +550,9 @@ __device__ __forceinline__ void stale_search(const Cst& c, const Ptr& P, int i, 
 // whose candidates overflowed gets all its pairs from the stale-bin search instead; past
 // K of those, the rest go in order to a run of the overflow pool (the search runs a
 // second time to write it).
+template <bool kPlain>
 __global__ void SPH_BOUNDS(SPH_OCC_FILTER) k_nbr_filter(Cst c, Ptr P) {
+    using S = Shape<kPlain>;
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= c.n) return;
     const int vc = __ldg(P.vl_cnt + i);
@@ -574,7 +576,7 @@ __global__ void SPH_BOUNDS(SPH_OCC_FILTER) k_nbr_filter(Cst c, Ptr P) {
         // accepted entries go after the deep rows; near ones fill the list from its last
         // row down (deep + accepted + near <= the candidates <= Kv = K rows)
         list_entries(P.vl + i, (size_t)n, ne, [&](int e) {
-            const int j = e & kIdxMask, mir = (int)((unsigned)e >> kMirShift);
+            const int j = S::idx(e), mir = S::mir(e);
             if (mir && (((mir & 1) && !ny) || ((mir & 2) && !nz))) return;
             const float4 pj = __ldg(pos + j);
             F3 xj = f3(pj);
@@ -622,34 +624,36 @@ __global__ void SPH_BOUNDS(SPH_OCC_FILTER) k_nbr_filter(Cst c, Ptr P) {
 
 // Calls f(j, mirror, pos_j) for this step's neighbours of i, requesting the next entry's
 // position while the current pair is evaluated (the passes stall on that gather).
-template <class F>
+template <bool kPlain = false, class F>
 __device__ __forceinline__ void for_each_neighbour_pos(const Cst& c, const Ptr& P, int i,
                                                        const float4* __restrict__ pos, F&& f) {
+    using S = Shape<kPlain>;
     const int cnt = __ldg(P.nbr_cnt + i);
     const int m = cnt < c.K ? cnt : c.K;
     const size_t n = (size_t)c.n;
     const int* __restrict__ nb = P.nbr + i;
     int e0 = m > 0 ? __ldg(nb) : 0;
     int e1 = m > 1 ? __ldg(nb + n) : 0;
-    float4 p0 = m > 0 ? __ldg(pos + (e0 & kIdxMask)) : make_float4(0.f, 0.f, 0.f, 0.f);
+    float4 p0 = m > 0 ? __ldg(pos + S::idx(e0)) : make_float4(0.f, 0.f, 0.f, 0.f);
     for (int k = 0; k < m; ++k) {
         const int e = e0;
         const float4 pj = p0;
         e0 = e1;
         if (k + 2 < m) e1 = __ldg(nb + (size_t)(k + 2) * n);
-        if (k + 1 < m) p0 = __ldg(pos + (e0 & kIdxMask));
-        f(e & kIdxMask, (int)((unsigned)e >> kMirShift), pj);
+        if (k + 1 < m) p0 = __ldg(pos + S::idx(e0));
+        f(S::idx(e), S::mir(e), pj);
     }
     if (cnt > c.K)
-        list_pairs(P.ovf + __ldg(P.ovf_off + i), 1, cnt - c.K, [&](int j, int mir) { f(j, mir, __ldg(pos + j)); });
+        list_pairs<kPlain>(P.ovf + __ldg(P.ovf_off + i), 1, cnt - c.K,
+                           [&](int j, int mir) { f(j, mir, __ldg(pos + j)); });
 }
 
 // Calls f(j, mirror) for this step's neighbours of i: the list, then any overflow run.
-template <class F>
+template <bool kPlain = false, class F>
 __device__ __forceinline__ void for_each_neighbour(const Cst& c, const Ptr& P, int i, F&& f) {
     const int cnt = __ldg(P.nbr_cnt + i);
-    list_pairs(P.nbr + i, (size_t)c.n, cnt < c.K ? cnt : c.K, f);
-    if (cnt > c.K) list_pairs(P.ovf + __ldg(P.ovf_off + i), 1, cnt - c.K, f);
+    list_pairs<kPlain>(P.nbr + i, (size_t)c.n, cnt < c.K ? cnt : c.K, f);
+    if (cnt > c.K) list_pairs<kPlain>(P.ovf + __ldg(P.ovf_off + i), 1, cnt - c.K, f);
 }
 
 

@@ -393,19 +393,21 @@ __device__ __forceinline__ void store_kc_inverse(const Cst& c, const Ptr& P, int
     P.aux[6 * i + 4] = b;
 }
 
+template <bool kPlain>
 __global__ void __launch_bounds__(kBlock) k_kc_inverse(Cst c, Ptr P) {
+    using S = Shape<kPlain>;
     int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= c.n) return;
     const float4* __restrict__ pos = as4c(P.cur.pos);
     F3 xi = f3(pos[i]);
     // E = sum V_j (x_j - x_i) (x) grad W, symmetric (grad W = f r): six entries
     float e00 = 0.f, e11 = 0.f, e22 = 0.f, e01 = 0.f, e02 = 0.f, e12 = 0.f;
-    for_each_neighbour(c, P, i, [&](int j, int mir) {
+    for_each_neighbour<kPlain>(c, P, i, [&](int j, int mir) {
         float4 pj = __ldg(pos + j);
         F3 xj = f3(pj);
         if (mir) xj = mirror3(mir, xj);
         const F3 r = xi - xj;
-        const F3 sr = (-(w_of(pj, c) * wendland_dW_factor(dot3(r, r), c))) * r;
+        const F3 sr = (-(S::w(pj, c) * wendland_dW_factor(dot3(r, r), c))) * r;
         e00 += sr.x * r.x; e01 += sr.x * r.y; e02 += sr.x * r.z;
         e11 += sr.y * r.y; e12 += sr.y * r.z; e22 += sr.z * r.z;
     });
@@ -414,7 +416,9 @@ __global__ void __launch_bounds__(kBlock) k_kc_inverse(Cst c, Ptr P) {
 }
 
 // ------------------------------------------------------------------ pass A
+template <bool kPlain>
 __global__ void SPH_BOUNDS(SPH_OCC_SOLID_A) k_solid_a(Cst c, Ptr P) {
+    using S = Shape<kPlain>;
     int i = blockIdx.x * blockDim.x + threadIdx.x;
     double wdiff = 0.0;
     if (i < c.n) {
@@ -436,14 +440,14 @@ __global__ void SPH_BOUNDS(SPH_OCC_SOLID_A) k_solid_a(Cst c, Ptr P) {
         F3 lg = {0, 0, 0};
         float r0 = 0.0f, r1 = 0.0f;
         float G[3][3] = {{0, 0, 0}, {0, 0, 0}, {0, 0, 0}};
-        for_each_neighbour(c, P, i, [&](int j, int mir) {
+        for_each_neighbour<kPlain>(c, P, i, [&](int j, int mir) {
             float4 pj = __ldg(pos + j), vj4 = __ldg(vel + j);
             F3 xj = f3(pj), vj = f3(vj4);
             if (mir) { xj = mirror3(mir, xj); vj = mirror3(mir, vj); }
             F3 r = xi - xj;
             float rn2 = dot3(r, r), rn;
             F3 g = wendland_dW2(r, rn2, rn, c);
-            float Vj = w_of(pj, c);
+            float Vj = S::w(pj, c);
             float ld = __ldg(lam + j) - lam_i;
             F3 Lg = {L00 * g.x + L01 * g.y + L02 * g.z, L01 * g.x + L11 * g.y + L12 * g.z,
                      L02 * g.x + L12 * g.y + L22 * g.z};
@@ -480,10 +484,10 @@ __global__ void SPH_BOUNDS(SPH_OCC_SOLID_A) k_solid_a(Cst c, Ptr P) {
                 }
             }
         });
-        if (c.p.two_d) lg.z = 0.0f;
+        if (S::two_d(c)) lg.z = 0.0f;
         P.lgrad[i] = make_float4(lg.x, lg.y, lg.z, 0.0f);
         float dvg = r0;
-        if (c.p.axisymmetric) dvg -= vi.y / r_axi_of(pi.y, c);
+        if (S::axi(c)) dvg -= vi.y / r_axi_of(pi.y, c);
         P.div[i] = make_float4(dvg, r1, 0.0f, 0.0f);
         wdiff = -(double)pi.w * (double)__ldg(P.cur.disp + 4 * i + 3) * (double)r1;
         grad_v_finish<NoExtra>(c, P, i, G, pi, vi.y);
@@ -492,7 +496,9 @@ __global__ void SPH_BOUNDS(SPH_OCC_SOLID_A) k_solid_a(Cst c, Ptr P) {
 }
 
 // ------------------------------------------------------------------ grad v alone (damper refresh)
+template <bool kPlain>
 __global__ void SPH_PAIR_BOUNDS_OCC4 k_gradv(Cst c, Ptr P) {
+    using S = Shape<kPlain>;
     int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= c.n) return;
     const float4* __restrict__ pos = as4c(P.cur.pos);
@@ -500,14 +506,14 @@ __global__ void SPH_PAIR_BOUNDS_OCC4 k_gradv(Cst c, Ptr P) {
     float4 pi = pos[i];
     F3 xi = f3(pi), vi = f3(vel[i]);
     float G[3][3] = {{0, 0, 0}, {0, 0, 0}, {0, 0, 0}};
-    for_each_neighbour(c, P, i, [&](int j, int mir) {
+    for_each_neighbour<kPlain>(c, P, i, [&](int j, int mir) {
         float4 pj = __ldg(pos + j);
         F3 xj = f3(pj), vj = f3(__ldg(vel + j));
         if (mir) { xj = mirror3(mir, xj); vj = mirror3(mir, vj); }
         F3 r = xi - xj;
         float rn;
         F3 g = wendland_dW2(r, dot3(r, r), rn, c);
-        const F3 vd = w_of(pj, c) * (vj - vi);
+        const F3 vd = S::w(pj, c) * (vj - vi);
         G[0][0] += vd.x * g.x; G[0][1] += vd.x * g.y; G[0][2] += vd.x * g.z;
         G[1][0] += vd.y * g.x; G[1][1] += vd.y * g.y; G[1][2] += vd.y * g.z;
         G[2][0] += vd.z * g.x; G[2][1] += vd.z * g.y; G[2][2] += vd.z * g.z;
@@ -639,7 +645,9 @@ __device__ __forceinline__ void block_count_add(unsigned v, unsigned long long* 
     if (threadIdx.x == 0 && s_cnt && dst) atomicAdd(dst, (unsigned long long)s_cnt);
 }
 
+template <bool kPlain>
 __global__ void SPH_BOUNDS(SPH_OCC_SOLID_B) k_solid_b(Cst c, Ptr P) {
+    using S = Shape<kPlain>;
     int i = blockIdx.x * blockDim.x + threadIdx.x;
     double pw = 0.0, wl = 0.0;
     bool capped_any = false;
@@ -665,7 +673,7 @@ __global__ void SPH_BOUNDS(SPH_OCC_SOLID_B) k_solid_b(Cst c, Ptr P) {
         Sym A = {0, 0, 0, 0, 0, 0};
         float dep = 0.0f, adv = 0.0f, dif = 0.0f;
         if (ale) {
-            for_each_neighbour(c, P, i, [&](int j, int mir) {
+            for_each_neighbour<kPlain>(c, P, i, [&](int j, int mir) {
                 float4 pj = __ldg(pos + j), vj4 = __ldg(vel + j), shj = __ldg(shf + j);
                 F3 xj = f3(pj);
                 F3 du_j = {shj.x * inv_dt, shj.y * inv_dt, shj.z * inv_dt};
@@ -675,8 +683,9 @@ __global__ void SPH_BOUNDS(SPH_OCC_SOLID_B) k_solid_b(Cst c, Ptr P) {
                 F3 r = xi - xj;
                 float rn2 = dot3(r, r), rn;
                 F3 g = wendland_dW2(r, rn2, rn, c);
-                float rho_j = vj4.w / pj.w;
-                float wj = w_of(pj, c);
+                // rho_j only in products and sums here: the rounded quotient (2 ulp) suffices
+                const float rho_j = __fdividef(vj4.w, pj.w);
+                float wj = S::w(pj, c);
                 // w_j [(rho_j du_j . gW) phi_j - (rho_i du_i . gW) phi_i - phi_i div(rho du)]
                 // / rho_i (SOLID.py:1799-1862), whose rho_i du_i parts cancel:
                 // w_j rho_j (du_j . gW) (phi_j - phi_i) / rho_i
@@ -961,8 +970,9 @@ __global__ void __launch_bounds__(kBlock) k_solid_commit(Cst c, Ptr P) {
 // kVisc: a deck with the bulk viscosity q or Monaghan's Pi_ij (SOLID.py:3386-3401,
 // :3560-3570, :3727-3766); kAxi: an axisymmetric deck (its pair-radius forms and
 // geometric sources).  The plain instances keep the registers of the common case.
-template <bool kVisc, bool kAxi>
+template <bool kVisc, bool kAxi, bool kPlain>
 __global__ void SPH_BOUNDS(SPH_OCC_SOLID_FORCE) k_solid_force(Cst c, Ptr P) {
+    using S = Shape<kPlain>;
     int i = blockIdx.x * blockDim.x + threadIdx.x;
     float amag = 0.0f, csq = 0.0f, cvisc = 0.0f;
     double hgp = 0.0, vpw = 0.0;
@@ -986,7 +996,7 @@ __global__ void SPH_BOUNDS(SPH_OCC_SOLID_FORCE) k_solid_force(Cst c, Ptr P) {
             ce_q = qc.y;
         }
         const float rho_i = vi4.w / pi.w, inv_rho_i = 1.0f / rho_i;
-        const float w_i = w_of(pi, c), mw_i = mw_of(vi4.w, pi, c), inv_mw = 1.0f / mw_i;
+        const float w_i = S::w(pi, c), mw_i = S::mw(vi4.w, pi, c), inv_mw = 1.0f / mw_i;
         const int ki = eos_of(P, i);
         const float dt = dt_at(c, P, ki), inv_dt = 1.0f / dt;
         const Sym s = load_s(sdev, i);
@@ -1008,14 +1018,14 @@ __global__ void SPH_BOUNDS(SPH_OCC_SOLID_FORCE) k_solid_force(Cst c, Ptr P) {
         const float c_i = kVisc ? P.mat[ki].cp : 0.0f;
         F3 a = {0, 0, 0};
         float dei = 0.0f, dhg = 0.0f, dvisc = 0.0f, mu_max = 0.0f;
-        for_each_neighbour(c, P, i, [&](int j, int mir) {
+        for_each_neighbour<kPlain>(c, P, i, [&](int j, int mir) {
             float4 pj = __ldg(pos + j), vj4 = __ldg(vel + j);
             F3 xj = f3(pj), vj = f3(vj4);
             if (mir) { xj = mirror3(mir, xj); vj = mirror3(mir, vj); }
             F3 r = xi - xj;
             float rn2 = dot3(r, r), rn;
             F3 g = wendland_dW2(r, rn2, rn, c);
-            float w_j = w_of(pj, c);
+            float w_j = S::w(pj, c);
             const float rj = r_axi_of(pj.y, c);
             // the pair radius over r_i, on the axial (axc) and radial (axr) pair forces
             const float ratio = (axc || axr) ? 0.5f * (ri + rj) * inv_ri : 1.0f;
@@ -1074,7 +1084,10 @@ __global__ void SPH_BOUNDS(SPH_OCC_SOLID_FORCE) k_solid_force(Cst c, Ptr P) {
             // the viscous work conjugates are summed once, as de_visc = -(their part of
             // de_int), and folded into de_int after the loop: one add per pair fewer
             if (c.p.viscosity > 0.0f) dvisc += 0.5f * dot3(am, vij);
-            float rho_j = vj4.w / pj.w;
+            // rho_j to within 2 ulp for the products and sums below; the dt pair test, which
+            // takes the difference rho_i - rho_j, forms the exact quotient whenever the
+            // rounded one is within 1% of its threshold (as the fluid's force pass)
+            const float rho_j = __fdividef(vj4.w, pj.w);
             if (av_on && vxy < 0.0f) {
                 // Pi_ij = (-alpha cbar mu + beta mu^2) / rhobar on an approaching pair
                 const float mu = c.h * vxy / (rn * rn + c.p.av_eps * c.h * c.h);
@@ -1082,7 +1095,7 @@ __global__ void SPH_BOUNDS(SPH_OCC_SOLID_FORCE) k_solid_force(Cst c, Ptr P) {
                 const float c_j = c.one_material ? c_i : P.mat[eos_of(P, j)].cp;
                 const float c_bar = 0.5f * (c_i + c_j);
                 const float pij = (-c.p.av_alpha * c_bar * mu + c.p.av_beta * mu * mu) / rho_bar;
-                F3 ap = (-mw_of(vj4.w, pj, c) * pij) * g;
+                F3 ap = (-S::mw(vj4.w, pj, c) * pij) * g;
                 float mu_cfl = -mu;
                 if (axc || axr) {
                     if (axc) ap.x *= ratio;
@@ -1101,8 +1114,9 @@ __global__ void SPH_BOUNDS(SPH_OCC_SOLID_FORCE) k_solid_force(Cst c, Ptr P) {
                 if (mir) du_j = mirror3(mir, du_j);
                 a += (-(w_j * inv_rho_i) * (rho_j * dot3(du_j, g))) * vij;
             }
-            if (c.p.dt_pair_mode != 0 && (c.p.dt_pair_mode != 2 || same_material(c, P, j, ki))) {
-                float drho = fabsf(rho_i - rho_j);
+            if (c.p.dt_pair_mode != 0 && fabsf(rho_i - rho_j) > eps_rho * (1.0f - 1e-2f) &&
+                (c.p.dt_pair_mode != 2 || same_material(c, P, j, ki))) {
+                const float drho = fabsf(rho_i - vj4.w / pj.w);   // exact, as the reference's test
                 if (drho > eps_rho) {
                     // the quotient only where it can beat the running maximum: the product
                     // rounds within 1e-6 of cl drho, so the pre-test never drops a larger one
@@ -1264,7 +1278,9 @@ __global__ void __launch_bounds__(kBlock) k_half_kick(Cst c, Ptr P) {
     block_sum_atomic(ke, &P.sc->hg_work);   // + KE before the damper
 }
 
+template <bool kPlain>
 __global__ void __launch_bounds__(kBlock) k_hg_stage(Cst c, Ptr P, int stage) {
+    using S = Shape<kPlain>;
     if (c.n_inst == 0 && stage >= P.sc->sts_stages) return;
     int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= c.n) return;
@@ -1279,13 +1295,13 @@ __global__ void __launch_bounds__(kBlock) k_hg_stage(Cst c, Ptr P, int stage) {
     F3 yi = y_load(P, i, rb);
     const float rho_i = __ldg(&vel[i].w) / pi.w;
     const SymG Si = own_gsym(P, i);
-    const bool axc = c.p.axisymmetric && c.p.axi_conservative_x;
-    const bool axr = c.p.axisymmetric && c.p.axi_conservative_r;
+    const bool axc = S::axi(c) && c.p.axi_conservative_x;
+    const bool axr = S::axi(c) && c.p.axi_conservative_r;
     const float ri = r_axi_of(pi.y, c), inv_ri = 1.0f / ri;
     const float hg_pre = c.p.hourglass_alpha * (P.mat[ki].rho0 / rho_i) * (P.mat[ki].cp * c.inv_h)
                          / (c.p.V0 * (float)c.p.hg_W_dx0);
     F3 acc = {0, 0, 0};
-    for_each_neighbour(c, P, i, [&](int j, int mir) {
+    for_each_neighbour<kPlain>(c, P, i, [&](int j, int mir) {
         float4 pj = __ldg(pos + j);
         F3 xj = f3(pj);
         F3 yj = y_load(P, j, rb);
@@ -1301,7 +1317,7 @@ __global__ void __launch_bounds__(kBlock) k_hg_stage(Cst c, Ptr P, int stage) {
         // as the in-loop damper: (y_j - y_i) . rhat - |r| rhat^T <S> rhat
         const SymG Ss = {Si.xx + Sj.xx, Si.yy + Sj.yy, Si.zz + Sj.zz, Si.xy + Sj.xy, Si.xz + Sj.xz, Si.yz + Sj.yz};
         float hg = dot3(yj - yi, rh) - 0.5f * rn * quad_sym(Ss, rh);
-        float damp = hg_pre * w_of(pj, c) * wendland_W(rn, c) * hg;
+        float damp = hg_pre * S::w(pj, c) * wendland_W(rn, c) * hg;
         if (c.p.hg_mixed_impedance) damp *= hg_impedance_ratio(P, ki, j);
         F3 ah = damp * rh;
         if (axc || axr) {
@@ -1549,10 +1565,10 @@ inline int solid_substep_launch(const Cst& c, const Ptr& P, int n, cudaStream_t 
     const int nb = grid_of(n, bs);
     auto in = [&](int s) { return s >= first_stage && s <= last_stage; };
     if (in(SPH_STAGE_LAM)) {
-        k_lam<<<nb, bs, 0, st>>>(c, P); mark("k_lam");
-        if (c.p.kernel_correction) { k_kc_inverse<<<nb, bs, 0, st>>>(c, P); mark("k_kc_inverse"); }
-        k_solid_a<<<nb, bs, 0, st>>>(c, P); mark("k_solid_a");
-        k_solid_b<<<nb, bs, 0, st>>>(c, P); mark("k_solid_b");
+        SHAPED(plain_shape(c), k_lam, <<<nb, bs, 0, st>>>(c, P)); mark("k_lam");
+        if (c.p.kernel_correction) { SHAPED(plain_shape(c), k_kc_inverse, <<<nb, bs, 0, st>>>(c, P)); mark("k_kc_inverse"); }
+        SHAPED(plain_shape(c), k_solid_a, <<<nb, bs, 0, st>>>(c, P)); mark("k_solid_a");
+        SHAPED(plain_shape(c), k_solid_b, <<<nb, bs, 0, st>>>(c, P)); mark("k_solid_b");
         if (c.p.jc_surrogate && P.jc.count) {
             const int tiles = (n + kMlpTileRows - 1) / kMlpTileRows;
             const int g = std::min(kMlpCtasPerSm * 148, std::max(tiles, 1));
@@ -1566,11 +1582,14 @@ inline int solid_substep_launch(const Cst& c, const Ptr& P, int n, cudaStream_t 
     if (in(SPH_STAGE_FORCES)) {
         const bool visc = c.p.q_l2 > 0.0f || c.p.av_alpha > 0.0f || c.p.av_beta > 0.0f;
         if (c.p.axisymmetric) {
-            if (visc) k_solid_force<true, true><<<nb, bs, 0, st>>>(c, P);
-            else k_solid_force<false, true><<<nb, bs, 0, st>>>(c, P);
+            if (visc) k_solid_force<true, true, false><<<nb, bs, 0, st>>>(c, P);
+            else k_solid_force<false, true, false><<<nb, bs, 0, st>>>(c, P);
+        } else if (plain_shape(c)) {
+            if (visc) k_solid_force<true, false, true><<<nb, bs, 0, st>>>(c, P);
+            else k_solid_force<false, false, true><<<nb, bs, 0, st>>>(c, P);
         } else {
-            if (visc) k_solid_force<true, false><<<nb, bs, 0, st>>>(c, P);
-            else k_solid_force<false, false><<<nb, bs, 0, st>>>(c, P);
+            if (visc) k_solid_force<true, false, false><<<nb, bs, 0, st>>>(c, P);
+            else k_solid_force<false, false, false><<<nb, bs, 0, st>>>(c, P);
         }
         mark("k_solid_force");
     }
@@ -1578,8 +1597,11 @@ inline int solid_substep_launch(const Cst& c, const Ptr& P, int n, cudaStream_t 
     if (in(SPH_STAGE_ADVECT)) {
         if (c.p.hourglass_sts && c.p.hourglass_alpha > 0.0f) {
             k_half_kick<<<nb, bs, 0, st>>>(c, P); mark("k_half_kick");
-            if (c.p.hg_sts_refresh) { k_gradv<<<nb, bs, 0, st>>>(c, P); mark("k_gradv"); }
-            for (int s = 0; s < kStsMaxStages; ++s) { k_hg_stage<<<nb, bs, 0, st>>>(c, P, s); mark("k_hg_stage"); }
+            if (c.p.hg_sts_refresh) { SHAPED(plain_shape(c), k_gradv, <<<nb, bs, 0, st>>>(c, P)); mark("k_gradv"); }
+            for (int s = 0; s < kStsMaxStages; ++s) {
+                SHAPED(plain_shape(c), k_hg_stage, <<<nb, bs, 0, st>>>(c, P, s));
+                mark("k_hg_stage");
+            }
             k_sts_finish<<<nb, bs, 0, st>>>(c, P); mark("k_sts_finish");
         } else {
             k_solid_advect<<<nb, bs, 0, st>>>(c, P); mark("k_solid_advect");
@@ -1587,7 +1609,7 @@ inline int solid_substep_launch(const Cst& c, const Ptr& P, int n, cudaStream_t 
         k_constraints<<<nb, bs, 0, st>>>(c, P); mark("k_constraints");
     }
     if (in(SPH_STAGE_PST) && c.p.pst_enabled) {
-        k_pst<<<nb, bs, 0, st>>>(c, P); mark("k_pst");
+        SHAPED(plain_shape(c), k_pst, <<<nb, bs, 0, st>>>(c, P)); mark("k_pst");
         k_finish<<<nb, bs, 0, st>>>(c, P, last_stage >= SPH_STAGE_BOUNDARY ? 3 : 1); mark("k_finish");
     } else if (in(SPH_STAGE_BOUNDARY)) {
         k_finish<<<nb, bs, 0, st>>>(c, P, 2); mark("k_finish");
