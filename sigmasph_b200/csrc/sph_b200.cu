@@ -157,6 +157,14 @@ int apply_force(SphHandle* h, cudaStream_t st) {
     return SPH_OK;
 }
 
+// The fluid force pass runs its plain instance on standard decks too: its standard one
+// measured slower on the 1M dam break (0.455 against 0.414 ms; the gradient pass's standard
+// instance gains 0.433 -> 0.387 ms there).
+inline int force_shape(const Cst& c) {
+    const int s = shape_of(c);
+    return s == 2 ? 1 : s;
+}
+
 // update_grid_id / counting_sort / the neighbour search of every step
 // (particle_system.py:1300-1490): the step-start bins, the candidate lists when the
 // displacement bound asks for a build (the sort kernels return at once otherwise), and
@@ -182,7 +190,7 @@ int rebuild(SphHandle* h, cudaStream_t st) {
     LAUNCH("k_gather", k_gather<<<nb, kBlock, 0, st>>>(c, P));
     LAUNCH("k_gather_back", k_gather_back<<<nb, kBlock, 0, st>>>(c, P));
     LAUNCH("k_vlist_build", k_vlist_build<<<nb, kBlock, 0, st>>>(c, P));
-    LAUNCH("k_nbr_filter", SHAPED(plain_shape(c), k_nbr_filter, <<<nb, kBlock, 0, st>>>(c, P)));
+    LAUNCH("k_nbr_filter", SHAPED(shape_of(c), k_nbr_filter, <<<nb, kBlock, 0, st>>>(c, P)));
     return SPH_OK;
 }
 
@@ -190,15 +198,15 @@ int fluid_substep_and_boundary(SphHandle* h, cudaStream_t st) {
     const int nb = blocks_for(h->n);
     const Cst& c = h->c;
     Ptr P = make_ptr(h);
-    const bool plain = plain_shape(c);
-    LAUNCH("k_lam", SHAPED(plain, k_lam, <<<nb, kBlock, 0, st>>>(c, P)));
-    LAUNCH("k_lamgrad_cont", SHAPED(plain, k_lamgrad_cont, <<<nb, kBlock, 0, st>>>(c, P)));
+    const int shape = shape_of(c);
+    LAUNCH("k_lam", SHAPED(shape, k_lam, <<<nb, kBlock, 0, st>>>(c, P)));
+    LAUNCH("k_lamgrad_cont", SHAPED(shape, k_lamgrad_cont, <<<nb, kBlock, 0, st>>>(c, P)));
     LAUNCH("k_eos", k_eos<<<nb, kBlock, 0, st>>>(c, P));
-    LAUNCH("k_force", SHAPED(plain, k_force, <<<nb, kBlock, 0, st>>>(c, P)));
+    LAUNCH("k_force", SHAPED(force_shape(c), k_force, <<<nb, kBlock, 0, st>>>(c, P)));
     LAUNCH("k_dt", k_dt<<<1, 32, 0, st>>>(c, P));
     LAUNCH("k_advect", k_advect<<<nb, kBlock, 0, st>>>(c, P));
     if (h->p.pst_enabled) {
-        LAUNCH("k_pst", SHAPED(plain, k_pst, <<<nb, kBlock, 0, st>>>(c, P)));
+        LAUNCH("k_pst", SHAPED(shape, k_pst, <<<nb, kBlock, 0, st>>>(c, P)));
         LAUNCH("k_finish", k_finish<<<nb, kBlock, 0, st>>>(c, P, 3));
     } else {
         LAUNCH("k_finish", k_finish<<<nb, kBlock, 0, st>>>(c, P, 2));
@@ -518,16 +526,16 @@ int sph_run_stage(SphHandle* h, int stage, void* stream) {
     switch (stage) {
         case SPH_STAGE_SORT: { int r = rebuild(h, st); if (r) return r; break; }
         case SPH_STAGE_LAM:
-            SHAPED(plain_shape(c), k_lam, <<<nb, kBlock, 0, st>>>(c, P));
-            SHAPED(plain_shape(c), k_lamgrad_cont, <<<nb, kBlock, 0, st>>>(c, P));
+            SHAPED(shape_of(c), k_lam, <<<nb, kBlock, 0, st>>>(c, P));
+            SHAPED(shape_of(c), k_lamgrad_cont, <<<nb, kBlock, 0, st>>>(c, P));
             break;
         case SPH_STAGE_CONTINUITY: k_eos<<<nb, kBlock, 0, st>>>(c, P); break;
-        case SPH_STAGE_FORCES: SHAPED(plain_shape(c), k_force, <<<nb, kBlock, 0, st>>>(c, P)); break;
+        case SPH_STAGE_FORCES: SHAPED(force_shape(c), k_force, <<<nb, kBlock, 0, st>>>(c, P)); break;
         case SPH_STAGE_DT: k_dt<<<1, 32, 0, st>>>(c, P); break;
         case SPH_STAGE_ADVECT: k_advect<<<nb, kBlock, 0, st>>>(c, P); break;
         case SPH_STAGE_PST:
             if (h->p.pst_enabled) {
-                SHAPED(plain_shape(c), k_pst, <<<nb, kBlock, 0, st>>>(c, P));
+                SHAPED(shape_of(c), k_pst, <<<nb, kBlock, 0, st>>>(c, P));
                 k_finish<<<nb, kBlock, 0, st>>>(c, P, 1);
             }
             break;
@@ -743,7 +751,7 @@ extern "C" int sph_relax_pass(SphHandle* h, float beta, float* residual, float* 
     if (int r = rebuild(h, st)) return r;
     Ptr P = make_ptr(h);
     const Cst& c = h->c;
-    k_lam<false><<<nb, kBlock, 0, st>>>(c, P);
+    k_lam<0><<<nb, kBlock, 0, st>>>(c, P);
     if (!h->p.pst_normal_eigvec) k_relax_lamgrad<<<nb, kBlock, 0, st>>>(c, P);
     CK(cudaMemsetAsync(&h->ac->relax_max_bits, 0, sizeof(unsigned int), st));
     k_relax<<<nb, kBlock, 0, st>>>(c, P, beta, residual_each);

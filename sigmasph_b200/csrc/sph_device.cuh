@@ -353,15 +353,34 @@ __device__ __forceinline__ float mw_of(float m, float4 pos, const Cst& c) {
     return c.p.axisymmetric ? m / fmaxf(pos.y, c.p.axi_r_min) : m;
 }
 
-// The deck's shape as the pair passes see it.  Shape<true> is a 3D deck with no mirror
-// plane and no axisymmetry (the dam break, the round bar): neighbour entries carry no
-// mirror code and the weights are the stored volumes, known when the pass is compiled.
-// Shape<false> reads those switches from the parameters.
+// The deck as the pair passes see it, fixed when a pass is compiled (Shape<kShape>):
+//  0  every switch read from the parameters;
+//  1  plain: a 3D deck with no mirror plane and no axisymmetry (neighbour entries carry
+//     no mirror code; the weights are the stored volumes);
+//  2  plain and standard: also every term of the default step on -- delta+-SPH with the
+//     shift, its ALE terms, the gradient-lambda surface normal, delta diffusion and the dt
+//     pair limit; for a solid also one material, the in-loop hourglass damper, Morris
+//     viscosity, plasticity and the ALE transport of the history and of e -- no ensemble.
+// A uniform switch inside a pair loop costs issue slots and splits the loop body the
+// compiler schedules; the dam break and the round bar run instance 2.
 __host__ __device__ __forceinline__ bool plain_shape(const Cst& c) {
     return !c.mirror_y && !c.mirror_z && !c.p.axisymmetric && !c.p.two_d;
 }
-template <bool kPlain>
+__host__ __device__ __forceinline__ bool std_form(const Cst& c) {
+    const SphParams& p = c.p;
+    const bool fluid = p.pst_enabled && p.pst_ale_momentum && !p.pst_normal_eigvec && p.delta_sph > 0.0f &&
+                       p.dt_pair_mode != 0 && c.n_inst == 0 && !p.delta_pairs_all && !p.c0_mixed &&
+                       !p.hg_mixed_impedance;
+    if (!p.is_solid) return fluid;
+    return fluid && p.hourglass_alpha > 0.0f && !p.hourglass_sts && p.viscosity > 0.0f && c.one_material &&
+           c.any_plastic && p.ale_history && p.transport_e && p.ale_diffusion > 0.0f;
+}
+__host__ __device__ __forceinline__ int shape_of(const Cst& c) {
+    return plain_shape(c) ? (std_form(c) ? 2 : 1) : 0;
+}
+template <int kShape>
 struct Shape {
+    static constexpr bool kPlain = kShape >= 1, kStd = kShape == 2;
     __device__ static __forceinline__ bool two_d(const Cst& c) { return !kPlain && c.p.two_d; }
     __device__ static __forceinline__ bool axi(const Cst& c) { return !kPlain && c.p.axisymmetric; }
     __device__ static __forceinline__ float w(float4 pos, const Cst& c) { return kPlain ? pos.w : w_of(pos, c); }
@@ -370,12 +389,36 @@ struct Shape {
     }
     __device__ static __forceinline__ int idx(int e) { return kPlain ? e : (e & kIdxMask); }
     __device__ static __forceinline__ int mir(int e) { return kPlain ? 0 : (int)((unsigned)e >> kMirShift); }
+    // the step's terms
+    __device__ static __forceinline__ bool pst(const Cst& c) { return kStd || c.p.pst_enabled; }
+    __device__ static __forceinline__ bool lgrad(const Cst& c) { return kStd || !c.p.pst_normal_eigvec; }
+    __device__ static __forceinline__ bool delta(const Cst& c) { return kStd || c.p.delta_sph > 0.0f; }
+    __device__ static __forceinline__ bool ale_mom(const Cst& c) {
+        return kStd || (c.p.pst_enabled && c.p.pst_ale_momentum);
+    }
+    __device__ static __forceinline__ bool dt_pairs(const Cst& c) { return kStd || c.p.dt_pair_mode != 0; }
+    __device__ static __forceinline__ bool ensemble(const Cst& c) { return !kStd && c.n_inst > 0; }
+    __device__ static __forceinline__ bool pairs_all(const Cst& c) { return !kStd && c.p.delta_pairs_all; }
+    __device__ static __forceinline__ bool c0_mixed(const Cst& c) { return !kStd && c.p.c0_mixed; }
+    // the solid's
+    __device__ static __forceinline__ bool hg_inloop(const Cst& c) {
+        return kStd || (c.p.hourglass_alpha > 0.0f && !c.p.hourglass_sts);
+    }
+    __device__ static __forceinline__ bool hg_mixed(const Cst& c) { return !kStd && c.p.hg_mixed_impedance; }
+    __device__ static __forceinline__ bool visc(const Cst& c) { return kStd || c.p.viscosity > 0.0f; }
+    __device__ static __forceinline__ bool one(const Cst& c) { return kStd || c.one_material; }
+    __device__ static __forceinline__ bool plastic(const Cst& c) { return kStd || c.any_plastic; }
+    __device__ static __forceinline__ bool ale_hist(const Cst& c) { return kStd || c.p.ale_history; }
+    __device__ static __forceinline__ bool transport_e(const Cst& c) { return kStd || c.p.transport_e; }
+    __device__ static __forceinline__ bool ale_diff(const Cst& c) { return kStd || c.p.ale_diffusion > 0.0f; }
 };
-// Launches the instance of a shape-templated pass for the deck.
-#define SHAPED(plain, kernel, ...)            \
-    do {                                      \
-        if (plain) kernel<true> __VA_ARGS__;  \
-        else kernel<false> __VA_ARGS__;       \
+// Launches the instance of a shape-templated pass for the deck (shape_of).
+#define SHAPED(shape, kernel, ...)                   \
+    do {                                             \
+        const int shape_ = (shape);                  \
+        if (shape_ == 2) kernel<2> __VA_ARGS__;      \
+        else if (shape_ == 1) kernel<1> __VA_ARGS__; \
+        else kernel<0> __VA_ARGS__;                  \
     } while (0)
 
 // One particle's terms of every FP64 reduction.

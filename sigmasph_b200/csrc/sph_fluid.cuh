@@ -26,9 +26,10 @@ __device__ __forceinline__ float4* as4(float* p) { return reinterpret_cast<float
 __device__ __forceinline__ const float4* as4c(const float* p) { return reinterpret_cast<const float4*>(p); }
 
 // ------------------------------------------------------------------ compute_lam pass 1
-template <bool kPlain>
+template <int kShape>
 __global__ void SPH_BOUNDS(SPH_OCC_LAM) k_lam(Cst c, Ptr P) {
-    using S = Shape<kPlain>;
+    using S = Shape<kShape>;
+    constexpr bool kPlain = S::kPlain;
     int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= c.n) return;
     const float4* __restrict__ pos = as4c(P.cur.pos);
@@ -105,9 +106,10 @@ __global__ void SPH_BOUNDS(SPH_OCC_LAM) k_lam(Cst c, Ptr P) {
 }
 
 // ------------------------------------------------------------------ grad lambda + continuity
-template <bool kPlain>
+template <int kShape>
 __global__ void SPH_BOUNDS(SPH_OCC_LAMGRAD) k_lamgrad_cont(Cst c, Ptr P) {
-    using S = Shape<kPlain>;
+    using S = Shape<kShape>;
+    constexpr bool kPlain = S::kPlain;
     int i = blockIdx.x * blockDim.x + threadIdx.x;
     double wdiff = 0.0;
     if (i < c.n) {
@@ -124,8 +126,8 @@ __global__ void SPH_BOUNDS(SPH_OCC_LAMGRAD) k_lamgrad_cont(Cst c, Ptr P) {
         const float inv_rho_i = 1.0f / rho_i;
         const float dt = P.sc->dt;
         const float inv_dt = 1.0f / dt;
-        const bool pst = c.p.pst_enabled;
-        const bool need_lgrad = !c.p.pst_normal_eigvec;
+        const bool pst = S::pst(c);
+        const bool need_lgrad = S::lgrad(c);
         F3 lg = {0, 0, 0};
         float r0 = 0.0f, r1 = 0.0f;
         // the next neighbour's position is requested while this pair is evaluated
@@ -157,7 +159,7 @@ __global__ void SPH_BOUNDS(SPH_OCC_LAMGRAD) k_lamgrad_cont(Cst c, Ptr P) {
                 rr += (rho_j - rho_i) * inv_rho_i * dot3(du_j, g);
             }
             r0 += Vj * rr;
-            if (c.p.delta_sph > 0.0f) {
+            if (S::delta(c)) {
                 // psi . grad W = 2 (rho_j - rho_i) (-r . grad W) / (|r|^2 + eta^2)
                 float psig = __fdividef(2.0f * (rho_j - rho_i) * (-dot3(r, g)), rn2 + c.eta2);
                 float rate = c.delta_coef * Vj * psig * inv_rho_i;
@@ -218,9 +220,10 @@ __global__ void __launch_bounds__(kBlock) k_eos(Cst c, Ptr P) {
 }
 
 // ------------------------------------------------------------------ pressure + viscosity + dt pairs
-template <bool kPlain>
+template <int kShape>
 __global__ void SPH_BOUNDS(SPH_OCC_FORCE) k_force(Cst c, Ptr P) {
-    using S = Shape<kPlain>;
+    using S = Shape<kShape>;
+    constexpr bool kPlain = S::kPlain;
     int i = blockIdx.x * blockDim.x + threadIdx.x;
     float amag = 0.0f, csq = 0.0f;
     if (i < c.n) {
@@ -235,7 +238,7 @@ __global__ void SPH_BOUNDS(SPH_OCC_FORCE) k_force(Cst c, Ptr P) {
         const float w_i = S::w(pi, c);
         const float mw_i = S::mw(vi4.w, pi, c);
         const float dt = P.sc->dt;
-        const bool ale = c.p.pst_enabled && c.p.pst_ale_momentum;
+        const bool ale = S::ale_mom(c);
         const float eps_rho = 1e-3f * c.p.density0;
         const float inv_mw_i = 1.0f / mw_i, inv_rho_i = 1.0f / rho_i, inv_dt = 1.0f / dt;
         const float wi_mw = w_i * inv_mw_i;
@@ -272,7 +275,7 @@ __global__ void SPH_BOUNDS(SPH_OCC_FORCE) k_force(Cst c, Ptr P) {
                 if (mir) du_j = mirror3(mir, du_j);
                 a += (-(w_j * inv_rho_i) * (rho_j * dot3(du_j, g))) * vij;
             }
-            if (c.p.dt_pair_mode != 0 && fabsf(rho_i - rho_j) > eps_rho * (1.0f - 1e-2f)) {
+            if (S::dt_pairs(c) && fabsf(rho_i - rho_j) > eps_rho * (1.0f - 1e-2f)) {
                 float drho = fabsf(rho_i - vj4.w / pj.w);   // exact, as the reference's test
                 if (drho > eps_rho) {
                     // the quotient only where it can beat the running maximum: the product
@@ -290,7 +293,7 @@ __global__ void SPH_BOUNDS(SPH_OCC_FORCE) k_force(Cst c, Ptr P) {
         P.acc[i] = make_float4(an.x, an.y, an.z, c.p.track_visc_work ? dvisc : 0.0f);
         bool ongrid = !(isnan(pi.x) || isnan(pi.y) || isnan(pi.z));
         if (ongrid) amag = norm3(an);
-        if (c.p.dt_pair_mode != 0) csq = cl;
+        if (S::dt_pairs(c)) csq = cl;
     }
     block_max_atomic(amag, &P.ac->max_accel_bits);
     block_max_atomic(csq, &P.ac->max_c_sq_bits);
@@ -386,7 +389,7 @@ __global__ void __launch_bounds__(kBlock) k_advect(Cst c, Ptr P) {
 // (or when the candidate list overflowed) the stale-bin search.  f(j, mirror, pos_j).
 template <bool kPlain, class F>
 __device__ __forceinline__ void for_each_pst_neighbour(const Cst& c, const Ptr& P, int i, F3 xi, F&& f) {
-    using S = Shape<kPlain>;
+    using S = Shape<kPlain ? 1 : 0>;
     if (isnan(xi.x) || isnan(xi.y) || isnan(xi.z)) return;
     const float dtot = __uint_as_float(P.ac->d_start_bits) + __uint_as_float(P.ac->max_disp_bits) +
                        __uint_as_float(P.ac->max_grip_disp_bits);
@@ -453,11 +456,11 @@ __device__ __forceinline__ F3 pst_term_d2(const Cst& c, const float4* __restrict
         f = c.p.pst_R * ipow_or_pow(Wij * inv_Wd, c.p.pst_n);
     }
     if (kForm == kPstColle4 || (kForm == kPstAny && c.p.pst_colle)) {
-        const float Vj = Shape<kPlain>::w(pj, c);
+        const float Vj = Shape<kPlain ? 1 : 0>::w(pj, c);
         if (Vj > 1e-30f) return ((1.0f + f) * Vj) * g;
     } else {
         const float mj_raw = m_uni ? m_u : __ldg(&vel[j].w);
-        const float mj = Shape<kPlain>::mw(mj_raw, pj, c);
+        const float mj = Shape<kPlain ? 1 : 0>::mw(mj_raw, pj, c);
         if (mj > 1e-10f) {
             // m_j / mean rho: a sum of densities, rounded quotients suffice (no cancellation)
             const float rho_j = __fdividef(mj_raw, pj.w);
@@ -523,8 +526,9 @@ __device__ __forceinline__ F3 pst_constrain(const Cst& c, const Ptr& P, int i, F
     return dr;
 }
 
-template <bool kPlain>
+template <int kShape>
 __global__ void SPH_BOUNDS(SPH_OCC_PST) k_pst(Cst c, Ptr P) {
+    constexpr bool kPlain = kShape >= 1;
     int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i == 0) {   // steps whose shift could not use the candidate lists
         const float dtot = __uint_as_float(P.ac->d_start_bits) + __uint_as_float(P.ac->max_disp_bits) +

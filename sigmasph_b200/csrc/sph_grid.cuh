@@ -501,7 +501,7 @@ __device__ __forceinline__ void list_entries(const int* __restrict__ nb, size_t 
 }
 template <bool kPlain = false, class F>
 __device__ __forceinline__ void list_pairs(const int* __restrict__ nb, size_t n, int m, F&& f) {
-    list_entries(nb, n, m, [&](int e) { f(Shape<kPlain>::idx(e), Shape<kPlain>::mir(e)); });
+    list_entries(nb, n, m, [&](int e) { f(Shape<kPlain ? 1 : 0>::idx(e), Shape<kPlain ? 1 : 0>::mir(e)); });
 }
 
 // Entries 0 .. m-1 of a list made of pieces, with the same two-entry prefetch: at(k)
@@ -550,9 +550,10 @@ __device__ __forceinline__ void stale_search(const Cst& c, const Ptr& P, int i, 
 // whose candidates overflowed gets all its pairs from the stale-bin search instead; past
 // K of those, the rest go in order to a run of the overflow pool (the search runs a
 // second time to write it).
-template <bool kPlain>
+template <int kShape>
 __global__ void SPH_BOUNDS(SPH_OCC_FILTER) k_nbr_filter(Cst c, Ptr P) {
-    using S = Shape<kPlain>;
+    using S = Shape<kShape>;
+    constexpr bool kPlain = S::kPlain;
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= c.n) return;
     const int vc = __ldg(P.vl_cnt + i);
@@ -627,7 +628,7 @@ __global__ void SPH_BOUNDS(SPH_OCC_FILTER) k_nbr_filter(Cst c, Ptr P) {
 template <bool kPlain = false, class F>
 __device__ __forceinline__ void for_each_neighbour_pos(const Cst& c, const Ptr& P, int i,
                                                        const float4* __restrict__ pos, F&& f) {
-    using S = Shape<kPlain>;
+    using S = Shape<kPlain ? 1 : 0>;
     const int cnt = __ldg(P.nbr_cnt + i);
     const int m = cnt < c.K ? cnt : c.K;
     const size_t n = (size_t)c.n;

@@ -393,9 +393,10 @@ __device__ __forceinline__ void store_kc_inverse(const Cst& c, const Ptr& P, int
     P.aux[6 * i + 4] = b;
 }
 
-template <bool kPlain>
+template <int kShape>
 __global__ void __launch_bounds__(kBlock) k_kc_inverse(Cst c, Ptr P) {
-    using S = Shape<kPlain>;
+    using S = Shape<kShape>;
+    constexpr bool kPlain = S::kPlain;
     int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= c.n) return;
     const float4* __restrict__ pos = as4c(P.cur.pos);
@@ -416,9 +417,10 @@ __global__ void __launch_bounds__(kBlock) k_kc_inverse(Cst c, Ptr P) {
 }
 
 // ------------------------------------------------------------------ pass A
-template <bool kPlain>
+template <int kShape>
 __global__ void SPH_BOUNDS(SPH_OCC_SOLID_A) k_solid_a(Cst c, Ptr P) {
-    using S = Shape<kPlain>;
+    using S = Shape<kShape>;
+    constexpr bool kPlain = S::kPlain;
     int i = blockIdx.x * blockDim.x + threadIdx.x;
     double wdiff = 0.0;
     if (i < c.n) {
@@ -432,11 +434,11 @@ __global__ void SPH_BOUNDS(SPH_OCC_SOLID_A) k_solid_a(Cst c, Ptr P) {
         const float L00 = l0.x, L11 = l0.y, L22 = l0.z, L01 = l0.w, L02 = l1.x, L12 = l1.y;
         const float lam_i = lam[i];
         const float rho_i = vi4.w / pi.w, inv_rho_i = 1.0f / rho_i;
-        const bool pst = c.p.pst_enabled;
+        const bool pst = S::pst(c);
         const int ki = eos_of(P, i);
         const float dt = dt_at(c, P, ki), inv_dt = 1.0f / dt;
         const float di = P.mat[ki].delta;
-        const float c0i = c.n_inst > 0 ? P.irow[ki].c0 : c.p.c0;
+        const float c0i = S::ensemble(c) ? P.irow[ki].c0 : c.p.c0;
         F3 lg = {0, 0, 0};
         float r0 = 0.0f, r1 = 0.0f;
         float G[3][3] = {{0, 0, 0}, {0, 0, 0}, {0, 0, 0}};
@@ -470,13 +472,13 @@ __global__ void SPH_BOUNDS(SPH_OCC_SOLID_A) k_solid_a(Cst c, Ptr P) {
             r0 += Vj * rr;
             // pair_delta and pair_c0 (SOLID.py:4102-4114, DSPH.py:483-511) on same-material
             // pairs, or on every pair under Diffusion.pairs "all" (DSPH.py:1271-1282)
-            const int kj = c.one_material ? ki : eos_of(P, j);
-            if (kj == ki || c.p.delta_pairs_all) {
+            const int kj = S::one(c) ? ki : eos_of(P, j);
+            if (kj == ki || S::pairs_all(c)) {
                 const float dj = kj == ki ? di : P.mat[kj].delta;
                 float den = di + dj;
                 float dl = den > 1e-12f ? 2.0f * di * dj / den : 0.0f;
                 if (dl > 0.0f) {
-                    const float c0p = c.p.c0_mixed ? 0.5f * (P.mat[ki].c0 + P.mat[kj].c0) : c0i;
+                    const float c0p = S::c0_mixed(c) ? 0.5f * (P.mat[ki].c0 + P.mat[kj].c0) : c0i;
                     float psig = __fdividef(2.0f * (rho_j - rho_i) * (-dot3(r, g)), rn2 + c.eta2);
                     float rate = dl * c.h * c0p * Vj * psig * inv_rho_i;
                     r0 += rate;
@@ -496,9 +498,10 @@ __global__ void SPH_BOUNDS(SPH_OCC_SOLID_A) k_solid_a(Cst c, Ptr P) {
 }
 
 // ------------------------------------------------------------------ grad v alone (damper refresh)
-template <bool kPlain>
+template <int kShape>
 __global__ void SPH_PAIR_BOUNDS_OCC4 k_gradv(Cst c, Ptr P) {
-    using S = Shape<kPlain>;
+    using S = Shape<kShape>;
+    constexpr bool kPlain = S::kPlain;
     int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= c.n) return;
     const float4* __restrict__ pos = as4c(P.cur.pos);
@@ -645,9 +648,10 @@ __device__ __forceinline__ void block_count_add(unsigned v, unsigned long long* 
     if (threadIdx.x == 0 && s_cnt && dst) atomicAdd(dst, (unsigned long long)s_cnt);
 }
 
-template <bool kPlain>
+template <int kShape>
 __global__ void SPH_BOUNDS(SPH_OCC_SOLID_B) k_solid_b(Cst c, Ptr P) {
-    using S = Shape<kPlain>;
+    using S = Shape<kShape>;
+    constexpr bool kPlain = S::kPlain;
     int i = blockIdx.x * blockDim.x + threadIdx.x;
     double pw = 0.0, wl = 0.0;
     bool capped_any = false;
@@ -667,8 +671,8 @@ __global__ void SPH_BOUNDS(SPH_OCC_SOLID_B) k_solid_b(Cst c, Ptr P) {
         float ep = sd1.z;
         const float T_old = sd1.w;
         const float e_i = shi.w;
-        const bool ale = c.p.ale_history != 0;
-        const bool plastic_any = c.any_plastic != 0;
+        const bool ale = S::ale_hist(c);
+        const bool plastic_any = S::plastic(c);
         const F3 du_i = {shi.x * inv_dt, shi.y * inv_dt, shi.z * inv_dt};
         Sym A = {0, 0, 0, 0, 0, 0};
         float dep = 0.0f, adv = 0.0f, dif = 0.0f;
@@ -697,10 +701,10 @@ __global__ void SPH_BOUNDS(SPH_OCC_SOLID_B) k_solid_b(Cst c, Ptr P) {
                 A.xz += ka * (sj.xz - s.xz);
                 A.yz += ka * (sj.yz - s.yz);
                 if (plastic_any) dep += ka * (epj - ep);
-                if (c.p.transport_e) {
+                if (S::transport_e(c)) {
                     float e_j = shj.w;
                     adv += wj * rho_j * (e_j - e_i) * dot3(du_j, g) * inv_rho_i;
-                    if (c.p.ale_diffusion > 0.0f && same_material(c, P, j, ki)) {
+                    if (S::ale_diff(c) && (S::one(c) || same_material(c, P, j, ki))) {
                         float psig = __fdividef(2.0f * (e_j - e_i) * (-dot3(r, g)), rn2 + c.eta2);
                         float rb = 0.5f * (rho_i + rho_j);
                         F3 su = du_i + du_j;
@@ -970,9 +974,10 @@ __global__ void __launch_bounds__(kBlock) k_solid_commit(Cst c, Ptr P) {
 // kVisc: a deck with the bulk viscosity q or Monaghan's Pi_ij (SOLID.py:3386-3401,
 // :3560-3570, :3727-3766); kAxi: an axisymmetric deck (its pair-radius forms and
 // geometric sources).  The plain instances keep the registers of the common case.
-template <bool kVisc, bool kAxi, bool kPlain>
+template <bool kVisc, bool kAxi, int kShape>
 __global__ void SPH_BOUNDS(SPH_OCC_SOLID_FORCE) k_solid_force(Cst c, Ptr P) {
-    using S = Shape<kPlain>;
+    using S = Shape<kShape>;
+    constexpr bool kPlain = S::kPlain;
     int i = blockIdx.x * blockDim.x + threadIdx.x;
     float amag = 0.0f, csq = 0.0f, cvisc = 0.0f;
     double hgp = 0.0, vpw = 0.0;
@@ -1000,8 +1005,8 @@ __global__ void SPH_BOUNDS(SPH_OCC_SOLID_FORCE) k_solid_force(Cst c, Ptr P) {
         const int ki = eos_of(P, i);
         const float dt = dt_at(c, P, ki), inv_dt = 1.0f / dt;
         const Sym s = load_s(sdev, i);
-        const bool ale = c.p.pst_enabled && c.p.pst_ale_momentum;
-        const bool hg_inloop = c.p.hourglass_alpha > 0.0f && !c.p.hourglass_sts;
+        const bool ale = S::ale_mom(c);
+        const bool hg_inloop = S::hg_inloop(c);
         const bool axc = kAxi && c.p.axi_conservative_x;
         const bool axr = kAxi && c.p.axi_conservative_r;
         const float ri = r_axi_of(pi.y, c), inv_ri = 1.0f / ri;
@@ -1013,7 +1018,7 @@ __global__ void SPH_BOUNDS(SPH_OCC_SOLID_FORCE) k_solid_force(Cst c, Ptr P) {
         kinst = ki;
         on = true;
         const float eps_rho = 1e-3f * c.p.density0;
-        const float csig = c.n_inst > 0 ? P.irow[ki].c_signal : c.p.c_signal;
+        const float csig = S::ensemble(c) ? P.irow[ki].c_signal : c.p.c_signal;
         float cl = csig * csig;
         const float c_i = kVisc ? P.mat[ki].cp : 0.0f;
         F3 a = {0, 0, 0};
@@ -1047,7 +1052,7 @@ __global__ void SPH_BOUNDS(SPH_OCC_SOLID_FORCE) k_solid_force(Cst c, Ptr P) {
                                      Si.xz + Sj.xz, Si.yz + Sj.yz};
                     float hg = dot3(vj - vi, rh) - 0.5f * rn * quad_sym(Ss, rh);
                     float damp = hg_pre * w_j * wendland_W(rn, c) * hg;
-                    if (c.p.hg_mixed_impedance) damp *= hg_impedance_ratio(P, ki, j);
+                    if (S::hg_mixed(c)) damp *= hg_impedance_ratio(P, ki, j);
                     F3 ah = damp * rh;
                     if (axc) ah.x *= ratio;
                     if (axr) ah.y *= ratio;
@@ -1083,7 +1088,7 @@ __global__ void SPH_BOUNDS(SPH_OCC_SOLID_FORCE) k_solid_force(Cst c, Ptr P) {
             a += am;
             // the viscous work conjugates are summed once, as de_visc = -(their part of
             // de_int), and folded into de_int after the loop: one add per pair fewer
-            if (c.p.viscosity > 0.0f) dvisc += 0.5f * dot3(am, vij);
+            if (S::visc(c)) dvisc += 0.5f * dot3(am, vij);
             // rho_j to within 2 ulp for the products and sums below; the dt pair test, which
             // takes the difference rho_i - rho_j, forms the exact quotient whenever the
             // rounded one is within 1% of its threshold (as the fluid's force pass)
@@ -1114,8 +1119,8 @@ __global__ void SPH_BOUNDS(SPH_OCC_SOLID_FORCE) k_solid_force(Cst c, Ptr P) {
                 if (mir) du_j = mirror3(mir, du_j);
                 a += (-(w_j * inv_rho_i) * (rho_j * dot3(du_j, g))) * vij;
             }
-            if (c.p.dt_pair_mode != 0 && fabsf(rho_i - rho_j) > eps_rho * (1.0f - 1e-2f) &&
-                (c.p.dt_pair_mode != 2 || same_material(c, P, j, ki))) {
+            if (S::dt_pairs(c) && fabsf(rho_i - rho_j) > eps_rho * (1.0f - 1e-2f) &&
+                (c.p.dt_pair_mode != 2 || S::one(c) || same_material(c, P, j, ki))) {
                 const float drho = fabsf(rho_i - vj4.w / pj.w);   // exact, as the reference's test
                 if (drho > eps_rho) {
                     // the quotient only where it can beat the running maximum: the product
@@ -1142,7 +1147,7 @@ __global__ void SPH_BOUNDS(SPH_OCC_SOLID_FORCE) k_solid_force(Cst c, Ptr P) {
         P.acc[i] = make_float4(an.x, an.y, an.z, dei);
         bool ongrid = !(isnan(pi.x) || isnan(pi.y) || isnan(pi.z));
         if (ongrid) amag = norm3(an);
-        if (c.p.dt_pair_mode != 0) csq = cl;
+        if (S::dt_pairs(c)) csq = cl;
         hgp = (double)(mw_i * dhg);
         vpw = (double)vi4.w * (double)dvisc;
         if (kVisc) {
@@ -1152,14 +1157,14 @@ __global__ void SPH_BOUNDS(SPH_OCC_SOLID_FORCE) k_solid_force(Cst c, Ptr P) {
             cvisc = fmaxf(ce_q, ce_av);
         }
     }
-    if (c.n_inst > 0) {
+    if (S::ensemble(c)) {
         inst_max_atomic(amag, kinst, on, &SphInstState::max_accel_bits, P.inst);
         inst_max_atomic(csq, kinst, on, &SphInstState::max_c_sq_bits, P.inst);
         return;
     }
     block_max_atomic(amag, &P.ac->max_accel_bits);
     block_max_atomic(csq, &P.ac->max_c_sq_bits);
-    if (c.p.hourglass_alpha > 0.0f && !c.p.hourglass_sts) block_sum_atomic(hgp, &P.ac->hg_power);
+    if (S::hg_inloop(c)) block_sum_atomic(hgp, &P.ac->hg_power);
     if (kVisc) block_max_atomic(cvisc, &P.ac->visc_c_bits);
     if (c.p.track_visc_work) block_sum_atomic(vpw, &P.ac->visc_power);
 }
@@ -1278,9 +1283,10 @@ __global__ void __launch_bounds__(kBlock) k_half_kick(Cst c, Ptr P) {
     block_sum_atomic(ke, &P.sc->hg_work);   // + KE before the damper
 }
 
-template <bool kPlain>
+template <int kShape>
 __global__ void __launch_bounds__(kBlock) k_hg_stage(Cst c, Ptr P, int stage) {
-    using S = Shape<kPlain>;
+    using S = Shape<kShape>;
+    constexpr bool kPlain = S::kPlain;
     if (c.n_inst == 0 && stage >= P.sc->sts_stages) return;
     int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= c.n) return;
@@ -1318,7 +1324,7 @@ __global__ void __launch_bounds__(kBlock) k_hg_stage(Cst c, Ptr P, int stage) {
         const SymG Ss = {Si.xx + Sj.xx, Si.yy + Sj.yy, Si.zz + Sj.zz, Si.xy + Sj.xy, Si.xz + Sj.xz, Si.yz + Sj.yz};
         float hg = dot3(yj - yi, rh) - 0.5f * rn * quad_sym(Ss, rh);
         float damp = hg_pre * S::w(pj, c) * wendland_W(rn, c) * hg;
-        if (c.p.hg_mixed_impedance) damp *= hg_impedance_ratio(P, ki, j);
+        if (S::hg_mixed(c)) damp *= hg_impedance_ratio(P, ki, j);
         F3 ah = damp * rh;
         if (axc || axr) {
             const float ratio = 0.5f * (ri + r_axi_of(pj.y, c)) * inv_ri;
@@ -1565,10 +1571,10 @@ inline int solid_substep_launch(const Cst& c, const Ptr& P, int n, cudaStream_t 
     const int nb = grid_of(n, bs);
     auto in = [&](int s) { return s >= first_stage && s <= last_stage; };
     if (in(SPH_STAGE_LAM)) {
-        SHAPED(plain_shape(c), k_lam, <<<nb, bs, 0, st>>>(c, P)); mark("k_lam");
-        if (c.p.kernel_correction) { SHAPED(plain_shape(c), k_kc_inverse, <<<nb, bs, 0, st>>>(c, P)); mark("k_kc_inverse"); }
-        SHAPED(plain_shape(c), k_solid_a, <<<nb, bs, 0, st>>>(c, P)); mark("k_solid_a");
-        SHAPED(plain_shape(c), k_solid_b, <<<nb, bs, 0, st>>>(c, P)); mark("k_solid_b");
+        SHAPED(shape_of(c), k_lam, <<<nb, bs, 0, st>>>(c, P)); mark("k_lam");
+        if (c.p.kernel_correction) { SHAPED(shape_of(c), k_kc_inverse, <<<nb, bs, 0, st>>>(c, P)); mark("k_kc_inverse"); }
+        SHAPED(shape_of(c), k_solid_a, <<<nb, bs, 0, st>>>(c, P)); mark("k_solid_a");
+        SHAPED(shape_of(c), k_solid_b, <<<nb, bs, 0, st>>>(c, P)); mark("k_solid_b");
         if (c.p.jc_surrogate && P.jc.count) {
             const int tiles = (n + kMlpTileRows - 1) / kMlpTileRows;
             const int g = std::min(kMlpCtasPerSm * 148, std::max(tiles, 1));
@@ -1582,14 +1588,17 @@ inline int solid_substep_launch(const Cst& c, const Ptr& P, int n, cudaStream_t 
     if (in(SPH_STAGE_FORCES)) {
         const bool visc = c.p.q_l2 > 0.0f || c.p.av_alpha > 0.0f || c.p.av_beta > 0.0f;
         if (c.p.axisymmetric) {
-            if (visc) k_solid_force<true, true, false><<<nb, bs, 0, st>>>(c, P);
-            else k_solid_force<false, true, false><<<nb, bs, 0, st>>>(c, P);
-        } else if (plain_shape(c)) {
-            if (visc) k_solid_force<true, false, true><<<nb, bs, 0, st>>>(c, P);
-            else k_solid_force<false, false, true><<<nb, bs, 0, st>>>(c, P);
+            if (visc) k_solid_force<true, true, 0><<<nb, bs, 0, st>>>(c, P);
+            else k_solid_force<false, true, 0><<<nb, bs, 0, st>>>(c, P);
+        } else if (shape_of(c) == 2) {
+            if (visc) k_solid_force<true, false, 2><<<nb, bs, 0, st>>>(c, P);
+            else k_solid_force<false, false, 2><<<nb, bs, 0, st>>>(c, P);
+        } else if (shape_of(c) == 1) {
+            if (visc) k_solid_force<true, false, 1><<<nb, bs, 0, st>>>(c, P);
+            else k_solid_force<false, false, 1><<<nb, bs, 0, st>>>(c, P);
         } else {
-            if (visc) k_solid_force<true, false, false><<<nb, bs, 0, st>>>(c, P);
-            else k_solid_force<false, false, false><<<nb, bs, 0, st>>>(c, P);
+            if (visc) k_solid_force<true, false, 0><<<nb, bs, 0, st>>>(c, P);
+            else k_solid_force<false, false, 0><<<nb, bs, 0, st>>>(c, P);
         }
         mark("k_solid_force");
     }
@@ -1597,9 +1606,9 @@ inline int solid_substep_launch(const Cst& c, const Ptr& P, int n, cudaStream_t 
     if (in(SPH_STAGE_ADVECT)) {
         if (c.p.hourglass_sts && c.p.hourglass_alpha > 0.0f) {
             k_half_kick<<<nb, bs, 0, st>>>(c, P); mark("k_half_kick");
-            if (c.p.hg_sts_refresh) { SHAPED(plain_shape(c), k_gradv, <<<nb, bs, 0, st>>>(c, P)); mark("k_gradv"); }
+            if (c.p.hg_sts_refresh) { SHAPED(shape_of(c), k_gradv, <<<nb, bs, 0, st>>>(c, P)); mark("k_gradv"); }
             for (int s = 0; s < kStsMaxStages; ++s) {
-                SHAPED(plain_shape(c), k_hg_stage, <<<nb, bs, 0, st>>>(c, P, s));
+                SHAPED(shape_of(c), k_hg_stage, <<<nb, bs, 0, st>>>(c, P, s));
                 mark("k_hg_stage");
             }
             k_sts_finish<<<nb, bs, 0, st>>>(c, P); mark("k_sts_finish");
@@ -1609,7 +1618,7 @@ inline int solid_substep_launch(const Cst& c, const Ptr& P, int n, cudaStream_t 
         k_constraints<<<nb, bs, 0, st>>>(c, P); mark("k_constraints");
     }
     if (in(SPH_STAGE_PST) && c.p.pst_enabled) {
-        SHAPED(plain_shape(c), k_pst, <<<nb, bs, 0, st>>>(c, P)); mark("k_pst");
+        SHAPED(shape_of(c), k_pst, <<<nb, bs, 0, st>>>(c, P)); mark("k_pst");
         k_finish<<<nb, bs, 0, st>>>(c, P, last_stage >= SPH_STAGE_BOUNDARY ? 3 : 1); mark("k_finish");
     } else if (in(SPH_STAGE_BOUNDARY)) {
         k_finish<<<nb, bs, 0, st>>>(c, P, 2); mark("k_finish");
