@@ -104,13 +104,14 @@ def load_peaks():
 
 # DRAM bytes per particle of one launch of the dominant kernels (ncu dram__bytes_read.sum
 # + dram__bytes_write.sum over the particles of the captured case, in the workload's own
-# configuration at 256k particles: a --set full capture at full size is too large to run
-# safely).  The traffic of these kernels grows in proportion to the particles, so the line
+# configuration at 256k (dam break) and 219k (bar) particles: a --set full capture at full
+# size is too large to run safely).  The traffic of these kernels grows in proportion to the particles, so the line
 # scales them by the particle count.  Measured with the commands recorded beside the
 # figures under profiles/.
 NCU_DRAM_BYTES_PER_PARTICLE = {
-    "dambreak3d": {},
-    "tensile_bar3d": {},
+    "dambreak3d": {"k_pst": 425.3, "k_force": 421.8, "k_lamgrad_cont": 443.3, "k_lam": 354.8,
+                   "k_nbr_filter": 230.3},
+    "tensile_bar3d": {"k_solid_force": 559.6, "k_solid_b": 678.6, "k_solid_a": 542.3, "k_pst": 630.5},
 }
 
 
@@ -522,8 +523,10 @@ def main():
                 "unit": "GB/s", "frac": achieved / peak, "peak_source": peak_kind,
                 "algorithmic_bytes_per_particle": ALGO_BYTES[dom],
                 "launch_ms": dom_ms, "traffic": traffic,
-                "traffic_source": ("ncu dram__bytes_read.sum + dram__bytes_write.sum of a launch at "
-                                   "256k particles, scaled by the particle count") if traffic else None}
+                "traffic_source": ("ncu dram__bytes_read.sum + dram__bytes_write.sum of one launch of "
+                                   "the same kernel on the same workload at %s particles, scaled by "
+                                   "the particle count" % ("256,000" if tag == "dambreak3d" else "218,573"))
+                                  if traffic else None}
     import ctypes as C
     fma = C.c_double(0.0)
     abi.check(abi.lib().sph_fma_peak(C.byref(fma), None), "sph_fma_peak")
