@@ -12,9 +12,16 @@ what differs between them is arithmetic.  Checked every 100 steps:
     both relative to |pe(0)| (the column's potential energy, the budget's largest term);
   * linear momentum (gravity and the walls change it; the three runs must agree);
   * x (over dx0), v, V and p, field-wide and per particle (floor 1% of the largest).
-The GPU must stay within 4x the FP32 oracle's distance to FP64 (plus a floor).  With
-SPH_DRIFT_REPORT set, the table is written there as JSON.
+Until the column's front reaches the far wall and splashes (step ~300 here) the flow is
+smooth and the two float32 runs stay equally close to FP64: every row of the GPU must be
+within 2x the FP32 oracle's distance (plus a floor).  After it the flow is chaotic: each
+float32 run leaves the FP64 trajectory along its own path and a single row's distance
+fluctuates by several times between rows (momentum: 5.5e-5, 8.4e-5, 3.0e-5, 2.4e-5 for the
+FP32 oracle at steps 700-1000 of one run), so the GPU's largest distance over the run must
+stay within 4x the FP32 oracle's largest (plus a floor).  With SPH_DRIFT_REPORT set, the
+table is written there as JSON.
 """
+SMOOTH_UNTIL = 300
 import json
 import os
 
@@ -120,9 +127,15 @@ def test_dambreak_128k_drift_against_fp64(cuda):
         with open(out, "w") as f:
             json.dump({"scene": "3D dam break", "dx_m": DX_128K, "particles": n, "steps": STEPS,
                        "E_ref": e_ref, "rows": rows}, f, indent=1)
-    last = rows[-1]
-    assert abs(last["E_bal_gpu_minus_fp64"]) <= 4.0 * abs(last["E_bal_fp32_minus_fp64"]) + 1e-6, last
-    assert last["P_gpu_minus_fp64"] <= 4.0 * last["P_fp32_minus_fp64"] + 1e-6, last
-    for key in keys:
-        assert last["field_gpu"][key] <= 4.0 * last["field_fp32"][key] + 1e-5, (key, last)
+    def series(name, key=None):
+        if key is None:
+            return np.array([abs(r[name]) for r in rows])
+        return np.array([r[name][key] for r in rows])
+    smooth = np.array([r["step"] <= SMOOTH_UNTIL for r in rows])
+    checks = [("E_bal", series("E_bal_gpu_minus_fp64"), series("E_bal_fp32_minus_fp64"), 1e-7),
+              ("P", series("P_gpu_minus_fp64"), series("P_fp32_minus_fp64"), 1e-6)]
+    checks += [(key, series("field_gpu", key), series("field_fp32", key), 1e-5) for key in keys]
+    for name, g_d, f_d, floor in checks:
+        assert np.all(g_d[smooth] <= 2.0 * f_d[smooth] + floor), (name, g_d[smooth], f_d[smooth])
+        assert g_d.max() <= 4.0 * f_d.max() + floor, (name, g_d, f_d)
     assert solver.error_word() & ~0x2 == 0
