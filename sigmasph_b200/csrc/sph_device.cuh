@@ -61,6 +61,7 @@ struct GridLayout {
     int cmax[3];
     int bits[3];       // Morton bits per axis (dense mode)
     int total_bits;
+    unsigned mask[3];  // the key bits each axis occupies (dense mode)
 };
 
 // Device copy of SphScalars (identical layout, so one memcpy returns it).
@@ -238,17 +239,19 @@ __device__ __forceinline__ int hash_cell(int cx, int cy, int cz, int mcap) {
 
 // Compact Morton code of a cell offset inside the occupied box: bits are interleaved
 // from the least significant end, x then y then z, each axis contributing only the
-// bits its extent needs.
+// bits its extent needs.  The key is the OR of the three axes' dilated offsets: each
+// offset's bits deposited, lowest first, at the key bits its axis occupies (mask[a]).
+__device__ __forceinline__ unsigned dilate(unsigned v, unsigned mask) {
+    unsigned r = 0u;
+    for (unsigned m = mask; m != 0u && v != 0u; m &= m - 1u, v >>= 1) r |= (v & 1u) ? (m & (0u - m)) : 0u;
+    return r;
+}
+// The dilated offset one step further along the same axis: the carry skips the other
+// axes' bits (which the OR with ~mask fills).
+__device__ __forceinline__ unsigned dilated_next(unsigned d, unsigned mask) { return ((d | ~mask) + 1u) & mask; }
 __device__ __forceinline__ int morton_key(int ox, int oy, int oz, const GridLayout& L) {
-    unsigned key = 0;
-    int pos = 0;
-    int nb = max(L.bits[0], max(L.bits[1], L.bits[2]));
-    for (int b = 0; b < nb; ++b) {
-        if (b < L.bits[0]) { key |= ((unsigned)(ox >> b) & 1u) << pos; ++pos; }
-        if (b < L.bits[1]) { key |= ((unsigned)(oy >> b) & 1u) << pos; ++pos; }
-        if (b < L.bits[2]) { key |= ((unsigned)(oz >> b) & 1u) << pos; ++pos; }
-    }
-    return (int)key;
+    return (int)(dilate((unsigned)ox, L.mask[0]) | dilate((unsigned)oy, L.mask[1]) |
+                 dilate((unsigned)oz, L.mask[2]));
 }
 
 // Bucket of a cell, or -1 if no particle can be binned there (outside the dense box).

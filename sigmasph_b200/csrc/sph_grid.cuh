@@ -158,6 +158,17 @@ __global__ void k_layout(Cst c, Ptr P) {
         tb += b;
     }
     L.total_bits = tb;
+    {
+        // the key bits of each axis: x, y, z in turn from the least significant end,
+        // each while it has bits left
+        unsigned m[3] = {0u, 0u, 0u};
+        int pos = 0;
+        const int nb = max(L.bits[0], max(L.bits[1], L.bits[2]));
+        for (int b = 0; b < nb && pos < 32; ++b)
+            for (int a = 0; a < 3; ++a)
+                if (b < L.bits[a] && pos < 32) m[a] |= 1u << pos++;
+        for (int a = 0; a < 3; ++a) L.mask[a] = m[a];
+    }
     if (tb <= c.mcap_log2) {
         L.mode = 0;
         L.nbuckets = 1 << tb;
@@ -392,9 +403,7 @@ __device__ __forceinline__ void sweep_coarse(const Cst& c, const Ptr& P, const G
                                              float d2cut, float hcut, F&& f) {
     const float4* __restrict__ pos = reinterpret_cast<const float4*>(P.cur.pos);
     const bool hashed = L.mode != 0;
-    auto cell = [&](int mir, F3 xs, int nx, int ny, int nz) {
-        const int b = bucket_of(nx, ny, nz, L, c.mcap);
-        if (b < 0) return;
+    auto cell_b = [&](int mir, F3 xs, int b, int nx, int ny, int nz) {
         bucket_candidates(P, hashed, b, nx, ny, nz, [&](int j) {
             if (mir == 0 && j == self_idx) return;
             const float4 pj = __ldg(pos + j);
@@ -402,12 +411,40 @@ __device__ __forceinline__ void sweep_coarse(const Cst& c, const Ptr& P, const G
             if (d2 < d2cut) f(j, mir, pj, d2);
         });
     };
+    auto cell = [&](int mir, F3 xs, int nx, int ny, int nz) {
+        const int b = bucket_of(nx, ny, nz, L, c.mcap);
+        if (b >= 0) cell_b(mir, xs, b, nx, ny, nz);
+    };
+    if (!hashed) {
+        // the real sweep over the dense table, in the same cell order: x and y dilated once
+        // per row, z stepped with dilated_next along the row
+        const int z_lo = max(bz - w, L.cmin[2]), z_hi = min(bz + w, L.cmax[2]);
 #pragma unroll 1
-    for (int o0 = -w; o0 <= w; ++o0)
+        for (int o0 = -w; o0 <= w; ++o0) {
+            const int nx = bx + o0;
+            if (nx < L.cmin[0] || nx > L.cmax[0]) continue;
+            const unsigned kx = dilate((unsigned)(nx - L.cmin[0]), L.mask[0]);
 #pragma unroll 1
-        for (int o1 = -w; o1 <= w; ++o1)
+            for (int o1 = -w; o1 <= w; ++o1) {
+                const int ny = by + o1;
+                if (ny < L.cmin[1] || ny > L.cmax[1] || z_lo > z_hi) continue;
+                const unsigned kxy = kx | dilate((unsigned)(ny - L.cmin[1]), L.mask[1]);
+                unsigned kz = dilate((unsigned)(z_lo - L.cmin[2]), L.mask[2]);
 #pragma unroll 1
-            for (int o2 = -w; o2 <= w; ++o2) cell(0, xq, bx + o0, by + o1, bz + o2);
+                for (int nz = z_lo; nz <= z_hi; ++nz) {
+                    cell_b(0, xq, (int)(kxy | kz), nx, ny, nz);
+                    kz = dilated_next(kz, L.mask[2]);
+                }
+            }
+        }
+    } else {
+#pragma unroll 1
+        for (int o0 = -w; o0 <= w; ++o0)
+#pragma unroll 1
+            for (int o1 = -w; o1 <= w; ++o1)
+#pragma unroll 1
+                for (int o2 = -w; o2 <= w; ++o2) cell(0, xq, bx + o0, by + o1, bz + o2);
+    }
     const bool my = c.mirror_y && xq.y < hcut, mz = c.mirror_z && xq.z < hcut;
     if (my) {
         const F3 xm = mirror3(1, xq);
@@ -553,7 +590,6 @@ __device__ __forceinline__ void stale_search(const Cst& c, const Ptr& P, int i, 
 template <int kShape>
 __global__ void SPH_BOUNDS(SPH_OCC_FILTER) k_nbr_filter(Cst c, Ptr P) {
     using S = Shape<kShape>;
-    constexpr bool kPlain = S::kPlain;
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= c.n) return;
     const int vc = __ldg(P.vl_cnt + i);
