@@ -25,9 +25,9 @@ traffic), `step_roofline` (the whole step's algorithmic bytes), `fp32_bound` (th
 estimated FP32 work against the FP32 FMA peak that `sph_fma_peak` measures on the same
 GPU), `kernel_ms_per_step` (CUDA events around every kernel of eager steps on a copy of
 the workload warmed up the same way: the same steps of the simulation as the timed
-window), `neighbour_lists` (list builds among the timed steps), `steady_state` (a longer
-window after the timed one, where the flow is faster and the lists are built more often:
-the build cost amortised), `drift` (the energy balance over the timed window from the
+window), `neighbour_lists` (list builds among the timed steps), `steady_state` (200 steps
+from step 400 on, or right after the timed window if that ends later: the flow is faster
+there and the lists are built more often, so the build cost is amortised), `drift` (the energy balance over the timed window from the
 library's FP64 reductions) and `clocks`.
 
 Under torchrun (N > 1) every rank runs an independent replica of a single scene (it does
@@ -370,6 +370,8 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--profile-steps", type=int, default=0,
                     help="eager profiled steps (0: as many as the timed window)")
+    ap.add_argument("--steady-after", type=int, default=400,
+                    help="the steady window starts at this step (or after the timed one)")
     ap.add_argument("--steady-steps", type=int, default=200,
                     help="a longer window after the timed one, for the amortised build cost")
     args = ap.parse_args()
@@ -444,11 +446,16 @@ def main():
 
     # ---------------------------------------------------------------- steady state
     # The window above starts right after the warm-up, while the flow is slow and the
-    # candidate lists are rarely built; a longer window after it shows the build cost
-    # amortised at the rate the flow sets later on.
+    # candidate lists are rarely built; a window that starts at step --steady-after (or
+    # right after the timed one, if later) shows the build cost amortised at the rate the
+    # flow sets later on.
     Ks = args.steady_steps
     steady = None
     if Ks > 0:
+        done = W + K
+        if args.steady_after > done:
+            solver.step_many(args.steady_after - done)
+            done = args.steady_after
         solver.list_stats(reset=True)
         rep.barrier()
         torch.cuda.synchronize()
@@ -458,7 +465,7 @@ def main():
         torch.cuda.synchronize()
         ms_s = rep.max_over_ranks(e0.elapsed_time(e1))
         ls = solver.list_stats()
-        steady = {"steps": Ks, "after_steps": W + K, "builds": ls["builds"],
+        steady = {"steps": Ks, "after_steps": done, "builds": ls["builds"],
                   "ms_per_step": ms_s / Ks, "value": rep.throughput(n * Ks, ms_s / 1000.0),
                   "unit": UNIT}
 
