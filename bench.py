@@ -21,7 +21,9 @@ packed ensembles.
 
 Besides `value` and `e2e`, the line carries `roofline` (the dominant kernel's algorithmic
 bytes over its event-timed launch, against the measured HBM copy peak, with its ncu DRAM
-traffic), `step_roofline` (the whole step's algorithmic bytes), `fp32_bound` (the step's
+traffic), `issue_roofline` (the same kernel's warp instructions, from ncu, over its launch
+against the GPU's instruction issue rate: the bound the pair passes sit at),
+`step_roofline` (the whole step's algorithmic bytes), `fp32_bound` (the step's
 estimated FP32 work against the FP32 FMA peak that `sph_fma_peak` measures on the same
 GPU), `kernel_ms_per_step` (CUDA events around every kernel of eager steps on a copy of
 the workload warmed up the same way: the same steps of the simulation as the timed
@@ -112,6 +114,17 @@ NCU_DRAM_BYTES_PER_PARTICLE = {
     "dambreak3d": {"k_pst": 425.3, "k_force": 421.8, "k_lamgrad_cont": 443.3, "k_lam": 354.8,
                    "k_nbr_filter": 230.3},
     "tensile_bar3d": {"k_solid_force": 559.6, "k_solid_b": 678.6, "k_solid_a": 542.3, "k_pst": 630.5},
+}
+
+
+# Warp instructions per particle of one launch (ncu smsp__inst_executed.sum over the
+# particles of the same captures).  The pair passes are bound by instruction issue, not by
+# DRAM: the issue roofline is the GPU's SMs x 4 schedulers x one warp instruction per
+# cycle at the clock sampled during the timed window.
+NCU_WARP_INST_PER_PARTICLE = {
+    "dambreak3d": {"k_pst": 337.4, "k_force": 341.7, "k_lamgrad_cont": 292.6, "k_lam": 127.7,
+                   "k_nbr_filter": 114.2},
+    "tensile_bar3d": {"k_solid_force": 593.8, "k_solid_b": 391.0, "k_solid_a": 372.5, "k_pst": 347.6},
 }
 
 
@@ -546,6 +559,21 @@ def main():
                                    "the same kernel on the same workload at %s particles, scaled by "
                                    "the particle count" % ("256,000" if tag == "dambreak3d" else "218,573"))
                                   if traffic else None}
+    issue_roofline = None
+    wi = NCU_WARP_INST_PER_PARTICLE.get(tag, {}).get(dom)
+    if wi is not None:
+        sms = torch.cuda.get_device_properties(local).multi_processor_count
+        mhz = (ck or {}).get("sm_mhz") or (ck or {}).get("sm_max_mhz")
+        if mhz:
+            peak_i = sms * 4 * mhz * 1e6
+            ach_i = wi * n / (dom_ms / 1000.0)
+            issue_roofline = {"bound": "issue", "kernel": dom, "achieved": ach_i, "peak": peak_i,
+                              "unit": "warp-instructions/s", "frac": ach_i / peak_i,
+                              "warp_instructions_per_particle": wi,
+                              "peak_source": "%d SMs x 4 schedulers x the sampled %g MHz" % (sms, mhz),
+                              "source": "ncu smsp__inst_executed.sum of one launch on the same workload "
+                                        "at %s particles, scaled by the particle count"
+                                        % ("256,000" if tag == "dambreak3d" else "218,573")}
     import ctypes as C
     fma = C.c_double(0.0)
     abi.check(abi.lib().sph_fma_peak(C.byref(fma), None), "sph_fma_peak")
@@ -573,7 +601,8 @@ def main():
                                     "shift_searches": lists["shift_searches"]},
                 "steady_state": steady, "drift": drift,
                 "kernel_profile_window": f"{Kp} eager steps, the same steps of the simulation as the timed window",
-                "roofline": roofline, "step_roofline": step_roofline, "fp32_bound": fp32_bound,
+                "roofline": roofline, "issue_roofline": issue_roofline,
+                "step_roofline": step_roofline, "fp32_bound": fp32_bound,
                 "kernel_ms_per_step": {k: round(v, 5) for k, v in sorted(per_step_ms.items(),
                                                                        key=lambda t: -t[1])},
                 "error_word": err}
