@@ -363,7 +363,9 @@ __device__ __forceinline__ float mw_of(float m, float4 pos, const Cst& c) {
 //  2  plain and standard: also every term of the default step on -- delta+-SPH with the
 //     shift, its ALE terms, the gradient-lambda surface normal, delta diffusion and the dt
 //     pair limit; for a solid also one material, the in-loop hourglass damper, Morris
-//     viscosity, plasticity and the ALE transport of the history and of e -- no ensemble.
+//     viscosity, plasticity and the ALE transport of the history and of e -- no ensemble;
+//  3  plain 2D: a single-layer (plane-strain or 2D) deck with no mirror plane and no
+//     axisymmetry (the strip ensembles).
 // A uniform switch inside a pair loop costs issue slots and splits the loop body the
 // compiler schedules; the dam break and the round bar run instance 2.
 __host__ __device__ __forceinline__ bool plain_shape(const Cst& c) {
@@ -378,13 +380,16 @@ __host__ __device__ __forceinline__ bool std_form(const Cst& c) {
     return fluid && p.hourglass_alpha > 0.0f && !p.hourglass_sts && p.viscosity > 0.0f && c.one_material &&
            c.any_plastic && p.ale_history && p.transport_e && p.ale_diffusion > 0.0f;
 }
+__host__ __device__ __forceinline__ bool plain2d_shape(const Cst& c) {
+    return !c.mirror_y && !c.mirror_z && !c.p.axisymmetric && c.p.two_d;
+}
 __host__ __device__ __forceinline__ int shape_of(const Cst& c) {
-    return plain_shape(c) ? (std_form(c) ? 2 : 1) : 0;
+    return plain_shape(c) ? (std_form(c) ? 2 : 1) : (plain2d_shape(c) ? 3 : 0);
 }
 template <int kShape>
 struct Shape {
-    static constexpr bool kPlain = kShape >= 1, kStd = kShape == 2;
-    __device__ static __forceinline__ bool two_d(const Cst& c) { return !kPlain && c.p.two_d; }
+    static constexpr bool kPlain = kShape >= 1, kStd = kShape == 2, k2D = kShape == 3;
+    __device__ static __forceinline__ bool two_d(const Cst& c) { return k2D || (!kPlain && c.p.two_d); }
     __device__ static __forceinline__ bool axi(const Cst& c) { return !kPlain && c.p.axisymmetric; }
     __device__ static __forceinline__ float w(float4 pos, const Cst& c) { return kPlain ? pos.w : w_of(pos, c); }
     __device__ static __forceinline__ float mw(float m, float4 pos, const Cst& c) {
@@ -421,6 +426,7 @@ struct Shape {
         const int shape_ = (shape);                  \
         if (shape_ == 2) kernel<2> __VA_ARGS__;      \
         else if (shape_ == 1) kernel<1> __VA_ARGS__; \
+        else if (shape_ == 3) kernel<3> __VA_ARGS__; \
         else kernel<0> __VA_ARGS__;                  \
     } while (0)
 
