@@ -241,6 +241,7 @@ __global__ void SPH_BOUNDS(SPH_OCC_FORCE) k_force(Cst c, Ptr P) {
         const bool ale = S::ale_mom(c);
         const float eps_rho = 1e-3f * c.p.density0;
         const float inv_mw_i = 1.0f / mw_i, inv_rho_i = 1.0f / rho_i, inv_dt = 1.0f / dt;
+        const float inv_rho_dt = inv_rho_i * inv_dt;
         const float wi_mw = w_i * inv_mw_i;
         float cl = c.p.c_signal * c.p.c_signal;
         F3 a = {0, 0, 0};
@@ -270,10 +271,15 @@ __global__ void SPH_BOUNDS(SPH_OCC_FORCE) k_force(Cst c, Ptr P) {
             if (ale) {
                 // the ALE momentum term w_j [div(rho v du) - v_i div(rho du)] / rho_i
                 // (DSPH.py:1630-1640), whose rho_i du_i parts cancel:
-                // w_j rho_j (du_j . gW) (v_j - v_i) / rho_i
-                F3 du_j = {sj.x * inv_dt, sj.y * inv_dt, sj.z * inv_dt};
-                if (mir) du_j = mirror3(mir, du_j);
-                a += (-(w_j * inv_rho_i) * (rho_j * dot3(du_j, g))) * vij;
+                // w_j rho_j (du_j . gW) (v_j - v_i) / rho_i; with w_j = V_j (plain decks)
+                // w_j rho_j is the mass m_j, and du_j = shift_j / dt
+                if (kPlain) {
+                    a += (-(vj4.w * inv_rho_dt) * dot3(f3(sj), g)) * vij;
+                } else {
+                    F3 du_j = {sj.x * inv_dt, sj.y * inv_dt, sj.z * inv_dt};
+                    if (mir) du_j = mirror3(mir, du_j);
+                    a += (-(w_j * inv_rho_i) * (rho_j * dot3(du_j, g))) * vij;
+                }
             }
             if (S::dt_pairs(c) && fabsf(rho_i - rho_j) > eps_rho * (1.0f - 1e-2f)) {
                 float drho = fabsf(rho_i - vj4.w / pj.w);   // exact, as the reference's test
@@ -439,8 +445,9 @@ __device__ __forceinline__ void for_each_pst_neighbour(const Cst& c, const Ptr& 
 // The disorder sum's pair term from the shift pass's own test: the mirrored position xj and
 // the squared separation d2 the neighbour test formed.  Arithmetic of pst_pair_term below.
 // kForm 1 (Sun) and 2 (Colle) fix the deck's exponent n = 4 with W(dx0) > 0 when the pass
-// is compiled; kForm 0 reads the form, n and W(dx0) from the parameters.
-constexpr int kPstAny = 0, kPstSun4 = 1, kPstColle4 = 2;
+// is compiled, 3 is Sun's with every particle of mass m_u; kForm 0 reads the form, n and
+// W(dx0) from the parameters.
+constexpr int kPstAny = 0, kPstSun4 = 1, kPstColle4 = 2, kPstSun4Uni = 3;
 template <bool kPlain, int kForm>
 __device__ __forceinline__ F3 pst_term_d2(const Cst& c, const float4* __restrict__ vel, F3 xi, float rho_i,
                                           float inv_Wd, int j, float4 pj, F3 xj, float d2, bool m_uni,
@@ -459,7 +466,7 @@ __device__ __forceinline__ F3 pst_term_d2(const Cst& c, const float4* __restrict
         const float Vj = Shape<kPlain ? 1 : 0>::w(pj, c);
         if (Vj > 1e-30f) return ((1.0f + f) * Vj) * g;
     } else {
-        const float mj_raw = m_uni ? m_u : __ldg(&vel[j].w);
+        const float mj_raw = (kForm == kPstSun4Uni || m_uni) ? m_u : __ldg(&vel[j].w);
         const float mj = Shape<kPlain ? 1 : 0>::mw(mj_raw, pj, c);
         if (mj > 1e-10f) {
             // m_j / mean rho: a sum of densities, rounded quotients suffice (no cancellation)
@@ -556,11 +563,13 @@ __global__ void SPH_BOUNDS(SPH_OCC_PST) k_pst(Cst c, Ptr P) {
                 sr += pst_term_d2<kPlain, kForm>(c, vel, xi, rho_i, inv_Wd, j, pj, xj, d2, m_uni, m_u);
             });
         };
-        if (c.W_dx0 > 1e-10f && c.p.pst_n == 4)
-            c.p.pst_colle ? walk(std::integral_constant<int, kPstColle4>())
-                          : walk(std::integral_constant<int, kPstSun4>());
-        else
+        if (c.W_dx0 > 1e-10f && c.p.pst_n == 4) {
+            if (c.p.pst_colle) walk(std::integral_constant<int, kPstColle4>());
+            else if (m_uni) walk(std::integral_constant<int, kPstSun4Uni>());
+            else walk(std::integral_constant<int, kPstSun4>());
+        } else {
             walk(std::integral_constant<int, kPstAny>());
+        }
     }
     float4 vi4 = vel[i];
     F3 vi = f3(vi4);
