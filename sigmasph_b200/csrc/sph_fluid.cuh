@@ -552,7 +552,7 @@ __global__ void SPH_BOUNDS(SPH_OCC_PST) k_pst(Cst c, Ptr P) {
     const float rho_i = m_i / pi.w;
     {
         const float inv_Wd = c.W_dx0 > 0.0f ? 1.0f / c.W_dx0 : 0.0f;
-        // filled by this step's fluid advect; a solid step leaves them unequal
+        // filled by this step's fluid advect (a solid's: by k_solid_a)
         const unsigned int mlo = P.ac->m_min_bits;
         const bool m_uni = !c.p.pst_colle && mlo == P.ac->m_max_bits;
         const float m_u = __uint_as_float(mlo);

@@ -423,6 +423,7 @@ __global__ void SPH_BOUNDS(SPH_OCC_SOLID_A) k_solid_a(Cst c, Ptr P) {
     constexpr bool kPlain = S::kPlain;
     int i = blockIdx.x * blockDim.x + threadIdx.x;
     double wdiff = 0.0;
+    unsigned int mlo = 0xffffffffu, mhi = 0u;   // this particle's mass bits, for the range
     if (i < c.n) {
         const float4* __restrict__ pos = as4c(P.cur.pos);
         const float4* __restrict__ vel = as4c(P.cur.vel);
@@ -430,6 +431,7 @@ __global__ void SPH_BOUNDS(SPH_OCC_SOLID_A) k_solid_a(Cst c, Ptr P) {
         const float* __restrict__ lam = P.lam;
         float4 pi = pos[i], vi4 = vel[i];
         F3 xi = f3(pi), vi = f3(vi4);
+        mlo = mhi = __float_as_uint(vi4.w);
         float4 l0 = P.lsym[2 * i], l1 = P.lsym[2 * i + 1];
         const float L00 = l0.x, L11 = l0.y, L22 = l0.z, L01 = l0.w, L02 = l1.x, L12 = l1.y;
         const float lam_i = lam[i];
@@ -495,6 +497,9 @@ __global__ void SPH_BOUNDS(SPH_OCC_SOLID_A) k_solid_a(Cst c, Ptr P) {
         grad_v_finish<NoExtra>(c, P, i, G, pi, vi.y);
     }
     block_sum_atomic(wdiff, &P.ac->w_diff_step);
+    // the range of this step's masses (equal bits: every particle has that mass), for the
+    // stress pass's sweep
+    block_minmax_bits(mlo, mhi, &P.ac->m_min_bits, &P.ac->m_max_bits);
 }
 
 // ------------------------------------------------------------------ grad v alone (damper refresh)
@@ -676,9 +681,16 @@ __global__ void SPH_BOUNDS(SPH_OCC_SOLID_B) k_solid_b(Cst c, Ptr P) {
         const F3 du_i = {shi.x * inv_dt, shi.y * inv_dt, shi.z * inv_dt};
         Sym A = {0, 0, 0, 0, 0, 0};
         float dep = 0.0f, adv = 0.0f, dif = 0.0f;
-        if (ale) {
+        // one mass for every particle (k_solid_a recorded the range): the sweep reads no
+        // neighbour's velocity record, whose mass is all it needs
+        const unsigned int m_lo = P.ac->m_min_bits;
+        const bool m_uni = m_lo == P.ac->m_max_bits;
+        const float m_u = __uint_as_float(m_lo);
+        auto sweep = [&](auto uni) {
+            constexpr bool kUni = decltype(uni)::value;
             for_each_neighbour<kPlain>(c, P, i, [&](int j, int mir) {
-                float4 pj = __ldg(pos + j), vj4 = __ldg(vel + j), shj = __ldg(shf + j);
+                float4 pj = __ldg(pos + j), shj = __ldg(shf + j);
+                const float m_j = kUni ? m_u : __ldg(&vel[j].w);
                 F3 xj = f3(pj);
                 F3 du_j = {shj.x * inv_dt, shj.y * inv_dt, shj.z * inv_dt};
                 float epj;
@@ -688,7 +700,7 @@ __global__ void SPH_BOUNDS(SPH_OCC_SOLID_B) k_solid_b(Cst c, Ptr P) {
                 float rn2 = dot3(r, r), rn;
                 F3 g = wendland_dW2(r, rn2, rn, c);
                 // rho_j only in products and sums here: the rounded quotient (2 ulp) suffices
-                const float rho_j = __fdividef(vj4.w, pj.w);
+                const float rho_j = __fdividef(m_j, pj.w);
                 float wj = S::w(pj, c);
                 // w_j [(rho_j du_j . gW) phi_j - (rho_i du_i . gW) phi_i - phi_i div(rho du)]
                 // / rho_i (SOLID.py:1799-1862), whose rho_i du_i parts cancel:
@@ -713,6 +725,10 @@ __global__ void SPH_BOUNDS(SPH_OCC_SOLID_B) k_solid_b(Cst c, Ptr P) {
                     }
                 }
             });
+        };
+        if (ale) {
+            if (m_uni) sweep(std::true_type());
+            else sweep(std::false_type());
         }
         // update_stress (SOLID.py:2691-3004): Jaumann rate, trace-free symmetric update
         float Lg[3][3];
