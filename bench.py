@@ -111,9 +111,9 @@ def load_peaks():
 # scales them by the particle count.  Measured with the commands recorded beside the
 # figures under profiles/.
 NCU_DRAM_BYTES_PER_PARTICLE = {
-    "dambreak3d": {"k_pst": 425.3, "k_force": 421.8, "k_lamgrad_cont": 443.3, "k_lam": 354.8,
+    "dambreak3d": {"k_pst": 421.7, "k_force": 421.8, "k_lamgrad_cont": 443.3, "k_lam": 354.8,
                    "k_nbr_filter": 230.3},
-    "tensile_bar3d": {"k_solid_force": 559.6, "k_solid_b": 678.6, "k_solid_a": 542.3, "k_pst": 630.5},
+    "tensile_bar3d": {"k_solid_force": 559.6, "k_solid_b": 665.3, "k_solid_a": 542.3, "k_pst": 630.5},
 }
 
 
@@ -122,9 +122,9 @@ NCU_DRAM_BYTES_PER_PARTICLE = {
 # DRAM: the issue roofline is the GPU's SMs x 4 schedulers x one warp instruction per
 # cycle at the clock sampled during the timed window.
 NCU_WARP_INST_PER_PARTICLE = {
-    "dambreak3d": {"k_pst": 337.4, "k_force": 341.7, "k_lamgrad_cont": 292.6, "k_lam": 127.7,
+    "dambreak3d": {"k_pst": 326.0, "k_force": 341.7, "k_lamgrad_cont": 292.6, "k_lam": 127.7,
                    "k_nbr_filter": 114.2},
-    "tensile_bar3d": {"k_solid_force": 593.8, "k_solid_b": 391.0, "k_solid_a": 372.5, "k_pst": 347.6},
+    "tensile_bar3d": {"k_solid_force": 593.8, "k_solid_b": 386.8, "k_solid_a": 372.5, "k_pst": 347.6},
 }
 
 
