@@ -217,7 +217,7 @@ typedef struct SphScalars {
     float   max_v;            /* solver.max_v[None]                                      */
     int32_t off_grid_num;     /* ps.off_grid_num[None]                                   */
     int32_t err;              /* SPH_EW_* bits accumulated since the last reset           */
-    int32_t sts_stages;       /* last hourglass sub-cycle count                           */
+    int32_t sts_stages;       /* last hourglass sub-cycle count (ensembles: the largest)  */
     int32_t pad0;
     double  off_grid_mass;    /* ps.off_grid_mass[None]                                  */
     double  wall_work;        /* SPHBase.wall_work                                       */

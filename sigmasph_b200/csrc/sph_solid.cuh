@@ -258,7 +258,10 @@ __global__ void k_solid_load(Cst c, Ptr P) {
             S.max_c_sq_bits = __float_as_uint(cs * cs);
             S.max_accel_bits = __float_as_uint(1e-10f);
         }
-        if (blockIdx.x == 0 && threadIdx.x == 0 && P.jc.count) *P.jc.count = 0;
+        if (blockIdx.x == 0 && threadIdx.x == 0) {
+            if (P.jc.count) *P.jc.count = 0;
+            P.sc->sts_stages = 0;   // the largest instance's stage count, from k_solid_dt
+        }
         return;
     }
     if (threadIdx.x != 0 || blockIdx.x != 0) return;
@@ -1230,6 +1233,7 @@ __global__ void k_solid_dt(Cst c, Ptr P) {
             }
             S.dt = dt;
             S.sts_stages = s;
+            if (s > 0) atomicMax(&P.sc->sts_stages, s);
             for (int g = 0; g < 2; ++g)
                 for (int d = 0; d < 3; ++d) { S.constraint_force[g][d] = 0.0; S.constraint_disp[g][d] = 0.0; }
         }
@@ -1303,7 +1307,8 @@ template <int kShape>
 __global__ void __launch_bounds__(kBlock) k_hg_stage(Cst c, Ptr P, int stage) {
     using S = Shape<kShape>;
     constexpr bool kPlain = S::kPlain;
-    if (c.n_inst == 0 && stage >= P.sc->sts_stages) return;
+    // the stage count (an ensemble: its largest instance's) -- later stages return at once
+    if (stage >= P.sc->sts_stages) return;
     int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= c.n) return;
     const int ki = eos_of(P, i);
