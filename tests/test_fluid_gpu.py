@@ -533,3 +533,47 @@ def test_full_size_properties(cuda):
     assert np.isfinite(st["pos"]).all() and np.isfinite(st["vel"]).all()
     assert sv.compute_total_mass() == m0
     assert sv.error_word() & ~abi.EW_HASHED_GRID == 0
+
+
+def _linear_field_scene(n=8000):
+    sc = dambreak3d(dx=dx_for_particles(n), pst=False, viscosity=0.0)
+    sc["Load"]["gravitation"] = [0.0, 0.0, 0.0]
+    ps = ParticleSystem(SimConfig(sc), device="cuda")
+    x = ps.x.to_numpy().astype(np.float64)
+    h = float(ps.support_radius)
+    return ps, x, (x.min(0) + h, x.max(0) - h)
+
+
+def test_linear_fields_pin_the_gpu_pair_sums(cuda):
+    """The analytic identities tests/test_oracle.py checks on the oracle, on the CUDA path
+    itself: for v = A x the interior volumetric strain rate is -lambda tr(A), and for a
+    linear pressure p = p0 + G . x (set through the volumes) the interior pressure
+    acceleration is -lambda G / rho.  Float32 bounds: 1e-3 for the rate; 1e-2 for the
+    acceleration (the Tait EOS's (rho/rho0)^7 - 1 cancels to ~2e-3, and neighbour
+    pressure differences are ~3% of p)."""
+    ps, x, box = _linear_field_scene()
+    A = np.random.default_rng(3).normal(size=(3, 3)) * 0.1
+    ps.v.from_numpy((x @ A.T).astype(np.float32))
+    solver = ps.build_solver()
+    for s in (abi.STAGE_SORT, abi.STAGE_LAM, abi.STAGE_CONTINUITY):
+        solver.run_stage(s)
+    g = gpu_fields(ps)
+    inn = np.all((g["x"] > box[0]) & (g["x"] < box[1]), axis=1)
+    assert inn.sum() > 2000
+    want = -g["lam"][inn] * np.trace(A)
+    assert np.abs(g["divergence"][inn] - want).max() <= 1e-3 * np.abs(want).max()
+
+    ps, x, box = _linear_field_scene()
+    p = build_params(ps)
+    G = np.array([300.0, -200.0, 150.0])
+    pt = 20.0 - (x @ G).min() + x @ G
+    S, gam, rho0 = float(p.stiffness), float(p.exponent), float(p.density0)
+    m = ps.m.to_numpy().astype(np.float64)
+    ps.V.from_numpy((m / (rho0 * (1.0 + pt / S) ** (1.0 / gam))).astype(np.float32))
+    solver = ps.build_solver()
+    for s in (abi.STAGE_SORT, abi.STAGE_LAM, abi.STAGE_CONTINUITY, abi.STAGE_FORCES):
+        solver.run_stage(s)
+    g = gpu_fields(ps)
+    inn = np.all((g["x"] > box[0]) & (g["x"] < box[1]), axis=1)
+    want = -(g["lam"][:, None] * G[None, :]) / (g["m"] / g["V"])[:, None]
+    assert np.abs(g["acc"][inn] - want[inn]).max() <= 1e-2 * np.abs(want[inn]).max()

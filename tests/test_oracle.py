@@ -119,3 +119,86 @@ def test_fp32_oracle_tracks_fp64_oracle():
         s = o.get_state()
         res.append(s["x"][np.argsort(s["pid"])])
     assert np.abs(res[0] - res[1]).max() < 1e-6 * ps.particle_diameter * 100
+
+
+# ------------------------------------------------------------------ analytic identities
+# The oracle's pair sums restate the reference's kernel bodies; these identities pin them
+# to the physics they discretise, independently of the restatement: on a lattice interior
+# the kernel's first moment sum_j V_j (x_j - x_i) (x) grad W_ij is lambda I (lambda: the
+# lambda pass's value there, 0.979 at 2.6 dx in 3D), so a linear field's SPH derivative
+# is lambda times the exact one.
+
+def _linear_field_oracle(n=8000):
+    sc = dambreak3d(dx=dx_for_particles(n), pst=False, viscosity=0.0)
+    sc["Load"]["gravitation"] = [0.0, 0.0, 0.0]
+    ps = ParticleSystem(SimConfig(sc), device="cpu")
+    st = state_from_sets(ps.state_numpy())
+    x = st["x"].astype(np.float64)
+    h = float(ps.support_radius)
+    box = (x.min(0) + h, x.max(0) - h)
+    return ps, build_params(ps), st, x, box
+
+
+def _interior(x, box):
+    return np.all((x > box[0]) & (x < box[1]), axis=1)
+
+
+def test_continuity_of_a_linear_velocity_field():
+    """v = A x: the continuity pass's volumetric strain rate sum_j V_j (v_i - v_j) . grad W
+    (DSPH.py:1208-1338) is -lambda tr(A) in the interior (dV/dt = -V times it: a field
+    that spreads grows the volume)."""
+    ps, p, st, x, box = _linear_field_oracle()
+    A = np.random.default_rng(3).normal(size=(3, 3)) * 0.1
+    st["v"] = x @ A.T
+    o = Oracle(p, ps.particle_max_num, fp64=True)
+    o.set_state(st, 1e-4)
+    for s in (abi.STAGE_SORT, abi.STAGE_LAM, abi.STAGE_CONTINUITY):
+        o.stage(s)
+    g = o.get_state()
+    inn = _interior(g["x"], box)
+    assert inn.sum() > 2000
+    want = -g["lam"][inn] * np.trace(A)
+    assert np.abs(g["divergence"][inn] - want).max() <= 1e-4 * np.abs(want).max()
+    V0 = dict(zip(st["pid"], st["V"]))
+    V_before = np.array([V0[k] for k in g["pid"][inn]])
+    assert np.all(np.sign(g["V"][inn] - V_before) == np.sign(np.trace(A)))
+
+
+def test_pressure_acceleration_of_a_linear_pressure_field():
+    """p = p0 + G . x (set through the volumes, the Tait EOS inverted): the symmetric
+    pressure force -sum_j w_i w_j (p_i + p_j) grad W / mw_i (DSPH.py:1523-1560) is
+    -lambda G / rho in the interior.  The volumes' 1e-4 spread leaves a p_i sum_j V_j grad W
+    of ~6e-4 of the result."""
+    ps, p, st, x, box = _linear_field_oracle()
+    G = np.array([300.0, -200.0, 150.0])
+    pt = 20.0 - (x @ G).min() + x @ G
+    S, gam, rho0 = float(p.stiffness), float(p.exponent), float(p.density0)
+    st["V"] = st["m"] / (rho0 * (1.0 + pt / S) ** (1.0 / gam))
+    o = Oracle(p, ps.particle_max_num, fp64=True)
+    o.set_state(st, 1e-7)
+    for s in (abi.STAGE_SORT, abi.STAGE_LAM, abi.STAGE_CONTINUITY, abi.STAGE_FORCES):
+        o.stage(s)
+    g = o.get_state()
+    inn = _interior(g["x"], box)
+    want = -(g["lam"][:, None] * G[None, :]) / (g["m"] / g["V"])[:, None]
+    assert np.abs(g["acc"][inn] - want[inn]).max() <= 2e-3 * np.abs(want[inn]).max()
+
+
+def test_kernel_corrected_velocity_gradient_is_exact_for_linear_fields():
+    """Solver.kernelCorrection: grad v = sum_j V_j (v_j - v_i) (x) grad W times the FP64
+    regularised inverse of the moment (SOLID.py:1757-1771, spd_inverse.py:45-101) is
+    exact for v = A x at every particle, the free surface included (where the moment is
+    far from lambda I)."""
+    from tests.test_solid_gpu import bar3d_kc_deck
+    ps = ParticleSystem(SimConfig(bar3d_kc_deck()), device="cpu")
+    st = state_from_sets(ps.state_numpy())
+    A = np.random.default_rng(5).normal(size=(3, 3)) * 1e-3
+    st["v"] = st["x"].astype(np.float64) @ A.T
+    o = Oracle(build_params(ps), ps.particle_max_num, fp64=True)
+    o.set_state(st, 1e-6)
+    o.stage(abi.STAGE_SORT)
+    o.stage(abi.STAGE_LAM)
+    g = o.get_state()
+    assert g["lam"].min() < 0.3            # the surface and its edges are in the sample
+    G = g["grad_v"].reshape(-1, 3, 3)
+    assert np.abs(G - A[None]).max() <= 1e-12 * np.abs(A).max()

@@ -464,3 +464,19 @@ def test_solid_reductions_match_numpy(cuda):
     assert sv.compute_total_mass() == pytest.approx(m.sum(), rel=1e-6)
     P = sv.compute_momentum()
     assert np.abs(P - (m[:, None] * v).sum(0)).max() <= 1e-5 * (m[:, None] * np.abs(v)).sum()
+
+
+def test_kernel_corrected_gradient_is_exact_on_the_gpu(cuda):
+    """v = A x on the kernel-corrected bar: the CUDA path's grad v (float32 pair sums, the
+    FP64 regularised inverse) is A at every particle, the free surface included, to float32
+    rounding amplified by the inverse where lambda falls to ~0.2 (bound 1e-3 of |A|)."""
+    ps = ParticleSystem(SimConfig(bar3d_kc_deck()), device="cuda")
+    A = np.random.default_rng(5).normal(size=(3, 3)) * 1e-3
+    ps.v.from_numpy((ps.x.to_numpy().astype(np.float64) @ A.T).astype(np.float32))
+    solver = ps.build_solver()
+    solver.run_stage(abi.STAGE_SORT)
+    solver.run_stage(abi.STAGE_LAM)
+    g = solid_gpu_fields(ps)
+    assert g["lam"].min() < 0.3
+    G = g["grad_v"].reshape(-1, 3, 3)
+    assert np.abs(G - A[None]).max() <= 1e-3 * np.abs(A).max()
