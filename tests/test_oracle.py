@@ -202,3 +202,28 @@ def test_kernel_corrected_velocity_gradient_is_exact_for_linear_fields():
     assert g["lam"].min() < 0.3            # the surface and its edges are in the sample
     G = g["grad_v"].reshape(-1, 3, 3)
     assert np.abs(G - A[None]).max() <= 1e-12 * np.abs(A).max()
+
+
+def test_morris_viscosity_vanishes_for_a_linear_velocity_field():
+    """The Morris viscous term 2 (dim + 2) nu sum_j w_j (v_ij . r_ij) / (|r_ij|^2 + eta^2)
+    grad W_ij (DSPH.py:1560-1600) discretises nu lap(v); lap(A x) = 0, and on a lattice
+    interior each pair's even (v_ij . r) against the odd grad W cancels with its mirror
+    neighbour: the interior acceleration vanishes (to 1e-3 of nu |A| / dx, a single pair
+    term's scale; the float32 lattice positions are symmetric to ~1e-7)."""
+    sc = dambreak3d(dx=dx_for_particles(8000), pst=False, viscosity=1e-3)
+    sc["Load"]["gravitation"] = [0.0, 0.0, 0.0]
+    ps = ParticleSystem(SimConfig(sc), device="cpu")
+    p = build_params(ps)
+    st = state_from_sets(ps.state_numpy())
+    x = st["x"].astype(np.float64)
+    h, dx = float(ps.support_radius), float(ps.particle_diameter)
+    box = (x.min(0) + h, x.max(0) - h)
+    A = np.random.default_rng(3).normal(size=(3, 3)) * 0.1
+    st["v"] = x @ A.T
+    o = Oracle(p, ps.particle_max_num, fp64=True)
+    o.set_state(st, 1e-7)
+    for s in (abi.STAGE_SORT, abi.STAGE_LAM, abi.STAGE_CONTINUITY, abi.STAGE_FORCES):
+        o.stage(s)
+    g = o.get_state()
+    inn = _interior(g["x"], box)
+    assert np.abs(g["acc"][inn]).max() <= 1e-3 * float(p.viscosity) * np.abs(A).max() / dx
