@@ -367,3 +367,63 @@ def test_conservative_radial_form_closes_the_ring_power():
     reciprocal pairs)."""
     plain, radial = _axi_power_imbalance(False), _axi_power_imbalance(True)
     assert plain > 1e-3 and radial < 0.02 * plain, (plain, radial)
+
+
+# ------------------------------------------------------------------ analytic identities
+def _bar_after_forces(sc, v_of=None, s_of=None):
+    """The FP64 oracle's state after the sort, lambda / stress and force stages of one step
+    on the deck, with the velocity and deviatoric stress set from functions of position."""
+    ps = ParticleSystem(SimConfig(sc), device="cpu")
+    st = state_from_sets(ps.state_numpy())
+    x = st["x"].astype(np.float64)
+    if v_of is not None:
+        st["v"] = v_of(x)
+    if s_of is not None:
+        st["sdev"] = s_of(x)
+    o = Oracle(build_params(ps), ps.particle_max_num, fp64=True)
+    o.set_state(st, 1e-7)
+    for s in (abi.STAGE_SORT, abi.STAGE_LAM, abi.STAGE_CONTINUITY, abi.STAGE_FORCES):
+        o.stage(s)
+    g = o.get_state()
+    order = np.argsort(g["pid"])
+    return {k: (v[order] if hasattr(v, "shape") and v.shape and v.shape[0] == len(order) else v)
+            for k, v in g.items()}
+
+
+def test_hourglass_damper_does_not_resist_a_linear_deformation():
+    """The in-loop damper's pair term [(v_j - v_i) - <G> (x_j - x_i)] . rhat (SOLID.py:
+    3768-3816) measures the departure from the linear field the velocity gradient G
+    predicts ("dv_ij vanishes for any affine motion").  With the kernel-corrected G exact for v = A x, the term vanishes on every
+    pair, so switching the damper on changes no acceleration (to 1e-10 of its scale)."""
+    from tests.test_solid_gpu import bar3d_kc_deck
+    A = np.random.default_rng(5).normal(size=(3, 3)) * 1e-3
+    out = {}
+    for alpha in (4.0, 0.0):
+        sc = bar3d_kc_deck()
+        sc["Hourglass"] = dict(sc.get("Hourglass", {}), alpha=alpha)
+        out[alpha] = _bar_after_forces(sc, v_of=lambda x: x @ A.T)
+    scale = np.abs(out[0.0]["acc"]).max()
+    assert scale > 0.0
+    assert np.abs(out[4.0]["acc"] - out[0.0]["acc"]).max() <= 1e-10 * scale
+
+
+def test_stress_acceleration_of_a_linear_stress_field():
+    """A deviatoric stress linear in position (s_xx = -s_yy = c x, s_xy = b y; the density
+    at rho0, so p = 0; at rest, so no damper, viscosity or rate): the symmetric stress
+    force sum_j w_i w_j (s_i + s_j) . grad W / mw_i (SOLID.py:3545-3700) is
+    lambda div(s) / rho = lambda (b + c, 0, 0) / rho where the kernel's moment is lambda I
+    (the bar's interior, lambda at its plateau: to 5e-3, the moment's anisotropy there)."""
+    from tests.test_solid_gpu import bar3d_deck
+    b, c = 2e-3, 1e-3
+
+    def s_of(x):
+        s = np.zeros((len(x), 6))
+        s[:, 0], s[:, 1], s[:, 3] = c * x[:, 0], -c * x[:, 0], b * x[:, 1]
+        return s
+    sc = bar3d_deck()
+    sc["Solver"]["viscosity"] = 0.0
+    g = _bar_after_forces(sc, s_of=s_of)
+    inn = g["lam"] >= 0.9999
+    assert inn.sum() > 5000
+    want = g["lam"][:, None] * np.array([b + c, 0.0, 0.0])[None, :] / (g["m"] / g["V"])[:, None]
+    assert np.abs(g["acc"][inn] - want[inn]).max() <= 5e-3 * np.abs(want[inn]).max()
