@@ -227,3 +227,55 @@ def test_morris_viscosity_vanishes_for_a_linear_velocity_field():
     g = o.get_state()
     inn = _interior(g["x"], box)
     assert np.abs(g["acc"][inn]).max() <= 1e-3 * float(p.viscosity) * np.abs(A).max() / dx
+
+
+def test_delta_diffusion_of_linear_and_quadratic_densities():
+    """delta-SPH density diffusion delta h c0 sum_j V_j psi_ij . grad W / rho_i with
+    psi_ij = 2 (rho_j - rho_i)(-r_ij) / (|r_ij|^2 + eta^2) (DSPH.py:1269-1300, Molteni &
+    Colagrossi) discretises delta h c0 lap(rho) / rho: at rest it is the whole continuity
+    rate.  A linear density has no Laplacian and the interior rate vanishes (to 1e-3 of a
+    single pair term's scale delta h c0 |grad rho| / (rho dx)); a quadratic one,
+    rho = rho0 + a (y - y_mid)^2, gives a positive rate within 10% of delta h c0 2a / rho
+    (the lattice and the eta^2 regularisation take ~6%)."""
+    ps, p, st, x, box = _linear_field_oracle()
+    hdc = float(p.delta_sph) * float(ps.support_radius) * float(p.c0)
+    G = np.array([1.0, -0.5, 0.7])
+    for name, rho in (("linear", 1000.0 + x @ G),
+                      ("quadratic", 1000.0 + 50.0 * (x[:, 1] - x[:, 1].mean()) ** 2)):
+        s = dict(st)
+        s["V"] = st["m"] / rho
+        o = Oracle(p, ps.particle_max_num, fp64=True)
+        o.set_state(s, 1e-7)
+        for k in (abi.STAGE_SORT, abi.STAGE_LAM, abi.STAGE_CONTINUITY):
+            o.stage(k)
+        g = o.get_state()
+        inn = _interior(g["x"], box)
+        rate = g["divergence"][inn]
+        if name == "linear":
+            scale = hdc * np.abs(G).max() / 1000.0 / float(ps.particle_diameter)
+            assert np.abs(rate).max() <= 1e-3 * scale
+        else:
+            want = hdc * 100.0 / (g["m"][inn] / g["V"][inn])
+            assert np.all(rate > 0.9 * want) and np.all(rate < 1.0 * want)
+
+
+def test_shift_vanishes_on_an_undisturbed_lattice():
+    """The particle shift (Sun form, DSPH.py:712-1049) is driven by the kernel-weighted
+    disorder sum sum_j (1 + R (W / W(dx0))^n) m_j / rho_ij grad W, which the symmetric
+    lattice cancels: after one step of the column at rest without gravity, the interior
+    shift is zero (1e-12 of the spacing)."""
+    sc = dambreak3d(dx=dx_for_particles(8000), viscosity=0.0)
+    sc["Load"]["gravitation"] = [0.0, 0.0, 0.0]
+    ps = ParticleSystem(SimConfig(sc), device="cpu")
+    st = state_from_sets(ps.state_numpy())
+    x = st["x"].astype(np.float64)
+    h = float(ps.support_radius)
+    box = (x.min(0) + h, x.max(0) - h)
+    o = Oracle(build_params(ps), ps.particle_max_num, fp64=True)
+    o.set_state(st, 1e-4)
+    for k in range(8):
+        o.stage(k)
+    g = o.get_state()
+    inn = _interior(g["x"], box)
+    assert inn.sum() > 2000
+    assert np.abs(g["pst_shift"][inn]).max() <= 1e-12 * float(ps.particle_diameter)
