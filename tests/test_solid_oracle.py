@@ -427,3 +427,36 @@ def test_stress_acceleration_of_a_linear_stress_field():
     assert inn.sum() > 5000
     want = g["lam"][:, None] * np.array([b + c, 0.0, 0.0])[None, :] / (g["m"] / g["V"])[:, None]
     assert np.abs(g["acc"][inn] - want[inn]).max() <= 5e-3 * np.abs(want[inn]).max()
+
+
+def test_jaumann_update_only_rotates_under_a_rigid_spin():
+    """Objectivity of the Jaumann rate s_dot = 2 G dev(D) + W s - s W (SOLID.py:2691-2760):
+    under a rigid spin v = W x the strain rate D vanishes (the kernel-corrected gradient is
+    exact), so a uniform stress below yield is only rotated, s + dt (W s - s W), with no
+    plastic strain (to float64 rounding of the stress, 1e-12 of |s|: 1e-8 of the 4e-5
+    rotation)."""
+    from tests.test_solid_gpu import bar3d_kc_deck
+    sc = bar3d_kc_deck()
+    sc["Solver"]["viscosity"] = 0.0
+    ps = ParticleSystem(SimConfig(sc), device="cpu")
+    st = state_from_sets(ps.state_numpy())
+    x = st["x"].astype(np.float64)
+    w = np.array([0.3, -0.2, 0.5]) * 10.0
+    W = np.array([[0.0, -w[2], w[1]], [w[2], 0.0, -w[0]], [-w[1], w[0], 0.0]])
+    st["v"] = x @ W.T
+    s0 = np.array([[0.05, 0.02, -0.01], [0.02, -0.03, 0.015], [-0.01, 0.015, -0.02]])
+    six = lambda m: np.array([m[0, 0], m[1, 1], m[2, 2], m[0, 1], m[0, 2], m[1, 2]])
+    st["sdev"] = np.tile(six(s0), (len(x), 1))
+    o = Oracle(build_params(ps), ps.particle_max_num, fp64=True)
+    o.set_state(st, 1e-4)
+    o.stage(abi.STAGE_SORT)
+    o.stage(abi.STAGE_LAM)
+    g = o.get_state()
+    dt = o.scalars()["dt"]
+    S = s0 + dt * (W @ s0 - s0 @ W)
+    S -= np.trace(S) / 3.0 * np.eye(3)
+    change = np.abs(six(S) - six(s0)).max()
+    err = np.abs(g["sdev"] - six(S)[None]).max()
+    assert change > 1e-5
+    assert err <= 1e-12 * np.abs(s0).max() and err <= 1e-8 * change
+    assert g["eps_p"].max() == 0.0
