@@ -279,3 +279,24 @@ def test_shift_vanishes_on_an_undisturbed_lattice():
     inn = _interior(g["x"], box)
     assert inn.sum() > 2000
     assert np.abs(g["pst_shift"][inn]).max() <= 1e-12 * float(ps.particle_diameter)
+
+
+def test_pressure_force_conserves_momentum():
+    """The symmetric pressure force w_i w_j (p_i + p_j) grad W_ij / mw_i (DSPH.py:1523-1560)
+    is antisymmetric in the pair once multiplied by m_i = mw_i: for any pressure field
+    (random densities here, at rest, no gravity, no viscosity or shift) the accelerations
+    carry no net momentum, sum_i m_i a_i = 0 (to 1e-12 of sum_i m_i |a_i|)."""
+    ps, p, st, x, box = _linear_field_oracle()
+    rng = np.random.default_rng(4)
+    S, gam, rho0 = float(p.stiffness), float(p.exponent), float(p.density0)
+    pt = rng.uniform(10.0, 500.0, len(x))
+    st["V"] = st["m"] / (rho0 * (1.0 + pt / S) ** (1.0 / gam))
+    o = Oracle(p, ps.particle_max_num, fp64=True)
+    o.set_state(st, 1e-7)
+    for k in (abi.STAGE_SORT, abi.STAGE_LAM, abi.STAGE_CONTINUITY, abi.STAGE_FORCES):
+        o.stage(k)
+    g = o.get_state()
+    ma = g["m"][:, None] * g["acc"]
+    gross = np.abs(ma).sum()
+    assert gross > 0.0
+    assert np.abs(ma.sum(axis=0)).max() <= 1e-12 * gross
